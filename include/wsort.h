@@ -1,0 +1,213 @@
+/*
+ * wsort: the Gaussian-splat depth-key + stable counting sort of the Winding
+ * engine, as a C-ABI shared library (libwsort.so) running sm_100a CUDA.
+ *
+ * Inputs and outputs are the reference's: 32-byte .splat records in, and for
+ * each view the survivor count, the u32 permutation of splat indices (back to
+ * front) and the matching 16-bit keys out. Citations are to files of the
+ * reference project (winding-engine 1.9.0).
+ *
+ * Conventions
+ *   - Every function returns WS_OK (0) or a negative WS_ERR_* code; the text
+ *     of the last failure on a context is ws_last_error(ctx). Messages that
+ *     have a counterpart in the reference use its wording.
+ *   - Plain pointers and sizes only. `stream` is a cudaStream_t passed as
+ *     void* (NULL: the context's own stream).
+ *   - One context per host thread; a context's calls are not synchronised.
+ *     The server object (ws_server_*) is internally synchronised.
+ *   - Clouds belong to the context that made them. Output buffers belong to
+ *     the caller.
+ *
+ * Order contract. The reference appends survivors through atomics and
+ * scatters ties through atomics (src/render/splats.js:182, :218), so its order
+ * within a key varies run to run. This library returns the one deterministic
+ * order that the reference's own stable CPU sort gives (DrawList.sort,
+ * src/render/drawlist.js:186-229, with survivors pushed in index order):
+ * survivors ordered by (key ascending, splat index ascending).
+ */
+#ifndef WSORT_H
+#define WSORT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define WS_VERSION 1
+
+enum {
+    WS_OK = 0,
+    WS_ERR_ARG = -1,          /* an argument is invalid (null, negative cull, ...) */
+    WS_ERR_FORMAT = -2,       /* the bytes are not .splat records */
+    WS_ERR_NAN = -3,          /* a splat position is not a finite number */
+    WS_ERR_CAPACITY = -4,     /* more splats than one cloud holds */
+    WS_ERR_CUDA = -5,         /* a CUDA runtime call failed */
+    WS_ERR_NOMEM = -6,        /* device memory (or the server's budget) exhausted */
+    WS_ERR_TIMEOUT = -7,      /* a bounded device-side wait expired; results invalid */
+    WS_ERR_UNLOADED = -8,     /* the cloud was freed */
+    WS_ERR_BUSY = -9,         /* the server's queue is full, or it is stopping */
+    WS_ERR_PENDING = -10      /* ws_server_wait timed out: the request is not done yet */
+};
+
+/* Most splats one cloud holds (look-back counts are 30-bit). */
+#define WS_MAX_SPLATS ((uint32_t)1 << 30)
+/* Number of distinct keys: render/splats.js:64 (BUCKETS). */
+#define WS_BUCKETS 65536u
+
+typedef struct ws_ctx ws_ctx;
+typedef struct ws_cloud ws_cloud;
+typedef struct ws_plan ws_plan;
+typedef struct ws_server ws_server;
+
+/*
+ * One view of a cloud: exactly the f32 values the reference writes into its
+ * Cloud uniform for a sort (src/render/splats.js:80-92, filled at :574-587).
+ * Matrices are column-major. depthMin / depthScale are not passed: the
+ * library computes them from the cloud's box in FP64 as prepare does
+ * (:561-582). cull is Renderer.splatCull (src/render/renderer.js:340-344):
+ * 0 keeps every splat the frustum and faintness tests keep.
+ */
+typedef struct ws_view {
+    float model_view[16];
+    float projection[16];
+    float viewport[2];
+    float cull;
+} ws_view;
+
+/* ------------------------------------------------------------ context */
+
+/* Replaces SplatPass.create (src/render/splats.js:418-501): a context on
+ * CUDA device `device`, with its stream and scratch. */
+int ws_create(ws_ctx** out, int device);
+/* Replaces SplatPass.destroy (src/render/splats.js:724-727). */
+int ws_destroy(ws_ctx* ctx);
+/* The message of the last failure on ctx ("" if none). */
+const char* ws_last_error(const ws_ctx* ctx);
+/* Waits for the context's stream and reports any device-side error raised by
+ * sorts queued with WS_DEVICE_OUTPUT since the last check. */
+int ws_sync(ws_ctx* ctx);
+
+/* ------------------------------------------------------------ clouds */
+
+/*
+ * Replaces parseSplats / parseSplatFile (src/scene/splats.js:60-76, :373-388)
+ * followed by new Splats (src/render/splats.js:389-409): the records are
+ * copied to the device, decoded there (centres, colour word, and each
+ * covariance R S S^T R^T in FP64 rounded to f32, as put() computes it at
+ * src/scene/splats.js:335-369) and kept resident. Refusals mirror the
+ * reference: a zip, gzip, zstd .spz or .ply header (a .ply is not read by
+ * this library), a length that is zero or not a multiple of 32, a position
+ * that is not finite, or more than WS_MAX_SPLATS splats.
+ */
+int ws_cloud_from_splat(ws_ctx* ctx, const uint8_t* bytes, size_t nbytes, ws_cloud** out);
+/* As ws_cloud_from_splat for records already in device memory. */
+int ws_cloud_from_device(ws_ctx* ctx, const void* device_bytes, size_t nbytes, ws_cloud** out);
+/* Splats.count / .min / .max (src/render/splats.js:401-403). min/max may be NULL. */
+int ws_cloud_info(const ws_cloud* cloud, uint32_t* count, double min[3], double max[3]);
+/* Copies the decoded arrays to host memory: centers 4 f32 a splat (the 4th
+ * holds the colour word's bits), covariances 6 f32 a splat (xx xy xz yy yz
+ * zz): the `centers` / `covariances` of parseSplats. Either may be NULL. */
+int ws_cloud_download(const ws_cloud* cloud, float* centers, float* covariances);
+/* Replaces Splats.destroy (src/render/splats.js:411-415). */
+int ws_cloud_free(ws_cloud* cloud);
+
+/*
+ * The per-cloud depth range of prepare (src/render/splats.js:561-582), in
+ * FP64: *visible is 0 when the cloud is wholly behind the camera (the
+ * reference skips it), else depth_min / depth_scale are the f32 values of
+ * Cloud.depthMin / Cloud.depthScale.
+ */
+int ws_depth_range(const ws_cloud* cloud, const float model_view[16], int* visible, float* depth_min,
+                   float* depth_scale);
+
+/* ------------------------------------------------------------ sorting */
+
+/* Output placement for ws_sort. */
+#define WS_HOST_OUTPUT 0   /* order/keys/count are host memory; returns when they are filled */
+#define WS_DEVICE_OUTPUT 1 /* device memory; returns once the work is queued on `stream` */
+
+/*
+ * One cloud, one view. Replaces SplatPass._encodeSort's three dispatches for
+ * a cloud (makeKeys, scanCounts, place: src/render/splats.js:676-697, WGSL
+ * :155-219) and its outputs: `order` (binding 6) and args.instanceCount
+ * (binding 7), here `count`. order and keys (keys may be NULL) must hold the
+ * cloud's count of u32; entries [0, *count) are written: order[j] is a splat
+ * index, keys[j] its key (65535 - depth bucket, so the farthest first).
+ * A cloud wholly behind the camera yields *count == 0.
+ * Errors: WS_ERR_ARG for a cull that is negative or not finite, with the
+ * reference's message "splatCull must be 0 or more, got <cull>"
+ * (src/render/renderer.js:1529); WS_ERR_UNLOADED for a freed cloud
+ * (src/render/splats.js:556).
+ */
+int ws_sort(ws_ctx* ctx, const ws_cloud* cloud, const ws_view* view, uint32_t* order, uint32_t* keys,
+            uint32_t* count, int flags, void* stream);
+
+/* One job of a batch: device-memory outputs, as ws_sort with WS_DEVICE_OUTPUT. */
+typedef struct ws_job {
+    const ws_cloud* cloud;
+    ws_view view;
+    uint32_t* order;
+    uint32_t* keys;      /* may be NULL */
+    uint32_t* count;
+} ws_job;
+
+/*
+ * Many (cloud, view) jobs in one persistent launch. Replaces the per-cloud
+ * loop of SplatPass._encodeSort (src/render/splats.js:678-696), which
+ * dispatches three kernels per cloud. Each job's result is identical to what
+ * ws_sort gives for it alone. Queued on `stream`; returns once queued.
+ */
+int ws_sort_batch(ws_ctx* ctx, int njobs, const ws_job* jobs, void* stream);
+
+/*
+ * A batch frozen into a CUDA graph: the job set (clouds, output buffers) is
+ * fixed at creation; views can change between launches with
+ * ws_plan_set_views, which waits for the plan's previous launch to finish
+ * reading them. The graph holds the upload of the views, the reset of the
+ * counters and the one persistent launch.
+ */
+int ws_plan_create(ws_ctx* ctx, int njobs, const ws_job* jobs, ws_plan** out);
+int ws_plan_set_views(ws_plan* plan, const ws_view* views);
+int ws_plan_launch(ws_plan* plan, void* stream);
+int ws_plan_destroy(ws_plan* plan);
+
+/* ------------------------------------------------------------ device buffers */
+
+/*
+ * Device memory for per-cloud sort outputs, for callers without a CUDA
+ * allocator of their own (a JavaScript host, for one). Replaces the
+ * createBuffer calls of SplatPass._stateFor (src/render/splats.js:629-652):
+ * the `order` buffer and the count word of `args`.
+ */
+int ws_device_alloc(ws_ctx* ctx, size_t bytes, void** out);
+int ws_device_free(ws_ctx* ctx, void* ptr);
+/* Copies `bytes` from device memory to host memory, after the context's
+ * queued work (and `stream`'s, if given) has finished. */
+int ws_device_download(ws_ctx* ctx, const void* device_src, void* host_dst, size_t bytes, void* stream);
+
+/* ------------------------------------------------------------ tuning */
+
+/*
+ * Kernel parameters. keys_tile: splats a key work item covers (multiple of
+ * 256, at most 8192). pass_tile: elements a digit-pass work item covers
+ * (2048 or 4096). ctas_per_sm: resident CTAs per SM of the persistent grid
+ * (0: as many as fit). spin_limit: iterations a device-side wait spins
+ * before it gives up with WS_ERR_TIMEOUT.
+ */
+typedef struct ws_params {
+    uint32_t keys_tile;
+    uint32_t pass_tile;
+    uint32_t ctas_per_sm;
+    uint32_t spin_limit;
+} ws_params;
+
+int ws_get_params(const ws_ctx* ctx, ws_params* out);
+int ws_set_params(ws_ctx* ctx, const ws_params* params);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WSORT_H */

@@ -1,0 +1,351 @@
+// CPU oracle for the splat depth-key + stable counting-sort path.
+//
+// TEST INFRASTRUCTURE ONLY: the checker that tests, the smoke check and the
+// benchmark's CPU-baseline leg compare the CUDA library against. Nothing in
+// the product library links or calls this file.
+//
+// Build: g++ -std=c++17 -O2 -ffp-contract=off -fno-fast-math (see Makefile).
+// Every f32 operation below is a separately rounded IEEE single op; every
+// double operation a separately rounded IEEE double op, evaluated left to
+// right as the reference's JavaScript evaluates it.
+
+#include "oracle.h"
+
+#include <cmath>
+#include <cstdio>
+#include <algorithm>
+#include <cstring>
+#include <thread>
+#include <vector>
+
+namespace {
+
+// Math.hypot as V8 evaluates it (the reference's loader runs under V8):
+// the largest magnitude is factored out, the squares of the quotients are
+// summed with Kahan compensation, and sqrt(sum) * max is returned. Returns
+// +0 when every argument is zero (the caller's `|| 1` then applies).
+double v8_hypot4(double a, double b, double c, double d) {
+    const double v[4] = {std::fabs(a), std::fabs(b), std::fabs(c), std::fabs(d)};
+    double max = 0.0;
+    for (double x : v)
+        if (x > max) max = x;
+    if (max == 0.0) return 0.0;
+    double sum = 0.0, compensation = 0.0;
+    for (double x : v) {
+        const double n = x / max;
+        const double summand = n * n - compensation;
+        const double preliminary = sum + summand;
+        compensation = (preliminary - sum) - summand;
+        sum = preliminary;
+    }
+    return std::sqrt(sum) * max;
+}
+
+float le_f32(const uint8_t* p) {
+    float f;
+    std::memcpy(&f, p, 4);
+    return f;
+}
+
+// One decoded splat into the output arrays: put() at scene/splats.js:335-369.
+void put(float* centers, float* cov, uint32_t i, const uint8_t* rec) {
+    const double x = le_f32(rec + 0), y = le_f32(rec + 4), z = le_f32(rec + 8);
+    const double sx = le_f32(rec + 12), sy = le_f32(rec + 16), sz = le_f32(rec + 20);
+    centers[size_t(i) * 4 + 0] = static_cast<float>(x);
+    centers[size_t(i) * 4 + 1] = static_cast<float>(y);
+    centers[size_t(i) * 4 + 2] = static_cast<float>(z);
+    const uint32_t word = uint32_t(rec[24]) | (uint32_t(rec[25]) << 8) |
+                          (uint32_t(rec[26]) << 16) | (uint32_t(rec[27]) << 24);
+    std::memcpy(&centers[size_t(i) * 4 + 3], &word, 4);
+
+    // (b - 128) / 128: exact in double.
+    const double qw = (double(rec[28]) - 128.0) / 128.0;
+    const double qx = (double(rec[29]) - 128.0) / 128.0;
+    const double qy = (double(rec[30]) - 128.0) / 128.0;
+    const double qz = (double(rec[31]) - 128.0) / 128.0;
+    double length = v8_hypot4(qw, qx, qy, qz);
+    if (length == 0.0 || std::isnan(length)) length = 1.0;  // `|| 1`
+    const double w = qw / length, u = qx / length, v = qy / length, t = qz / length;
+    const double r00 = 1.0 - 2.0 * (v * v + t * t), r01 = 2.0 * (u * v - w * t),
+                 r02 = 2.0 * (u * t + w * v);
+    const double r10 = 2.0 * (u * v + w * t), r11 = 1.0 - 2.0 * (u * u + t * t),
+                 r12 = 2.0 * (v * t - w * u);
+    const double r20 = 2.0 * (u * t - w * v), r21 = 2.0 * (v * t + w * u),
+                 r22 = 1.0 - 2.0 * (u * u + v * v);
+    const double m00 = r00 * sx, m01 = r01 * sy, m02 = r02 * sz;
+    const double m10 = r10 * sx, m11 = r11 * sy, m12 = r12 * sz;
+    const double m20 = r20 * sx, m21 = r21 * sy, m22 = r22 * sz;
+    float* c = cov + size_t(i) * 6;
+    c[0] = static_cast<float>(m00 * m00 + m01 * m01 + m02 * m02);
+    c[1] = static_cast<float>(m00 * m10 + m01 * m11 + m02 * m12);
+    c[2] = static_cast<float>(m00 * m20 + m01 * m21 + m02 * m22);
+    c[3] = static_cast<float>(m10 * m10 + m11 * m11 + m12 * m12);
+    c[4] = static_cast<float>(m10 * m20 + m11 * m21 + m12 * m22);
+    c[5] = static_cast<float>(m20 * m20 + m21 * m21 + m22 * m22);
+}
+
+// WGSL clamp(e, low, high) = min(max(e, low), high); max/min return the
+// non-NaN operand, as fmaxf/fminf do.
+inline float clampf(float e, float lo, float hi) { return std::fmin(std::fmax(e, lo), hi); }
+
+}  // namespace
+
+extern "C" int or_parse_splat(const uint8_t* data, size_t nbytes, float* centers, float* cov,
+                              double bmin[3], double bmax[3], uint32_t* bad_index, char* err,
+                              size_t errlen) {
+    // The sniffing order of parseSplats (scene/splats.js:60-76).
+    if (nbytes >= 8 && data[0] == 0x4e && data[1] == 0x47 && data[2] == 0x53 && data[3] == 0x50) {
+        uint32_t version;
+        std::memcpy(&version, data + 4, 4);
+        if (version >= 4) {
+            std::snprintf(err, errlen,
+                          "splats: a .spz of version 4, compressed with zstd, which browsers cannot "
+                          "unpack; save it as version 3, or as a .ply or .splat");
+            return -6;
+        }
+    }
+    if (nbytes >= 4 && data[0] == 0x70 && data[1] == 0x6c && data[2] == 0x79 &&
+        (data[3] == 0x0a || data[3] == 0x0d)) {
+        std::snprintf(err, errlen, "splats: a .ply is not read here: only .splat records are");
+        return -5;
+    }
+    if (nbytes >= 4 && data[0] == 0x50 && data[1] == 0x4b && data[2] == 0x03 && data[3] == 0x04) {
+        std::snprintf(err, errlen, "splats: this is a zip: unpack it with readSplats, which reads a .sog");
+        return -2;
+    }
+    if (nbytes >= 2 && data[0] == 0x1f && data[1] == 0x8b) {
+        std::snprintf(err, errlen, "splats: this is gzipped: unpack it with readSplats, which reads a .spz");
+        return -3;
+    }
+    if (nbytes == 0 || nbytes % 32 != 0) {
+        std::snprintf(err, errlen,
+                      "splats: not a .ply, and %zu bytes is not a whole number of 32-byte .splat records",
+                      nbytes);
+        return -1;
+    }
+    const uint32_t count = uint32_t(nbytes / 32);
+    for (int k = 0; k < 3; ++k) {
+        bmin[k] = INFINITY;
+        bmax[k] = -INFINITY;
+    }
+    for (uint32_t i = 0; i < count; ++i) {
+        const uint8_t* rec = data + size_t(i) * 32;
+        const double p[3] = {le_f32(rec), le_f32(rec + 4), le_f32(rec + 8)};
+        if (!(std::isfinite(p[0]) && std::isfinite(p[1]) && std::isfinite(p[2]))) {
+            if (bad_index) *bad_index = i;
+            std::snprintf(err, errlen, "splats: splat %u has a position that is not a number", i);
+            return -4;
+        }
+        put(centers, cov, i, rec);
+        for (int k = 0; k < 3; ++k) {
+            if (p[k] < bmin[k]) bmin[k] = p[k];
+            if (p[k] > bmax[k]) bmax[k] = p[k];
+        }
+    }
+    return 0;
+}
+
+extern "C" int or_depth_range(const float mv[16], const double bmin[3], const double bmax[3],
+                              float* depth_min, float* depth_scale) {
+    // render/splats.js:561-582, in doubles, the box's eight corners.
+    double near = INFINITY, far = -INFINITY;
+    for (int k = 0; k < 8; ++k) {
+        const double x = (k & 1) ? bmax[0] : bmin[0];
+        const double y = (k & 2) ? bmax[1] : bmin[1];
+        const double z = (k & 4) ? bmax[2] : bmin[2];
+        const double depth = -(double(mv[2]) * x + double(mv[6]) * y + double(mv[10]) * z + double(mv[14]));
+        if (depth < near) near = depth;
+        if (depth > far) far = depth;
+    }
+    if (far <= 0.0) return 1;
+    // Math.max(near, 0): +0 when near is a zero of either sign.
+    near = (near > 0.0) ? near : 0.0;
+    const double span = far - near;
+    *depth_min = static_cast<float>(near);
+    *depth_scale = static_cast<float>(65535.0 / (span > 1e-6 ? span : 1e-6));
+    return 0;
+}
+
+extern "C" void or_footprint(const or_cloud* c, const float* cov, uint32_t i, const float view[4],
+                             float f[3]) {
+    // render/splats.js:102-124. Matrices are indexed [row][col] here; the
+    // WGSL source builds them column by column.
+    const float* s6 = cov + size_t(i) * 6;
+    const float S[3][3] = {{s6[0], s6[1], s6[2]}, {s6[1], s6[3], s6[4]}, {s6[2], s6[4], s6[5]}};
+    const float* P = c->projection;
+    const float fx = (P[0] * c->viewport[0]) * 0.5f;
+    const float fy = (P[5] * c->viewport[1]) * 0.5f;
+    float J[3][3] = {{fx, 0.0f, 0.0f}, {0.0f, fy, 0.0f}, {0.0f, 0.0f, 0.0f}};
+    if (P[15] == 0.0f) {
+        const float d = -view[2];
+        const float x = clampf(view[0] / d, -1.3f / P[0], 1.3f / P[0]) * d;
+        const float y = clampf(view[1] / d, -1.3f / P[5], 1.3f / P[5]) * d;
+        const float dd = d * d;
+        J[0][0] = fx / d;
+        J[1][1] = fy / d;
+        J[0][2] = (fx * x) / dd;
+        J[1][2] = (fy * y) / dd;
+    }
+    const float* mv = c->model_view;
+    float W[3][3];
+    for (int r = 0; r < 3; ++r)
+        for (int col = 0; col < 3; ++col) W[r][col] = mv[col * 4 + r];
+    float T[2][3], U[2][3];
+    for (int r = 0; r < 2; ++r)
+        for (int col = 0; col < 3; ++col)
+            T[r][col] = (J[r][0] * W[0][col] + J[r][1] * W[1][col]) + J[r][2] * W[2][col];
+    for (int r = 0; r < 2; ++r)
+        for (int col = 0; col < 3; ++col)
+            U[r][col] = (T[r][0] * S[0][col] + T[r][1] * S[1][col]) + T[r][2] * S[2][col];
+    // cov = U * transpose(T); the WGSL returns cov[0][0], cov[0][1] (column 0,
+    // row 1) and cov[1][1].
+    f[0] = (U[0][0] * T[0][0] + U[0][1] * T[0][1]) + U[0][2] * T[0][2];
+    f[1] = (U[1][0] * T[0][0] + U[1][1] * T[0][1]) + U[1][2] * T[0][2];
+    f[2] = (U[1][0] * T[1][0] + U[1][1] * T[1][1]) + U[1][2] * T[1][2];
+}
+
+extern "C" uint32_t or_key(const or_cloud* c, const float* centers, const float* cov, uint32_t i) {
+    // makeKeys, render/splats.js:155-186.
+    const float x = centers[size_t(i) * 4 + 0];
+    const float y = centers[size_t(i) * 4 + 1];
+    const float z = centers[size_t(i) * 4 + 2];
+    uint32_t word;
+    std::memcpy(&word, &centers[size_t(i) * 4 + 3], 4);
+    const float* M = c->model_view;
+    float view[4];
+    for (int j = 0; j < 4; ++j) view[j] = ((M[j] * x + M[4 + j] * y) + M[8 + j] * z) + M[12 + j] * 1.0f;
+    const float* P = c->projection;
+    float clip[4];
+    for (int j = 0; j < 4; ++j)
+        clip[j] = ((P[j] * view[0] + P[4 + j] * view[1]) + P[8 + j] * view[2]) + P[12 + j] * view[3];
+    const float w = clip[3];
+    if (view[2] >= 0.0f || clip[2] > w || std::fabs(clip[0]) > 1.3f * w || std::fabs(clip[1]) > 1.3f * w)
+        return OR_CULLED;
+    // unpack4x8unorm(center.w).a
+    const float alpha = float(word >> 24) / 255.0f;
+    if (alpha * 255.0f <= 1.0f) return OR_CULLED;
+    if (c->cull > 0.0f) {
+        float f[3];
+        or_footprint(c, cov, i, view, f);
+        const float det = (f[0] + 0.3f) * (f[2] + 0.3f) - f[1] * f[1];
+        const float area = 6.2831853f * std::sqrt(std::fmax(det, 0.0f));
+        if (alpha * area < c->cull) return OR_CULLED;
+    }
+    const float scaled = (-view[2] - c->depth_min) * c->depth_scale;
+    const uint32_t bucket = uint32_t(clampf(scaled, 0.0f, float(OR_BUCKETS - 1u)));
+    return OR_BUCKETS - 1u - bucket;
+}
+
+extern "C" void or_make_keys(const or_cloud* c, const float* centers, const float* cov, uint32_t begin,
+                             uint32_t end, uint32_t* keys) {
+    for (uint32_t i = begin; i < end; ++i) keys[i] = or_key(c, centers, cov, i);
+}
+
+extern "C" uint32_t or_counting_sort(const uint32_t* keys, uint32_t n, uint32_t* order,
+                                     uint32_t* sorted_keys) {
+    std::vector<uint32_t> start(OR_BUCKETS + 1, 0);
+    for (uint32_t i = 0; i < n; ++i)
+        if (keys[i] != OR_CULLED) ++start[keys[i] + 1];
+    for (uint32_t b = 0; b < OR_BUCKETS; ++b) start[b + 1] += start[b];
+    const uint32_t survivors = start[OR_BUCKETS];
+    for (uint32_t i = 0; i < n; ++i) {
+        const uint32_t k = keys[i];
+        if (k == OR_CULLED) continue;
+        const uint32_t at = start[k]++;
+        order[at] = i;
+        if (sorted_keys) sorted_keys[at] = k;
+    }
+    return survivors;
+}
+
+extern "C" void or_drawlist_sort(uint32_t* keys_in, uint32_t* payloads_in, uint32_t n,
+                                 uint32_t* keys_alt_in, uint32_t* payloads_alt_in) {
+    if (n < 2) return;
+    uint32_t* keys = keys_in;
+    uint32_t* payloads = payloads_in;
+    uint32_t* keys_alt = keys_alt_in;
+    uint32_t* payloads_alt = payloads_alt_in;
+    uint32_t counts[256];
+    for (int pass = 0; pass < 4; ++pass) {
+        const int shift = pass * 8;
+        std::memset(counts, 0, sizeof(counts));
+        for (uint32_t i = 0; i < n; ++i) ++counts[(keys[i] >> shift) & 0xff];
+        if (counts[(keys[0] >> shift) & 0xff] == n) continue;
+        uint32_t total = 0;
+        for (int b = 0; b < 256; ++b) {
+            const uint32_t cnt = counts[b];
+            counts[b] = total;
+            total += cnt;
+        }
+        for (uint32_t i = 0; i < n; ++i) {
+            const uint32_t dst = counts[(keys[i] >> shift) & 0xff]++;
+            keys_alt[dst] = keys[i];
+            payloads_alt[dst] = payloads[i];
+        }
+        std::swap(keys, keys_alt);
+        std::swap(payloads, payloads_alt);
+    }
+    // The reference repoints its public arrays at whichever pair holds the
+    // result; here the result is copied back into the caller's arrays.
+    if (keys != keys_in) {
+        std::memcpy(keys_in, keys, size_t(n) * 4);
+        std::memcpy(payloads_in, payloads, size_t(n) * 4);
+    }
+}
+
+extern "C" uint32_t or_sort_view(const float* centers, const float* cov, uint32_t n, const double bmin[3],
+                                 const double bmax[3], const float model_view[16],
+                                 const float projection[16], const float viewport[2], float cull,
+                                 uint32_t* order, uint32_t* sorted_keys, int threads) {
+    or_cloud c;
+    std::memcpy(c.model_view, model_view, sizeof(c.model_view));
+    std::memcpy(c.projection, projection, sizeof(c.projection));
+    c.viewport[0] = viewport[0];
+    c.viewport[1] = viewport[1];
+    c.count = n;
+    c.cull = cull;
+    if (or_depth_range(model_view, bmin, bmax, &c.depth_min, &c.depth_scale) != 0) return 0;
+    std::vector<uint32_t> keys(n);
+    if (threads <= 1 || n < 65536) {
+        or_make_keys(&c, centers, cov, 0, n, keys.data());
+        return or_counting_sort(keys.data(), n, order, sorted_keys);
+    }
+    // Parallel: keys by index chunks, then a per-chunk histogram, a
+    // (bucket, chunk)-major prefix and a per-chunk scatter, which keeps the
+    // result identical to the sequential stable sort.
+    const uint32_t T = uint32_t(threads);
+    const uint32_t chunk = (n + T - 1) / T;
+    std::vector<std::vector<uint32_t>> hist(T, std::vector<uint32_t>(OR_BUCKETS, 0));
+    std::vector<std::thread> pool;
+    for (uint32_t t = 0; t < T; ++t)
+        pool.emplace_back([&, t] {
+            const uint32_t b = t * chunk, e = std::min(n, b + chunk);
+            if (b >= e) return;
+            or_make_keys(&c, centers, cov, b, e, keys.data());
+            for (uint32_t i = b; i < e; ++i)
+                if (keys[i] != OR_CULLED) ++hist[t][keys[i]];
+        });
+    for (auto& th : pool) th.join();
+    pool.clear();
+    uint32_t total = 0;
+    for (uint32_t k = 0; k < OR_BUCKETS; ++k)
+        for (uint32_t t = 0; t < T; ++t) {
+            const uint32_t cnt = hist[t][k];
+            hist[t][k] = total;
+            total += cnt;
+        }
+    for (uint32_t t = 0; t < T; ++t)
+        pool.emplace_back([&, t] {
+            const uint32_t b = t * chunk, e = std::min(n, b + chunk);
+            uint32_t* at = hist[t].data();
+            for (uint32_t i = b; i < e; ++i) {
+                const uint32_t k = keys[i];
+                if (k == OR_CULLED) continue;
+                const uint32_t dst = at[k]++;
+                order[dst] = i;
+                if (sorted_keys) sorted_keys[dst] = k;
+            }
+        });
+    for (auto& th : pool) th.join();
+    return total;
+}

@@ -1,0 +1,114 @@
+/*
+ * CPU oracle for the splat depth-key + stable counting-sort path.
+ *
+ * TEST INFRASTRUCTURE ONLY. This is a plain C++ restatement of the
+ * reference's arithmetic, used by the tests, by the smoke check and by the
+ * CPU-baseline leg of the benchmark as the checker. The product library
+ * (winding_b200/libwsort.so) never links, loads or calls it.
+ *
+ * What it restates (paths relative to the reference project):
+ *   - the .splat record decode and covariance:   src/scene/splats.js:335-388
+ *   - the per-cloud depth range (FP64):          src/render/splats.js:559-587
+ *   - makeKeys and footprint (f32):              src/render/splats.js:102-124, :155-186
+ *   - the stable order of survivors:             src/render/drawlist.js:186-229
+ *
+ * Pinned evaluation order. WGSL lets a driver fuse and reorder f32 work, so
+ * the oracle fixes one order and the CUDA kernels follow it bit for bit:
+ * every f32 operation is a separately rounded IEEE op (built with
+ * -ffp-contract=off, no fast-math), sums are taken left to right in the
+ * order the WGSL source writes them, matrix-vector products are the
+ * column sums col0*v0 + col1*v1 + col2*v2 + col3*v3, and divisions and
+ * square roots are correctly rounded.
+ */
+#ifndef WSORT_ORACLE_H
+#define WSORT_ORACLE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Number of 16-bit keys: render/splats.js:64 (BUCKETS). */
+#define OR_BUCKETS 65536u
+/* Marks a culled splat in the per-splat key array the oracle returns. */
+#define OR_CULLED 0xFFFFFFFFu
+
+/* The fields of the reference's Cloud uniform a sort depends on
+ * (render/splats.js:80-92, filled at :574-587). */
+typedef struct or_cloud {
+    float model_view[16];
+    float projection[16];
+    float viewport[2];
+    float depth_min;
+    float depth_scale;
+    uint32_t count;
+    float cull;
+} or_cloud;
+
+/*
+ * Decodes `nbytes` of .splat records (scene/splats.js:373-388, put :335-369).
+ * centers: 4 f32 per splat (x, y, z, colour word bits); cov: 6 f32 per splat
+ * (xx xy xz yy yz zz); bmin/bmax: the box around the centres, as doubles.
+ * Returns 0, or -1 (length not a whole number of records, or zero),
+ * -2 (a zip), -3 (gzip), -4 (non-finite position; *bad_index set),
+ * -5 (a .ply header), -6 (a zstd .spz). The message text is left in err.
+ */
+int or_parse_splat(const uint8_t* bytes, size_t nbytes, float* centers, float* cov,
+                   double bmin[3], double bmax[3], uint32_t* bad_index,
+                   char* err, size_t errlen);
+
+/*
+ * The per-cloud depth range in FP64 (render/splats.js:561-582).
+ * Returns 1 when the cloud is wholly behind the camera (far <= 0: the
+ * reference skips it), else 0 with depth_min / depth_scale as the f32 values
+ * the Cloud uniform holds.
+ */
+int or_depth_range(const float model_view[16], const double bmin[3], const double bmax[3],
+                   float* depth_min, float* depth_scale);
+
+/* Splat i's key (0..65535) or OR_CULLED: makeKeys (render/splats.js:155-186). */
+uint32_t or_key(const or_cloud* c, const float* centers, const float* cov, uint32_t i);
+
+/* footprint (render/splats.js:102-124): f[0]=xx, f[1]=xy, f[2]=yy. */
+void or_footprint(const or_cloud* c, const float* cov, uint32_t i,
+                  const float view[4], float f[3]);
+
+/* Keys for splats [begin, end) into keys[i]. */
+void or_make_keys(const or_cloud* c, const float* centers, const float* cov,
+                  uint32_t begin, uint32_t end, uint32_t* keys);
+
+/*
+ * Stable counting sort of the survivors by (key, splat index): the order the
+ * reference's DrawList.sort gives when survivors are pushed in index order.
+ * Returns the survivor count S; order[0..S) and sorted_keys[0..S) are written.
+ */
+uint32_t or_counting_sort(const uint32_t* keys, uint32_t n, uint32_t* order,
+                          uint32_t* sorted_keys);
+
+/*
+ * DrawList.sort restated as written (render/drawlist.js:186-229): LSD radix
+ * over 4 bytes, skipping passes whose byte is constant. Sorts keys/payloads
+ * in place (using the alt buffers as ping-pong space).
+ */
+void or_drawlist_sort(uint32_t* keys, uint32_t* payloads, uint32_t n,
+                      uint32_t* keys_alt, uint32_t* payloads_alt);
+
+/*
+ * The whole per-view path: depth range, keys and the stable sort.
+ * view_* are what a caller writes into the Cloud uniform; the range is
+ * computed here. Returns S. threads > 1 splits the work across host threads
+ * (deterministic: same output as threads == 1).
+ */
+uint32_t or_sort_view(const float* centers, const float* cov, uint32_t n,
+                      const double bmin[3], const double bmax[3],
+                      const float model_view[16], const float projection[16],
+                      const float viewport[2], float cull,
+                      uint32_t* order, uint32_t* sorted_keys, int threads);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

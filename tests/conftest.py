@@ -1,0 +1,20 @@
+import os
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200) and libwsort.so")
+
+
+@pytest.fixture(scope="session")
+def ctx():
+    from winding_b200 import Context
+    c = Context(0)
+    yield c
+    c.close()

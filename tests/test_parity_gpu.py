@@ -1,0 +1,230 @@
+"""GPU parity: libwsort.so against the CPU oracle, bit for bit.
+
+Every comparison is exact (np.array_equal on u32 / the f32 bit patterns):
+the only floating-point steps are pinned to separately rounded IEEE ops on
+both sides, and everything after them is integer work.
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests import kats
+from winding_b200 import WsError, make_view, parse_splats, workloads as W
+from winding_b200 import _lib
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def oracle_sort(parsed, view_src, cull):
+    return O.sort_view(parsed, view_src.model_view, view_src.projection, view_src.viewport, cull)
+
+
+def check_job(ctx, job, culls=(0.0, 0.5)):
+    splats = parse_splats(job.records, ctx)
+    parsed = O.parse_splat(job.bytes())
+    try:
+        for cull in culls:
+            view = make_view(job.view.model_view, job.view.projection, job.view.viewport, cull)
+            order, keys = ctx.sort(splats, view)
+            want_o, want_k = oracle_sort(parsed, job.view, cull)
+            assert order.size == want_o.size, (cull, order.size, want_o.size)
+            assert np.array_equal(order, want_o), cull
+            assert np.array_equal(keys, want_k), cull
+    finally:
+        splats.destroy()
+
+
+def test_decode_matches_the_oracle(ctx):
+    job = W.clusters_1m(seed=31, n=50_000)
+    splats = parse_splats(job.records, ctx)
+    parsed = O.parse_splat(job.bytes())
+    c, v = splats.download()
+    assert np.array_equal(c.view(np.uint32), parsed.centers.view(np.uint32))
+    assert np.array_equal(v.view(np.uint32), parsed.covariances.view(np.uint32))
+    assert splats.min == list(parsed.min) and splats.max == list(parsed.max)
+    splats.destroy()
+
+
+def test_decode_known_answers(ctx):
+    s = parse_splats(kats.UNTURNED, ctx)
+    c, v = s.download()
+    assert list(c[0, :3]) == [1, 2, 3]
+    assert list(c.view(np.uint8).reshape(-1, 16)[0, 12:]) == [10, 20, 30, 200]
+    assert np.allclose(v[0], kats.UNTURNED_COV, atol=1e-4)
+    q = parse_splats(kats.QUARTER, ctx)
+    _, v = q.download()
+    assert abs(v[0, 0] - 4) <= 1e-2 and abs(v[0, 3] - 0.25) <= 1e-2 and abs(v[0, 1]) <= 1e-2
+
+
+@pytest.mark.parametrize("data,message", kats.REFUSED)
+def test_refusals_by_message(ctx, data, message):
+    with pytest.raises(WsError, match=message):
+        parse_splats(data, ctx)
+
+
+@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLDEN, "*.npz"))))
+def test_golden_fixtures(ctx, path):
+    g = np.load(path)
+    splats = parse_splats(g["records"], ctx)
+    for tag, cull in (("0p0", 0.0), ("0p5", 0.5)):
+        order, keys = ctx.sort(splats, make_view(g["model_view"], g["projection"], g["viewport"], cull))
+        assert np.array_equal(order, g[f"order_{tag}"]), (path, cull)
+        assert np.array_equal(keys, g[f"keys_{tag}"]), (path, cull)
+    splats.destroy()
+
+
+@pytest.mark.parametrize("n", [1, 2, 31, 32, 33, 255, 256, 257, 2047, 2048, 2049, 4095, 4096, 4097, 12289])
+def test_ragged_sizes(ctx, n):
+    check_job(ctx, W.uniform_100k(seed=100 + n, n=n))
+
+
+def test_uniform_100k(ctx):
+    check_job(ctx, W.uniform_100k(seed=0), culls=(0.0, 0.5, 2.0))
+
+
+def test_clusters_300k(ctx):
+    check_job(ctx, W.clusters_1m(seed=1, n=300_000))
+
+
+def test_slab_heavy_collisions(ctx):
+    check_job(ctx, W.slab_6m(seed=2, n=400_000))
+
+
+@pytest.mark.parametrize("red_first", [True, False])
+def test_two_splats_back_to_front(ctx, red_first):
+    s = parse_splats(kats.two_splats(red_first), ctx)
+    red, blue = (0, 1) if red_first else (1, 0)
+    mv, proj, vp = kats.gpu_test_camera(5.0)
+    order, keys = ctx.sort(s, make_view(mv, proj, vp, 0.5))
+    assert list(order) == [blue, red] and list(keys) == [0, 65535]
+    mv, proj, vp = kats.gpu_test_camera(-5.0)
+    order, _ = ctx.sort(s, make_view(mv, proj, vp, 0.5))
+    assert list(order) == [red, blue]
+    s.destroy()
+
+
+def test_single_splat_and_speck(ctx):
+    mv, proj, vp = kats.gpu_test_camera(5.0)
+    one = parse_splats(kats.two_splats(True)[:32], ctx)
+    order, keys = ctx.sort(one, make_view(mv, proj, vp, 0.5))
+    assert list(order) == [0] and list(keys) == [65535]
+    speck = parse_splats(kats.speck_file(), ctx)
+    assert list(ctx.sort(speck, make_view(mv, proj, vp, 0.5))[0]) == [1]
+    assert sorted(ctx.sort(speck, make_view(mv, proj, vp, 0.0))[0]) == [0, 1]
+
+
+def test_behind_the_camera_and_all_culled(ctx):
+    from winding_b200.camera import look_at, perspective
+    s = parse_splats(kats.two_splats(True), ctx)
+    order, _ = ctx.sort(s, make_view(look_at((0, 0, 5), (0, 0, 10)), perspective(0.8, 4 / 3, 0.1), (160, 120), 0.5))
+    assert order.size == 0
+    # In front, but every splat too faint.
+    job = W.uniform_100k(seed=9, n=5000)
+    job.records["rgba"][:, 3] = 1
+    check_job(ctx, job)
+
+
+def test_cull_errors_and_unloaded(ctx):
+    s = parse_splats(kats.two_splats(True), ctx)
+    mv, proj, vp = kats.gpu_test_camera(5.0)
+    with pytest.raises(WsError, match="splatCull must be 0 or more, got -1"):
+        ctx.sort(s, make_view(mv, proj, vp, -1.0))
+    s.destroy()
+    with pytest.raises(WsError, match="unloaded"):
+        ctx.sort(s, make_view(mv, proj, vp, 0.5))
+    rc = ctx.lib.ws_sort(ctx.handle, s.handle, None, None, None, None, 0, None)
+    assert rc == _lib.WS_ERR_UNLOADED
+
+
+def _device_jobs(ctx, jobs, culls):
+    import torch
+    outs = []
+    specs = []
+    for job, cull in zip(jobs, culls):
+        sp = parse_splats(job.records, ctx)
+        n = max(sp.count, 1)
+        o = torch.empty(n, dtype=torch.int32, device="cuda")
+        k = torch.empty(n, dtype=torch.int32, device="cuda")
+        c = torch.zeros(1, dtype=torch.int32, device="cuda")
+        outs.append((sp, o, k, c))
+        specs.append((sp, make_view(job.view.model_view, job.view.projection, job.view.viewport, cull),
+                       o.data_ptr(), k.data_ptr(), c.data_ptr()))
+    return outs, specs
+
+
+def _results(outs):
+    import torch
+    torch.cuda.synchronize()
+    res = []
+    for sp, o, k, c in outs:
+        s = int(c.item())
+        res.append((o[:s].cpu().numpy().view(np.uint32), k[:s].cpu().numpy().view(np.uint32)))
+    return res
+
+
+def test_batch_equals_each_job_alone(ctx):
+    import torch
+    rng = np.random.default_rng(7)
+    jobs = []
+    for j in range(9):
+        n = int(np.exp(rng.uniform(np.log(3_000), np.log(200_000))))
+        rec = W.scene(W.KINDS[j % 3], n, 700 + j)
+        jobs.append(W.Job(rec, W.View(W.random_pose(rng), W.perspective(W.FOV_Y, W.ASPECT, W.NEAR))))
+    culls = [0.5 if j % 2 else 0.0 for j in range(len(jobs))]
+    outs, specs = _device_jobs(ctx, jobs, culls)
+    ctx.sort_batch(specs, stream=torch.cuda.current_stream().cuda_stream)
+    got = _results(outs)
+    ctx.sync()
+    for (order, keys), job, cull in zip(got, jobs, culls):
+        want_o, want_k = oracle_sort(O.parse_splat(job.bytes()), job.view, cull)
+        assert np.array_equal(order, want_o) and np.array_equal(keys, want_k)
+    # the graph-captured plan, twice, with new views the second time
+    plan = ctx.plan(specs)
+    plan.launch(torch.cuda.current_stream().cuda_stream)
+    got2 = _results(outs)
+    assert all(np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]) for a, b in zip(got, got2))
+    views = []
+    for job, cull in zip(jobs, culls):
+        job.view.model_view = W.random_pose(rng)
+        views.append(make_view(job.view.model_view, job.view.projection, job.view.viewport, cull))
+    plan.set_views(views)
+    plan.launch(torch.cuda.current_stream().cuda_stream)
+    got3 = _results(outs)
+    for (order, keys), job, cull in zip(got3, jobs, culls):
+        want_o, want_k = oracle_sort(O.parse_splat(job.bytes()), job.view, cull)
+        assert np.array_equal(order, want_o) and np.array_equal(keys, want_k)
+    plan.close()
+    for sp, *_ in outs:
+        sp.destroy()
+
+
+@pytest.mark.parametrize("keys_tile,pass_tile", [(256, 2048), (1024, 4096), (4096, 2048), (8192, 4096)])
+def test_tile_parameters_do_not_change_the_result(ctx, keys_tile, pass_tile):
+    old = ctx.params
+    try:
+        ctx.set_params(keys_tile=keys_tile, pass_tile=pass_tile)
+        check_job(ctx, W.clusters_1m(seed=41, n=120_001))
+    finally:
+        ctx.set_params(keys_tile=old.keys_tile, pass_tile=old.pass_tile)
+
+
+def test_full_size_slab_properties(ctx):
+    """6M splats: the oracle's result at full size, checked exactly, plus
+    size-independent properties of the permutation."""
+    job = W.slab_6m(seed=2)
+    splats = parse_splats(job.records, ctx)
+    parsed = O.parse_splat(job.bytes())
+    view = make_view(job.view.model_view, job.view.projection, job.view.viewport, 0.5)
+    order, keys = ctx.sort(splats, view)
+    assert np.all(np.diff(keys.astype(np.int64)) >= 0)
+    same = keys[1:] == keys[:-1]
+    assert np.all(order[1:][same] > order[:-1][same])          # stable: index order within a key
+    assert np.unique(order).size == order.size
+    want_o, want_k = O.sort_view(parsed, job.view.model_view, job.view.projection, job.view.viewport, 0.5,
+                                 threads=os.cpu_count() or 1)
+    assert np.array_equal(order, want_o) and np.array_equal(keys, want_k)
+    splats.destroy()

@@ -1,0 +1,762 @@
+// The C ABI of libwsort.so (include/wsort.h): contexts, resident clouds,
+// single and batched sorts, and graph-captured plans.
+#include "wsort.h"
+#include "wsort_dev.cuh"
+#include "wsort_host.h"
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+namespace wsort {
+cudaError_t launch_sort(const JobDesc* jobs, const uint2* items, uint32_t n_items, LaunchCtl* lctl, uint32_t* err,
+                        uint32_t t1, uint32_t pass_tile, uint32_t spin_limit, int grid, cudaStream_t stream);
+int sort_occupancy(uint32_t pass_tile);
+cudaError_t launch_decode(const void* records, uint32_t n, float4* centers, float2* cov, uint32_t* bounds,
+                          uint32_t* bad, int sms, cudaStream_t stream);
+
+int set_error(ws_ctx* ctx, int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    std::vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    if (ctx) ctx->err = buf;
+    return code;
+}
+
+int cuda_error(ws_ctx* ctx, cudaError_t e, const char* what) {
+    if (e == cudaErrorMemoryAllocation)
+        return set_error(ctx, WS_ERR_NOMEM, "%s: out of device memory (%s)", what, cudaGetErrorString(e));
+    return set_error(ctx, WS_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+cudaError_t DevBuf::ensure(size_t n) {
+    if (n <= bytes) return cudaSuccess;
+    release();
+    const cudaError_t e = cudaMalloc(&p, n);
+    if (e != cudaSuccess) {
+        p = nullptr;
+        cudaGetLastError();
+        return e;
+    }
+    bytes = n;
+    return cudaSuccess;
+}
+void DevBuf::release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+}
+cudaError_t HostBuf::ensure(size_t n) {
+    if (n <= bytes) return cudaSuccess;
+    release();
+    const cudaError_t e = cudaHostAlloc(&p, n, cudaHostAllocDefault);
+    if (e != cudaSuccess) {
+        p = nullptr;
+        cudaGetLastError();
+        return e;
+    }
+    bytes = n;
+    return cudaSuccess;
+}
+void HostBuf::release() {
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    bytes = 0;
+}
+
+static size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+uint32_t pad_splats(uint32_t n) { return (uint32_t)align_up(n ? n : 1, kPadSplats); }
+
+// Tile counts and scratch footprint of one job.
+void job_shape(uint32_t n, const ws_params& p, uint32_t* t1, uint32_t* t2, uint32_t* t3, size_t* bytes) {
+    const uint32_t n1 = n ? n : 1;
+    *t1 = (n1 + p.keys_tile - 1) / p.keys_tile;
+    *t2 = (n1 + p.pass_tile - 1) / p.pass_tile;
+    *t3 = *t2;
+    const size_t np = pad_splats(n);
+    size_t b = 0;
+    b += align_up(np * 2, 256);                 // k16
+    b += align_up(np / 8, 256);                 // mask
+    b += align_up(np * 2, 256);                 // key_b
+    b += align_up(np * 4, 256);                 // idx_b
+    b += align_up((size_t)(*t2 + *t3) * 1024, 256);   // status
+    *bytes = b;
+}
+
+size_t launch_scratch_bytes(const uint32_t* ns, int njobs, const ws_params& p) {
+    size_t total = align_up(sizeof(LaunchCtl) + (size_t)njobs * sizeof(JobCtl), 256);
+    for (int j = 0; j < njobs; ++j) {
+        uint32_t t1, t2, t3;
+        size_t b;
+        job_shape(ns[j], p, &t1, &t2, &t3, &b);
+        total += b;
+    }
+    return total;
+}
+
+// Fills job descriptors and lays the scratch out from `scratch`.
+void layout_jobs(JobDesc* out, const ws_job* jobs, int njobs, const ws_params& p, char* scratch) {
+    char* at = scratch + align_up(sizeof(LaunchCtl) + (size_t)njobs * sizeof(JobCtl), 256);
+    JobCtl* ctls = reinterpret_cast<JobCtl*>(scratch + sizeof(LaunchCtl));
+    for (int j = 0; j < njobs; ++j) {
+        const ws_cloud* c = jobs[j].cloud;
+        JobDesc& d = out[j];
+        std::memset(&d, 0, sizeof(d));
+        d.centers = c->centers;
+        d.cov = c->cov;
+        for (int k = 0; k < 3; ++k) {
+            d.bmin[k] = c->bmin[k];
+            d.bmax[k] = c->bmax[k];
+        }
+        d.n = c->n;
+        std::memcpy(d.mv, jobs[j].view.model_view, sizeof(d.mv));
+        std::memcpy(d.proj, jobs[j].view.projection, sizeof(d.proj));
+        d.viewport[0] = jobs[j].view.viewport[0];
+        d.viewport[1] = jobs[j].view.viewport[1];
+        d.cull = jobs[j].view.cull;
+        d.order = jobs[j].order;
+        d.keys = jobs[j].keys;
+        d.count = jobs[j].count;
+        size_t bytes;
+        job_shape(c->n, p, &d.tiles1, &d.tiles2, &d.tiles3, &bytes);
+        const size_t np = pad_splats(c->n);
+        d.k16 = reinterpret_cast<uint16_t*>(at);
+        at += align_up(np * 2, 256);
+        d.mask = reinterpret_cast<uint32_t*>(at);
+        at += align_up(np / 8, 256);
+        d.key_b = reinterpret_cast<uint16_t*>(at);
+        at += align_up(np * 2, 256);
+        d.idx_b = reinterpret_cast<uint32_t*>(at);
+        at += align_up(np * 4, 256);
+        d.status = reinterpret_cast<uint32_t*>(at);
+        at += align_up((size_t)(d.tiles2 + d.tiles3) * 1024, 256);
+        d.ctl = reinterpret_cast<uint32_t*>(&ctls[j]);
+    }
+}
+
+// Work items, software-pipelined across jobs: the keys of job s, then the
+// low pass of job s-1, then the high pass of job s-2, so that a digit pass
+// rarely waits for the phase before it.
+void build_items(std::vector<uint2>& items, const JobDesc* jobs, int njobs) {
+    items.clear();
+    for (int s = 0; s < njobs + 2; ++s) {
+        if (s < njobs)
+            for (uint32_t t = 0; t < jobs[s].tiles1; ++t) items.push_back(make_uint2(s, (kPhaseKeys << 30) | t));
+        if (s - 1 >= 0 && s - 1 < njobs)
+            for (uint32_t t = 0; t < jobs[s - 1].tiles2; ++t)
+                items.push_back(make_uint2(s - 1, (kPhaseLow << 30) | t));
+        if (s - 2 >= 0 && s - 2 < njobs)
+            for (uint32_t t = 0; t < jobs[s - 2].tiles3; ++t)
+                items.push_back(make_uint2(s - 2, (kPhaseHigh << 30) | t));
+    }
+}
+
+int grid_for(ws_ctx* ctx, size_t n_items) {
+    int per_sm = sort_occupancy(ctx->params.pass_tile);
+    if (per_sm < 1) per_sm = 1;
+    if (ctx->params.ctas_per_sm && (int)ctx->params.ctas_per_sm < per_sm) per_sm = (int)ctx->params.ctas_per_sm;
+    size_t g = (size_t)ctx->sms * per_sm;
+    if (g > n_items) g = n_items ? n_items : 1;
+    return (int)g;
+}
+
+int check_view(ws_ctx* ctx, const ws_view* v) {
+    if (!v) return set_error(ctx, WS_ERR_ARG, "ws_sort: view is null");
+    const float cull = v->cull;
+    if (!(cull >= 0.0f && std::isfinite(cull))) {
+        // The reference prints the number as JavaScript would; %g is close.
+        return set_error(ctx, WS_ERR_ARG, "splatCull must be 0 or more, got %g", (double)cull);
+    }
+    return WS_OK;
+}
+
+int check_cloud(ws_ctx* ctx, const ws_cloud* c) {
+    if (!c) return set_error(ctx, WS_ERR_ARG, "ws_sort: cloud is null");
+    if (c->magic != kCloudMagic) return set_error(ctx, WS_ERR_ARG, "ws_sort: not a cloud handle");
+    if (!c->alive)
+        return set_error(ctx, WS_ERR_UNLOADED, "addSplats: these splats were unloaded; remove the node first");
+    if (c->ctx != ctx) return set_error(ctx, WS_ERR_ARG, "ws_sort: the cloud belongs to another context");
+    return WS_OK;
+}
+
+// Stages, uploads and launches a batch on ctx's scratch. The stream waits for
+// the context's previous launch, so one scratch is never shared by two
+// launches in flight.
+int run_batch(ws_ctx* ctx, const ws_job* jobs, int njobs, cudaStream_t stream) {
+    cudaError_t e;
+    std::vector<uint32_t> ns(njobs);
+    for (int j = 0; j < njobs; ++j) ns[j] = jobs[j].cloud->n;
+    const size_t need = launch_scratch_bytes(ns.data(), njobs, ctx->params);
+    if (need > ctx->scratch.bytes) {
+        // The old scratch may still be read by a launch in flight.
+        if ((e = cudaEventSynchronize(ctx->launched)) != cudaSuccess) return cuda_error(ctx, e, "ws_sort");
+        if ((e = ctx->scratch.ensure(need)) != cudaSuccess) return cuda_error(ctx, e, "ws_sort scratch");
+    }
+    // Pinned staging is rewritten only after its previous upload finished.
+    if ((e = cudaEventSynchronize(ctx->staged)) != cudaSuccess) return cuda_error(ctx, e, "ws_sort");
+    if ((e = ctx->jobs_h.ensure((size_t)njobs * sizeof(JobDesc))) != cudaSuccess)
+        return cuda_error(ctx, e, "ws_sort staging");
+    if ((e = ctx->jobs_d.ensure((size_t)njobs * sizeof(JobDesc))) != cudaSuccess)
+        return cuda_error(ctx, e, "ws_sort job table");
+    JobDesc* hj = static_cast<JobDesc*>(ctx->jobs_h.p);
+    layout_jobs(hj, jobs, njobs, ctx->params, static_cast<char*>(ctx->scratch.p));
+
+    // Items depend only on the job sizes and the tiles: reuse the last upload
+    // when they are unchanged.
+    bool same = ctx->items_valid && ctx->last_ns == ns && ctx->last_keys_tile == ctx->params.keys_tile &&
+                ctx->last_pass_tile == ctx->params.pass_tile;
+    if (!same) {
+        build_items(ctx->items, hj, njobs);
+        if ((e = ctx->items_h.ensure(ctx->items.size() * sizeof(uint2))) != cudaSuccess)
+            return cuda_error(ctx, e, "ws_sort staging");
+        if (ctx->items.size() * sizeof(uint2) > ctx->items_d.bytes) {
+            if ((e = cudaEventSynchronize(ctx->launched)) != cudaSuccess) return cuda_error(ctx, e, "ws_sort");
+            if ((e = ctx->items_d.ensure(ctx->items.size() * sizeof(uint2))) != cudaSuccess)
+                return cuda_error(ctx, e, "ws_sort items");
+        }
+        std::memcpy(ctx->items_h.p, ctx->items.data(), ctx->items.size() * sizeof(uint2));
+    }
+    if (stream != ctx->stream) cudaStreamWaitEvent(stream, ctx->launched, 0);
+    if ((e = cudaMemcpyAsync(ctx->jobs_d.p, hj, (size_t)njobs * sizeof(JobDesc), cudaMemcpyHostToDevice, stream)) !=
+        cudaSuccess)
+        return cuda_error(ctx, e, "ws_sort upload");
+    if (!same) {
+        if ((e = cudaMemcpyAsync(ctx->items_d.p, ctx->items_h.p, ctx->items.size() * sizeof(uint2),
+                                 cudaMemcpyHostToDevice, stream)) != cudaSuccess)
+            return cuda_error(ctx, e, "ws_sort upload");
+        ctx->last_ns = ns;
+        ctx->last_keys_tile = ctx->params.keys_tile;
+        ctx->last_pass_tile = ctx->params.pass_tile;
+        ctx->items_valid = true;
+    }
+    cudaEventRecord(ctx->staged, stream);
+    const size_t ctl_bytes = sizeof(LaunchCtl) + (size_t)njobs * sizeof(JobCtl);
+    if ((e = cudaMemsetAsync(ctx->scratch.p, 0, ctl_bytes, stream)) != cudaSuccess)
+        return cuda_error(ctx, e, "ws_sort reset");
+    const size_t n_items = ctx->items.size();
+    e = launch_sort(static_cast<JobDesc*>(ctx->jobs_d.p), static_cast<uint2*>(ctx->items_d.p), (uint32_t)n_items,
+                    static_cast<LaunchCtl*>(ctx->scratch.p), ctx->err_d, ctx->params.keys_tile,
+                    ctx->params.pass_tile, ctx->params.spin_limit, grid_for(ctx, n_items), stream);
+    if (e != cudaSuccess) return cuda_error(ctx, e, "ws_sort launch");
+    cudaEventRecord(ctx->launched, stream);
+    ++ctx->launches;
+    return WS_OK;
+}
+
+// Reads and clears the sticky device error words. Call after a sync.
+int take_device_error(ws_ctx* ctx) {
+    uint32_t words[2] = {0, 0};
+    cudaError_t e = cudaMemcpy(words, ctx->err_d, sizeof(words), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_error(ctx, e, "ws_sync");
+    if (words[0]) {
+        cudaMemset(ctx->err_d, 0, 2 * sizeof(uint32_t));
+        return set_error(ctx, WS_ERR_TIMEOUT,
+                         "a device-side wait gave up (code %u at work item %u); the results of that launch "
+                         "are invalid",
+                         words[0], words[1]);
+    }
+    return WS_OK;
+}
+
+double host_depth_range(const float mv[16], const double bmin[3], const double bmax[3], int* visible,
+                        float* depth_min, float* depth_scale) {
+    double nearv = INFINITY, farv = -INFINITY;
+    for (int k = 0; k < 8; ++k) {
+        const double x = (k & 1) ? bmax[0] : bmin[0];
+        const double y = (k & 2) ? bmax[1] : bmin[1];
+        const double z = (k & 4) ? bmax[2] : bmin[2];
+        const double depth = -(double(mv[2]) * x + double(mv[6]) * y + double(mv[10]) * z + double(mv[14]));
+        if (depth < nearv) nearv = depth;
+        if (depth > farv) farv = depth;
+    }
+    *visible = farv > 0.0;
+    nearv = nearv > 0.0 ? nearv : 0.0;
+    const double span = farv - nearv;
+    *depth_min = (float)nearv;
+    *depth_scale = (float)(65535.0 / (span > 1e-6 ? span : 1e-6));
+    return nearv;
+}
+
+}  // namespace wsort
+
+using namespace wsort;
+
+// ------------------------------------------------------------------ context
+
+extern "C" int ws_create(ws_ctx** out, int device) {
+    if (!out) return WS_ERR_ARG;
+    *out = nullptr;
+    ws_ctx* ctx = new (std::nothrow) ws_ctx();
+    if (!ctx) return WS_ERR_NOMEM;
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) {
+        delete ctx;
+        return WS_ERR_CUDA;
+    }
+    ctx->device = device;
+    cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, device);
+    if ((e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&ctx->staged, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&ctx->launched, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaMalloc(&ctx->err_d, 4 * sizeof(uint32_t))) != cudaSuccess ||
+        (e = ctx->count_h.ensure(64)) != cudaSuccess) {
+        ws_destroy(ctx);
+        return WS_ERR_CUDA;
+    }
+    cudaMemset(ctx->err_d, 0, 4 * sizeof(uint32_t));
+    ctx->params.keys_tile = 2048;
+    ctx->params.pass_tile = 4096;
+    ctx->params.ctas_per_sm = 0;
+    ctx->params.spin_limit = 1u << 22;
+    *out = ctx;
+    return WS_OK;
+}
+
+extern "C" int ws_destroy(ws_ctx* ctx) {
+    if (!ctx) return WS_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    cudaDeviceSynchronize();
+    ctx->scratch.release();
+    ctx->jobs_d.release();
+    ctx->items_d.release();
+    ctx->out_d.release();
+    ctx->jobs_h.release();
+    ctx->items_h.release();
+    ctx->count_h.release();
+    if (ctx->err_d) cudaFree(ctx->err_d);
+    if (ctx->staged) cudaEventDestroy(ctx->staged);
+    if (ctx->launched) cudaEventDestroy(ctx->launched);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    for (ws_cloud* c : ctx->freed) delete c;
+    delete ctx;
+    return WS_OK;
+}
+
+extern "C" const char* ws_last_error(const ws_ctx* ctx) { return ctx ? ctx->err.c_str() : "no context"; }
+
+extern "C" int ws_sync(ws_ctx* ctx) {
+    if (!ctx) return WS_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return cuda_error(ctx, e, "ws_sync");
+    return take_device_error(ctx);
+}
+
+extern "C" int ws_get_params(const ws_ctx* ctx, ws_params* out) {
+    if (!ctx || !out) return WS_ERR_ARG;
+    *out = ctx->params;
+    return WS_OK;
+}
+
+extern "C" int ws_set_params(ws_ctx* ctx, const ws_params* p) {
+    if (!ctx || !p) return WS_ERR_ARG;
+    if (p->keys_tile == 0 || p->keys_tile % kThreads || p->keys_tile > 8192)
+        return set_error(ctx, WS_ERR_ARG, "ws_set_params: keys_tile must be a multiple of %d, at most 8192", kThreads);
+    if (p->pass_tile != 2048 && p->pass_tile != 4096)
+        return set_error(ctx, WS_ERR_ARG, "ws_set_params: pass_tile must be 2048 or 4096");
+    if (p->spin_limit == 0) return set_error(ctx, WS_ERR_ARG, "ws_set_params: spin_limit must be positive");
+    ctx->params = *p;
+    ctx->items_valid = false;
+    return WS_OK;
+}
+
+// ------------------------------------------------------------------ clouds
+
+static int sniff(ws_ctx* ctx, const uint8_t* d, size_t nbytes) {
+    // The order of parseSplats (src/scene/splats.js:60-76).
+    if (nbytes >= 8 && d[0] == 0x4e && d[1] == 0x47 && d[2] == 0x53 && d[3] == 0x50) {
+        uint32_t version;
+        std::memcpy(&version, d + 4, 4);
+        if (version >= 4)
+            return set_error(ctx, WS_ERR_FORMAT,
+                             "splats: a .spz of version 4, compressed with zstd, which browsers cannot unpack; "
+                             "save it as version 3, or as a .ply or .splat");
+    }
+    if (nbytes >= 4 && d[0] == 0x70 && d[1] == 0x6c && d[2] == 0x79 && (d[3] == 0x0a || d[3] == 0x0d))
+        return set_error(ctx, WS_ERR_FORMAT, "splats: a .ply is not read here: only .splat records are");
+    if (nbytes >= 4 && d[0] == 0x50 && d[1] == 0x4b && d[2] == 0x03 && d[3] == 0x04)
+        return set_error(ctx, WS_ERR_FORMAT, "splats: this is a zip: unpack it with readSplats, which reads a .sog");
+    if (nbytes >= 2 && d[0] == 0x1f && d[1] == 0x8b)
+        return set_error(ctx, WS_ERR_FORMAT, "splats: this is gzipped: unpack it with readSplats, which reads a .spz");
+    if (nbytes == 0 || nbytes % 32 != 0)
+        return set_error(ctx, WS_ERR_FORMAT,
+                         "splats: not a .ply, and %zu bytes is not a whole number of 32-byte .splat records", nbytes);
+    if (nbytes / 32 > WS_MAX_SPLATS)
+        return set_error(ctx, WS_ERR_CAPACITY, "splats: %zu splats are more than this device holds in one buffer, %u",
+                         nbytes / 32, WS_MAX_SPLATS);
+    return WS_OK;
+}
+
+static int decode_cloud(ws_ctx* ctx, const void* dev_records, uint32_t n, ws_cloud** out) {
+    cudaError_t e;
+    ws_cloud* c = new (std::nothrow) ws_cloud();
+    if (!c) return set_error(ctx, WS_ERR_NOMEM, "ws_cloud: out of host memory");
+    c->ctx = ctx;
+    c->n = n;
+    const size_t np = pad_splats(n);
+    if ((e = cudaMalloc(&c->centers, np * sizeof(float4))) != cudaSuccess ||
+        (e = cudaMalloc(&c->cov, np * 3 * sizeof(float2))) != cudaSuccess) {
+        ws_cloud_free(c);
+        return cuda_error(ctx, e, "ws_cloud");
+    }
+    uint32_t* words = nullptr;   // bounds[6], bad
+    if ((e = cudaMalloc(&words, 8 * sizeof(uint32_t))) != cudaSuccess) {
+        ws_cloud_free(c);
+        return cuda_error(ctx, e, "ws_cloud");
+    }
+    const uint32_t init[8] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0u, 0u, 0u, 0xFFFFFFFFu, 0u};
+    cudaMemcpyAsync(words, init, sizeof(init), cudaMemcpyHostToDevice, ctx->stream);
+    cudaMemsetAsync(c->centers, 0, np * sizeof(float4), ctx->stream);
+    cudaMemsetAsync(c->cov, 0, np * 3 * sizeof(float2), ctx->stream);
+    e = launch_decode(dev_records, n, c->centers, c->cov, words, words + 6, ctx->sms, ctx->stream);
+    uint32_t back[8];
+    if (e == cudaSuccess) e = cudaMemcpyAsync(back, words, sizeof(back), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    cudaFree(words);
+    if (e != cudaSuccess) {
+        ws_cloud_free(c);
+        return cuda_error(ctx, e, "ws_cloud decode");
+    }
+    if (back[6] != 0xFFFFFFFFu) {
+        ws_cloud_free(c);
+        return set_error(ctx, WS_ERR_NAN, "splats: splat %u has a position that is not a number", back[6]);
+    }
+    for (int k = 0; k < 3; ++k) {
+        uint32_t lo = back[k], hi = back[3 + k];
+        lo = (lo & 0x80000000u) ? (lo & 0x7FFFFFFFu) : ~lo;
+        hi = (hi & 0x80000000u) ? (hi & 0x7FFFFFFFu) : ~hi;
+        float flo, fhi;
+        std::memcpy(&flo, &lo, 4);
+        std::memcpy(&fhi, &hi, 4);
+        c->bmin[k] = flo;
+        c->bmax[k] = fhi;
+    }
+    c->magic = kCloudMagic;
+    c->alive = true;
+    *out = c;
+    return WS_OK;
+}
+
+extern "C" int ws_cloud_from_splat(ws_ctx* ctx, const uint8_t* bytes, size_t nbytes, ws_cloud** out) {
+    if (!ctx || !out || (!bytes && nbytes)) return set_error(ctx, WS_ERR_ARG, "ws_cloud_from_splat: null argument");
+    *out = nullptr;
+    cudaSetDevice(ctx->device);
+    int rc = sniff(ctx, bytes, nbytes);
+    if (rc) return rc;
+    void* staging = nullptr;
+    cudaError_t e = cudaMalloc(&staging, nbytes);
+    if (e != cudaSuccess) return cuda_error(ctx, e, "ws_cloud_from_splat");
+    e = cudaMemcpyAsync(staging, bytes, nbytes, cudaMemcpyHostToDevice, ctx->stream);
+    if (e != cudaSuccess) {
+        cudaFree(staging);
+        return cuda_error(ctx, e, "ws_cloud_from_splat upload");
+    }
+    rc = decode_cloud(ctx, staging, (uint32_t)(nbytes / 32), out);
+    cudaFree(staging);
+    return rc;
+}
+
+extern "C" int ws_cloud_from_device(ws_ctx* ctx, const void* dev, size_t nbytes, ws_cloud** out) {
+    if (!ctx || !out || (!dev && nbytes)) return set_error(ctx, WS_ERR_ARG, "ws_cloud_from_device: null argument");
+    *out = nullptr;
+    cudaSetDevice(ctx->device);
+    if (reinterpret_cast<uintptr_t>(dev) % 16)
+        return set_error(ctx, WS_ERR_ARG, "ws_cloud_from_device: records must be 16-byte aligned");
+    uint8_t head[8] = {0};
+    if (nbytes) {
+        cudaError_t e = cudaMemcpy(head, dev, nbytes < 8 ? nbytes : 8, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return cuda_error(ctx, e, "ws_cloud_from_device");
+    }
+    int rc = sniff(ctx, head, nbytes);
+    if (rc) return rc;
+    return decode_cloud(ctx, dev, (uint32_t)(nbytes / 32), out);
+}
+
+extern "C" int ws_cloud_info(const ws_cloud* c, uint32_t* count, double mn[3], double mx[3]) {
+    if (!c || c->magic != kCloudMagic) return WS_ERR_ARG;
+    if (!c->alive) return WS_ERR_UNLOADED;
+    if (count) *count = c->n;
+    for (int k = 0; k < 3; ++k) {
+        if (mn) mn[k] = c->bmin[k];
+        if (mx) mx[k] = c->bmax[k];
+    }
+    return WS_OK;
+}
+
+extern "C" int ws_cloud_download(const ws_cloud* c, float* centers, float* covariances) {
+    if (!c || c->magic != kCloudMagic) return WS_ERR_ARG;
+    if (!c->alive) return WS_ERR_UNLOADED;
+    cudaSetDevice(c->ctx->device);
+    cudaError_t e = cudaStreamSynchronize(c->ctx->stream);
+    if (e == cudaSuccess && centers) e = cudaMemcpy(centers, c->centers, (size_t)c->n * 16, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && covariances)
+        e = cudaMemcpy(covariances, c->cov, (size_t)c->n * 24, cudaMemcpyDeviceToHost);
+    return e == cudaSuccess ? WS_OK : cuda_error(c->ctx, e, "ws_cloud_download");
+}
+
+extern "C" int ws_cloud_free(ws_cloud* c) {
+    if (!c) return WS_ERR_ARG;
+    if (c->magic != kCloudMagic) {   // a half-built cloud from a failed load
+        if (c->centers) cudaFree(c->centers);
+        if (c->cov) cudaFree(c->cov);
+        delete c;
+        return WS_OK;
+    }
+    if (!c->alive) return WS_ERR_UNLOADED;
+    cudaSetDevice(c->ctx->device);
+    // A sort in flight may still read the cloud.
+    cudaDeviceSynchronize();
+    if (c->centers) cudaFree(c->centers);
+    if (c->cov) cudaFree(c->cov);
+    c->centers = nullptr;
+    c->cov = nullptr;
+    // The handle stays valid (and refused by every call) until its context
+    // is destroyed, so a sort of a freed cloud is an error, not a crash.
+    c->alive = false;
+    c->ctx->freed.push_back(c);
+    return WS_OK;
+}
+
+extern "C" int ws_depth_range(const ws_cloud* c, const float mv[16], int* visible, float* dmin, float* dscale) {
+    if (!c || !mv || !visible || !dmin || !dscale || c->magic != kCloudMagic) return WS_ERR_ARG;
+    if (!c->alive) return WS_ERR_UNLOADED;
+    host_depth_range(mv, c->bmin, c->bmax, visible, dmin, dscale);
+    return WS_OK;
+}
+
+// ------------------------------------------------------------------ sorting
+
+extern "C" int ws_sort(ws_ctx* ctx, const ws_cloud* cloud, const ws_view* view, uint32_t* order, uint32_t* keys,
+                       uint32_t* count, int flags, void* stream_p) {
+    if (!ctx) return WS_ERR_ARG;
+    int rc;
+    if ((rc = check_cloud(ctx, cloud)) || (rc = check_view(ctx, view))) return rc;
+    if (!order || !count) return set_error(ctx, WS_ERR_ARG, "ws_sort: order and count are required");
+    if (flags != WS_HOST_OUTPUT && flags != WS_DEVICE_OUTPUT) return set_error(ctx, WS_ERR_ARG, "ws_sort: bad flags");
+    cudaSetDevice(ctx->device);
+    cudaStream_t stream = stream_p ? static_cast<cudaStream_t>(stream_p) : ctx->stream;
+    ws_job job;
+    job.cloud = cloud;
+    job.view = *view;
+    if (flags == WS_DEVICE_OUTPUT) {
+        job.order = order;
+        job.keys = keys;
+        job.count = count;
+        return run_batch(ctx, &job, 1, stream);
+    }
+    // Host output: sort into the context's device buffers, then copy back
+    // the survivors only.
+    const size_t n = cloud->n;
+    cudaError_t e;
+    if ((e = cudaEventSynchronize(ctx->launched)) != cudaSuccess) return cuda_error(ctx, e, "ws_sort");
+    if ((e = ctx->out_d.ensure(align_up((2 * n + 1) * sizeof(uint32_t), 256))) != cudaSuccess)
+        return cuda_error(ctx, e, "ws_sort output");
+    uint32_t* d = static_cast<uint32_t*>(ctx->out_d.p);
+    job.order = d;
+    job.keys = keys ? d + n : nullptr;
+    job.count = d + 2 * n;
+    if ((rc = run_batch(ctx, &job, 1, stream))) return rc;
+    uint32_t* hc = static_cast<uint32_t*>(ctx->count_h.p);
+    if ((e = cudaMemcpyAsync(hc, job.count, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(hc + 1, ctx->err_d, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(stream)) != cudaSuccess)
+        return cuda_error(ctx, e, "ws_sort");
+    if (hc[1]) return take_device_error(ctx);
+    const uint32_t s = hc[0];
+    *count = s;
+    if (s) {
+        if ((e = cudaMemcpyAsync(order, job.order, (size_t)s * 4, cudaMemcpyDeviceToHost, stream)) != cudaSuccess)
+            return cuda_error(ctx, e, "ws_sort download");
+        if (keys && (e = cudaMemcpyAsync(keys, job.keys, (size_t)s * 4, cudaMemcpyDeviceToHost, stream)) != cudaSuccess)
+            return cuda_error(ctx, e, "ws_sort download");
+        if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return cuda_error(ctx, e, "ws_sort download");
+    }
+    return WS_OK;
+}
+
+extern "C" int ws_sort_batch(ws_ctx* ctx, int njobs, const ws_job* jobs, void* stream_p) {
+    if (!ctx) return WS_ERR_ARG;
+    if (njobs < 0 || (njobs && !jobs)) return set_error(ctx, WS_ERR_ARG, "ws_sort_batch: bad job list");
+    if (njobs == 0) return WS_OK;
+    if (njobs > (1 << 20)) return set_error(ctx, WS_ERR_ARG, "ws_sort_batch: too many jobs");
+    for (int j = 0; j < njobs; ++j) {
+        int rc;
+        if ((rc = check_cloud(ctx, jobs[j].cloud)) || (rc = check_view(ctx, &jobs[j].view))) return rc;
+        if (!jobs[j].order || !jobs[j].count) return set_error(ctx, WS_ERR_ARG, "ws_sort_batch: job %d has no output", j);
+    }
+    cudaSetDevice(ctx->device);
+    return run_batch(ctx, jobs, njobs, stream_p ? static_cast<cudaStream_t>(stream_p) : ctx->stream);
+}
+
+// ------------------------------------------------------------------ plans
+
+struct ws_plan {
+    ws_ctx* ctx;
+    int njobs;
+    std::vector<ws_job> jobs;
+    DevBuf scratch, jobs_d, items_d;
+    HostBuf jobs_h;
+    uint32_t n_items;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaEvent_t done = nullptr;
+    int grid;
+};
+
+extern "C" int ws_plan_create(ws_ctx* ctx, int njobs, const ws_job* jobs, ws_plan** out) {
+    if (!ctx || !out) return WS_ERR_ARG;
+    *out = nullptr;
+    if (njobs <= 0 || !jobs) return set_error(ctx, WS_ERR_ARG, "ws_plan_create: no jobs");
+    for (int j = 0; j < njobs; ++j) {
+        int rc;
+        if ((rc = check_cloud(ctx, jobs[j].cloud)) || (rc = check_view(ctx, &jobs[j].view))) return rc;
+        if (!jobs[j].order || !jobs[j].count) return set_error(ctx, WS_ERR_ARG, "ws_plan_create: job %d has no output", j);
+    }
+    cudaSetDevice(ctx->device);
+    ws_plan* p = new (std::nothrow) ws_plan();
+    if (!p) return set_error(ctx, WS_ERR_NOMEM, "ws_plan_create: out of host memory");
+    p->ctx = ctx;
+    p->njobs = njobs;
+    p->jobs.assign(jobs, jobs + njobs);
+    std::vector<uint32_t> ns(njobs);
+    for (int j = 0; j < njobs; ++j) ns[j] = jobs[j].cloud->n;
+    cudaError_t e;
+    const size_t need = launch_scratch_bytes(ns.data(), njobs, ctx->params);
+    if ((e = p->scratch.ensure(need)) != cudaSuccess || (e = p->jobs_d.ensure(njobs * sizeof(JobDesc))) != cudaSuccess ||
+        (e = p->jobs_h.ensure(njobs * sizeof(JobDesc))) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&p->done, cudaEventDisableTiming)) != cudaSuccess) {
+        ws_plan_destroy(p);
+        return cuda_error(ctx, e, "ws_plan_create");
+    }
+    JobDesc* hj = static_cast<JobDesc*>(p->jobs_h.p);
+    layout_jobs(hj, jobs, njobs, ctx->params, static_cast<char*>(p->scratch.p));
+    std::vector<uint2> items;
+    build_items(items, hj, njobs);
+    p->n_items = (uint32_t)items.size();
+    if ((e = p->items_d.ensure(items.size() * sizeof(uint2))) != cudaSuccess ||
+        (e = cudaMemcpy(p->items_d.p, items.data(), items.size() * sizeof(uint2), cudaMemcpyHostToDevice)) !=
+            cudaSuccess) {
+        ws_plan_destroy(p);
+        return cuda_error(ctx, e, "ws_plan_create");
+    }
+    p->grid = grid_for(ctx, items.size());
+    // Capture: upload the job table from pinned memory, reset the counters,
+    // launch.
+    cudaStream_t cs;
+    if ((e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking)) != cudaSuccess) {
+        ws_plan_destroy(p);
+        return cuda_error(ctx, e, "ws_plan_create");
+    }
+    e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        cudaMemcpyAsync(p->jobs_d.p, hj, njobs * sizeof(JobDesc), cudaMemcpyHostToDevice, cs);
+        cudaMemsetAsync(p->scratch.p, 0, sizeof(LaunchCtl) + (size_t)njobs * sizeof(JobCtl), cs);
+        launch_sort(static_cast<JobDesc*>(p->jobs_d.p), static_cast<uint2*>(p->items_d.p), p->n_items,
+                    static_cast<LaunchCtl*>(p->scratch.p), ctx->err_d, ctx->params.keys_tile, ctx->params.pass_tile,
+                    ctx->params.spin_limit, p->grid, cs);
+        e = cudaStreamEndCapture(cs, &p->graph);
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&p->exec, p->graph, 0);
+    cudaStreamDestroy(cs);
+    if (e != cudaSuccess) {
+        ws_plan_destroy(p);
+        return cuda_error(ctx, e, "ws_plan_create capture");
+    }
+    *out = p;
+    return WS_OK;
+}
+
+extern "C" int ws_plan_set_views(ws_plan* p, const ws_view* views) {
+    if (!p || !views) return WS_ERR_ARG;
+    for (int j = 0; j < p->njobs; ++j) {
+        int rc = check_view(p->ctx, &views[j]);
+        if (rc) return rc;
+    }
+    cudaSetDevice(p->ctx->device);
+    cudaError_t e = cudaEventSynchronize(p->done);
+    if (e != cudaSuccess) return cuda_error(p->ctx, e, "ws_plan_set_views");
+    JobDesc* hj = static_cast<JobDesc*>(p->jobs_h.p);
+    for (int j = 0; j < p->njobs; ++j) {
+        std::memcpy(hj[j].mv, views[j].model_view, sizeof(hj[j].mv));
+        std::memcpy(hj[j].proj, views[j].projection, sizeof(hj[j].proj));
+        hj[j].viewport[0] = views[j].viewport[0];
+        hj[j].viewport[1] = views[j].viewport[1];
+        hj[j].cull = views[j].cull;
+        p->jobs[j].view = views[j];
+    }
+    return WS_OK;
+}
+
+extern "C" int ws_plan_launch(ws_plan* p, void* stream_p) {
+    if (!p) return WS_ERR_ARG;
+    for (int j = 0; j < p->njobs; ++j) {
+        int rc = check_cloud(p->ctx, p->jobs[j].cloud);
+        if (rc) return rc;
+    }
+    cudaSetDevice(p->ctx->device);
+    cudaStream_t stream = stream_p ? static_cast<cudaStream_t>(stream_p) : p->ctx->stream;
+    // One launch of a plan at a time on the device: it owns one scratch.
+    cudaStreamWaitEvent(stream, p->done, 0);
+    cudaError_t e = cudaGraphLaunch(p->exec, stream);
+    if (e != cudaSuccess) return cuda_error(p->ctx, e, "ws_plan_launch");
+    cudaEventRecord(p->done, stream);
+    return WS_OK;
+}
+
+extern "C" int ws_plan_destroy(ws_plan* p) {
+    if (!p) return WS_ERR_ARG;
+    cudaSetDevice(p->ctx->device);
+    if (p->done) {
+        cudaEventSynchronize(p->done);
+        cudaEventDestroy(p->done);
+    }
+    if (p->exec) cudaGraphExecDestroy(p->exec);
+    if (p->graph) cudaGraphDestroy(p->graph);
+    p->scratch.release();
+    p->jobs_d.release();
+    p->items_d.release();
+    p->jobs_h.release();
+    delete p;
+    return WS_OK;
+}
+
+// ------------------------------------------------------------------ buffers
+
+extern "C" int ws_device_alloc(ws_ctx* ctx, size_t bytes, void** out) {
+    if (!ctx || !out) return WS_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    *out = nullptr;
+    cudaError_t e = cudaMalloc(out, bytes ? bytes : 4);
+    if (e != cudaSuccess) {
+        *out = nullptr;
+        return cuda_error(ctx, e, "ws_device_alloc");
+    }
+    return WS_OK;
+}
+
+extern "C" int ws_device_free(ws_ctx* ctx, void* ptr) {
+    if (!ctx) return WS_ERR_ARG;
+    if (!ptr) return WS_OK;
+    cudaSetDevice(ctx->device);
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e == cudaSuccess) e = cudaFree(ptr);
+    return e == cudaSuccess ? WS_OK : cuda_error(ctx, e, "ws_device_free");
+}
+
+extern "C" int ws_device_download(ws_ctx* ctx, const void* src, void* dst, size_t bytes, void* stream_p) {
+    if (!ctx || (bytes && (!src || !dst))) return WS_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e == cudaSuccess && stream_p) e = cudaStreamSynchronize(static_cast<cudaStream_t>(stream_p));
+    if (e == cudaSuccess && bytes) e = cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_error(ctx, e, "ws_device_download");
+    return take_device_error(ctx);
+}

@@ -1,0 +1,62 @@
+// Host-side state behind the opaque handles of include/wsort.h.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "wsort.h"
+
+namespace wsort {
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    cudaError_t ensure(size_t n);
+    void release();
+};
+
+struct HostBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    cudaError_t ensure(size_t n);
+    void release();
+};
+
+constexpr uint32_t kCloudMagic = 0x57534F52u;   // "WSOR"
+
+int set_error(ws_ctx* ctx, int code, const char* fmt, ...);
+int cuda_error(ws_ctx* ctx, cudaError_t e, const char* what);
+
+}  // namespace wsort
+
+struct ws_ctx {
+    int device = 0;
+    int sms = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t staged = nullptr;     // the last upload from pinned staging finished
+    cudaEvent_t launched = nullptr;   // the last launch on this context's scratch finished
+    std::string err;
+    ws_params params{};
+    wsort::DevBuf scratch, jobs_d, items_d, out_d;
+    wsort::HostBuf jobs_h, items_h, count_h;
+    uint32_t* err_d = nullptr;        // sticky device error: code, work item
+    std::vector<uint2> items;
+    std::vector<uint32_t> last_ns;
+    uint32_t last_keys_tile = 0, last_pass_tile = 0;
+    bool items_valid = false;
+    uint64_t launches = 0;
+    std::vector<struct ws_cloud*> freed;   // freed clouds, kept as refusable handles
+};
+
+struct ws_cloud {
+    uint32_t magic = 0;
+    bool alive = false;
+    ws_ctx* ctx = nullptr;
+    uint32_t n = 0;
+    float4* centers = nullptr;
+    float2* cov = nullptr;
+    double bmin[3] = {0, 0, 0}, bmax[3] = {0, 0, 0};
+};
