@@ -1,0 +1,456 @@
+"""Benchmark of the splat depth-key + stable counting sort on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+                    [--workload clusters-1M|uniform-100k|slab-6M|mixed-64] [--cull C]
+
+One step is one sort of one batch of synthetic splats: for the default
+workload (clusters-1M: 1,000,000 splats from 32 Gaussian clusters, one view
+framing them, cull 0.5) one plain ws_sort of the resident cloud. Prints one
+JSON line:
+
+  value        Msplats/s (whole job, all ranks), cloud resident in HBM,
+               outputs to device memory, CUDA events on the launching stream,
+               L2 flushed (a 256 MiB write) before every timed step
+  e2e          the same metric through the public call a user makes
+               (ws_sort with host outputs): per step the view goes up and the
+               count, permutation and keys come back to pinned host memory
+  roofline     the sort kernel's algorithmic bytes / its event-timed duration
+               against the measured HBM copy bandwidth
+  cpu_baseline the CPU oracle (C++ restatement of the reference's path, all
+               host threads) on a bounded sample of the same workload
+  suite        the other measured targets: the plain kernel at 6M splats
+               (slab-6M) and batched vs plain on the 64-job mixed workload
+
+--impl reference times the reference's algorithm on the host CPU instead
+(the oracle port; the reference's own JavaScript needs Node, which this
+machine does not have) and prints the same line with "impl": "reference".
+With N > 1 (torchrun), every rank sorts its own replica of the workload
+(weak scaling, no collective on the data path); the time is the max over
+ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+FALLBACK_HBM_GBS = 6650.0
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="wsort", choices=["wsort", "reference"])
+    ap.add_argument("--workload", default="clusters-1M",
+                    choices=["clusters-1M", "uniform-100k", "slab-6M", "mixed-64"])
+    ap.add_argument("--cull", type=float, default=0.5)
+    ap.add_argument("--no-suite", action="store_true", help="skip the slab-6M / mixed-64 side measurements")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU baseline sample length")
+    return ap.parse_args()
+
+
+def peak_hbm():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def ncu_traffic(workload: str, cull: float):
+    """DRAM bytes per launch of the sort kernel from the committed ncu summary
+    (profiles/traffic.txt: `<workload> <cull> <bytes>` lines), or None."""
+    path = os.path.join(ROOT, "profiles", "traffic.txt")
+    try:
+        for line in open(path):
+            parts = line.split()
+            if len(parts) >= 3 and not line.startswith("#") and parts[0] == workload and float(parts[1]) == cull:
+                return int(float(parts[2]))
+    except OSError:
+        pass
+    return None
+
+
+def make_jobs(workload: str, cull: float, seed_offset: int = 0):
+    from winding_b200 import workloads as W
+    if workload == "clusters-1M":
+        return [W.clusters_1m(seed=1 + seed_offset, cull=cull)]
+    if workload == "uniform-100k":
+        return [W.uniform_100k(seed=0 + seed_offset, cull=cull)]
+    if workload == "slab-6M":
+        return [W.slab_6m(seed=2 + seed_offset, cull=cull)]
+    return W.mixed_64(seed=3 + seed_offset, cull=cull)
+
+
+class Clocks:
+    """nvidia-smi samples of the SM clock and throttle reasons during a region."""
+
+    FIELDS = "clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown," \
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown," \
+             "clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        out, _ = self.proc.communicate(timeout=10)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax = float(parts[1])
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[4:8]):
+                if flag.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_baseline(jobs, seconds: float, threads: int):
+    """The oracle on the host cores: full views of the workload, repeated for
+    about `seconds` (at least once). Returns (Msplats/s, sample text)."""
+    from oracle import oracle as O
+    parsed = [O.parse_splat(j.bytes()) for j in jobs]
+    done = 0
+    sorts = 0
+    t0 = time.perf_counter()
+    while True:
+        for p, j in zip(parsed, jobs):
+            O.sort_view(p, j.view.model_view, j.view.projection, j.view.viewport, j.view.cull, threads=threads)
+            done += p.count
+            sorts += 1
+            if time.perf_counter() - t0 >= seconds:
+                break
+        if time.perf_counter() - t0 >= seconds:
+            break
+    dt = time.perf_counter() - t0
+    return done / dt / 1e6, f"{sorts} full-view sorts ({done} splats) in {dt:.1f} s"
+
+
+def run_reference(args, rank: int):
+    if rank != 0:
+        return
+    jobs = make_jobs(args.workload, args.cull)
+    threads = os.cpu_count() or 1
+    # Each step: one full pass of the workload's views on the host cores.
+    from oracle import oracle as O
+    parsed = [O.parse_splat(j.bytes()) for j in jobs]
+
+    def step():
+        n = 0
+        for p, j in zip(parsed, jobs):
+            O.sort_view(p, j.view.model_view, j.view.projection, j.view.viewport, j.view.cull, threads=threads)
+            n += p.count
+        return n
+
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    total = 0
+    for _ in range(args.steps):
+        total += step()
+    dt = time.perf_counter() - t0
+    value = total / dt / 1e6
+    line = {
+        "impl": "reference", "metric": "Msplats/s sorted (bit-exact stable order)", "value": value,
+        "unit": "Msplats/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 keys, u32 sort", "data": "synthetic (seeded)",
+        "config": {"workload": args.workload, "splats_per_step": total // args.steps, "cull": args.cull,
+                   "viewport": [1920, 1080]},
+        "cpu_baseline": {"value": value, "unit": "Msplats/s", "cores": threads, "kind": "port",
+                         "sample": f"{args.steps} steps of the full workload; C++ restatement of the reference's "
+                                   f"makeKeys + stable counting sort (the reference's JavaScript needs Node, absent)"},
+        "e2e": {"value": value, "unit": "Msplats/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def timed_sorts(ctx, torch, steps, flush, fn):
+    """Runs fn() `steps` times, each bracketed by CUDA events on torch's
+    current stream with an L2 flush before it. Returns total ms."""
+    stream = torch.cuda.current_stream()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for a, b in evs:
+        flush.zero_()
+        a.record(stream)
+        fn()
+        b.record(stream)
+    torch.cuda.synchronize()
+    return sum(a.elapsed_time(b) for a, b in evs)
+
+
+def plain_measure(ctx, torch, jobs, steps, warmup, flush):
+    """Plain ws_sort per job (device outputs). Returns dict with totals."""
+    from winding_b200 import make_view, parse_splats
+    stream = torch.cuda.current_stream().cuda_stream
+    clouds, outs, views = [], [], []
+    for j in jobs:
+        sp = parse_splats(j.records, ctx)
+        n = max(sp.count, 1)
+        o = torch.empty(n, dtype=torch.int32, device="cuda")
+        k = torch.empty(n, dtype=torch.int32, device="cuda")
+        c = torch.zeros(1, dtype=torch.int32, device="cuda")
+        clouds.append(sp)
+        outs.append((o, k, c))
+        views.append(make_view(j.view.model_view, j.view.projection, j.view.viewport, j.view.cull))
+
+    def one():
+        for sp, v, (o, k, c) in zip(clouds, views, outs):
+            ctx.sort_device(sp, v, o.data_ptr(), k.data_ptr(), c.data_ptr(), stream)
+
+    for _ in range(warmup):
+        one()
+    torch.cuda.synchronize()
+    ctx.timing(True)
+    ms = timed_sorts(ctx, torch, steps, flush, one)
+    kms, launches = ctx.timing_read()
+    ctx.timing(False)
+    survivors = [int(c.item()) for _, _, c in outs]
+    return {"clouds": clouds, "views": views, "outs": outs, "ms": ms, "kernel_ms": kms, "launches": launches,
+            "survivors": survivors, "splats": sum(sp.count for sp in clouds)}
+
+
+def survivors_at_cull0(ctx, torch, plain):
+    """Splats that pass the frustum and faintness tests (the ones whose
+    covariance the footprint cull reads): the survivor count at cull 0."""
+    from winding_b200 import make_view
+    stream = torch.cuda.current_stream().cuda_stream
+    out = []
+    for sp, v, (o, k, c) in zip(plain["clouds"], plain["views"], plain["outs"]):
+        v0 = make_view(np.ctypeslib.as_array(v.model_view), np.ctypeslib.as_array(v.projection),
+                       (v.viewport[0], v.viewport[1]), 0.0)
+        ctx.sort_device(sp, v0, o.data_ptr(), k.data_ptr(), c.data_ptr(), stream)
+        torch.cuda.synchronize()
+        out.append(int(c.item()))
+    return out
+
+
+def algorithmic_bytes(n, s):
+    """The per-(cloud, view) figure the roofline uses: every 32-byte .splat
+    record read once and a u32 index plus a u32 key written per survivor,
+    32 N + 8 S."""
+    return 32 * n + 8 * s
+
+
+def layout_bytes(n, n_front, s, cull):
+    """The same work in the resident layout the reference's GPU path (and
+    this library) keeps: each splat's 16-byte centre, the 24-byte covariance
+    of every splat the footprint cull examines (cull > 0), and 8 bytes per
+    survivor."""
+    return 16 * n + (24 * n_front if cull > 0 else 0) + 8 * s
+
+
+def run_wsort(args, rank, world, local_rank):
+    import torch
+    torch.cuda.set_device(local_rank)
+    # One explicit stream for the flush, the sorts and the events.
+    with torch.cuda.stream(torch.cuda.Stream()):
+        _run_wsort(args, rank, world, local_rank, torch)
+
+
+def _run_wsort(args, rank, world, local_rank, torch):
+    from winding_b200 import Context
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+    ctx = Context(local_rank)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device="cuda")
+    jobs = make_jobs(args.workload, args.cull, seed_offset=0)
+
+    plain = plain_measure(ctx, torch, jobs, 0, args.warmup, flush)   # load + warm
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(local_rank)
+    clocks.start()
+    ctx.timing(True)
+    stream = torch.cuda.current_stream().cuda_stream
+
+    def one():
+        for sp, v, (o, k, c) in zip(plain["clouds"], plain["views"], plain["outs"]):
+            ctx.sort_device(sp, v, o.data_ptr(), k.data_ptr(), c.data_ptr(), stream)
+
+    ms = timed_sorts(ctx, torch, args.steps, flush, one)
+    kms, launches = ctx.timing_read()
+    ctx.timing(False)
+    clk = clocks.stop()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    splats_per_step = plain["splats"]
+    value = splats_per_step * world * args.steps / (ms_max / 1e3) / 1e6
+    survivors = [int(c.item()) for _, _, c in plain["outs"]]
+
+    # End to end through the public call: host outputs, every step.
+    n_max = max(sp.count for sp in plain["clouds"])
+    host_order = torch.empty(n_max, dtype=torch.int32).pin_memory()
+    host_keys = torch.empty(n_max, dtype=torch.int32).pin_memory()
+    import ctypes
+    cnt = ctypes.c_uint32()
+    from winding_b200 import _lib
+
+    def one_e2e():
+        for sp, v in zip(plain["clouds"], plain["views"]):
+            ctx.check(ctx.lib.ws_sort(ctx.handle, sp.handle, ctypes.byref(v), host_order.data_ptr(),
+                                      host_keys.data_ptr(), ctypes.byref(cnt), _lib.WS_HOST_OUTPUT, stream))
+
+    for _ in range(2):
+        one_e2e()
+    e2e_steps = max(3, min(args.steps, 20))
+    e2e_ms = timed_sorts(ctx, torch, e2e_steps, flush, one_e2e)
+    view_bytes = 35 * 4 * len(jobs)
+    e2e_value = splats_per_step * e2e_steps / (e2e_ms / 1e3) / 1e6
+    d2h = sum(4 + 8 * s for s in survivors)
+
+    line = {
+        "metric": "Msplats/s sorted (bit-exact stable order)", "value": value, "unit": "Msplats/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 keys, u32 sort",
+        "data": "synthetic (seeded)",
+        "config": {"workload": args.workload, "splats_per_step": splats_per_step, "survivors_per_step": sum(survivors),
+                   "cull": args.cull, "viewport": [1920, 1080], "l2": "flushed (256 MiB write) before each step",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "e2e": {"value": e2e_value, "unit": "Msplats/s", "h2d_bytes_per_step": view_bytes, "d2h_bytes_per_step": d2h,
+                "call": "ws_sort(WS_HOST_OUTPUT) into pinned host buffers"},
+        "gpu_launches": launches,
+        "clocks": clk,
+    }
+    if rank == 0:
+        peak, src = peak_hbm()
+        front = survivors_at_cull0(ctx, torch, plain) if args.cull > 0 else survivors
+        algo = sum(algorithmic_bytes(sp.count, s) for sp, s in zip(plain["clouds"], survivors))
+        lay = sum(layout_bytes(sp.count, f, s, args.cull) for sp, f, s in zip(plain["clouds"], front, survivors))
+        kernel_s = kms / max(launches, 1) / 1e3 * len(jobs)   # per step
+        achieved = algo / kernel_s / 1e9
+        traffic = ncu_traffic(args.workload, args.cull)
+        p = ctx.params
+        line["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                            "frac": achieved / peak, "traffic": traffic, "peak_source": src,
+                            "kernel": f"wsort::sort_kernel (tile {p.tile}, {p.ctas_per_sm} CTAs/SM)",
+                            "kernel_us_per_step": kernel_s * 1e6, "algorithmic_bytes_per_step": algo,
+                            "algorithmic_bytes": "32 N + 8 S",
+                            "layout_bytes_per_step": lay,
+                            "layout_frac": lay / kernel_s / 1e9 / peak}
+        if world == 1:
+            v, sample = cpu_baseline(jobs, args.cpu_seconds, os.cpu_count() or 1)
+            line["cpu_baseline"] = {"value": v, "unit": "Msplats/s", "cores": os.cpu_count() or 1, "kind": "port",
+                                    "sample": sample + "; C++ restatement of the reference's makeKeys + stable "
+                                                       "counting sort, all host threads"}
+        if not args.no_suite and world == 1:
+            try:
+                line["suite"] = suite(ctx, torch, flush, args)
+            except Exception as exc:   # the headline line still prints
+                line["suite"] = {"error": f"{type(exc).__name__}: {exc}"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    for sp in plain["clouds"]:
+        sp.destroy()
+    ctx.close()
+
+
+def suite(ctx, torch, flush, args):
+    """Side measurements of the two targets: the plain kernel at 6M splats
+    against the HBM roofline, and batched vs plain on the mixed workload."""
+    out = {}
+    peak, src = peak_hbm()
+    # slab-6M, plain kernel
+    jobs = make_jobs("slab-6M", 0.5)
+    p = plain_measure(ctx, torch, jobs, 20, 3, flush)
+    n = p["splats"]
+    algo = sum(algorithmic_bytes(sp.count, s) for sp, s in zip(p["clouds"], p["survivors"]))
+    kernel_s = p["kernel_ms"] / p["launches"] / 1e3
+    out["slab-6M"] = {"splats": n, "survivors": p["survivors"][0], "kernel_us": kernel_s * 1e6,
+                      "step_us": p["ms"] / 20 * 1e3, "msplats_s": n / (p["ms"] / 20 / 1e3) / 1e6,
+                      "achieved_gbs": algo / kernel_s / 1e9, "frac": algo / kernel_s / 1e9 / peak,
+                      "peak_source": src, "traffic": ncu_traffic("slab-6M", 0.5)}
+    for sp in p["clouds"]:
+        sp.destroy()
+    del p
+    # mixed-64: 64 plain calls vs one batched launch vs the graph-captured plan
+    jobs = make_jobs("mixed-64", 0.5)
+    p = plain_measure(ctx, torch, jobs, 10, 2, flush)
+    total = p["splats"]
+    specs = [(sp, v, o.data_ptr(), k.data_ptr(), c.data_ptr())
+             for sp, v, (o, k, c) in zip(p["clouds"], p["views"], p["outs"])]
+    stream = torch.cuda.current_stream().cuda_stream
+    for _ in range(2):
+        ctx.sort_batch(specs, stream)
+    b_ms = timed_sorts(ctx, torch, 10, flush, lambda: ctx.sort_batch(specs, stream))
+    plan = ctx.plan(specs)
+    for _ in range(2):
+        plan.launch(stream)
+    g_ms = timed_sorts(ctx, torch, 10, flush, lambda: plan.launch(stream))
+    plan.close()
+    plain_rate = total * 10 / (p["ms"] / 1e3) / 1e6
+    batch_rate = total * 10 / (b_ms / 1e3) / 1e6
+    graph_rate = total * 10 / (g_ms / 1e3) / 1e6
+    out["mixed-64"] = {"jobs": len(jobs), "splats": total, "plain_msplats_s": plain_rate,
+                       "batched_msplats_s": batch_rate, "graph_msplats_s": graph_rate,
+                       "batched_vs_plain": batch_rate / plain_rate, "graph_vs_plain": graph_rate / plain_rate,
+                       "plain_ms_per_step": p["ms"] / 10, "graph_ms_per_step": g_ms / 10}
+    for sp in p["clouds"]:
+        sp.destroy()
+    return out
+
+
+def main():
+    args = parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        run_wsort(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

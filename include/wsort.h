@@ -12,7 +12,8 @@
  *     of the last failure on a context is ws_last_error(ctx). Messages that
  *     have a counterpart in the reference use its wording.
  *   - Plain pointers and sizes only. `stream` is a cudaStream_t passed as
- *     void* (NULL: the context's own stream).
+ *     void* (NULL: the context's own stream, a blocking stream, so work on
+ *     the legacy default stream is ordered before it).
  *   - One context per host thread; a context's calls are not synchronised.
  *     The server object (ws_server_*) is internally synchronised.
  *   - Clouds belong to the context that made them. Output buffers belong to
@@ -190,21 +191,51 @@ int ws_device_download(ws_ctx* ctx, const void* device_src, void* host_dst, size
 /* ------------------------------------------------------------ tuning */
 
 /*
- * Kernel parameters. keys_tile: splats a key work item covers (multiple of
- * 256, at most 8192). pass_tile: elements a digit-pass work item covers
- * (2048 or 4096). ctas_per_sm: resident CTAs per SM of the persistent grid
- * (0: as many as fit). spin_limit: iterations a device-side wait spins
- * before it gives up with WS_ERR_TIMEOUT.
+ * Kernel parameters. tile: splats one work item of the key and digit passes
+ * covers (1024, 2048 or 4096). ctas_per_sm: the kernel variant's resident
+ * CTAs per SM (2, 3 or 4; 0 picks 3), which bounds its registers per
+ * thread. spin_limit: polls a device-side wait makes before it gives up
+ * with WS_ERR_TIMEOUT.
  */
 typedef struct ws_params {
-    uint32_t keys_tile;
-    uint32_t pass_tile;
+    uint32_t tile;
     uint32_t ctas_per_sm;
     uint32_t spin_limit;
+    uint32_t reserved;
 } ws_params;
 
 int ws_get_params(const ws_ctx* ctx, ws_params* out);
 int ws_set_params(ws_ctx* ctx, const ws_params* params);
+
+/* ------------------------------------------------------------ measurement */
+
+/*
+ * Kernel timing for benchmarks (the reference's GpuProfiler role,
+ * src/render/timing.js:1-33): while enabled, every sort launch on ctx is
+ * bracketed by CUDA events recorded on its own stream. ws_timing_read waits
+ * for them and returns the summed kernel time in ms and the number of sort
+ * kernels launched since the previous read (or since enabling).
+ */
+int ws_timing(ws_ctx* ctx, int enable);
+int ws_timing_read(ws_ctx* ctx, double* kernel_ms, uint64_t* launches);
+
+/*
+ * Work-item tracing: while enabled, each sort launch of ctx (not plans)
+ * stamps every work item with the GPU's global timer when its ticket was
+ * claimed, when its dependency wait ended and when it finished, and the SM
+ * it ran on. ws_trace_read waits for the last launch and copies up to `cap`
+ * records of it; *n receives how many it has. phase: 0 keys, 1 low-digit
+ * scan, 2 low-digit scatter, 3 high-digit counts, 4 high-digit scan,
+ * 5 high-digit scatter.
+ */
+typedef struct ws_trace_rec {
+    uint64_t claim_ns, start_ns, end_ns;
+    uint32_t job, phase, tile, sm;
+    uint64_t mark_ns[3];   /* digit passes: inputs staged, ranked, staged for writing (0: none) */
+} ws_trace_rec;
+
+int ws_trace(ws_ctx* ctx, int enable);
+int ws_trace_read(ws_ctx* ctx, ws_trace_rec* out, size_t cap, size_t* n);
 
 #ifdef __cplusplus
 }

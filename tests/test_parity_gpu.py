@@ -202,14 +202,14 @@ def test_batch_equals_each_job_alone(ctx):
         sp.destroy()
 
 
-@pytest.mark.parametrize("keys_tile,pass_tile", [(256, 2048), (1024, 4096), (4096, 2048), (8192, 4096)])
-def test_tile_parameters_do_not_change_the_result(ctx, keys_tile, pass_tile):
+@pytest.mark.parametrize("tile", [1024, 2048, 4096])
+def test_tile_parameters_do_not_change_the_result(ctx, tile):
     old = ctx.params
     try:
-        ctx.set_params(keys_tile=keys_tile, pass_tile=pass_tile)
+        ctx.set_params(tile=tile)
         check_job(ctx, W.clusters_1m(seed=41, n=120_001))
     finally:
-        ctx.set_params(keys_tile=old.keys_tile, pass_tile=old.pass_tile)
+        ctx.set_params(tile=old.tile)
 
 
 def test_full_size_slab_properties(ctx):

@@ -65,10 +65,10 @@ class WsJob(ctypes.Structure):
 
 class WsParams(ctypes.Structure):
     _fields_ = [
-        ("keys_tile", ctypes.c_uint32),
-        ("pass_tile", ctypes.c_uint32),
+        ("tile", ctypes.c_uint32),
         ("ctas_per_sm", ctypes.c_uint32),
         ("spin_limit", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32),
     ]
 
 
@@ -102,6 +102,19 @@ class WsServerStats(ctypes.Structure):
     ]
 
 
+class WsTraceRec(ctypes.Structure):
+    _fields_ = [
+        ("claim_ns", ctypes.c_uint64),
+        ("start_ns", ctypes.c_uint64),
+        ("end_ns", ctypes.c_uint64),
+        ("job", ctypes.c_uint32),
+        ("phase", ctypes.c_uint32),
+        ("tile", ctypes.c_uint32),
+        ("sm", ctypes.c_uint32),
+        ("mark_ns", ctypes.c_uint64 * 3),
+    ]
+
+
 vp = ctypes.c_void_p
 u32p = ctypes.POINTER(ctypes.c_uint32)
 f32p = ctypes.POINTER(ctypes.c_float)
@@ -130,6 +143,11 @@ SIGNATURES = {
     "ws_device_download": (ctypes.c_int, [vp, vp, vp, ctypes.c_size_t, vp]),
     "ws_get_params": (ctypes.c_int, [vp, ctypes.POINTER(WsParams)]),
     "ws_set_params": (ctypes.c_int, [vp, ctypes.POINTER(WsParams)]),
+    "ws_timing": (ctypes.c_int, [vp, ctypes.c_int]),
+    "ws_timing_read": (ctypes.c_int, [vp, f64p, ctypes.POINTER(ctypes.c_uint64)]),
+    "ws_trace": (ctypes.c_int, [vp, ctypes.c_int]),
+    "ws_trace_read": (ctypes.c_int, [vp, ctypes.POINTER(WsTraceRec), ctypes.c_size_t,
+                                     ctypes.POINTER(ctypes.c_size_t)]),
 }
 
 _lib = None

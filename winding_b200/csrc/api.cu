@@ -14,8 +14,9 @@
 
 namespace wsort {
 cudaError_t launch_sort(const JobDesc* jobs, const uint2* items, uint32_t n_items, LaunchCtl* lctl, uint32_t* err,
-                        uint32_t t1, uint32_t pass_tile, uint32_t spin_limit, int grid, cudaStream_t stream);
-int sort_occupancy(uint32_t pass_tile);
+                        uint32_t tile, int minb, uint32_t spin_limit, int grid, cudaStream_t stream,
+                        TraceRec* trace);
+int sort_occupancy(uint32_t tile, int minb);
 cudaError_t launch_decode(const void* records, uint32_t n, float4* centers, float2* cov, uint32_t* bounds,
                           uint32_t* bad, int sms, cudaStream_t stream);
 
@@ -74,31 +75,86 @@ static size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 uint32_t pad_splats(uint32_t n) { return (uint32_t)align_up(n ? n : 1, kPadSplats); }
 
-// Tile counts and scratch footprint of one job.
-void job_shape(uint32_t n, const ws_params& p, uint32_t* t1, uint32_t* t2, uint32_t* t3, size_t* bytes) {
+// Tile count and scratch footprint of one job.
+void job_shape(uint32_t n, const ws_params& p, uint32_t* tiles, size_t* bytes) {
     const uint32_t n1 = n ? n : 1;
-    *t1 = (n1 + p.keys_tile - 1) / p.keys_tile;
-    *t2 = (n1 + p.pass_tile - 1) / p.pass_tile;
-    *t3 = *t2;
+    *tiles = (n1 + p.tile - 1) / p.tile;
     const size_t np = pad_splats(n);
     size_t b = 0;
-    b += align_up(np * 2, 256);                 // k16
-    b += align_up(np / 8, 256);                 // mask
-    b += align_up(np * 2, 256);                 // key_b
-    b += align_up(np * 4, 256);                 // idx_b
-    b += align_up((size_t)(*t2 + *t3) * 1024, 256);   // status
+    b += align_up(np * 2, 256);                        // k16
+    b += align_up(np / 8, 256);                        // mask
+    b += align_up(np * 2, 256);                        // key_b
+    b += align_up(np * 4, 256);                        // idx_b
+    b += 2 * align_up((size_t)*tiles * 1024, 256);     // cnt_lo, cnt_hi
     *bytes = b;
 }
 
 size_t launch_scratch_bytes(const uint32_t* ns, int njobs, const ws_params& p) {
     size_t total = align_up(sizeof(LaunchCtl) + (size_t)njobs * sizeof(JobCtl), 256);
     for (int j = 0; j < njobs; ++j) {
-        uint32_t t1, t2, t3;
+        uint32_t tiles;
         size_t b;
-        job_shape(ns[j], p, &t1, &t2, &t3, &b);
+        job_shape(ns[j], p, &tiles, &b);
         total += b;
     }
     return total;
+}
+
+// The per-view shortcuts the keys phase may take, proved here on the host:
+//
+// fast_transform: the model-view's last row is (0, 0, 0, 1) and the
+// projection has the zero pattern of a perspective (entries 1, 2, 3, 4, 6,
+// 7, 12, 13, 15 are zero), every entry is finite, and no view-space
+// coordinate of the cloud can overflow (|view_j| <= sum_k |m_jk| R + |m_j3|
+// well below FLT_MAX, R the largest box coordinate). Then view.w is exactly
+// 1 and the dropped projection terms are zeros times finite numbers.
+//
+// keep_byte / keep_q: the footprint shortcut of the keys phase. With
+// A = fx (|W row 0|_1 + |1.3 / p00| |W row 2|_1) and the same for y, and
+// smax the largest |covariance entry| of the cloud, every entry of
+// |T| |Sigma| |T|^T is at most 1.02 max(A)^2 smax / d^2 =: keep_q / d^2.
+// keep_byte is the least alpha byte with RN(alpha * 1.85) >= cull.
+void view_shortcuts(const ws_view& v, const ws_cloud* c, uint32_t* fast, uint32_t* keep_byte, float* keep_q) {
+    const float* M = v.model_view;
+    const float* P = v.projection;
+    bool finite = true;
+    for (int k = 0; k < 16; ++k) finite = finite && std::isfinite(M[k]) && std::isfinite(P[k]);
+    *fast = 0;
+    if (finite && M[3] == 0.0f && M[7] == 0.0f && M[11] == 0.0f && M[15] == 1.0f && P[1] == 0.0f &&
+        P[2] == 0.0f && P[3] == 0.0f && P[4] == 0.0f && P[6] == 0.0f && P[7] == 0.0f && P[12] == 0.0f &&
+        P[13] == 0.0f && P[15] == 0.0f) {
+        double R = 0.0;
+        for (int k = 0; k < 3; ++k) R = std::fmax(R, std::fmax(std::fabs(c->bmin[k]), std::fabs(c->bmax[k])));
+        double vmax = 0.0;
+        for (int j = 0; j < 3; ++j)
+            vmax = std::fmax(vmax, (std::fabs((double)M[j]) + std::fabs((double)M[4 + j]) + std::fabs((double)M[8 + j])) * R +
+                                       std::fabs((double)M[12 + j]));
+        if (std::isfinite(R) && vmax * 1.01 < 1e37) *fast = 1;
+    }
+    *keep_byte = 256;
+    *keep_q = INFINITY;
+    if (!(v.cull > 0.0f) || P[15] != 0.0f || !finite || !(c->smax >= 0.0f) || !std::isfinite(c->smax)) return;
+    const float fx = (P[0] * v.viewport[0]) * 0.5f;
+    const float fy = (P[5] * v.viewport[1]) * 0.5f;
+    const double xhi = std::fabs((double)(1.3f / P[0])), yhi = std::fabs((double)(1.3f / P[5]));
+    const double r0 = std::fabs((double)M[0]) + std::fabs((double)M[4]) + std::fabs((double)M[8]);
+    const double r1 = std::fabs((double)M[1]) + std::fabs((double)M[5]) + std::fabs((double)M[9]);
+    const double r2 = std::fabs((double)M[2]) + std::fabs((double)M[6]) + std::fabs((double)M[10]);
+    const double a0 = std::fabs((double)fx) * (r0 + xhi * r2);
+    const double a1 = std::fabs((double)fy) * (r1 + yhi * r2);
+    const double a = std::fmax(a0, a1);
+    const double q = 1.02 * a * a * (double)c->smax;
+    if (!std::isfinite(q) || q > 1e30) return;
+    float qf = (float)q;
+    if ((double)qf < q) qf = std::nextafter(qf, INFINITY);
+    for (uint32_t b = 0; b < 256; ++b) {
+        const float alpha = (float)b / 255.0f;
+        if (alpha * 1.85f >= v.cull && alpha * 255.0f > 1.0f) {
+            *keep_byte = b;
+            break;
+        }
+    }
+    *keep_q = qf;
 }
 
 // Fills job descriptors and lays the scratch out from `scratch`.
@@ -124,8 +180,9 @@ void layout_jobs(JobDesc* out, const ws_job* jobs, int njobs, const ws_params& p
         d.order = jobs[j].order;
         d.keys = jobs[j].keys;
         d.count = jobs[j].count;
+        view_shortcuts(jobs[j].view, c, &d.fast_transform, &d.keep_byte, &d.keep_q);
         size_t bytes;
-        job_shape(c->n, p, &d.tiles1, &d.tiles2, &d.tiles3, &bytes);
+        job_shape(c->n, p, &d.tiles, &bytes);
         const size_t np = pad_splats(c->n);
         d.k16 = reinterpret_cast<uint16_t*>(at);
         at += align_up(np * 2, 256);
@@ -135,33 +192,42 @@ void layout_jobs(JobDesc* out, const ws_job* jobs, int njobs, const ws_params& p
         at += align_up(np * 2, 256);
         d.idx_b = reinterpret_cast<uint32_t*>(at);
         at += align_up(np * 4, 256);
-        d.status = reinterpret_cast<uint32_t*>(at);
-        at += align_up((size_t)(d.tiles2 + d.tiles3) * 1024, 256);
+        d.cnt_lo = reinterpret_cast<uint32_t*>(at);
+        at += align_up((size_t)d.tiles * 1024, 256);
+        d.cnt_hi = reinterpret_cast<uint32_t*>(at);
+        at += align_up((size_t)d.tiles * 1024, 256);
         d.ctl = reinterpret_cast<uint32_t*>(&ctls[j]);
     }
 }
 
-// Work items, software-pipelined across jobs: the keys of job s, then the
-// low pass of job s-1, then the high pass of job s-2, so that a digit pass
-// rarely waits for the phase before it.
-void build_items(std::vector<uint2>& items, const JobDesc* jobs, int njobs) {
-    items.clear();
-    for (int s = 0; s < njobs + 2; ++s) {
-        if (s < njobs)
-            for (uint32_t t = 0; t < jobs[s].tiles1; ++t) items.push_back(make_uint2(s, (kPhaseKeys << 30) | t));
-        if (s - 1 >= 0 && s - 1 < njobs)
-            for (uint32_t t = 0; t < jobs[s - 1].tiles2; ++t)
-                items.push_back(make_uint2(s - 1, (kPhaseLow << 30) | t));
-        if (s - 2 >= 0 && s - 2 < njobs)
-            for (uint32_t t = 0; t < jobs[s - 2].tiles3; ++t)
-                items.push_back(make_uint2(s - 2, (kPhaseHigh << 30) | t));
-    }
+// Items of one phase of one job.
+static void push_phase(std::vector<uint2>& items, const JobDesc& d, uint32_t job, uint32_t phase) {
+    const uint32_t count = (phase == kPhaseScanLo || phase == kPhaseScanHi) ? kScanItems
+                           : phase == kPhaseCountHi ? (d.tiles + kCountSpan - 1) / kCountSpan
+                                                    : d.tiles;
+    for (uint32_t t = 0; t < count; ++t) items.push_back(make_uint2(job, (phase << kPhaseShift) | t));
 }
 
+// Work items, software-pipelined across jobs: at step s, phase k of job
+// s - k for k = 0..5, so that an item rarely waits for the phase before it.
+void build_items(std::vector<uint2>& items, const JobDesc* jobs, int njobs) {
+    items.clear();
+    for (int s = 0; s < njobs + (int)kPhases - 1; ++s)
+        for (uint32_t k = 0; k < kPhases; ++k) {
+            const int j = s - (int)k;
+            if (j >= 0 && j < njobs) push_phase(items, jobs[j], (uint32_t)j, k);
+        }
+}
+
+// Resident CTAs per SM the kernel variant is built for: ctas_per_sm, or 3.
+int variant_minb(const ws_params& p) { return p.ctas_per_sm >= 2 && p.ctas_per_sm <= 4 ? (int)p.ctas_per_sm : 3; }
+
 int grid_for(ws_ctx* ctx, size_t n_items) {
-    int per_sm = sort_occupancy(ctx->params.pass_tile);
-    if (per_sm < 1) per_sm = 1;
-    if (ctx->params.ctas_per_sm && (int)ctx->params.ctas_per_sm < per_sm) per_sm = (int)ctx->params.ctas_per_sm;
+    const int minb = variant_minb(ctx->params);
+    const int ti = ctx->params.tile == 1024 ? 0 : ctx->params.tile == 2048 ? 1 : 2;
+    int& cached = ctx->occupancy[ti][minb - 2];
+    if (cached == 0) cached = sort_occupancy(ctx->params.tile, minb);
+    int per_sm = cached < 1 ? 1 : cached;
     size_t g = (size_t)ctx->sms * per_sm;
     if (g > n_items) g = n_items ? n_items : 1;
     return (int)g;
@@ -210,8 +276,7 @@ int run_batch(ws_ctx* ctx, const ws_job* jobs, int njobs, cudaStream_t stream) {
 
     // Items depend only on the job sizes and the tiles: reuse the last upload
     // when they are unchanged.
-    bool same = ctx->items_valid && ctx->last_ns == ns && ctx->last_keys_tile == ctx->params.keys_tile &&
-                ctx->last_pass_tile == ctx->params.pass_tile;
+    bool same = ctx->items_valid && ctx->last_ns == ns && ctx->last_tile == ctx->params.tile;
     if (!same) {
         build_items(ctx->items, hj, njobs);
         if ((e = ctx->items_h.ensure(ctx->items.size() * sizeof(uint2))) != cudaSuccess)
@@ -232,8 +297,7 @@ int run_batch(ws_ctx* ctx, const ws_job* jobs, int njobs, cudaStream_t stream) {
                                  cudaMemcpyHostToDevice, stream)) != cudaSuccess)
             return cuda_error(ctx, e, "ws_sort upload");
         ctx->last_ns = ns;
-        ctx->last_keys_tile = ctx->params.keys_tile;
-        ctx->last_pass_tile = ctx->params.pass_tile;
+        ctx->last_tile = ctx->params.tile;
         ctx->items_valid = true;
     }
     cudaEventRecord(ctx->staged, stream);
@@ -241,12 +305,33 @@ int run_batch(ws_ctx* ctx, const ws_job* jobs, int njobs, cudaStream_t stream) {
     if ((e = cudaMemsetAsync(ctx->scratch.p, 0, ctl_bytes, stream)) != cudaSuccess)
         return cuda_error(ctx, e, "ws_sort reset");
     const size_t n_items = ctx->items.size();
+    cudaEvent_t t_stop = nullptr;
+    if (ctx->timing) {
+        if (ctx->timing_used == ctx->timing_events.size()) {
+            cudaEvent_t a, b;
+            if ((e = cudaEventCreate(&a)) != cudaSuccess) return cuda_error(ctx, e, "ws_timing");
+            if ((e = cudaEventCreate(&b)) != cudaSuccess) return cuda_error(ctx, e, "ws_timing");
+            ctx->timing_events.emplace_back(a, b);
+        }
+        cudaEventRecord(ctx->timing_events[ctx->timing_used].first, stream);
+        t_stop = ctx->timing_events[ctx->timing_used].second;
+        ++ctx->timing_used;
+    }
+    TraceRec* trace = nullptr;
+    if (ctx->tracing) {
+        if ((e = ctx->trace_d.ensure(n_items * sizeof(TraceRec))) != cudaSuccess) return cuda_error(ctx, e, "ws_trace");
+        trace = static_cast<TraceRec*>(ctx->trace_d.p);
+        ctx->trace_items = ctx->items;
+        ctx->trace_grid = grid_for(ctx, n_items);
+    }
     e = launch_sort(static_cast<JobDesc*>(ctx->jobs_d.p), static_cast<uint2*>(ctx->items_d.p), (uint32_t)n_items,
-                    static_cast<LaunchCtl*>(ctx->scratch.p), ctx->err_d, ctx->params.keys_tile,
-                    ctx->params.pass_tile, ctx->params.spin_limit, grid_for(ctx, n_items), stream);
+                    static_cast<LaunchCtl*>(ctx->scratch.p), ctx->err_d, ctx->params.tile,
+                    variant_minb(ctx->params), ctx->params.spin_limit, grid_for(ctx, n_items), stream, trace);
     if (e != cudaSuccess) return cuda_error(ctx, e, "ws_sort launch");
+    if (t_stop) cudaEventRecord(t_stop, stream);
     cudaEventRecord(ctx->launched, stream);
     ++ctx->launches;
+    ++ctx->timing_launches;
     return WS_OK;
 }
 
@@ -302,7 +387,9 @@ extern "C" int ws_create(ws_ctx** out, int device) {
     }
     ctx->device = device;
     cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, device);
-    if ((e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+    // A blocking stream: work a caller queued on the legacy default stream
+    // (where torch puts it unless told otherwise) is ordered before a sort.
+    if ((e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamDefault)) != cudaSuccess ||
         (e = cudaEventCreateWithFlags(&ctx->staged, cudaEventDisableTiming)) != cudaSuccess ||
         (e = cudaEventCreateWithFlags(&ctx->launched, cudaEventDisableTiming)) != cudaSuccess ||
         (e = cudaMalloc(&ctx->err_d, 4 * sizeof(uint32_t))) != cudaSuccess ||
@@ -311,9 +398,8 @@ extern "C" int ws_create(ws_ctx** out, int device) {
         return WS_ERR_CUDA;
     }
     cudaMemset(ctx->err_d, 0, 4 * sizeof(uint32_t));
-    ctx->params.keys_tile = 2048;
-    ctx->params.pass_tile = 4096;
-    ctx->params.ctas_per_sm = 0;
+    ctx->params.tile = 2048;
+    ctx->params.ctas_per_sm = 4;
     ctx->params.spin_limit = 1u << 22;
     *out = ctx;
     return WS_OK;
@@ -335,6 +421,10 @@ extern "C" int ws_destroy(ws_ctx* ctx) {
     if (ctx->staged) cudaEventDestroy(ctx->staged);
     if (ctx->launched) cudaEventDestroy(ctx->launched);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    for (auto& pr : ctx->timing_events) {
+        cudaEventDestroy(pr.first);
+        cudaEventDestroy(pr.second);
+    }
     for (ws_cloud* c : ctx->freed) delete c;
     delete ctx;
     return WS_OK;
@@ -358,11 +448,11 @@ extern "C" int ws_get_params(const ws_ctx* ctx, ws_params* out) {
 
 extern "C" int ws_set_params(ws_ctx* ctx, const ws_params* p) {
     if (!ctx || !p) return WS_ERR_ARG;
-    if (p->keys_tile == 0 || p->keys_tile % kThreads || p->keys_tile > 8192)
-        return set_error(ctx, WS_ERR_ARG, "ws_set_params: keys_tile must be a multiple of %d, at most 8192", kThreads);
-    if (p->pass_tile != 2048 && p->pass_tile != 4096)
-        return set_error(ctx, WS_ERR_ARG, "ws_set_params: pass_tile must be 2048 or 4096");
+    if (p->tile != 1024 && p->tile != 2048 && p->tile != 4096)
+        return set_error(ctx, WS_ERR_ARG, "ws_set_params: tile must be 1024, 2048 or 4096");
     if (p->spin_limit == 0) return set_error(ctx, WS_ERR_ARG, "ws_set_params: spin_limit must be positive");
+    if (p->ctas_per_sm != 0 && (p->ctas_per_sm < 2 || p->ctas_per_sm > 4))
+        return set_error(ctx, WS_ERR_ARG, "ws_set_params: ctas_per_sm must be 0, 2, 3 or 4");
     ctx->params = *p;
     ctx->items_valid = false;
     return WS_OK;
@@ -407,16 +497,16 @@ static int decode_cloud(ws_ctx* ctx, const void* dev_records, uint32_t n, ws_clo
         ws_cloud_free(c);
         return cuda_error(ctx, e, "ws_cloud");
     }
-    uint32_t* words = nullptr;   // bounds[6], bad
+    uint32_t* words = nullptr;   // bounds[6], max |covariance|, bad
     if ((e = cudaMalloc(&words, 8 * sizeof(uint32_t))) != cudaSuccess) {
         ws_cloud_free(c);
         return cuda_error(ctx, e, "ws_cloud");
     }
-    const uint32_t init[8] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0u, 0u, 0u, 0xFFFFFFFFu, 0u};
+    const uint32_t init[8] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0u, 0u, 0u, 0u, 0xFFFFFFFFu};
     cudaMemcpyAsync(words, init, sizeof(init), cudaMemcpyHostToDevice, ctx->stream);
     cudaMemsetAsync(c->centers, 0, np * sizeof(float4), ctx->stream);
     cudaMemsetAsync(c->cov, 0, np * 3 * sizeof(float2), ctx->stream);
-    e = launch_decode(dev_records, n, c->centers, c->cov, words, words + 6, ctx->sms, ctx->stream);
+    e = launch_decode(dev_records, n, c->centers, c->cov, words, words + 7, ctx->sms, ctx->stream);
     uint32_t back[8];
     if (e == cudaSuccess) e = cudaMemcpyAsync(back, words, sizeof(back), cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
@@ -425,9 +515,16 @@ static int decode_cloud(ws_ctx* ctx, const void* dev_records, uint32_t n, ws_clo
         ws_cloud_free(c);
         return cuda_error(ctx, e, "ws_cloud decode");
     }
-    if (back[6] != 0xFFFFFFFFu) {
+    if (back[7] != 0xFFFFFFFFu) {
         ws_cloud_free(c);
-        return set_error(ctx, WS_ERR_NAN, "splats: splat %u has a position that is not a number", back[6]);
+        return set_error(ctx, WS_ERR_NAN, "splats: splat %u has a position that is not a number", back[7]);
+    }
+    {
+        const uint32_t o = back[6];
+        const uint32_t u = (o & 0x80000000u) ? (o & 0x7FFFFFFFu) : ~o;
+        float f;
+        std::memcpy(&f, &u, 4);
+        c->smax = o ? f : 0.0f;   // NaN if any entry is NaN (then no shortcut applies)
     }
     for (int k = 0; k < 3; ++k) {
         uint32_t lo = back[k], hi = back[3 + k];
@@ -660,8 +757,8 @@ extern "C" int ws_plan_create(ws_ctx* ctx, int njobs, const ws_job* jobs, ws_pla
         cudaMemcpyAsync(p->jobs_d.p, hj, njobs * sizeof(JobDesc), cudaMemcpyHostToDevice, cs);
         cudaMemsetAsync(p->scratch.p, 0, sizeof(LaunchCtl) + (size_t)njobs * sizeof(JobCtl), cs);
         launch_sort(static_cast<JobDesc*>(p->jobs_d.p), static_cast<uint2*>(p->items_d.p), p->n_items,
-                    static_cast<LaunchCtl*>(p->scratch.p), ctx->err_d, ctx->params.keys_tile, ctx->params.pass_tile,
-                    ctx->params.spin_limit, p->grid, cs);
+                    static_cast<LaunchCtl*>(p->scratch.p), ctx->err_d, ctx->params.tile,
+                    variant_minb(ctx->params), ctx->params.spin_limit, p->grid, cs, nullptr);
         e = cudaStreamEndCapture(cs, &p->graph);
     }
     if (e == cudaSuccess) e = cudaGraphInstantiate(&p->exec, p->graph, 0);
@@ -759,4 +856,66 @@ extern "C" int ws_device_download(ws_ctx* ctx, const void* src, void* dst, size_
     if (e == cudaSuccess && bytes) e = cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return cuda_error(ctx, e, "ws_device_download");
     return take_device_error(ctx);
+}
+
+// ------------------------------------------------------------------ timing
+
+extern "C" int ws_timing(ws_ctx* ctx, int enable) {
+    if (!ctx) return WS_ERR_ARG;
+    ctx->timing = enable != 0;
+    ctx->timing_used = 0;
+    ctx->timing_launches = 0;
+    return WS_OK;
+}
+
+extern "C" int ws_timing_read(ws_ctx* ctx, double* kernel_ms, uint64_t* launches) {
+    if (!ctx) return WS_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    double total = 0.0;
+    for (size_t k = 0; k < ctx->timing_used; ++k) {
+        cudaError_t e = cudaEventSynchronize(ctx->timing_events[k].second);
+        if (e != cudaSuccess) return cuda_error(ctx, e, "ws_timing_read");
+        float ms = 0.0f;
+        e = cudaEventElapsedTime(&ms, ctx->timing_events[k].first, ctx->timing_events[k].second);
+        if (e != cudaSuccess) return cuda_error(ctx, e, "ws_timing_read");
+        total += ms;
+    }
+    if (kernel_ms) *kernel_ms = total;
+    if (launches) *launches = ctx->timing_launches;
+    ctx->timing_used = 0;
+    ctx->timing_launches = 0;
+    return WS_OK;
+}
+
+// ------------------------------------------------------------------ tracing
+
+extern "C" int ws_trace(ws_ctx* ctx, int enable) {
+    if (!ctx) return WS_ERR_ARG;
+    ctx->tracing = enable != 0;
+    return WS_OK;
+}
+
+extern "C" int ws_trace_read(ws_ctx* ctx, ws_trace_rec* out, size_t cap, size_t* n) {
+    if (!ctx || !n) return WS_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e == cudaSuccess) e = cudaEventSynchronize(ctx->launched);
+    if (e != cudaSuccess) return cuda_error(ctx, e, "ws_trace_read");
+    const size_t items = ctx->trace_items.size();
+    *n = items;
+    if (!out || cap == 0 || !ctx->trace_d.p) return WS_OK;
+    std::vector<TraceRec> recs(items);
+    e = cudaMemcpy(recs.data(), ctx->trace_d.p, items * sizeof(TraceRec), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_error(ctx, e, "ws_trace_read");
+    for (size_t k = 0; k < items && k < cap; ++k) {
+        out[k].claim_ns = recs[k].claim;
+        out[k].start_ns = recs[k].start;
+        out[k].end_ns = recs[k].end;
+        out[k].job = ctx->trace_items[k].x;
+        out[k].phase = ctx->trace_items[k].y >> kPhaseShift;
+        out[k].tile = ctx->trace_items[k].y & kTileMask;
+        out[k].sm = recs[k].sm;
+        for (int q = 0; q < 3; ++q) out[k].mark_ns[q] = recs[k].mark[q];
+    }
+    return WS_OK;
 }

@@ -10,20 +10,20 @@
 // stable CPU sort gives (src/render/drawlist.js:186-229): survivors by
 // (key, splat index).
 //
+// Each digit pass is reduce-then-scan: per-tile digit counts (stored digit
+// major), a scan over tiles for each digit (ScanLo / ScanHi) that turns them
+// into each tile's starting offset per digit, then a stable warp-ranked
+// scatter. The low pass's counts
+// come out of the key phase for free. There is no serial chain between
+// tiles, so a pass whose tiles all start at once (they do: each pass waits
+// for the whole of the one before) costs no look-back latency.
+//
 // Work is a queue of items, each (job, phase, tile), claimed in order through
-// one atomic ticket by a persistent grid of CTAs:
-//   phase 0, keys   a tile of splats: cull, key, survivor bit, both digit
-//                   histograms (warp-aggregated with __match_any_sync)
-//   phase 1, low    a tile of splats: rank survivors by the low key byte
-//                   (stable warp ranking), decoupled look-back across tiles
-//                   for each of the 256 digits, scatter (key, index)
-//   phase 2, high   a tile of the low pass's output, same by the high byte,
-//                   scattering the final order and keys
-// An item only ever waits for items with smaller tickets (the phase before
-// it of the same job, or the tiles before it in a look-back), which were
-// claimed by CTAs that are running, so the queue always drains. Every wait
-// is bounded: after spin_limit polls the kernel records an error and every
-// CTA drains the remaining items without work.
+// one atomic ticket by a persistent grid of CTAs. An item only waits for the
+// phase before it of the same job, whose items all have smaller tickets and
+// were claimed by CTAs that are running, so the queue always drains. Every
+// wait is bounded: after spin_limit polls the kernel records an error and
+// every CTA drains the remaining items without work.
 #include "wsort_dev.cuh"
 
 namespace wsort {
@@ -31,23 +31,65 @@ namespace wsort {
 template <int IPT>
 struct SortSmem {
     static constexpr int kTile = kThreads * IPT;
-    uint32_t hist[2][256];          // key-phase histograms accumulated across items
     ViewConsts vc;
+    float alpha[256];               // unpack4x8unorm(..).a: byte / 255, correctly rounded
     int vc_job;                     // job whose constants vc holds
-    int acc_job;                    // job whose key tiles hist accumulates, or -1
-    uint32_t acc_tiles;
-    uint32_t item;
+    int gb_job, gb_pass;            // job and pass whose digit starts gbase holds
+    uint32_t gtotal;                // that pass's survivor count
+    uint32_t gbase[256];            // global start of each digit of that pass
+    uint32_t next;                  // the ticket this CTA works on next
     uint32_t drain;
     uint32_t abort;
+    int pend_job;                   // items done but not yet published: their job,
+    uint32_t pend_phase, pend_n;    // phase and number
+    int ready_job;                  // (job, phase) whose dependency this CTA has seen met
+    uint32_t ready_phase;
+    uint64_t mark[4];               // tracing: timestamps inside an item
     uint32_t scan[kWarps];
-    uint32_t total;
-    uint16_t wcnt[kWarps][256];     // per-warp digit counts, then warp prefixes
-    uint32_t gbase[256];            // global start of each digit
-    uint32_t gofs[256];             // global position of tile slot 0 of each digit
-    uint32_t lstart[256];           // tile-local start of each digit
-    uint16_t stage_key[kTile];
-    uint32_t stage_idx[kTile];
+    uint32_t hist[256];             // a tile's digit counts
+    union {
+        struct {                    // Keys
+            float4 centers[kTile];
+            uint32_t res[kTile];            // per splat: key, kCulled, or kPending
+            uint16_t queue[kTile];          // splats whose footprint must be evaluated
+            uint32_t qn;
+        } k;
+        struct {                    // Low, CountHi, High
+            uint16_t in_key[2][kTile];      // inputs (CountHi uses both key buffers)
+            uint32_t in_idx[kTile];
+            uint32_t mask[kTile / 32];
+            uint16_t wcnt[kWarps][256];     // per-warp digit counts, then warp prefixes
+            uint32_t gofs[256];             // global position of tile slot 0 of each digit
+            uint32_t lstart[256];           // tile-local start of each digit
+            uint16_t stage_key[kTile];
+            uint32_t stage_idx[kTile];
+        } p;
+    } u;
 };
+
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// 16-byte asynchronous copies global -> shared (cp.async, cached in L2
+// only), and the wait for all of this thread's copies.
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
+    const uint32_t dst = (uint32_t)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
+// Copies `bytes` (a multiple of 16, both ends 16-byte aligned) with the whole
+// CTA; the caller waits and synchronises.
+__device__ __forceinline__ void cta_copy(void* smem_dst, const void* gsrc, uint32_t bytes) {
+    char* d = static_cast<char*>(smem_dst);
+    const char* g = static_cast<const char*>(gsrc);
+    for (uint32_t o = threadIdx.x * 16u; o < bytes; o += kThreads * 16u) cp_async16(d + o, g + o);
+}
 
 // Exclusive scan of one value per thread across the CTA. *total receives the
 // sum. Contains __syncthreads; every thread must call it.
@@ -80,94 +122,12 @@ __device__ __forceinline__ void raise_error(uint32_t* err, uint32_t code, uint32
     if (atomicCAS(err, 0u, code) == 0u) err[1] = item;
 }
 
+// Waits (thread 0, bounded) until `need` items of the phase before this one
+// are done. Returns false, uniformly across the CTA, if the wait gave up.
 template <int IPT>
-__device__ void flush_hist(const JobDesc* jobs, SortSmem<IPT>& sm) {
-    const int tid = threadIdx.x;
-    JobCtl* ctl = reinterpret_cast<JobCtl*>(jobs[sm.acc_job].ctl);
-    const uint32_t a = sm.hist[0][tid], b = sm.hist[1][tid];
-    if (a) atomicAdd(&ctl->hist[0][tid], a);
-    if (b) atomicAdd(&ctl->hist[1][tid], b);
-    sm.hist[0][tid] = 0;
-    sm.hist[1][tid] = 0;
-    __threadfence();
-    __syncthreads();
-    if (tid == 0) {
-        atomicAdd(&ctl->p1_done, sm.acc_tiles);
-        sm.acc_job = -1;
-        sm.acc_tiles = 0;
-    }
-    __syncthreads();
-}
-
-// Phase 0: keys, survivor bits and digit histograms for one tile of splats.
-template <int IPT>
-__device__ void keys_tile(const JobDesc& J, int job, uint32_t tile, uint32_t t1, SortSmem<IPT>& sm) {
-    const int tid = threadIdx.x;
-    const uint32_t lane = lane_id();
-    if (tid == 0) {
-        if (sm.vc_job != job) {
-            make_consts(J, sm.vc);
-            sm.vc_job = job;
-        }
-        sm.acc_job = job;
-        sm.acc_tiles += 1;
-    }
-    // Clear this tile's share of the job's look-back words; the digit passes
-    // read them only after every key tile is done.
-    {
-        const uint32_t words = (J.tiles2 + J.tiles3) * 256u;
-        const uint32_t per = (words + J.tiles1 - 1) / J.tiles1;
-        const uint32_t b = tile * per;
-        const uint32_t e = min(words, b + per);
-        for (uint32_t k = b + tid; k < e; k += kThreads) J.status[k] = 0;
-    }
-    __syncthreads();
-    const ViewConsts& c = sm.vc;
-    const uint32_t base = tile * t1;
-    const bool any = c.visible != 0;
-    for (uint32_t k = 0; k < t1; k += kThreads) {
-        const uint32_t i = base + k + tid;
-        uint32_t key = kCulled;
-        if (any && i < J.n) {
-            const float4 p = __ldcs(&J.centers[i]);
-            float view[4], clip[4];
-            transform(c, p.x, p.y, p.z, view, clip);
-            const float alpha = frustum_alpha(view, clip, __float_as_uint(p.w));
-            bool keep = alpha > 0.0f;
-            if (keep && c.cull > 0.0f) {
-                const float2 s0 = __ldg(&J.cov[3 * (size_t)i]);
-                const float2 s1 = __ldg(&J.cov[3 * (size_t)i + 1]);
-                const float2 s2 = __ldg(&J.cov[3 * (size_t)i + 2]);
-                const float s[6] = {s0.x, s0.y, s1.x, s1.y, s2.x, s2.y};
-                keep = footprint_keeps(c, view, s, alpha);
-            }
-            if (keep) key = depth_key(c, view);
-        }
-        const bool surv = key != kCulled;
-        const uint32_t ballot = __ballot_sync(0xffffffffu, surv);
-        if (i < J.n) J.k16[i] = surv ? (uint16_t)key : (uint16_t)0;
-        if (lane == 0 && i < J.n) J.mask[i >> 5] = ballot;
-        const uint32_t lo = key & 255u, hi = (key >> 8) & 255u;
-        uint32_t peers = __match_any_sync(0xffffffffu, surv ? lo : (0x100u | lane));
-        if (surv && lane == (uint32_t)(__ffs(peers) - 1)) atomicAdd(&sm.hist[0][lo], (uint32_t)__popc(peers));
-        peers = __match_any_sync(0xffffffffu, surv ? hi : (0x100u | lane));
-        if (surv && lane == (uint32_t)(__ffs(peers) - 1)) atomicAdd(&sm.hist[1][hi], (uint32_t)__popc(peers));
-    }
-}
-
-// Phases 1 and 2: one stable counting pass over 8 key bits for one tile.
-template <int PASS, int IPT>
-__device__ void digit_tile(const JobDesc& J, uint32_t tile, SortSmem<IPT>& sm, uint32_t* err, uint32_t item,
+__device__ bool wait_phase(const uint32_t* done, uint32_t need, SortSmem<IPT>& sm, uint32_t* err, uint32_t item,
                            uint32_t spin_limit) {
-    constexpr uint32_t T = SortSmem<IPT>::kTile;
-    const int tid = threadIdx.x;
-    const uint32_t lane = lane_id(), warp = tid >> 5;
-    JobCtl* ctl = reinterpret_cast<JobCtl*>(J.ctl);
-
-    // The phase this one reads must be complete.
-    if (tid == 0) {
-        const uint32_t* done = PASS == 0 ? &ctl->p1_done : &ctl->p2_done;
-        const uint32_t need = PASS == 0 ? J.tiles1 : J.tiles2;
+    if (threadIdx.x == 0) {
         uint32_t spins = 0;
         sm.abort = 0;
         while (ld_acquire(done) < need) {
@@ -176,193 +136,519 @@ __device__ void digit_tile(const JobDesc& J, uint32_t tile, SortSmem<IPT>& sm, u
                 sm.abort = 1;
                 break;
             }
-            __nanosleep(64);
+            __nanosleep(32);
         }
     }
     __syncthreads();
-    if (sm.abort) return;
+    return sm.abort == 0;
+}
+
+// Publishes the CTA's finished items of one (job, phase): the CTA barrier
+// orders every thread's writes before thread 0's release, whose acquire by a
+// waiting CTA (wait_phase) makes them visible there. Items are published in
+// bulk when the CTA moves on to another (job, phase) or leaves, never while
+// it waits, so the queue still drains.
+template <int IPT>
+__device__ void flush_pending(const JobDesc* jobs, SortSmem<IPT>& sm) {
+    if (sm.pend_job < 0) return;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        JobCtl* ctl = reinterpret_cast<JobCtl*>(jobs[sm.pend_job].ctl);
+        red_release_add(&ctl->done[sm.pend_phase], sm.pend_n);
+        sm.pend_job = -1;
+        sm.pend_n = 0;
+    }
+    __syncthreads();
+}
+
+// The lanes of the warp whose `on` is set and whose 8-bit digit equals this
+// lane's: one ballot per digit bit (faster than __match_any_sync here).
+__device__ __forceinline__ uint32_t match_digit8(uint32_t d, bool on) {
+    uint32_t m = __ballot_sync(0xffffffffu, on);
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+        const bool bit = (d >> b) & 1u;
+        const uint32_t v = __ballot_sync(0xffffffffu, bit);
+        m &= bit ? v : ~v;
+    }
+    return m;
+}
+
+// Warp-aggregated increment of hist[d] by the lanes whose `on` is set; for
+// digits that repeat within a warp (a skewed depth distribution).
+__device__ __forceinline__ void count_digit(uint32_t* hist, uint32_t d, bool on) {
+    const uint32_t peers = match_digit8(d, on);
+    if (on && lane_id() == (uint32_t)(__ffs(peers) - 1)) atomicAdd(&hist[d], (uint32_t)__popc(peers));
+}
+
+// Keys: keys, survivor bits and low-digit counts for one tile of splats.
+// The tile's centres are copied to shared memory at once. A first sweep
+// applies the frustum and faintness tests and the footprint shortcut; the
+// splats whose footprint must still be evaluated go to a queue that all
+// threads then work through densely (a warp does the footprint arithmetic
+// for 32 such splats, not for every warp that holds one), reading each one's
+// covariance only then.
+//
+// Footprint shortcut (exact): for a perspective view the host proves
+// keep_q <= 100 d^2 implies every entry of |T| |Sigma| |T|^T is at most 100
+// (T = J W, d = -view.z), and then the pinned computation of the area cannot
+// fall below 1.85, whatever the rounding: the 2D covariance differs from a
+// positive semi-definite one by at most 7.1 u * 100 per entry, which moves
+// (xx + .3)(yy + .3) - xy^2 at most 0.0025 below 0.09. So alpha * area >=
+// RN(alpha * 1.85) >= cull for every alpha byte >= keep_byte, and such a
+// splat is kept without its footprint (or its covariance) being computed.
+constexpr uint32_t kPending = 0xFFFFFFFEu;
+
+template <int IPT>
+__device__ void keys_tile(const JobDesc& J, int job, uint32_t tile, SortSmem<IPT>& sm) {
+    constexpr uint32_t T = SortSmem<IPT>::kTile;
+    const int tid = threadIdx.x;
+    const uint32_t lane = lane_id();
+    if (tid == 0) {
+        if (sm.vc_job != job) {
+            make_consts(J, sm.vc);
+            sm.vc_job = job;
+        }
+        sm.u.k.qn = 0;
+    }
+    sm.hist[tid] = 0;
+    __syncthreads();
+    const ViewConsts& c = sm.vc;
+    const uint32_t base = tile * T;
+    const bool any = c.visible != 0;
+    const bool fp = c.cull > 0.0f;
+    const uint32_t n = J.n;
+    // Every centre of the tile in flight at once: this thread copies the ones
+    // it will read (the cloud is padded to a whole number of tiles).
+    if (any) {
+#pragma unroll
+        for (int r = 0; r < IPT; ++r) cp_async16(&sm.u.k.centers[r * kThreads + tid], &J.centers[base + r * kThreads + tid]);
+        cp_async_wait_all();
+    }
+    // Sweep 1: tests and shortcut; footprints still to evaluate are queued.
+#pragma unroll 1
+    for (uint32_t k = 0; k < T; k += kThreads) {
+        const uint32_t at = k + tid;
+        uint32_t res = kCulled;
+        if (any && base + at < n) {
+            const float4 p = sm.u.k.centers[at];
+            float view[4];
+            view_of(c, p.x, p.y, p.z, view);
+            if (in_frustum(c, view)) {
+                const uint32_t byte = __float_as_uint(p.w) >> 24;
+                const float alpha = sm.alpha[byte];
+                if (!(fmul(alpha, 255.0f) <= 1.0f)) {   // else too faint to reach 1/255
+                    res = depth_key(c, view);
+                    if (fp) {
+                        const float d = -view[2];
+                        if (!(c.persp && byte >= c.keep_byte && c.keep_q <= fmul(100.0f, fmul(d, d)))) res = kPending;
+                    }
+                }
+            }
+        }
+        const uint32_t pend = __ballot_sync(0xffffffffu, res == kPending);
+        if (pend) {
+            uint32_t first = 0;
+            if (lane == (uint32_t)(__ffs(pend) - 1)) first = atomicAdd(&sm.u.k.qn, (uint32_t)__popc(pend));
+            first = __shfl_sync(0xffffffffu, first, __ffs(pend) - 1);
+            if (res == kPending) sm.u.k.queue[first + __popc(pend & lanemask_lt())] = (uint16_t)at;
+        }
+        sm.u.k.res[at] = res;
+    }
+    __syncthreads();
+    // Sweep 2: the queued footprints, densely.
+    const uint32_t qn = sm.u.k.qn;
+    for (uint32_t e = tid; e < qn; e += kThreads) {
+        const uint32_t at = sm.u.k.queue[e];
+        const size_t i = base + at;
+        const float4 p = sm.u.k.centers[at];
+        float view[4];
+        view_of(c, p.x, p.y, p.z, view);
+        const float2 a = __ldcs(&J.cov[3 * i]);
+        const float2 b2 = __ldcs(&J.cov[3 * i + 1]);
+        const float2 c2 = __ldcs(&J.cov[3 * i + 2]);
+        const float sg[6] = {a.x, a.y, b2.x, b2.y, c2.x, c2.y};
+        const float alpha = sm.alpha[__float_as_uint(p.w) >> 24];
+        sm.u.k.res[at] = footprint_keeps(c, view, sg, alpha) ? depth_key(c, view) : kCulled;
+    }
+    __syncthreads();
+    // Sweep 3: keys, survivor bits and low-digit counts.
+#pragma unroll 4
+    for (uint32_t k = 0; k < T; k += kThreads) {
+        const uint32_t i = base + k + tid;
+        const uint32_t key = sm.u.k.res[k + tid];
+        const bool surv = key != kCulled;
+        const uint32_t ballot = __ballot_sync(0xffffffffu, surv);
+        if (i < n) J.k16[i] = surv ? (uint16_t)key : (uint16_t)0;
+        if (lane == 0 && i < n) J.mask[i >> 5] = ballot;
+        if (surv) atomicAdd(&sm.hist[key & 255u], 1u);
+    }
+    __syncthreads();
+    J.cnt_lo[(size_t)tid * J.tiles + tile] = sm.hist[tid];
+}
+
+// The start of each digit in a pass's output (an exclusive scan of the
+// pass's digit totals), cached per (job, pass) for the CTA's next items.
+template <int IPT>
+__device__ void digit_starts(const JobDesc& J, int job, int pass, SortSmem<IPT>& sm) {
+    if (sm.gb_job == job && sm.gb_pass == pass) return;
+    JobCtl* ctl = reinterpret_cast<JobCtl*>(J.ctl);
+    uint32_t total;
+    const uint32_t g = block_exclusive_scan(__ldcg(&ctl->tot[pass][threadIdx.x]), sm.scan, &total);
+    sm.gbase[threadIdx.x] = g;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        sm.gtotal = total;
+        sm.gb_job = job;
+        sm.gb_pass = pass;
+    }
+    __syncthreads();
+}
+
+// CountHi: high-digit counts of tiles 2g and 2g + 1 of the low pass's
+// output. Both tiles' keys are copied at once, into the two key buffers of
+// the digit passes.
+template <int IPT>
+__device__ void count_hi_item(const JobDesc& J, int job, uint32_t g, SortSmem<IPT>& sm) {
+    constexpr uint32_t T = SortSmem<IPT>::kTile;
+    const int tid = threadIdx.x;
+    digit_starts(J, job, 0, sm);
+    const uint32_t s_total = sm.gtotal;
+    uint16_t* area[kCountSpan] = {sm.u.p.in_key[0], sm.u.p.in_key[1]};
+#pragma unroll
+    for (uint32_t q = 0; q < kCountSpan; ++q) {
+        const uint32_t tile = g * kCountSpan + q;
+        if (tile < J.tiles && tile * T < s_total) cta_copy(area[q], J.key_b + tile * T, T * 2);
+    }
+    cp_async_wait_all();
+    __syncthreads();
+#pragma unroll
+    for (uint32_t q = 0; q < kCountSpan; ++q) {
+        const uint32_t tile = g * kCountSpan + q;
+        if (tile >= J.tiles) break;
+        sm.hist[tid] = 0;
+        __syncthreads();
+        const uint32_t base = tile * T;
+        if (base < s_total) {
+#pragma unroll 4
+            for (int r = 0; r < IPT; ++r) {
+                const uint32_t at = r * kThreads + tid;
+                count_digit(sm.hist, area[q][at] >> 8, base + at < s_total);
+            }
+        }
+        __syncthreads();
+        J.cnt_hi[(size_t)tid * J.tiles + tile] = sm.hist[tid];
+    }
+}
+
+// ScanLo / ScanHi: for digit d, the exclusive prefix over tiles of its
+// per-tile counts (a contiguous row of the digit-major count matrix), in
+// place, and its total. Chunks of 256 x 16 tiles: all loads of a chunk are
+// in flight before the scan.
+template <int IPT>
+__device__ void scan_digit(uint32_t* cnt, uint32_t tiles, uint32_t d, uint32_t* tot, SortSmem<IPT>& sm) {
+    constexpr int V = 16;
+    const int tid = threadIdx.x;
+    uint32_t* row = cnt + (size_t)d * tiles;
+    uint32_t carry = 0;
+    for (uint32_t c0 = 0; c0 < tiles; c0 += kThreads * V) {
+        uint32_t v[V];
+        uint32_t local = 0;
+#pragma unroll
+        for (int q = 0; q < V; ++q) {
+            const uint32_t r = c0 + tid * V + q;
+            v[q] = r < tiles ? __ldcg(&row[r]) : 0u;
+        }
+#pragma unroll
+        for (int q = 0; q < V; ++q) local += v[q];
+        uint32_t chunk_total;
+        uint32_t run = carry + block_exclusive_scan(local, sm.scan, &chunk_total);
+#pragma unroll
+        for (int q = 0; q < V; ++q) {
+            const uint32_t r = c0 + tid * V + q;
+            if (r < tiles) row[r] = run;
+            run += v[q];
+        }
+        carry += chunk_total;
+    }
+    if (tid == 0) tot[d] = carry;
+}
+
+// Low / High: one stable counting pass over 8 key bits for one tile. The
+// tile's input is copied to shared memory first (cp.async, all at once);
+// each warp ranks its 32 x IPT consecutive elements in rounds of 32, stably.
+// Low / High: one stable counting pass over 8 key bits for one tile. The
+// tile's input is copied to shared memory first (cp.async, all at once);
+// each warp ranks its 32 x IPT consecutive elements in rounds of 32, stably.
+template <int PASS, int IPT>
+__device__ void digit_tile(const JobDesc& J, int job, uint32_t tile, SortSmem<IPT>& sm, uint32_t* err,
+                           uint32_t item) {
+    constexpr uint32_t T = SortSmem<IPT>::kTile;
+    const int tid = threadIdx.x;
+    const uint32_t lane = lane_id(), warp = tid >> 5;
 
     // Where each digit starts in this pass's output.
-    uint32_t total;
-    const uint32_t h = __ldcg(&ctl->hist[PASS][tid]);
-    sm.gbase[tid] = block_exclusive_scan(h, sm.scan, &total);
+    digit_starts(J, job, PASS, sm);
+    const uint32_t total = sm.gtotal;
+    const uint32_t gbase = sm.gbase[tid];
     if (PASS == 0 && tile == 0 && tid == 0) *J.count = total;
     const uint32_t n_in = PASS == 0 ? J.n : total;
     const uint32_t base = tile * T;
+    if (base >= n_in) return;
+    const uint32_t* cnt = PASS == 0 ? J.cnt_lo : J.cnt_hi;
+    const uint32_t excl = __ldcg(&cnt[(size_t)tid * J.tiles + tile]);
+    const uint32_t b = 0;
+    if (PASS == 0) {
+        cta_copy(sm.u.p.in_key[b], J.k16 + base, T * 2);
+        cta_copy(sm.u.p.mask, J.mask + base / 32, T / 8);
+    } else {
+        cta_copy(sm.u.p.in_key[b], J.key_b + base, T * 2);
+        cta_copy(sm.u.p.in_idx, J.idx_b + base, T * 4);
+    }
+    for (int k = tid; k < kWarps * 256; k += kThreads) (&sm.u.p.wcnt[0][0])[k] = 0;
+    cp_async_wait_all();
+    __syncthreads();
+    if (tid == 0) sm.mark[0] = global_ns();
 
-    if (base < n_in) {
-        for (int k = tid; k < kWarps * 256; k += kThreads) (&sm.wcnt[0][0])[k] = 0;
-        __syncthreads();
-
-        // Stable rank within the warp: rounds of 32 consecutive elements.
-        uint32_t packed[IPT];
-        uint32_t idxv[IPT];
-        const uint32_t wbase = base + warp * 32u * IPT;
+    // Stable rank within the warp.
+    uint32_t packed[IPT];
+    const uint32_t wlocal = warp * 32u * IPT;
+    const uint32_t lt = lanemask_lt();
+    // The rounds' matches are independent: all of them first, then the
+    // counter updates, which must run in round order.
+    uint32_t peersv[IPT];
 #pragma unroll
-        for (int r = 0; r < IPT; ++r) {
-            const uint32_t first = wbase + r * 32u;
-            const uint32_t pos = first + lane;
-            bool valid = pos < n_in;
-            uint32_t key = 0;
-            if (PASS == 0) {
-                const uint32_t m = first < n_in ? __ldcg(&J.mask[first >> 5]) : 0u;
-                valid = valid && ((m >> lane) & 1u);
-                if (valid) key = __ldcg(&J.k16[pos]);
-                idxv[r] = pos;
-            } else {
-                idxv[r] = 0;
-                if (valid) {
-                    key = __ldcg(&J.key_b[pos]);
-                    idxv[r] = __ldcg(&J.idx_b[pos]);
-                }
-            }
-            const uint32_t d = PASS == 0 ? (key & 255u) : (key >> 8);
-            const uint32_t peers = __match_any_sync(0xffffffffu, valid ? d : (0x100u | lane));
-            uint32_t prior = 0;
-            if (valid) prior = sm.wcnt[warp][d];
-            __syncwarp();
-            if (valid && lane == (uint32_t)(__ffs(peers) - 1)) sm.wcnt[warp][d] = (uint16_t)(prior + __popc(peers));
-            __syncwarp();
-            packed[r] = valid ? (key | ((prior + __popc(peers & lanemask_lt())) << 16)) : 0xFFFFFFFFu;
-        }
-        __syncthreads();
-
-        // Thread d: warp prefixes and the tile's count of digit d.
-        uint32_t tc = 0;
+    for (int r = 0; r < IPT; ++r) {
+        const uint32_t at = wlocal + r * 32u + lane;
+        bool valid = base + at < n_in;
+        if (PASS == 0) valid = valid && ((sm.u.p.mask[at >> 5] >> lane) & 1u);
+        const uint32_t key = sm.u.p.in_key[b][at];
+        const uint32_t d = PASS == 0 ? (key & 255u) : (key >> 8);
+        peersv[r] = match_digit8(d, valid);   // every lane takes part in the ballots
+        packed[r] = valid ? key : 0xFFFFFFFFu;
+    }
 #pragma unroll
-        for (int w = 0; w < kWarps; ++w) {
-            const uint32_t cnt = sm.wcnt[w][tid];
-            sm.wcnt[w][tid] = (uint16_t)tc;
-            tc += cnt;
-        }
+    for (int r = 0; r < IPT; ++r) {
+        const bool valid = packed[r] != 0xFFFFFFFFu;
+        const uint32_t key = packed[r] & 0xFFFFu;
+        const uint32_t d = PASS == 0 ? (key & 255u) : (key >> 8);
+        const uint32_t peers = peersv[r];
+        uint32_t prior = 0;
+        if (valid) prior = sm.u.p.wcnt[warp][d];
+        __syncwarp();
+        if (valid && lane == (uint32_t)(__ffs(peers) - 1)) sm.u.p.wcnt[warp][d] = (uint16_t)(prior + __popc(peers));
+        __syncwarp();
+        packed[r] = valid ? (key | ((prior + __popc(peers & lt)) << 16)) : 0xFFFFFFFFu;
+    }
+    __syncthreads();
 
-        // Decoupled look-back over this pass's tiles, one chain per digit.
-        uint32_t* st = J.status + (PASS == 0 ? 0u : J.tiles2 * 256u);
-        uint32_t excl = 0;
-        if (tile == 0) {
-            st_release(&st[tid], kFlagPrefix | tc);
+    // Thread d: warp prefixes and the tile's count of digit d.
+    uint32_t tc = 0;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) {
+        const uint32_t cnt_w = sm.u.p.wcnt[w][tid];
+        sm.u.p.wcnt[w][tid] = (uint16_t)tc;
+        tc += cnt_w;
+    }
+    if (tid == 0) sm.mark[1] = global_ns();
+    uint32_t tile_total;
+    const uint32_t ls = block_exclusive_scan(tc, sm.scan, &tile_total);
+    sm.u.p.lstart[tid] = ls;
+    sm.u.p.gofs[tid] = gbase + excl - ls;
+    __syncthreads();
+
+    // Stage in tile order (digit, then index), then write out runs.
+#pragma unroll
+    for (int r = 0; r < IPT; ++r) {
+        if (packed[r] == 0xFFFFFFFFu) continue;
+        const uint32_t key = packed[r] & 0xFFFFu;
+        const uint32_t d = PASS == 0 ? (key & 255u) : (key >> 8);
+        const uint32_t slot = sm.u.p.lstart[d] + sm.u.p.wcnt[warp][d] + (packed[r] >> 16);
+        const uint32_t at = wlocal + r * 32u + lane;
+        sm.u.p.stage_key[slot] = (uint16_t)key;
+        sm.u.p.stage_idx[slot] = PASS == 0 ? base + at : sm.u.p.in_idx[at];
+    }
+    __syncthreads();
+    if (tid == 0) sm.mark[2] = global_ns();
+    for (uint32_t s = tid; s < tile_total; s += kThreads) {
+        const uint32_t key = sm.u.p.stage_key[s];
+        const uint32_t d = PASS == 0 ? (key & 255u) : (key >> 8);
+        const uint32_t g = sm.u.p.gofs[d] + s;
+        if (g >= J.n) {   // only reachable if counts disagree: record, do not write
+            raise_error(err, kErrBounds, item);
+            continue;
+        }
+        if (PASS == 0) {
+            J.key_b[g] = (uint16_t)key;
+            J.idx_b[g] = sm.u.p.stage_idx[s];
         } else {
-            st_release(&st[tile * 256u + tid], kFlagAggregate | tc);
-            int j = (int)tile - 1;
-            uint32_t spins = 0;
-            while (j >= 0) {
-                const uint32_t s = ld_acquire(&st[(uint32_t)j * 256u + tid]);
-                if (s & (kFlagAggregate | kFlagPrefix)) {
-                    excl += s & kCountMask;
-                    if (s & kFlagPrefix) break;
-                    --j;
-                    spins = 0;
-                    continue;
-                }
-                if (++spins > spin_limit || ((spins & 1023u) == 0 && *(volatile uint32_t*)err)) {
-                    raise_error(err, kErrWaitLookback, item);
-                    break;
-                }
-            }
-            st_release(&st[tile * 256u + tid], kFlagPrefix | (excl + tc));
-        }
-
-        uint32_t tile_total;
-        const uint32_t ls = block_exclusive_scan(tc, sm.scan, &tile_total);
-        sm.lstart[tid] = ls;
-        sm.gofs[tid] = sm.gbase[tid] + excl - ls;
-        __syncthreads();
-
-        // Stage in tile order (digit, then index), then write out runs.
-#pragma unroll
-        for (int r = 0; r < IPT; ++r) {
-            if (packed[r] == 0xFFFFFFFFu) continue;
-            const uint32_t key = packed[r] & 0xFFFFu;
-            const uint32_t d = PASS == 0 ? (key & 255u) : (key >> 8);
-            const uint32_t slot = sm.lstart[d] + sm.wcnt[warp][d] + (packed[r] >> 16);
-            sm.stage_key[slot] = (uint16_t)key;
-            sm.stage_idx[slot] = idxv[r];
-        }
-        __syncthreads();
-        for (uint32_t s = tid; s < tile_total; s += kThreads) {
-            const uint32_t key = sm.stage_key[s];
-            const uint32_t d = PASS == 0 ? (key & 255u) : (key >> 8);
-            const uint32_t g = sm.gofs[d] + s;
-            if (g >= J.n) {   // only reachable if counts disagree: record, do not write
-                raise_error(err, kErrBounds, item);
-                continue;
-            }
-            if (PASS == 0) {
-                J.key_b[g] = (uint16_t)key;
-                J.idx_b[g] = sm.stage_idx[s];
-            } else {
-                __stcs(&J.order[g], sm.stage_idx[s]);
-                if (J.keys) __stcs(&J.keys[g], key);
-            }
+            __stcs(&J.order[g], sm.u.p.stage_idx[s]);
+            if (J.keys) __stcs(&J.keys[g], key);
         }
     }
-    __threadfence();
-    __syncthreads();
-    if (PASS == 0 && tid == 0) atomicAdd(&ctl->p2_done, 1u);
 }
 
-template <int IPT>
-__global__ void __launch_bounds__(kThreads) sort_kernel(const JobDesc* __restrict__ jobs,
+__device__ __forceinline__ uint32_t sm_id() {
+    uint32_t s;
+    asm("mov.u32 %0, %%smid;" : "=r"(s));
+    return s;
+}
+
+template <int IPT, int MINB>
+__global__ void __launch_bounds__(kThreads, MINB) sort_kernel(const JobDesc* __restrict__ jobs,
                                                         const uint2* __restrict__ items, uint32_t n_items,
                                                         LaunchCtl* __restrict__ lctl, uint32_t* __restrict__ err,
-                                                        uint32_t t1, uint32_t spin_limit) {
-    __shared__ SortSmem<IPT> sm;
+                                                        uint32_t spin_limit, TraceRec* __restrict__ trace) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    SortSmem<IPT>& sm = *reinterpret_cast<SortSmem<IPT>*>(smem_raw);
     const int tid = threadIdx.x;
-    sm.hist[0][tid] = 0;
-    sm.hist[1][tid] = 0;
+    sm.alpha[tid] = fdiv(float(tid), 255.0f);
     if (tid == 0) {
-        sm.acc_job = -1;
-        sm.acc_tiles = 0;
         sm.vc_job = -1;
+        sm.gb_job = -1;
+        sm.gb_pass = -1;
     }
-    __syncthreads();
+    if (tid == 0) {
+        sm.next = atomicAdd(&lctl->ticket, 1u);
+        sm.drain = *(volatile uint32_t*)err;
+        sm.pend_job = -1;
+        sm.pend_n = 0;
+        sm.ready_job = -1;
+    }
+    uint64_t t_claim = 0, t_start = 0;
+    if (trace && tid == 0) t_claim = global_ns();
     for (;;) {
         __syncthreads();   // the previous item's shared state is no longer read
-        if (tid == 0) {
-            sm.item = atomicAdd(&lctl->ticket, 1u);
-            sm.drain = *(volatile uint32_t*)err;
-        }
-        __syncthreads();
-        const uint32_t it = sm.item;
-        const uint2 item = it < n_items ? items[it] : make_uint2(0xFFFFFFFFu, 0u);
-        const uint32_t phase = item.y >> 30, tile = item.y & 0x3FFFFFFFu;
-        const int job = it < n_items ? (int)item.x : -1;
-        if (sm.acc_job >= 0 && !(phase == kPhaseKeys && job == sm.acc_job)) flush_hist(jobs, sm);
+        const uint32_t it = sm.next;
         if (it >= n_items) break;
-        if (sm.drain) continue;   // after an error: claim the remaining items, do no work
+        const uint2 item = items[it];
+        const uint32_t phase = item.y >> kPhaseShift, tile = item.y & kTileMask;
+        const int job = (int)item.x;
         const JobDesc& J = jobs[job];
-        if (phase == kPhaseKeys) {
-            keys_tile(J, job, tile, t1, sm);
-            __threadfence();
-        } else if (phase == kPhaseLow) {
-            digit_tile<0>(J, tile, sm, err, it, spin_limit);
-        } else {
-            digit_tile<1>(J, tile, sm, err, it, spin_limit);
+        JobCtl* ctl = reinterpret_cast<JobCtl*>(J.ctl);
+        if (job != sm.pend_job || phase != sm.pend_phase) flush_pending(jobs, sm);
+        bool work = !sm.drain;   // after an error: claim the remaining items, do no work
+        if (work && phase != kPhaseKeys && !(sm.ready_job == job && sm.ready_phase == phase)) {
+            // Items the phase before this one has: tiles, pairs of tiles, or
+            // one per digit.
+            const uint32_t need = (phase == kPhaseLow || phase == kPhaseHigh) ? kScanItems
+                                  : phase == kPhaseScanHi ? (J.tiles + kCountSpan - 1) / kCountSpan
+                                                          : J.tiles;
+            work = wait_phase(&ctl->done[phase - 1], need, sm, err, it, spin_limit);
+            if (work && tid == 0) {
+                sm.ready_job = job;
+                sm.ready_phase = phase;
+            }
+        }
+        if (work) {
+            if (trace && tid == 0) {
+                t_start = global_ns();
+                sm.mark[0] = sm.mark[1] = sm.mark[2] = 0;
+            }
+            switch (phase) {
+                case kPhaseKeys: keys_tile(J, job, tile, sm); break;
+                case kPhaseScanLo: scan_digit(J.cnt_lo, J.tiles, tile, ctl->tot[0], sm); break;
+                case kPhaseLow: digit_tile<0>(J, job, tile, sm, err, it); break;
+                case kPhaseCountHi: count_hi_item(J, job, tile, sm); break;
+                case kPhaseScanHi: scan_digit(J.cnt_hi, J.tiles, tile, ctl->tot[1], sm); break;
+                default: digit_tile<1>(J, job, tile, sm, err, it); break;
+            }
+            __syncthreads();
+        }
+        if (tid == 0) {
+            if (work) {
+                sm.pend_job = job;
+                sm.pend_phase = phase;
+                sm.pend_n += 1;
+                if (trace) {
+                    TraceRec r;
+                    r.claim = t_claim;
+                    r.start = t_start;
+                    r.end = global_ns();
+                    r.item = it;
+                    r.sm = sm_id();
+                    for (int q = 0; q < 3; ++q) r.mark[q] = sm.mark[q];
+                    trace[it] = r;
+                }
+            }
+            sm.next = atomicAdd(&lctl->ticket, 1u);
+            sm.drain = *(volatile uint32_t*)err;
+            if (trace) t_claim = global_ns();
         }
     }
+    flush_pending(jobs, sm);
+    cp_async_wait_all();   // no copy into this CTA's shared memory outlives it
     if (tid == 0) atomicAdd(&lctl->exited, 1u);
 }
 
-// Host-side launcher: the kernel variant for a digit-pass tile of
-// pass_tile elements.
-cudaError_t launch_sort(const JobDesc* jobs, const uint2* items, uint32_t n_items, LaunchCtl* lctl,
-                        uint32_t* err, uint32_t t1, uint32_t pass_tile, uint32_t spin_limit, int grid,
-                        cudaStream_t stream) {
-    if (pass_tile == 2048) {
-        sort_kernel<8><<<grid, kThreads, 0, stream>>>(jobs, items, n_items, lctl, err, t1, spin_limit);
-    } else {
-        sort_kernel<16><<<grid, kThreads, 0, stream>>>(jobs, items, n_items, lctl, err, t1, spin_limit);
-    }
+// The kernel variants: a tile of 256 * IPT elements, at least MINB resident
+// CTAs per SM (which caps the registers a thread may use).
+template <int IPT, int MINB>
+static cudaError_t prepare_variant() {
+    static bool done = false;   // the attribute is per function, set once per process
+    if (done) return cudaSuccess;
+    const cudaError_t e = cudaFuncSetAttribute(sort_kernel<IPT, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)sizeof(SortSmem<IPT>));
+    if (e == cudaSuccess) done = true;
+    return e;
+}
+
+template <int IPT, int MINB>
+static cudaError_t launch_variant(const JobDesc* jobs, const uint2* items, uint32_t n_items, LaunchCtl* lctl,
+                                  uint32_t* err, uint32_t spin_limit, int grid, cudaStream_t stream,
+                                  TraceRec* trace) {
+    cudaError_t e = prepare_variant<IPT, MINB>();
+    if (e != cudaSuccess) return e;
+    sort_kernel<IPT, MINB><<<grid, kThreads, sizeof(SortSmem<IPT>), stream>>>(jobs, items, n_items, lctl, err,
+                                                                               spin_limit, trace);
     return cudaGetLastError();
 }
 
-int sort_occupancy(uint32_t pass_tile) {
+template <int IPT>
+static cudaError_t launch_ipt(int minb, const JobDesc* jobs, const uint2* items, uint32_t n_items, LaunchCtl* lctl,
+                              uint32_t* err, uint32_t spin_limit, int grid, cudaStream_t stream, TraceRec* trace) {
+    switch (minb) {
+        case 2: return launch_variant<IPT, 2>(jobs, items, n_items, lctl, err, spin_limit, grid, stream, trace);
+        case 4: return launch_variant<IPT, 4>(jobs, items, n_items, lctl, err, spin_limit, grid, stream, trace);
+        default: return launch_variant<IPT, 3>(jobs, items, n_items, lctl, err, spin_limit, grid, stream, trace);
+    }
+}
+
+// Host-side launcher: the variant for a tile of `tile` elements and `minb`
+// resident CTAs per SM (2, 3 or 4).
+cudaError_t launch_sort(const JobDesc* jobs, const uint2* items, uint32_t n_items, LaunchCtl* lctl,
+                        uint32_t* err, uint32_t tile, int minb, uint32_t spin_limit, int grid, cudaStream_t stream,
+                        TraceRec* trace) {
+    switch (tile) {
+        case 1024: return launch_ipt<4>(minb, jobs, items, n_items, lctl, err, spin_limit, grid, stream, trace);
+        case 2048: return launch_ipt<8>(minb, jobs, items, n_items, lctl, err, spin_limit, grid, stream, trace);
+        default: return launch_ipt<16>(minb, jobs, items, n_items, lctl, err, spin_limit, grid, stream, trace);
+    }
+}
+
+template <int IPT, int MINB>
+static int occupancy_variant() {
     int blocks = 0;
-    if (pass_tile == 2048)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, sort_kernel<8>, kThreads, 0);
-    else
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, sort_kernel<16>, kThreads, 0);
+    if (prepare_variant<IPT, MINB>() != cudaSuccess) return 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, sort_kernel<IPT, MINB>, kThreads, sizeof(SortSmem<IPT>));
     return blocks;
+}
+
+template <int IPT>
+static int occupancy_ipt(int minb) {
+    switch (minb) {
+        case 2: return occupancy_variant<IPT, 2>();
+        case 4: return occupancy_variant<IPT, 4>();
+        default: return occupancy_variant<IPT, 3>();
+    }
+}
+
+int sort_occupancy(uint32_t tile, int minb) {
+    switch (tile) {
+        case 1024: return occupancy_ipt<4>(minb);
+        case 2048: return occupancy_ipt<8>(minb);
+        default: return occupancy_ipt<16>(minb);
+    }
 }
 
 }  // namespace wsort

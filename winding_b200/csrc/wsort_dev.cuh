@@ -22,15 +22,23 @@ constexpr int kThreads = 256;             // threads per CTA of every sort kerne
 constexpr int kWarps = kThreads / 32;
 constexpr uint32_t kPadSplats = 4096;     // resident clouds are padded to this multiple
 
-// Look-back status word: 2 flag bits over a 30-bit count.
-constexpr uint32_t kFlagAggregate = 1u << 30;
-constexpr uint32_t kFlagPrefix = 2u << 30;
-constexpr uint32_t kCountMask = (1u << 30) - 1;
-
-// Error codes a kernel leaves in LaunchCtl::error.
+// Error codes a kernel leaves in the context's error word.
 constexpr uint32_t kErrWaitPhase = 1;     // a phase dependency never completed
-constexpr uint32_t kErrWaitLookback = 2;  // a predecessor tile never published
 constexpr uint32_t kErrBounds = 3;        // a scatter position fell outside the output
+
+// Phases of one job, in dependency order. Each waits for the whole of the
+// one before it.
+//   Keys     per tile of splats: cull, key, survivor bit, low-digit counts
+//   ScanLo   per digit: scan over tiles of the low-digit counts
+//   Low      per tile of splats: stable rank by the low key byte, scatter
+//   CountHi  per two tiles of the low pass's output: high-digit counts
+//   ScanHi   per digit: scan over tiles of the high-digit counts
+//   High     per tile of the low pass's output: stable rank by the high
+//            byte, scatter the final order and keys
+constexpr uint32_t kPhaseKeys = 0, kPhaseScanLo = 1, kPhaseLow = 2, kPhaseCountHi = 3, kPhaseScanHi = 4,
+                   kPhaseHigh = 5, kPhases = 6;
+constexpr uint32_t kCountSpan = 2;        // tiles one CountHi item covers
+constexpr uint32_t kScanItems = 256;      // scan items per pass: one per digit value
 
 // One (cloud, view) to sort, as the persistent kernel reads it.
 struct alignas(16) JobDesc {
@@ -39,7 +47,12 @@ struct alignas(16) JobDesc {
     const float2* cov;          // 6 f32 a splat as 3 float2; padded likewise
     double bmin[3], bmax[3];    // box around the centres
     uint32_t n;
-    uint32_t tiles1, tiles2, tiles3;
+    uint32_t tiles;             // tiles of splats (Keys, Low) = tiles of the low pass's output (High)
+    // Per-view shortcuts the host proves exact (see keys_tile):
+    uint32_t fast_transform;    // affine model-view, reverse-Z perspective, no overflow possible
+    uint32_t keep_byte;         // alpha bytes at or above this pass the footprint cull when ...
+    float keep_q;               // ... keep_q <= 100 d^2 (+inf: never)
+    uint32_t pad1[3];
     // view: the values the reference writes into its Cloud uniform
     float mv[16];
     float proj[16];
@@ -51,34 +64,41 @@ struct alignas(16) JobDesc {
     uint32_t* keys;             // >= n, or null
     uint32_t* count;            // 1
     // scratch
-    uint16_t* k16;              // per splat key (survivors) ; n_pad
+    uint16_t* k16;              // per splat key (survivors)
     uint32_t* mask;             // survivor bits, one word per 32 splats
-    uint16_t* key_b;            // low-digit pass output: keys
-    uint32_t* idx_b;            // low-digit pass output: splat indices
-    uint32_t* status;           // look-back words: (tiles2 + tiles3) * 256
+    uint16_t* key_b;            // low pass output: keys
+    uint32_t* idx_b;            // low pass output: splat indices
+    uint32_t* cnt_lo;           // 256 x tiles (digit major): low-digit counts, then prefixes over tiles
+    uint32_t* cnt_hi;           // 256 x tiles: the same for the high digit
     uint32_t* ctl;              // JobCtl
 };
 
 // Per-job counters, zeroed before a launch.
 struct JobCtl {
-    uint32_t hist[2][256];      // survivor digit histograms: low byte, high byte
-    uint32_t p1_done;           // key tiles whose writes are visible
-    uint32_t p2_done;           // low-digit tiles whose writes are visible
-    uint32_t pad[14];
+    uint32_t tot[2][256];       // survivors per digit value: low byte, high byte
+    uint32_t done[8];           // items finished, per phase
+    uint32_t pad[8];
 };
 static_assert(sizeof(JobCtl) % 64 == 0, "JobCtl size");
 
 // Per-launch counters, zeroed before a launch.
 struct LaunchCtl {
     uint32_t ticket;            // next work item
-    uint32_t error;             // first error code
-    uint32_t error_item;        // the item that raised it
     uint32_t exited;            // CTAs that left the loop
-    uint32_t pad[12];
+    uint32_t pad[14];
 };
 
-// Work item: x = job, y = phase << 30 | tile.
-constexpr uint32_t kPhaseKeys = 0, kPhaseLow = 1, kPhaseHigh = 2;
+// One work item's timeline, when tracing: globaltimer ns at the claim of its
+// ticket, after its dependency wait, and at its end; and the SM it ran on.
+struct TraceRec {
+    uint64_t claim, start, end;
+    uint32_t item, sm;
+    uint64_t mark[3];           // digit passes: inputs staged, ranked, staged for writing
+};
+
+// Work item: x = job, y = phase << 29 | tile.
+constexpr uint32_t kPhaseShift = 29;
+constexpr uint32_t kTileMask = (1u << kPhaseShift) - 1;
 
 // ---------------------------------------------------------------- f32 ops
 __device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
@@ -95,6 +115,9 @@ __device__ __forceinline__ float fclamp(float e, float lo, float hi) { return fm
 struct ViewConsts {
     float mv[16];
     float proj[16];
+    float keep_q;
+    uint32_t keep_byte;
+    int fast;
     float fx, fy;               // p[0][0] * viewport.x * 0.5, p[1][1] * viewport.y * 0.5
     float xlo, xhi, ylo, yhi;   // -1.3 / p[0][0], 1.3 / p[0][0], and for p[1][1]
     float cull;
@@ -139,36 +162,55 @@ __device__ __forceinline__ void make_consts(const JobDesc& J, ViewConsts& c) {
     c.yhi = fdiv(1.3f, p5);
     c.cull = J.cull;
     c.persp = J.proj[15] == 0.0f;
+    c.keep_q = J.keep_q;
+    c.keep_byte = J.keep_byte;
+    c.fast = J.fast_transform != 0;
     depth_range(J, &c.depth_min, &c.depth_scale, &c.visible);
 }
 
-// view = modelView * (x, y, z, 1) and clip = projection * view.
-__device__ __forceinline__ void transform(const ViewConsts& c, float x, float y, float z, float view[4],
-                                          float clip[4]) {
+// view = modelView * (x, y, z, 1) (render/splats.js:160).
+__device__ __forceinline__ void view_of(const ViewConsts& c, float x, float y, float z, float view[4]) {
+    if (c.fast) {
+        // modelView's last row is (0, 0, 0, 1): view.w is exactly 1, and
+        // m[12 + j] * 1 is m[12 + j].
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+            view[j] = fadd(fadd(fadd(fmul(c.mv[j], x), fmul(c.mv[4 + j], y)), fmul(c.mv[8 + j], z)), c.mv[12 + j]);
+        view[3] = 1.0f;
+        return;
+    }
 #pragma unroll
     for (int j = 0; j < 4; ++j)
         view[j] = fadd(fadd(fadd(fmul(c.mv[j], x), fmul(c.mv[4 + j], y)), fmul(c.mv[8 + j], z)),
                        fmul(c.mv[12 + j], 1.0f));
-#pragma unroll
-    for (int j = 0; j < 4; ++j)
-        clip[j] = fadd(fadd(fadd(fmul(c.proj[j], view[0]), fmul(c.proj[4 + j], view[1])),
-                            fmul(c.proj[8 + j], view[2])),
-                       fmul(c.proj[12 + j], view[3]));
 }
 
-// Frustum and faintness tests (render/splats.js:163-170). Returns alpha, or a
-// negative value when culled.
-__device__ __forceinline__ float frustum_alpha(const float view[4], const float clip[4], uint32_t word) {
+// The frustum test (render/splats.js:161-167) on clip = projection * view.
+// With the fast transform the projection's zero entries are left out: each
+// dropped term is a zero times a finite number, which changes at most the
+// sign of a zero, and the tests below compare, so they decide the same.
+__device__ __forceinline__ bool in_frustum(const ViewConsts& c, const float view[4]) {
+    const float* P = c.proj;
+    float clip[4];
+    if (c.fast) {
+        clip[0] = fadd(fmul(P[0], view[0]), fmul(P[8], view[2]));
+        clip[1] = fadd(fmul(P[5], view[1]), fmul(P[9], view[2]));
+        clip[2] = fadd(fmul(P[10], view[2]), P[14]);
+        clip[3] = fmul(P[11], view[2]);
+    } else {
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            clip[j] = fadd(fadd(fadd(fmul(P[j], view[0]), fmul(P[4 + j], view[1])), fmul(P[8 + j], view[2])),
+                           fmul(P[12 + j], view[3]));
+    }
     const float w = clip[3];
-    if (view[2] >= 0.0f || clip[2] > w || fabsf(clip[0]) > fmul(1.3f, w) || fabsf(clip[1]) > fmul(1.3f, w))
-        return -1.0f;
-    const float alpha = fdiv(float(word >> 24), 255.0f);   // unpack4x8unorm(..).a
-    if (fmul(alpha, 255.0f) <= 1.0f) return -1.0f;
-    return alpha;
+    return !(view[2] >= 0.0f || clip[2] > w || fabsf(clip[0]) > fmul(1.3f, w) || fabsf(clip[1]) > fmul(1.3f, w));
 }
 
 // The footprint cull (render/splats.js:172-178 with footprint :102-124).
-// Returns true when the splat is kept. s[6] is its covariance.
+// Returns true when the splat is kept. s[6] is its covariance. J's entries
+// J[0][1] and J[1][0] are zero in both of its forms, so their products with
+// the (finite) model-view are zeros and are left out of T = J W.
 __device__ __forceinline__ bool footprint_keeps(const ViewConsts& c, const float view[4], const float s[6],
                                                 float alpha) {
     float J00 = c.fx, J11 = c.fy, J02 = 0.0f, J12 = 0.0f;
@@ -182,16 +224,14 @@ __device__ __forceinline__ bool footprint_keeps(const ViewConsts& c, const float
         J02 = fdiv(fmul(c.fx, x), dd);
         J12 = fdiv(fmul(c.fy, y), dd);
     }
-    // J = [[J00, 0, J02], [0, J11, J12], [0, 0, 0]];  W[r][col] = mv[col*4 + r].
-    const float J[2][3] = {{J00, 0.0f, J02}, {0.0f, J11, J12}};
-    const float S[3][3] = {{s[0], s[1], s[2]}, {s[1], s[3], s[4]}, {s[2], s[4], s[5]}};
+    // W[r][col] = mv[col*4 + r].
     float T[2][3], U[2][3];
 #pragma unroll
-    for (int r = 0; r < 2; ++r)
-#pragma unroll
-        for (int col = 0; col < 3; ++col)
-            T[r][col] = fadd(fadd(fmul(J[r][0], c.mv[col * 4 + 0]), fmul(J[r][1], c.mv[col * 4 + 1])),
-                             fmul(J[r][2], c.mv[col * 4 + 2]));
+    for (int col = 0; col < 3; ++col) {
+        T[0][col] = fadd(fmul(J00, c.mv[col * 4 + 0]), fmul(J02, c.mv[col * 4 + 2]));
+        T[1][col] = fadd(fmul(J11, c.mv[col * 4 + 1]), fmul(J12, c.mv[col * 4 + 2]));
+    }
+    const float S[3][3] = {{s[0], s[1], s[2]}, {s[1], s[3], s[4]}, {s[2], s[4], s[5]}};
 #pragma unroll
     for (int r = 0; r < 2; ++r)
 #pragma unroll
@@ -220,6 +260,9 @@ __device__ __forceinline__ uint32_t ld_acquire(const uint32_t* p) {
 }
 __device__ __forceinline__ void st_release(uint32_t* p, uint32_t v) {
     asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void red_release_add(uint32_t* p, uint32_t v) {
+    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31; }
 __device__ __forceinline__ uint32_t lanemask_lt() {

@@ -5,6 +5,7 @@
 
 #include <cstdint>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "wsort.h"
@@ -45,9 +46,20 @@ struct ws_ctx {
     uint32_t* err_d = nullptr;        // sticky device error: code, work item
     std::vector<uint2> items;
     std::vector<uint32_t> last_ns;
-    uint32_t last_keys_tile = 0, last_pass_tile = 0;
+    uint32_t last_tile = 0;
     bool items_valid = false;
+    int occupancy[3][3] = {};         // resident sort CTAs per SM, by tile and variant
     uint64_t launches = 0;
+    // kernel timing (ws_timing): event pairs recorded around each launch
+    bool timing = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> timing_events;
+    size_t timing_used = 0;
+    uint64_t timing_launches = 0;
+    // item tracing (ws_trace): the last traced launch's records and items
+    bool tracing = false;
+    wsort::DevBuf trace_d;
+    std::vector<uint2> trace_items;
+    int trace_grid = 0;
     std::vector<struct ws_cloud*> freed;   // freed clouds, kept as refusable handles
 };
 
@@ -59,4 +71,5 @@ struct ws_cloud {
     float4* centers = nullptr;
     float2* cov = nullptr;
     double bmin[3] = {0, 0, 0}, bmax[3] = {0, 0, 0};
+    float smax = 0.0f;              // largest |covariance entry| of the cloud
 };

@@ -88,12 +88,10 @@ class Context:
         self.check(self.lib.ws_get_params(self.handle, ctypes.byref(p)))
         return p
 
-    def set_params(self, keys_tile=None, pass_tile=None, ctas_per_sm=None, spin_limit=None) -> None:
+    def set_params(self, tile=None, ctas_per_sm=None, spin_limit=None) -> None:
         p = self.params
-        if keys_tile is not None:
-            p.keys_tile = keys_tile
-        if pass_tile is not None:
-            p.pass_tile = pass_tile
+        if tile is not None:
+            p.tile = tile
         if ctas_per_sm is not None:
             p.ctas_per_sm = ctas_per_sm
         if spin_limit is not None:
@@ -136,6 +134,30 @@ class Context:
 
     def plan(self, jobs: list[tuple]) -> "Plan":
         return Plan(self, jobs)
+
+    def timing(self, enable: bool = True) -> None:
+        self.check(self.lib.ws_timing(self.handle, int(enable)))
+
+    def timing_read(self) -> tuple[float, int]:
+        """(summed sort-kernel ms, sort kernels launched) since the last read."""
+        ms = ctypes.c_double()
+        n = ctypes.c_uint64()
+        self.check(self.lib.ws_timing_read(self.handle, ctypes.byref(ms), ctypes.byref(n)))
+        return ms.value, n.value
+
+    def trace(self, enable: bool = True) -> None:
+        self.check(self.lib.ws_trace(self.handle, int(enable)))
+
+    def trace_read(self) -> np.ndarray:
+        """The last traced launch's work items as a structured array
+        (claim_ns, start_ns, end_ns, job, phase, tile, sm, mark_ns)."""
+        n = ctypes.c_size_t()
+        self.check(self.lib.ws_trace_read(self.handle, None, 0, ctypes.byref(n)))
+        recs = (_lib.WsTraceRec * max(n.value, 1))()
+        self.check(self.lib.ws_trace_read(self.handle, recs, n.value, ctypes.byref(n)))
+        dt = np.dtype([("claim_ns", "<u8"), ("start_ns", "<u8"), ("end_ns", "<u8"), ("job", "<u4"),
+                       ("phase", "<u4"), ("tile", "<u4"), ("sm", "<u4"), ("mark_ns", "<u8", (3,))])
+        return np.frombuffer(bytes(recs), dtype=dt, count=n.value).copy()
 
     # device buffers, for callers without torch
     def alloc(self, nbytes: int) -> int:
