@@ -188,6 +188,30 @@ int ws_device_free(ws_ctx* ctx, void* ptr);
  * queued work (and `stream`'s, if given) has finished. */
 int ws_device_download(ws_ctx* ctx, const void* device_src, void* host_dst, size_t bytes, void* stream);
 
+/* ------------------------------------------------------------ without allocation */
+
+/*
+ * No counterpart in the reference (whose WebGPU path allocates its per-cloud
+ * sort buffers on first use). For callers that cannot allocate device memory
+ * when they sort -- a plugin whose device memory belongs to the host
+ * application's pool, a frame loop that may not stall on cudaMalloc or
+ * cudaFree -- this is ws_sort with WS_DEVICE_OUTPUT that allocates nothing:
+ * its scratch is one fixed array in the library's device memory, held by
+ * every GPU that loads the library until the process exits. It covers clouds
+ * of at most WS_NOALLOC_MAX_SPLATS splats (larger ones: WS_ERR_CAPACITY).
+ * The first call on a device takes the array's address (make it before any
+ * stream capture). All calls share the array and keep the last call's
+ * contents; calls whose GPU work overlaps (other streams or threads) race
+ * and must be serialised by the caller. order, keys (may be NULL) and count
+ * are device memory; the work is queued on `stream` (NULL: the cloud's
+ * context's stream). A device-side wait that gave up sets *count to
+ * 0xFFFFFFFF. Other errors: WS_ERR_ARG (null pointer, cull negative or not
+ * finite), WS_ERR_UNLOADED, WS_ERR_CUDA.
+ */
+#define WS_NOALLOC_MAX_SPLATS ((uint32_t)1 << 20)
+int ws_sort_noalloc(const ws_cloud* cloud, const ws_view* view, uint32_t* order, uint32_t* keys, uint32_t* count,
+                    void* stream);
+
 /* ------------------------------------------------------------ tuning */
 
 /*

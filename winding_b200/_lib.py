@@ -26,6 +26,7 @@ WS_ERR_PENDING = -10
 WS_HOST_OUTPUT = 0
 WS_DEVICE_OUTPUT = 1
 WS_MAX_SPLATS = 1 << 30
+WS_NOALLOC_MAX_SPLATS = 1 << 20
 
 ERROR_NAMES = {
     WS_ERR_ARG: "WS_ERR_ARG", WS_ERR_FORMAT: "WS_ERR_FORMAT", WS_ERR_NAN: "WS_ERR_NAN",
@@ -143,6 +144,7 @@ SIGNATURES = {
     "ws_device_download": (ctypes.c_int, [vp, vp, vp, ctypes.c_size_t, vp]),
     "ws_get_params": (ctypes.c_int, [vp, ctypes.POINTER(WsParams)]),
     "ws_set_params": (ctypes.c_int, [vp, ctypes.POINTER(WsParams)]),
+    "ws_sort_noalloc": (ctypes.c_int, [vp, ctypes.POINTER(WsView), vp, vp, vp, vp]),
     "ws_timing": (ctypes.c_int, [vp, ctypes.c_int]),
     "ws_timing_read": (ctypes.c_int, [vp, f64p, ctypes.POINTER(ctypes.c_uint64)]),
     "ws_trace": (ctypes.c_int, [vp, ctypes.c_int]),

@@ -1,0 +1,172 @@
+// ws_sort_noalloc: the plain one-cloud sort for callers that cannot allocate
+// device memory when they sort.
+//
+// Who needs it: a host whose device memory belongs to someone else -- a
+// renderer or engine plugin that must draw from the host application's own
+// pool, a real-time frame loop that may not stall on cudaMalloc/cudaFree
+// (both can synchronise the device), or code queued while another component
+// holds the device's allocator. ws_sort grows a per-context scratch buffer
+// with cudaMalloc on first use and whenever a larger cloud arrives; this entry
+// point never allocates. Its scratch is one file-scope __device__ array of a
+// fixed size (WS_NOALLOC_MAX_SPLATS splats' worth), which every GPU that
+// loads the library holds until the process exits.
+//
+// Set-up: the first call on a device (with that device current) takes the
+// array's device address with cudaGetSymbolAddress and keeps it; make that
+// first call before any stream capture. Every call then queues three kernels
+// on the stream: one that writes the job description and work list into the
+// array and clears the counters that must start at zero, the sort kernel of
+// ws_sort itself, and one that turns a device-side error into *count =
+// 0xFFFFFFFF. All calls share the one array, which keeps the last call's
+// contents: calls whose work overlaps on the GPU (other streams, other host
+// threads) race on it and must be serialised by the caller.
+#include "wsort.h"
+#include "wsort_dev.cuh"
+#include "wsort_host.h"
+
+#include <cmath>
+#include <cstring>
+#include <mutex>
+
+namespace wsort {
+
+cudaError_t launch_sort(const JobDesc* jobs, const uint2* items, uint32_t n_items, LaunchCtl* lctl, uint32_t* err,
+                        uint32_t tile, int minb, uint32_t spin_limit, int grid, cudaStream_t stream,
+                        TraceRec* trace);
+int sort_occupancy(uint32_t tile, int minb);
+size_t launch_scratch_bytes(const uint32_t* ns, int njobs, const ws_params& p);
+void layout_jobs(JobDesc* out, const ws_job* jobs, int njobs, const ws_params& p, char* scratch);
+
+namespace {
+
+// Fixed kernel parameters of this entry point (the library's defaults).
+constexpr uint32_t kTile = 2048;
+constexpr int kMinBlocks = 4;
+constexpr uint32_t kSpinLimit = 1u << 22;
+
+// Tiles of the largest cloud, and the work items of one job of that size:
+// keys, low pass and high pass one per tile, high-digit counts one per two
+// tiles, and the two scans one per digit value.
+constexpr uint32_t kMaxTiles = (WS_NOALLOC_MAX_SPLATS + kTile - 1) / kTile;
+constexpr uint32_t kMaxItems = 3 * kMaxTiles + (kMaxTiles + kCountSpan - 1) / kCountSpan + 2 * kScanItems;
+
+// Layout of the array: the sort's scratch for one job of up to
+// WS_NOALLOC_MAX_SPLATS splats (checked against launch_scratch_bytes on every
+// call), then the job description, the error words and the work items.
+constexpr size_t kSortBytes = 10u << 20;
+constexpr size_t kJobOffset = kSortBytes;
+constexpr size_t kErrOffset = kJobOffset + ((sizeof(JobDesc) + 255) / 256) * 256;
+constexpr size_t kItemsOffset = kErrOffset + 256;
+constexpr size_t kScratchBytes = kItemsOffset + (size_t)kMaxItems * sizeof(uint2);
+
+static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_setup_mutex;
+void* g_scratch_addr[kMaxDevices] = {};
+
+// Writes the job description and its work list into g_scratch and clears the
+// per-launch and per-job counters and the error words.
+__global__ void noalloc_setup_kernel(JobDesc desc, uint32_t tiles, uint32_t clear_bytes) {
+    JobDesc* job = reinterpret_cast<JobDesc*>(g_scratch + kJobOffset);
+    uint2* items = reinterpret_cast<uint2*>(g_scratch + kItemsOffset);
+    uint32_t* err = reinterpret_cast<uint32_t*>(g_scratch + kErrOffset);
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    if (tid == 0) *job = desc;
+    if (tid < 4) err[tid] = 0;
+    for (uint32_t k = tid; k < clear_bytes / 4; k += stride) reinterpret_cast<uint32_t*>(g_scratch)[k] = 0;
+    // The phases in order: keys, low scan, low pass, high counts, high scan,
+    // high pass (the order ws_sort's work list has for a single job).
+    const uint32_t counts[kPhases] = {tiles, kScanItems, tiles, (tiles + kCountSpan - 1) / kCountSpan, kScanItems,
+                                      tiles};
+    uint32_t first = 0;
+    for (uint32_t ph = 0; ph < kPhases; ++ph) {
+        for (uint32_t t = tid; t < counts[ph]; t += stride) items[first + t] = make_uint2(0u, (ph << kPhaseShift) | t);
+        first += counts[ph];
+    }
+}
+
+// A device-side wait that gave up leaves its code in the error words; the
+// caller sees it as *count == 0xFFFFFFFF.
+__global__ void noalloc_check_kernel(uint32_t* count) {
+    const uint32_t* err = reinterpret_cast<const uint32_t*>(g_scratch + kErrOffset);
+    if (err[0] != 0) *count = 0xFFFFFFFFu;
+}
+
+// The array's device address on the current device, taken once per device.
+int scratch_address(int device, char** out) {
+    if (device < 0 || device >= kMaxDevices) return WS_ERR_ARG;
+    std::lock_guard<std::mutex> lock(g_setup_mutex);
+    if (!g_scratch_addr[device]) {
+        void* ptr = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&ptr, g_scratch);
+        if (e != cudaSuccess || !ptr) {
+            cudaGetLastError();
+            return WS_ERR_CUDA;
+        }
+        g_scratch_addr[device] = ptr;
+    }
+    *out = static_cast<char*>(g_scratch_addr[device]);
+    return WS_OK;
+}
+
+}  // namespace
+}  // namespace wsort
+
+using namespace wsort;
+
+extern "C" int ws_sort_noalloc(const ws_cloud* cloud, const ws_view* view, uint32_t* order, uint32_t* keys,
+                               uint32_t* count, void* stream_p) {
+    if (!cloud || !view || !order || !count) return WS_ERR_ARG;
+    if (cloud->magic != kCloudMagic) return WS_ERR_ARG;
+    if (!cloud->alive) return WS_ERR_UNLOADED;
+    if (!(view->cull >= 0.0f && std::isfinite(view->cull))) return WS_ERR_ARG;
+    if (cloud->n > WS_NOALLOC_MAX_SPLATS) return WS_ERR_CAPACITY;
+
+    ws_params p{};
+    p.tile = kTile;
+    p.ctas_per_sm = kMinBlocks;
+    p.spin_limit = kSpinLimit;
+    const uint32_t n = cloud->n;
+    if (launch_scratch_bytes(&n, 1, p) > kSortBytes) return WS_ERR_CAPACITY;
+
+    const int device = cloud->ctx->device;
+    if (cudaSetDevice(device) != cudaSuccess) return WS_ERR_CUDA;
+    char* base = nullptr;
+    int rc = scratch_address(device, &base);
+    if (rc) return rc;
+    cudaStream_t stream = stream_p ? static_cast<cudaStream_t>(stream_p) : cloud->ctx->stream;
+
+    ws_job job;
+    job.cloud = cloud;
+    job.view = *view;
+    job.order = order;
+    job.keys = keys;
+    job.count = count;
+    JobDesc desc;
+    layout_jobs(&desc, &job, 1, p, base);
+
+    const uint32_t tiles = desc.tiles;
+    const uint32_t n_items = 3 * tiles + (tiles + kCountSpan - 1) / kCountSpan + 2 * kScanItems;
+    const uint32_t clear_bytes = (uint32_t)(((sizeof(LaunchCtl) + sizeof(JobCtl)) + 3) / 4 * 4);
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    int per_sm = sort_occupancy(kTile, kMinBlocks);
+    if (per_sm < 1) per_sm = 1;
+    int grid = sms * per_sm;
+    if ((uint32_t)grid > n_items) grid = (int)n_items;
+
+    noalloc_setup_kernel<<<8, 256, 0, stream>>>(desc, tiles, clear_bytes);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess)
+        e = launch_sort(reinterpret_cast<const JobDesc*>(base + kJobOffset),
+                        reinterpret_cast<const uint2*>(base + kItemsOffset), n_items,
+                        reinterpret_cast<LaunchCtl*>(base), reinterpret_cast<uint32_t*>(base + kErrOffset), kTile,
+                        kMinBlocks, kSpinLimit, grid, stream, nullptr);
+    if (e == cudaSuccess) {
+        noalloc_check_kernel<<<1, 1, 0, stream>>>(count);
+        e = cudaGetLastError();
+    }
+    return e == cudaSuccess ? WS_OK : WS_ERR_CUDA;
+}
