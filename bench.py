@@ -291,6 +291,8 @@ def _run_wsort(args, rank, world, local_rank, torch):
     jobs = make_jobs(args.workload, args.cull, seed_offset=0)
 
     plain = plain_measure(ctx, torch, jobs, 0, args.warmup, flush)   # load + warm
+    from winding_b200 import autotune
+    tuned = autotune.tune(ctx, [list(zip(plain["clouds"], plain["views"]))])
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
@@ -346,7 +348,8 @@ def _run_wsort(args, rank, world, local_rank, torch):
         "data": "synthetic (seeded)",
         "config": {"workload": args.workload, "splats_per_step": splats_per_step, "survivors_per_step": sum(survivors),
                    "cull": args.cull, "viewport": [1920, 1080], "l2": "flushed (256 MiB write) before each step",
-                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "tuned": {str(b): {"tile": t, "ctas_per_sm": c} for b, (t, c) in tuned.items()}},
         "e2e": {"value": e2e_value, "unit": "Msplats/s", "h2d_bytes_per_step": view_bytes, "d2h_bytes_per_step": d2h,
                 "call": "ws_sort(WS_HOST_OUTPUT) into pinned host buffers"},
         "gpu_launches": launches,
@@ -390,8 +393,13 @@ def suite(ctx, torch, flush, args):
     against the HBM roofline, and batched vs plain on the mixed workload."""
     out = {}
     peak, src = peak_hbm()
+    from winding_b200 import autotune
     # slab-6M, plain kernel
     jobs = make_jobs("slab-6M", 0.5)
+    p = plain_measure(ctx, torch, jobs, 0, 0, flush)
+    slab_tuned = autotune.tune(ctx, [list(zip(p["clouds"], p["views"]))])
+    for sp in p["clouds"]:
+        sp.destroy()
     p = plain_measure(ctx, torch, jobs, 20, 3, flush)
     n = p["splats"]
     algo = sum(algorithmic_bytes(sp.count, s) for sp, s in zip(p["clouds"], p["survivors"]))
@@ -399,12 +407,22 @@ def suite(ctx, torch, flush, args):
     out["slab-6M"] = {"splats": n, "survivors": p["survivors"][0], "kernel_us": kernel_s * 1e6,
                       "step_us": p["ms"] / 20 * 1e3, "msplats_s": n / (p["ms"] / 20 / 1e3) / 1e6,
                       "achieved_gbs": algo / kernel_s / 1e9, "frac": algo / kernel_s / 1e9 / peak,
-                      "peak_source": src, "traffic": ncu_traffic("slab-6M", 0.5)}
+                      "peak_source": src, "traffic": ncu_traffic("slab-6M", 0.5),
+                      "tuned": {str(b): list(v) for b, v in slab_tuned.items()}}
     for sp in p["clouds"]:
         sp.destroy()
     del p
-    # mixed-64: 64 plain calls vs one batched launch vs the graph-captured plan
+    # mixed-64: 64 plain calls vs one batched launch vs the graph-captured plan,
+    # each tuned for its own launch sizes
     jobs = make_jobs("mixed-64", 0.5)
+    p = plain_measure(ctx, torch, jobs, 0, 0, flush)
+    pairs = list(zip(p["clouds"], p["views"]))
+    per_bucket = {}
+    for pair in pairs:
+        per_bucket.setdefault(autotune.bucket(pair[0].count), pair)
+    mixed_tuned = autotune.tune(ctx, [[pr] for pr in per_bucket.values()] + [pairs])
+    for sp in p["clouds"]:
+        sp.destroy()
     p = plain_measure(ctx, torch, jobs, 10, 2, flush)
     total = p["splats"]
     specs = [(sp, v, o.data_ptr(), k.data_ptr(), c.data_ptr())
@@ -424,10 +442,95 @@ def suite(ctx, torch, flush, args):
     out["mixed-64"] = {"jobs": len(jobs), "splats": total, "plain_msplats_s": plain_rate,
                        "batched_msplats_s": batch_rate, "graph_msplats_s": graph_rate,
                        "batched_vs_plain": batch_rate / plain_rate, "graph_vs_plain": graph_rate / plain_rate,
-                       "plain_ms_per_step": p["ms"] / 10, "graph_ms_per_step": g_ms / 10}
+                       "plain_ms_per_step": p["ms"] / 10, "graph_ms_per_step": g_ms / 10,
+                       "tuned": {str(b): list(v) for b, v in mixed_tuned.items()}}
     for sp in p["clouds"]:
         sp.destroy()
+    try:
+        out["served-16"] = served(ctx, args)
+    except Exception as exc:
+        out["served-16"] = {"error": f"{type(exc).__name__}: {exc}"}
     return out
+
+
+def served(ctx, args, rate_hz: float = 2000.0, seconds: float = 2.0):
+    """Config 4: a Poisson stream of random-pose requests over 16 resident
+    scenes of 50k-4M splats, through the server (continuous batching) and,
+    on the same arrival schedule, through one plain ws_sort per request."""
+    import threading
+    from winding_b200 import make_view, parse_splats, workloads as W
+    from winding_b200.server import Server
+    scenes = [parse_splats(rec, ctx) for rec in W.served_16()]
+    resident = sum(sp.count for sp in scenes) * 40
+    arrivals = W.poisson_arrivals(rate_hz, seconds)
+    rng = np.random.default_rng(6)
+    proj = W.perspective(W.FOV_Y, W.ASPECT, W.NEAR)
+    reqs = [(int(rng.integers(0, len(scenes))), make_view(W.random_pose(rng), proj, W.VIEWPORT, 0.5))
+            for _ in arrivals]
+    splats = sum(scenes[k].count for k, _ in reqs)
+
+    def run(submit, collect):
+        """Submits on the arrival schedule from one thread, collects from another;
+        returns (seconds from the first arrival to the last result, latencies in
+        ms from each request's scheduled arrival to its result)."""
+        done = [None] * len(reqs)
+        tickets = [None] * len(reqs)
+        ready = threading.Semaphore(0)
+        t0 = time.perf_counter()
+
+        def producer():
+            for k, (at, (sc, v)) in enumerate(zip(arrivals, reqs)):
+                delay = t0 + at - time.perf_counter()
+                if delay > 0:
+                    time.sleep(delay)
+                tickets[k] = (t0 + at, submit(scenes[sc], v))
+                ready.release()
+
+        th = threading.Thread(target=producer)
+        th.start()
+        for k in range(len(reqs)):
+            ready.acquire()
+            t_sub, tk = tickets[k]
+            collect(tk)
+            done[k] = (time.perf_counter() - t_sub) * 1e3
+        th.join()
+        return time.perf_counter() - t0, done
+
+    def collect(srv, t):
+        srv.result(t)      # the result is on the device, as the reference's draw reads it
+        srv.release(t)
+
+    with Server(ctx, memory_budget=8 << 30, max_batch=64, streams=2) as srv:
+        wall, lat = run(lambda sp, v: srv.submit(sp, v), lambda t: collect(srv, t))
+        st = srv.stats()
+    import torch
+    n_max = max(sp.count for sp in scenes)
+    o = torch.empty(n_max, dtype=torch.int32, device="cuda")
+    k = torch.empty(n_max, dtype=torch.int32, device="cuda")
+    c = torch.zeros(1, dtype=torch.int32, device="cuda")
+    import ctypes as _ct
+    cnt = _ct.c_uint32()
+
+    def plain(sp, v):
+        """One plain ws_sort per request, device outputs, then its count."""
+        ctx.sort_device(sp, v, o.data_ptr(), k.data_ptr(), c.data_ptr())
+        ctx.check(ctx.lib.ws_device_download(ctx.handle, c.data_ptr(), _ct.byref(cnt), 4, None))
+
+    plain_wall, plain_lat = run(plain, lambda res: None)
+    for sp in scenes:
+        sp.destroy()
+    return {
+        "requests": len(reqs), "rate_hz": rate_hz, "scenes": len(scenes), "resident_bytes": resident,
+        "splats": splats,
+        "served_msplats_s": splats / wall / 1e6, "served_p50_ms": float(np.percentile(lat, 50)),
+        "served_p99_ms": float(np.percentile(lat, 99)),
+        "device_p50_ms": st["p50_ms"], "device_p99_ms": st["p99_ms"], "mean_batch": st["mean_batch"],
+        "batches": st["batches"], "overlapped_batches": st["overlapped_batches"],
+        "admission_waits": st["admission_waits"],
+        "plain_msplats_s": splats / plain_wall / 1e6, "plain_p50_ms": float(np.percentile(plain_lat, 50)),
+        "plain_p99_ms": float(np.percentile(plain_lat, 99)),
+        "latency": "scheduled arrival to the result ready in device memory, count known on the host",
+    }
 
 
 def main():

@@ -188,6 +188,61 @@ int ws_device_free(ws_ctx* ctx, void* ptr);
  * queued work (and `stream`'s, if given) has finished. */
 int ws_device_download(ws_ctx* ctx, const void* device_src, void* host_dst, size_t bytes, void* stream);
 
+/* ------------------------------------------------------------ serving */
+
+/*
+ * A request loop over resident clouds (no counterpart in
+ * the reference, which sorts once per frame on its own thread). Requests
+ * (cloud, view) are submitted from any thread; a dispatcher thread batches
+ * whatever has arrived into one persistent launch (continuous batching),
+ * admitting requests in arrival order while their device memory (outputs
+ * and sort scratch) fits the budget, with up to `streams` launches in flight
+ * so a batch that arrives while another runs overlaps with it on the device.
+ * Each result is identical to ws_sort's for the same request.
+ */
+typedef struct ws_server_opts {
+    size_t memory_budget;       /* device bytes for requests in flight; 0: 50% of free memory */
+    int max_batch;              /* most requests per launch (0: 64) */
+    uint64_t max_batch_splats;  /* most splats per launch (0: no limit) */
+    int streams;                /* launches in flight at once (0: 2) */
+    int queue_capacity;         /* queued requests before submit returns WS_ERR_BUSY (0: 65536) */
+    int collect_us;             /* after the first request of a batch, wait this long for more (0: none) */
+} ws_server_opts;
+
+typedef struct ws_server_stats {
+    uint64_t submitted, completed, failed, batches, splats;
+    uint64_t admission_waits;   /* times the head request waited for memory */
+    uint64_t in_flight;         /* requests admitted, not yet collected */
+    uint64_t peak_bytes;        /* most device memory in use by requests */
+    double p50_ms, p99_ms, mean_ms;   /* submit -> device completion */
+    double mean_batch;
+    uint64_t max_batch_seen;
+    uint64_t overlapped_batches; /* batches launched while another was still running */
+} ws_server_stats;
+
+int ws_server_create(ws_ctx* ctx, const ws_server_opts* opts, ws_server** out);
+/* Queues a request; *ticket identifies it. The cloud must stay loaded until
+ * the request is collected. WS_ERR_BUSY when the queue is full; WS_ERR_NOMEM
+ * when the request alone exceeds the memory budget. */
+int ws_server_submit(ws_server* server, const ws_cloud* cloud, const ws_view* view, uint64_t* ticket);
+/* *done = 1 once the request's result is ready. */
+int ws_server_poll(ws_server* server, uint64_t ticket, int* done);
+/* Waits up to timeout_ms (< 0: forever) for the request, copies its count,
+ * order and keys (keys may be NULL) to host memory and releases it.
+ * WS_ERR_PENDING if it is not done in time (it stays queued). */
+int ws_server_wait(ws_server* server, uint64_t ticket, uint32_t* order, uint32_t* keys, uint32_t* count,
+                   int timeout_ms);
+/* As ws_server_wait, but the result stays in device memory, as the
+ * reference's order buffer does for its draw (src/render/splats.js:716-721):
+ * *order / *keys point to it until ws_server_release(ticket); *count is the
+ * survivor count. */
+int ws_server_result(ws_server* server, uint64_t ticket, const uint32_t** order, const uint32_t** keys,
+                     uint32_t* count, int timeout_ms);
+int ws_server_release(ws_server* server, uint64_t ticket);
+int ws_server_get_stats(ws_server* server, ws_server_stats* out);
+/* Finishes the requests in flight, drops the queued ones, stops the threads. */
+int ws_server_destroy(ws_server* server);
+
 /* ------------------------------------------------------------ without allocation */
 
 /*
@@ -230,6 +285,14 @@ typedef struct ws_params {
 
 int ws_get_params(const ws_ctx* ctx, ws_params* out);
 int ws_set_params(ws_ctx* ctx, const ws_params* params);
+
+/*
+ * A tuning table (what winding_b200/autotune.py measures): entry b applies
+ * to launches whose total splat count has floor(log2) == b; entries with
+ * tile == 0, and sizes past the table, use ws_set_params's parameters.
+ * n <= 32 entries; n == 0 clears the table.
+ */
+int ws_set_tuning(ws_ctx* ctx, const ws_params* table, int n);
 
 /* ------------------------------------------------------------ measurement */
 

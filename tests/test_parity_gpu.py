@@ -228,3 +228,60 @@ def test_full_size_slab_properties(ctx):
                                  threads=os.cpu_count() or 1)
     assert np.array_equal(order, want_o) and np.array_equal(keys, want_k)
     splats.destroy()
+
+
+def _adversarial_cloud(n, seed, scale_mu, near_dist):
+    rng = np.random.default_rng(seed)
+    pos = rng.normal(size=(n, 3)) * np.array([2.0, 2.0, 2.0])
+    rec = W.records_from(pos, rng)
+    # wide spread of sizes: specks, thin needles and large blobs
+    rec["scale"] = np.exp(rng.normal(scale_mu, 2.0, size=(n, 3))).astype(np.float32)
+    flat = rng.random(n) < 0.2
+    rec["scale"][flat, rng.integers(0, 3)] = 0.0          # rank-deficient covariances
+    rec["rgba"][:, 3] = rng.integers(60, 80, size=n)      # alpha bytes around the shortcut's threshold
+    return rec
+
+
+@pytest.mark.parametrize("kind", ["persp-close", "persp-far", "ortho", "offcentre", "nonaffine"])
+def test_views_that_exercise_the_general_paths(ctx, kind):
+    from winding_b200.camera import look_at, perspective
+    rng = np.random.default_rng({"persp-close": 1, "persp-far": 2, "ortho": 3, "offcentre": 4, "nonaffine": 5}[kind])
+    rec = _adversarial_cloud(60_000, 70 + len(kind), -2.0 if kind == "persp-close" else -3.5, 1.0)
+    dist = 6.0 if kind == "persp-close" else 40.0
+    mv = look_at((dist * 0.3, dist * 0.2, dist), (0, 0, 0))
+    proj = perspective(1.0, 16 / 9, 0.1)
+    if kind == "ortho":
+        proj = np.zeros(16, np.float32)
+        proj[0], proj[5], proj[10], proj[14], proj[15] = 0.2, 0.35, -0.01, 0.5, 1.0
+    elif kind == "offcentre":
+        proj = proj.copy()
+        proj[8], proj[9] = np.float32(0.15), np.float32(-0.1)
+    elif kind == "nonaffine":
+        mv = mv.copy()
+        mv[3], mv[15] = np.float32(1e-3), np.float32(1.0001)
+    job = W.Job(rec, W.View(mv, proj, (1280.0, 720.0), 0.5))
+    check_job(ctx, job, culls=(0.0, 0.5, 1.0, 3.0))
+
+
+def test_cull_threshold_sweep(ctx):
+    """Culls around the footprint shortcut's bound; the same splats every time."""
+    rec = _adversarial_cloud(40_000, 91, -4.0, 30.0)
+    job = W.Job(rec, W.View(W.look_at((0, 0, 30), (0, 0, 0)), W.perspective(W.FOV_Y, W.ASPECT, W.NEAR)))
+    check_job(ctx, job, culls=(0.3, 0.45, 0.4999, 0.5, 0.5001, 0.55, 0.7))
+
+
+def test_tuning_table_changes_no_result(ctx):
+    from winding_b200 import autotune
+    job = W.clusters_1m(seed=81, n=150_000)
+    splats = parse_splats(job.records, ctx)
+    view = make_view(job.view.model_view, job.view.projection, job.view.viewport, 0.5)
+    want = ctx.sort(splats, view)
+    table = autotune.tune(ctx, [[(splats, view)]], reps=2)
+    assert autotune.bucket(splats.count) in table
+    got = ctx.sort(splats, view)
+    assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1])
+    bad = (_lib.WsParams * 1)()
+    bad[0].tile = 777
+    assert ctx.lib.ws_set_tuning(ctx.handle, bad, 1) == _lib.WS_ERR_ARG
+    autotune.install(ctx, {})
+    splats.destroy()

@@ -145,6 +145,16 @@ SIGNATURES = {
     "ws_get_params": (ctypes.c_int, [vp, ctypes.POINTER(WsParams)]),
     "ws_set_params": (ctypes.c_int, [vp, ctypes.POINTER(WsParams)]),
     "ws_sort_noalloc": (ctypes.c_int, [vp, ctypes.POINTER(WsView), vp, vp, vp, vp]),
+    "ws_server_create": (ctypes.c_int, [vp, ctypes.POINTER(WsServerOpts), ctypes.POINTER(vp)]),
+    "ws_server_submit": (ctypes.c_int, [vp, vp, ctypes.POINTER(WsView), ctypes.POINTER(ctypes.c_uint64)]),
+    "ws_server_poll": (ctypes.c_int, [vp, ctypes.c_uint64, ctypes.POINTER(ctypes.c_int)]),
+    "ws_server_wait": (ctypes.c_int, [vp, ctypes.c_uint64, vp, vp, vp, ctypes.c_int]),
+    "ws_server_result": (ctypes.c_int, [vp, ctypes.c_uint64, ctypes.POINTER(vp), ctypes.POINTER(vp),
+                                        ctypes.POINTER(ctypes.c_uint32), ctypes.c_int]),
+    "ws_server_release": (ctypes.c_int, [vp, ctypes.c_uint64]),
+    "ws_server_get_stats": (ctypes.c_int, [vp, ctypes.POINTER(WsServerStats)]),
+    "ws_server_destroy": (ctypes.c_int, [vp]),
+    "ws_set_tuning": (ctypes.c_int, [vp, ctypes.POINTER(WsParams), ctypes.c_int]),
     "ws_timing": (ctypes.c_int, [vp, ctypes.c_int]),
     "ws_timing_read": (ctypes.c_int, [vp, f64p, ctypes.POINTER(ctypes.c_uint64)]),
     "ws_trace": (ctypes.c_int, [vp, ctypes.c_int]),

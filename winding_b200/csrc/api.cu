@@ -255,10 +255,26 @@ int check_cloud(ws_ctx* ctx, const ws_cloud* c) {
 // Stages, uploads and launches a batch on ctx's scratch. The stream waits for
 // the context's previous launch, so one scratch is never shared by two
 // launches in flight.
+// The parameters a launch of `splats` splats in total runs with.
+const ws_params& params_for(const ws_ctx* ctx, uint64_t splats) {
+    int b = 0;
+    while (b < 63 && (splats >> (b + 1))) ++b;
+    if (b < ctx->tuning_n && ctx->tuning[b].tile) return ctx->tuning[b];
+    return ctx->params;
+}
+
 int run_batch(ws_ctx* ctx, const ws_job* jobs, int njobs, cudaStream_t stream) {
     cudaError_t e;
     std::vector<uint32_t> ns(njobs);
-    for (int j = 0; j < njobs; ++j) ns[j] = jobs[j].cloud->n;
+    uint64_t splats = 0;
+    for (int j = 0; j < njobs; ++j) splats += ns[j] = jobs[j].cloud->n;
+    const ws_params saved = ctx->params;
+    ctx->params = params_for(ctx, splats);   // restored below
+    struct Restore {
+        ws_ctx* c;
+        ws_params p;
+        ~Restore() { c->params = p; }
+    } restore{ctx, saved};
     const size_t need = launch_scratch_bytes(ns.data(), njobs, ctx->params);
     if (need > ctx->scratch.bytes) {
         // The old scratch may still be read by a launch in flight.
@@ -443,6 +459,28 @@ extern "C" int ws_sync(ws_ctx* ctx) {
 extern "C" int ws_get_params(const ws_ctx* ctx, ws_params* out) {
     if (!ctx || !out) return WS_ERR_ARG;
     *out = ctx->params;
+    return WS_OK;
+}
+
+static int valid_params(ws_ctx* ctx, const ws_params* p) {
+    if (p->tile != 1024 && p->tile != 2048 && p->tile != 4096)
+        return set_error(ctx, WS_ERR_ARG, "tile must be 1024, 2048 or 4096");
+    if (p->spin_limit == 0) return set_error(ctx, WS_ERR_ARG, "spin_limit must be positive");
+    if (p->ctas_per_sm != 0 && (p->ctas_per_sm < 2 || p->ctas_per_sm > 4))
+        return set_error(ctx, WS_ERR_ARG, "ctas_per_sm must be 0, 2, 3 or 4");
+    return WS_OK;
+}
+
+extern "C" int ws_set_tuning(ws_ctx* ctx, const ws_params* table, int n) {
+    if (!ctx || n < 0 || n > 32 || (n && !table)) return WS_ERR_ARG;
+    for (int b = 0; b < n; ++b)
+        if (table[b].tile) {
+            const int rc = valid_params(ctx, &table[b]);
+            if (rc) return rc;
+        }
+    for (int b = 0; b < 32; ++b) ctx->tuning[b] = b < n ? table[b] : ws_params{};
+    ctx->tuning_n = n;
+    ctx->items_valid = false;
     return WS_OK;
 }
 
@@ -718,6 +756,15 @@ extern "C" int ws_plan_create(ws_ctx* ctx, int njobs, const ws_job* jobs, ws_pla
         if (!jobs[j].order || !jobs[j].count) return set_error(ctx, WS_ERR_ARG, "ws_plan_create: job %d has no output", j);
     }
     cudaSetDevice(ctx->device);
+    uint64_t splats = 0;
+    for (int j = 0; j < njobs; ++j) splats += jobs[j].cloud->n;
+    const ws_params saved = ctx->params;
+    ctx->params = params_for(ctx, splats);   // restored below
+    struct Restore {
+        ws_ctx* c;
+        ws_params p;
+        ~Restore() { c->params = p; }
+    } restore{ctx, saved};
     ws_plan* p = new (std::nothrow) ws_plan();
     if (!p) return set_error(ctx, WS_ERR_NOMEM, "ws_plan_create: out of host memory");
     p->ctx = ctx;

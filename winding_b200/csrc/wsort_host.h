@@ -41,6 +41,8 @@ struct ws_ctx {
     cudaEvent_t launched = nullptr;   // the last launch on this context's scratch finished
     std::string err;
     ws_params params{};
+    ws_params tuning[32] = {};        // per floor(log2(splats)); tile 0: unset
+    int tuning_n = 0;
     wsort::DevBuf scratch, jobs_d, items_d, out_d;
     wsort::HostBuf jobs_h, items_h, count_h;
     uint32_t* err_d = nullptr;        // sticky device error: code, work item
