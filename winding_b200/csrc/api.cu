@@ -4,6 +4,7 @@
 #include "wsort_dev.cuh"
 #include "wsort_host.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -17,8 +18,8 @@ cudaError_t launch_sort(const JobDesc* jobs, const uint2* items, uint32_t n_item
                         uint32_t tile, int minb, uint32_t spin_limit, int grid, cudaStream_t stream,
                         TraceRec* trace);
 int sort_occupancy(uint32_t tile, int minb);
-cudaError_t launch_decode(const void* records, uint32_t n, float4* centers, float2* cov, uint32_t* bounds,
-                          uint32_t* bad, int sms, cudaStream_t stream);
+cudaError_t launch_decode(const void* records, uint32_t n, float4* centers, float2* cov, int8_t* sexp,
+                          uint32_t* bounds, uint32_t* bad, int sms, cudaStream_t stream);
 
 int set_error(ws_ctx* ctx, int code, const char* fmt, ...) {
     char buf[512];
@@ -110,9 +111,10 @@ size_t launch_scratch_bytes(const uint32_t* ns, int njobs, const ws_params& p) {
 // 1 and the dropped projection terms are zeros times finite numbers.
 //
 // keep_byte / keep_q: the footprint shortcut of the keys phase. With
-// A = fx (|W row 0|_1 + |1.3 / p00| |W row 2|_1) and the same for y, and
-// smax the largest |covariance entry| of the cloud, every entry of
-// |T| |Sigma| |T|^T is at most 1.02 max(A)^2 smax / d^2 =: keep_q / d^2.
+// A = fx (|W row 0|_1 + |1.3 / p00| |W row 2|_1) and the same for y, and a
+// splat's largest |covariance entry| at most 2^sexp, every entry of its
+// |T| |Sigma| |T|^T is at most 1.02 max(A)^2 2^sexp / d^2 =: keep_q 2^sexp / d^2
+// (keep_q is at least 2^-20, so keep_q 2^sexp stays a normal float).
 // keep_byte is the least alpha byte with RN(alpha * 1.85) >= cull.
 void view_shortcuts(const ws_view& v, const ws_cloud* c, uint32_t* fast, uint32_t* keep_byte, float* keep_q) {
     const float* M = v.model_view;
@@ -133,7 +135,7 @@ void view_shortcuts(const ws_view& v, const ws_cloud* c, uint32_t* fast, uint32_
     }
     *keep_byte = 256;
     *keep_q = INFINITY;
-    if (!(v.cull > 0.0f) || P[15] != 0.0f || !finite || !(c->smax >= 0.0f) || !std::isfinite(c->smax)) return;
+    if (!(v.cull > 0.0f) || P[15] != 0.0f || !finite) return;
     const float fx = (P[0] * v.viewport[0]) * 0.5f;
     const float fy = (P[5] * v.viewport[1]) * 0.5f;
     const double xhi = std::fabs((double)(1.3f / P[0])), yhi = std::fabs((double)(1.3f / P[5]));
@@ -143,7 +145,7 @@ void view_shortcuts(const ws_view& v, const ws_cloud* c, uint32_t* fast, uint32_
     const double a0 = std::fabs((double)fx) * (r0 + xhi * r2);
     const double a1 = std::fabs((double)fy) * (r1 + yhi * r2);
     const double a = std::fmax(a0, a1);
-    const double q = 1.02 * a * a * (double)c->smax;
+    const double q = std::fmax(1.02 * a * a, std::ldexp(1.0, -20));
     if (!std::isfinite(q) || q > 1e30) return;
     float qf = (float)q;
     if ((double)qf < q) qf = std::nextafter(qf, INFINITY);
@@ -167,6 +169,7 @@ void layout_jobs(JobDesc* out, const ws_job* jobs, int njobs, const ws_params& p
         std::memset(&d, 0, sizeof(d));
         d.centers = c->centers;
         d.cov = c->cov;
+        d.sexp = c->sexp;
         for (int k = 0; k < 3; ++k) {
             d.bmin[k] = c->bmin[k];
             d.bmax[k] = c->bmax[k];
@@ -183,6 +186,7 @@ void layout_jobs(JobDesc* out, const ws_job* jobs, int njobs, const ws_params& p
         view_shortcuts(jobs[j].view, c, &d.fast_transform, &d.keep_byte, &d.keep_q);
         size_t bytes;
         job_shape(c->n, p, &d.tiles, &bytes);
+        d.scan_items = d.tiles <= kSmallScanTiles ? 1u : kScanItems;
         const size_t np = pad_splats(c->n);
         d.k16 = reinterpret_cast<uint16_t*>(at);
         at += align_up(np * 2, 256);
@@ -202,21 +206,24 @@ void layout_jobs(JobDesc* out, const ws_job* jobs, int njobs, const ws_params& p
 
 // Items of one phase of one job.
 static void push_phase(std::vector<uint2>& items, const JobDesc& d, uint32_t job, uint32_t phase) {
-    const uint32_t count = (phase == kPhaseScanLo || phase == kPhaseScanHi) ? kScanItems
+    const uint32_t count = (phase == kPhaseScanLo || phase == kPhaseScanHi) ? d.scan_items
                            : phase == kPhaseCountHi ? (d.tiles + kCountSpan - 1) / kCountSpan
                                                     : d.tiles;
     for (uint32_t t = 0; t < count; ++t) items.push_back(make_uint2(job, (phase << kPhaseShift) | t));
 }
 
-// Work items, software-pipelined across jobs: at step s, phase k of job
-// s - k for k = 0..5, so that an item rarely waits for the phase before it.
+// Work items, phase major: every job's keys (largest job first), then every
+// job's low scan, low pass, and so on. An item's dependency (the phase
+// before it, of its job) was queued a whole phase earlier, so a CTA rarely
+// waits except at the end of a phase; within a phase the largest jobs come
+// first, whose dependencies finished first.
 void build_items(std::vector<uint2>& items, const JobDesc* jobs, int njobs) {
     items.clear();
-    for (int s = 0; s < njobs + (int)kPhases - 1; ++s)
-        for (uint32_t k = 0; k < kPhases; ++k) {
-            const int j = s - (int)k;
-            if (j >= 0 && j < njobs) push_phase(items, jobs[j], (uint32_t)j, k);
-        }
+    std::vector<int> by_size(njobs);
+    for (int j = 0; j < njobs; ++j) by_size[j] = j;
+    std::stable_sort(by_size.begin(), by_size.end(), [&](int a, int b) { return jobs[a].n > jobs[b].n; });
+    for (uint32_t k = 0; k < kPhases; ++k)
+        for (int j : by_size) push_phase(items, jobs[j], (uint32_t)j, k);
 }
 
 // Resident CTAs per SM the kernel variant is built for: ctas_per_sm, or 3.
@@ -531,7 +538,8 @@ static int decode_cloud(ws_ctx* ctx, const void* dev_records, uint32_t n, ws_clo
     c->n = n;
     const size_t np = pad_splats(n);
     if ((e = cudaMalloc(&c->centers, np * sizeof(float4))) != cudaSuccess ||
-        (e = cudaMalloc(&c->cov, np * 3 * sizeof(float2))) != cudaSuccess) {
+        (e = cudaMalloc(&c->cov, np * 3 * sizeof(float2))) != cudaSuccess ||
+        (e = cudaMalloc(&c->sexp, np)) != cudaSuccess) {
         ws_cloud_free(c);
         return cuda_error(ctx, e, "ws_cloud");
     }
@@ -544,7 +552,8 @@ static int decode_cloud(ws_ctx* ctx, const void* dev_records, uint32_t n, ws_clo
     cudaMemcpyAsync(words, init, sizeof(init), cudaMemcpyHostToDevice, ctx->stream);
     cudaMemsetAsync(c->centers, 0, np * sizeof(float4), ctx->stream);
     cudaMemsetAsync(c->cov, 0, np * 3 * sizeof(float2), ctx->stream);
-    e = launch_decode(dev_records, n, c->centers, c->cov, words, words + 7, ctx->sms, ctx->stream);
+    cudaMemsetAsync(c->sexp, 0x7f, np, ctx->stream);   // padding: no shortcut
+    e = launch_decode(dev_records, n, c->centers, c->cov, c->sexp, words, words + 7, ctx->sms, ctx->stream);
     uint32_t back[8];
     if (e == cudaSuccess) e = cudaMemcpyAsync(back, words, sizeof(back), cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
@@ -642,6 +651,7 @@ extern "C" int ws_cloud_free(ws_cloud* c) {
     if (c->magic != kCloudMagic) {   // a half-built cloud from a failed load
         if (c->centers) cudaFree(c->centers);
         if (c->cov) cudaFree(c->cov);
+        if (c->sexp) cudaFree(c->sexp);
         delete c;
         return WS_OK;
     }
@@ -651,8 +661,10 @@ extern "C" int ws_cloud_free(ws_cloud* c) {
     cudaDeviceSynchronize();
     if (c->centers) cudaFree(c->centers);
     if (c->cov) cudaFree(c->cov);
+    if (c->sexp) cudaFree(c->sexp);
     c->centers = nullptr;
     c->cov = nullptr;
+    c->sexp = nullptr;
     // The handle stays valid (and refused by every call) until its context
     // is destroyed, so a sort of a freed cloud is an error, not a crash.
     c->alive = false;

@@ -80,7 +80,8 @@ __device__ __forceinline__ void covariance(float fsx, float fsy, float fsz, uint
 // 0xFFFFFFFF).
 __global__ void __launch_bounds__(256) decode_kernel(const uint4* __restrict__ rec, uint32_t n,
                                                      float4* __restrict__ centers, float2* __restrict__ cov,
-                                                     uint32_t* __restrict__ bounds, uint32_t* __restrict__ bad) {
+                                                     int8_t* __restrict__ sexp, uint32_t* __restrict__ bounds,
+                                                     uint32_t* __restrict__ bad) {
     uint32_t lo[3] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu};
     uint32_t hi[3] = {0u, 0u, 0u};
     uint32_t smax = 0u;
@@ -98,6 +99,22 @@ __global__ void __launch_bounds__(256) decode_kernel(const uint4* __restrict__ r
         cov[3 * (size_t)i] = make_float2(c[0], c[1]);
         cov[3 * (size_t)i + 1] = make_float2(c[2], c[3]);
         cov[3 * (size_t)i + 2] = make_float2(c[4], c[5]);
+        float m = 0.0f;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) m = fmaxf(m, fabsf(c[k]));
+        bool finite = true;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) finite = finite && isfinite(c[k]);
+        // The least e with max |entry| <= 2^e (frexp: m = f 2^e, f in [.5, 1)),
+        // clamped to [-100, 127]; 127 for a non-finite entry.
+        int e = -100;
+        if (!finite) {
+            e = 127;
+        } else if (m > 0.0f) {
+            frexpf(m, &e);
+            e = e < -100 ? -100 : (e > 127 ? 127 : e);
+        }
+        sexp[i] = (int8_t)e;
 #pragma unroll
         for (int k = 0; k < 6; ++k) smax = max(smax, ordered(fabsf(c[k])));
         const uint32_t o[3] = {ordered(x), ordered(y), ordered(z)};
@@ -127,11 +144,11 @@ __global__ void __launch_bounds__(256) decode_kernel(const uint4* __restrict__ r
     }
 }
 
-cudaError_t launch_decode(const void* records, uint32_t n, float4* centers, float2* cov, uint32_t* bounds,
-                          uint32_t* bad, int sms, cudaStream_t stream) {
+cudaError_t launch_decode(const void* records, uint32_t n, float4* centers, float2* cov, int8_t* sexp,
+                          uint32_t* bounds, uint32_t* bad, int sms, cudaStream_t stream) {
     const uint32_t want = (n + 255) / 256;
     const uint32_t grid = want < (uint32_t)sms * 8u ? (want ? want : 1u) : (uint32_t)sms * 8u;
-    decode_kernel<<<grid, 256, 0, stream>>>(static_cast<const uint4*>(records), n, centers, cov, bounds, bad);
+    decode_kernel<<<grid, 256, 0, stream>>>(static_cast<const uint4*>(records), n, centers, cov, sexp, bounds, bad);
     return cudaGetLastError();
 }
 

@@ -78,8 +78,8 @@ __global__ void noalloc_setup_kernel(JobDesc desc, uint32_t tiles, uint32_t clea
     for (uint32_t k = tid; k < clear_bytes / 4; k += stride) reinterpret_cast<uint32_t*>(g_scratch)[k] = 0;
     // The phases in order: keys, low scan, low pass, high counts, high scan,
     // high pass (the order ws_sort's work list has for a single job).
-    const uint32_t counts[kPhases] = {tiles, kScanItems, tiles, (tiles + kCountSpan - 1) / kCountSpan, kScanItems,
-                                      tiles};
+    const uint32_t scans = desc.scan_items;
+    const uint32_t counts[kPhases] = {tiles, scans, tiles, (tiles + kCountSpan - 1) / kCountSpan, scans, tiles};
     uint32_t first = 0;
     for (uint32_t ph = 0; ph < kPhases; ++ph) {
         for (uint32_t t = tid; t < counts[ph]; t += stride) items[first + t] = make_uint2(0u, (ph << kPhaseShift) | t);
@@ -148,7 +148,7 @@ extern "C" int ws_sort_noalloc(const ws_cloud* cloud, const ws_view* view, uint3
     layout_jobs(&desc, &job, 1, p, base);
 
     const uint32_t tiles = desc.tiles;
-    const uint32_t n_items = 3 * tiles + (tiles + kCountSpan - 1) / kCountSpan + 2 * kScanItems;
+    const uint32_t n_items = 3 * tiles + (tiles + kCountSpan - 1) / kCountSpan + 2 * desc.scan_items;
     const uint32_t clear_bytes = (uint32_t)(((sizeof(LaunchCtl) + sizeof(JobCtl)) + 3) / 4 * 4);
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);

@@ -50,6 +50,7 @@ struct SortSmem {
     union {
         struct {                    // Keys
             float4 centers[kTile];
+            int8_t sexp[kTile];
             uint32_t res[kTile];            // per splat: key, kCulled, or kPending
             uint16_t queue[kTile];          // splats whose footprint must be evaluated
             uint32_t qn;
@@ -190,13 +191,19 @@ __device__ __forceinline__ void count_digit(uint32_t* hist, uint32_t d, bool on)
 // covariance only then.
 //
 // Footprint shortcut (exact): for a perspective view the host proves
-// keep_q <= 100 d^2 implies every entry of |T| |Sigma| |T|^T is at most 100
-// (T = J W, d = -view.z), and then the pinned computation of the area cannot
+// keep_q 2^sexp <= 100 d^2 implies every entry of |T| |Sigma| |T|^T is at most
+// 100 (T = J W, d = -view.z, sexp the splat's covariance exponent bound), and
+// then the pinned computation of the area cannot
 // fall below 1.85, whatever the rounding: the 2D covariance differs from a
 // positive semi-definite one by at most 7.1 u * 100 per entry, which moves
 // (xx + .3)(yy + .3) - xy^2 at most 0.0025 below 0.09. So alpha * area >=
 // RN(alpha * 1.85) >= cull for every alpha byte >= keep_byte, and such a
 // splat is kept without its footprint (or its covariance) being computed.
+// The same analysis bounds the pinned area from above for any G = the
+// largest entry of |T| |Sigma| |T|^T (G <= 1.002 keep_q 2^sexp / d^2): every
+// 2D entry is at most G (1 + 8.2u), so the area is at most
+// 2 pi (1.00001 G + 0.3)(1 + 5u); a splat with alpha times that below cull
+// is culled, again without its footprint.
 constexpr uint32_t kPending = 0xFFFFFFFEu;
 
 template <int IPT>
@@ -223,8 +230,11 @@ __device__ void keys_tile(const JobDesc& J, int job, uint32_t tile, SortSmem<IPT
     if (any) {
 #pragma unroll
         for (int r = 0; r < IPT; ++r) cp_async16(&sm.u.k.centers[r * kThreads + tid], &J.centers[base + r * kThreads + tid]);
+        if (fp) cta_copy(sm.u.k.sexp, J.sexp + base, T);
         cp_async_wait_all();
     }
+    __syncthreads();   // the exponents were copied by other threads
+    if (tid == 0) sm.mark[0] = global_ns();
     // Sweep 1: tests and shortcut; footprints still to evaluate are queued.
 #pragma unroll 1
     for (uint32_t k = 0; k < T; k += kThreads) {
@@ -240,8 +250,31 @@ __device__ void keys_tile(const JobDesc& J, int job, uint32_t tile, SortSmem<IPT
                 if (!(fmul(alpha, 255.0f) <= 1.0f)) {   // else too faint to reach 1/255
                     res = depth_key(c, view);
                     if (fp) {
-                        const float d = -view[2];
-                        if (!(c.persp && byte >= c.keep_byte && c.keep_q <= fmul(100.0f, fmul(d, d)))) res = kPending;
+                        // Decided without the footprint when the bounds allow
+                        // (see above); else queued.
+                        bool decided = false;
+                        if (c.persp) {
+                            const float d = -view[2];
+                            // keep_q 2^sexp, exactly: sexp is in [-100, 127] and
+                            // keep_q >= 2^-20, so the product is a normal float
+                            // (or +inf).
+                            const float pow2 = __int_as_float((int(sm.u.k.sexp[at]) + 127) << 23);
+                            const float q = fmul(c.keep_q, pow2);
+                            const float dd = fmul(d, d);
+                            if (byte >= c.keep_byte && q <= fmul(100.0f, dd)) {
+                                decided = true;   // kept
+                            } else if (dd > 1e-30f && dd < 1e30f && q < 1e30f) {
+                                // An upper bound of G: the approximate quotient is
+                                // within a few ulps, far inside the 1.002 margin.
+                                const float g = fmul(1.002f, __fdividef(q, dd));
+                                const float top = fmul(fmul(fmul(alpha, 6.2832f), fadd(fmul(g, 1.00001f), 0.3f)), 1.0001f);
+                                if (top < c.cull) {
+                                    res = kCulled;
+                                    decided = true;
+                                }
+                            }
+                        }
+                        if (!decided) res = kPending;
                     }
                 }
             }
@@ -256,6 +289,7 @@ __device__ void keys_tile(const JobDesc& J, int job, uint32_t tile, SortSmem<IPT
         sm.u.k.res[at] = res;
     }
     __syncthreads();
+    if (tid == 0) sm.mark[1] = global_ns();
     // Sweep 2: the queued footprints, densely.
     const uint32_t qn = sm.u.k.qn;
     for (uint32_t e = tid; e < qn; e += kThreads) {
@@ -272,6 +306,7 @@ __device__ void keys_tile(const JobDesc& J, int job, uint32_t tile, SortSmem<IPT
         sm.u.k.res[at] = footprint_keeps(c, view, sg, alpha) ? depth_key(c, view) : kCulled;
     }
     __syncthreads();
+    if (tid == 0) sm.mark[2] = global_ns();
     // Sweep 3: keys, survivor bits and low-digit counts.
 #pragma unroll 4
     for (uint32_t k = 0; k < T; k += kThreads) {
@@ -372,6 +407,22 @@ __device__ void scan_digit(uint32_t* cnt, uint32_t tiles, uint32_t d, uint32_t* 
         carry += chunk_total;
     }
     if (tid == 0) tot[d] = carry;
+}
+
+// ScanLo / ScanHi of a job of at most kSmallScanTiles tiles, in one item:
+// thread d scans its digit's row serially.
+__device__ void scan_small(uint32_t* cnt, uint32_t tiles, uint32_t* tot) {
+    uint32_t* row = cnt + (size_t)threadIdx.x * tiles;
+    uint32_t v[kSmallScanTiles];
+#pragma unroll
+    for (uint32_t r = 0; r < kSmallScanTiles; ++r) v[r] = r < tiles ? __ldcg(&row[r]) : 0u;
+    uint32_t run = 0;
+#pragma unroll
+    for (uint32_t r = 0; r < kSmallScanTiles; ++r) {
+        if (r < tiles) row[r] = run;
+        run += v[r];
+    }
+    tot[threadIdx.x] = run;
 }
 
 // Low / High: one stable counting pass over 8 key bits for one tile. The
@@ -531,7 +582,7 @@ __global__ void __launch_bounds__(kThreads, MINB) sort_kernel(const JobDesc* __r
         if (work && phase != kPhaseKeys && !(sm.ready_job == job && sm.ready_phase == phase)) {
             // Items the phase before this one has: tiles, pairs of tiles, or
             // one per digit.
-            const uint32_t need = (phase == kPhaseLow || phase == kPhaseHigh) ? kScanItems
+            const uint32_t need = (phase == kPhaseLow || phase == kPhaseHigh) ? J.scan_items
                                   : phase == kPhaseScanHi ? (J.tiles + kCountSpan - 1) / kCountSpan
                                                           : J.tiles;
             work = wait_phase(&ctl->done[phase - 1], need, sm, err, it, spin_limit);
@@ -547,10 +598,20 @@ __global__ void __launch_bounds__(kThreads, MINB) sort_kernel(const JobDesc* __r
             }
             switch (phase) {
                 case kPhaseKeys: keys_tile(J, job, tile, sm); break;
-                case kPhaseScanLo: scan_digit(J.cnt_lo, J.tiles, tile, ctl->tot[0], sm); break;
+                case kPhaseScanLo:
+                    if (J.scan_items == 1)
+                        scan_small(J.cnt_lo, J.tiles, ctl->tot[0]);
+                    else
+                        scan_digit(J.cnt_lo, J.tiles, tile, ctl->tot[0], sm);
+                    break;
                 case kPhaseLow: digit_tile<0>(J, job, tile, sm, err, it); break;
                 case kPhaseCountHi: count_hi_item(J, job, tile, sm); break;
-                case kPhaseScanHi: scan_digit(J.cnt_hi, J.tiles, tile, ctl->tot[1], sm); break;
+                case kPhaseScanHi:
+                    if (J.scan_items == 1)
+                        scan_small(J.cnt_hi, J.tiles, ctl->tot[1]);
+                    else
+                        scan_digit(J.cnt_hi, J.tiles, tile, ctl->tot[1], sm);
+                    break;
                 default: digit_tile<1>(J, job, tile, sm, err, it); break;
             }
             __syncthreads();

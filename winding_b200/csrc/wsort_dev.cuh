@@ -38,21 +38,24 @@ constexpr uint32_t kErrBounds = 3;        // a scatter position fell outside the
 constexpr uint32_t kPhaseKeys = 0, kPhaseScanLo = 1, kPhaseLow = 2, kPhaseCountHi = 3, kPhaseScanHi = 4,
                    kPhaseHigh = 5, kPhases = 6;
 constexpr uint32_t kCountSpan = 2;        // tiles one CountHi item covers
-constexpr uint32_t kScanItems = 256;      // scan items per pass: one per digit value
+constexpr uint32_t kScanItems = 256;      // scan items per pass of a large job: one per digit value
+constexpr uint32_t kSmallScanTiles = 64;  // a job of at most this many tiles scans in one item
 
 // One (cloud, view) to sort, as the persistent kernel reads it.
 struct alignas(16) JobDesc {
     // cloud (resident)
     const float4* centers;      // x, y, z, colour word bits; padded to kPadSplats
     const float2* cov;          // 6 f32 a splat as 3 float2; padded likewise
+    const int8_t* sexp;         // per splat: max |covariance entry| <= 2^sexp; padded likewise
     double bmin[3], bmax[3];    // box around the centres
     uint32_t n;
     uint32_t tiles;             // tiles of splats (Keys, Low) = tiles of the low pass's output (High)
     // Per-view shortcuts the host proves exact (see keys_tile):
     uint32_t fast_transform;    // affine model-view, reverse-Z perspective, no overflow possible
     uint32_t keep_byte;         // alpha bytes at or above this pass the footprint cull when ...
-    float keep_q;               // ... keep_q <= 100 d^2 (+inf: never)
-    uint32_t pad1[3];
+    float keep_q;               // ... keep_q 2^sexp <= 100 d^2 (+inf: never)
+    uint32_t scan_items;        // items of each scan phase: 1 (small job) or 256 (one per digit)
+    uint32_t pad1[2];
     // view: the values the reference writes into its Cloud uniform
     float mv[16];
     float proj[16];

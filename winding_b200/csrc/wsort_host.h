@@ -72,6 +72,7 @@ struct ws_cloud {
     uint32_t n = 0;
     float4* centers = nullptr;
     float2* cov = nullptr;
+    int8_t* sexp = nullptr;         // per splat: max |covariance entry| <= 2^sexp
     double bmin[3] = {0, 0, 0}, bmax[3] = {0, 0, 0};
     float smax = 0.0f;              // largest |covariance entry| of the cloud
 };
