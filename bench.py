@@ -58,6 +58,8 @@ def parse_args():
     ap.add_argument("--cull", type=float, default=0.5)
     ap.add_argument("--no-suite", action="store_true", help="skip the slab-6M / mixed-64 side measurements")
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU baseline sample length")
+    ap.add_argument("--tile", type=int, default=0, help="fixed tile size (skips the autotuner; with --ctas)")
+    ap.add_argument("--ctas", type=int, default=0, help="fixed resident CTAs per SM (with --tile)")
     return ap.parse_args()
 
 
@@ -292,7 +294,12 @@ def _run_wsort(args, rank, world, local_rank, torch):
 
     plain = plain_measure(ctx, torch, jobs, 0, args.warmup, flush)   # load + warm
     from winding_b200 import autotune
-    tuned = autotune.tune(ctx, [list(zip(plain["clouds"], plain["views"]))])
+    if args.tile and args.ctas:
+        ctx.set_params(tile=args.tile, ctas_per_sm=args.ctas)
+        autotune.install(ctx, {})
+        tuned = {autotune.bucket(plain["splats"]): (args.tile, args.ctas)}
+    else:
+        tuned = autotune.tune(ctx, [list(zip(plain["clouds"], plain["views"]))])
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
