@@ -51,7 +51,7 @@ struct SortSmem {
         struct {                    // Keys
             float4 centers[kTile];
             int8_t sexp[kTile];
-            uint32_t res[kTile];            // per splat: key, kCulled, or kPending
+            uint32_t maskw[kTile / 32];     // survivor bits
             uint16_t queue[kTile];          // splats whose footprint must be evaluated
             uint32_t qn;
         } k;
@@ -235,11 +235,15 @@ __device__ void keys_tile(const JobDesc& J, int job, uint32_t tile, SortSmem<IPT
     }
     __syncthreads();   // the exponents were copied by other threads
     if (tid == 0) sm.mark[0] = global_ns();
-    // Sweep 1: tests and shortcut; footprints still to evaluate are queued.
+    // Sweep 1: tests, keys and the footprint shortcut. Every splat's key slot
+    // is written now (the passes read only the slots whose survivor bit is
+    // set), with the survivor bits and digit counts of the splats already
+    // decided; the ones whose footprint must still be evaluated go to a queue.
 #pragma unroll 1
     for (uint32_t k = 0; k < T; k += kThreads) {
         const uint32_t at = k + tid;
-        uint32_t res = kCulled;
+        uint32_t key = 0;
+        bool kept = false, pending = false;
         if (any && base + at < n) {
             const float4 p = sm.u.k.centers[at];
             float view[4];
@@ -248,7 +252,8 @@ __device__ void keys_tile(const JobDesc& J, int job, uint32_t tile, SortSmem<IPT
                 const uint32_t byte = __float_as_uint(p.w) >> 24;
                 const float alpha = sm.alpha[byte];
                 if (!(fmul(alpha, 255.0f) <= 1.0f)) {   // else too faint to reach 1/255
-                    res = depth_key(c, view);
+                    key = depth_key(c, view);
+                    kept = true;
                     if (fp) {
                         // Decided without the footprint when the bounds allow
                         // (see above); else queued.
@@ -269,28 +274,36 @@ __device__ void keys_tile(const JobDesc& J, int job, uint32_t tile, SortSmem<IPT
                                 const float g = fmul(1.002f, __fdividef(q, dd));
                                 const float top = fmul(fmul(fmul(alpha, 6.2832f), fadd(fmul(g, 1.00001f), 0.3f)), 1.0001f);
                                 if (top < c.cull) {
-                                    res = kCulled;
+                                    kept = false;
                                     decided = true;
                                 }
                             }
                         }
-                        if (!decided) res = kPending;
+                        if (!decided) {
+                            kept = false;
+                            pending = true;
+                        }
                     }
                 }
             }
         }
-        const uint32_t pend = __ballot_sync(0xffffffffu, res == kPending);
+        const uint32_t i = base + at;
+        if (i < n) J.k16[i] = (uint16_t)key;
+        const uint32_t kb = __ballot_sync(0xffffffffu, kept);
+        if (lane == 0) sm.u.k.maskw[at >> 5] = kb;
+        if (kept) atomicAdd(&sm.hist[key & 255u], 1u);
+        const uint32_t pend = __ballot_sync(0xffffffffu, pending);
         if (pend) {
             uint32_t first = 0;
             if (lane == (uint32_t)(__ffs(pend) - 1)) first = atomicAdd(&sm.u.k.qn, (uint32_t)__popc(pend));
             first = __shfl_sync(0xffffffffu, first, __ffs(pend) - 1);
-            if (res == kPending) sm.u.k.queue[first + __popc(pend & lanemask_lt())] = (uint16_t)at;
+            if (pending) sm.u.k.queue[first + __popc(pend & lanemask_lt())] = (uint16_t)at;
         }
-        sm.u.k.res[at] = res;
     }
     __syncthreads();
     if (tid == 0) sm.mark[1] = global_ns();
-    // Sweep 2: the queued footprints, densely.
+    // Sweep 2: the queued footprints, densely; a kept splat sets its bit and
+    // counts its digit (its key is already out).
     const uint32_t qn = sm.u.k.qn;
     for (uint32_t e = tid; e < qn; e += kThreads) {
         const uint32_t at = sm.u.k.queue[e];
@@ -303,22 +316,15 @@ __device__ void keys_tile(const JobDesc& J, int job, uint32_t tile, SortSmem<IPT
         const float2 c2 = __ldcs(&J.cov[3 * i + 2]);
         const float sg[6] = {a.x, a.y, b2.x, b2.y, c2.x, c2.y};
         const float alpha = sm.alpha[__float_as_uint(p.w) >> 24];
-        sm.u.k.res[at] = footprint_keeps(c, view, sg, alpha) ? depth_key(c, view) : kCulled;
+        if (footprint_keeps(c, view, sg, alpha)) {
+            atomicOr(&sm.u.k.maskw[at >> 5], 1u << (at & 31u));
+            atomicAdd(&sm.hist[depth_key(c, view) & 255u], 1u);
+        }
     }
     __syncthreads();
     if (tid == 0) sm.mark[2] = global_ns();
-    // Sweep 3: keys, survivor bits and low-digit counts.
-#pragma unroll 4
-    for (uint32_t k = 0; k < T; k += kThreads) {
-        const uint32_t i = base + k + tid;
-        const uint32_t key = sm.u.k.res[k + tid];
-        const bool surv = key != kCulled;
-        const uint32_t ballot = __ballot_sync(0xffffffffu, surv);
-        if (i < n) J.k16[i] = surv ? (uint16_t)key : (uint16_t)0;
-        if (lane == 0 && i < n) J.mask[i >> 5] = ballot;
-        if (surv) atomicAdd(&sm.hist[key & 255u], 1u);
-    }
-    __syncthreads();
+    for (uint32_t w = tid; w < T / 32; w += kThreads)
+        if (base + w * 32 < n) J.mask[(base >> 5) + w] = sm.u.k.maskw[w];
     J.cnt_lo[(size_t)tid * J.tiles + tile] = sm.hist[tid];
 }
 
@@ -521,20 +527,37 @@ __device__ void digit_tile(const JobDesc& J, int job, uint32_t tile, SortSmem<IP
     }
     __syncthreads();
     if (tid == 0) sm.mark[2] = global_ns();
-    for (uint32_t s = tid; s < tile_total; s += kThreads) {
-        const uint32_t key = sm.u.p.stage_key[s];
-        const uint32_t d = PASS == 0 ? (key & 255u) : (key >> 8);
-        const uint32_t g = sm.u.p.gofs[d] + s;
-        if (g >= J.n) {   // only reachable if counts disagree: record, do not write
-            raise_error(err, kErrBounds, item);
-            continue;
+    // Write-out in chunks of four slots per thread: the chunk's staged
+    // entries are read first, so their shared-memory loads overlap.
+    constexpr int kChunk = 4;
+#pragma unroll 1
+    for (int r0 = 0; r0 < IPT && (uint32_t)r0 * kThreads < tile_total; r0 += kChunk) {
+        uint32_t kk[kChunk], ix[kChunk];
+#pragma unroll
+        for (int q = 0; q < kChunk; ++q) {
+            const uint32_t s = (uint32_t)(r0 + q) * kThreads + tid;
+            const bool on = s < tile_total;
+            kk[q] = on ? (uint32_t)sm.u.p.stage_key[s] : 0xFFFFFFFFu;
+            ix[q] = on ? sm.u.p.stage_idx[s] : 0u;
         }
-        if (PASS == 0) {
-            J.key_b[g] = (uint16_t)key;
-            J.idx_b[g] = sm.u.p.stage_idx[s];
-        } else {
-            __stcs(&J.order[g], sm.u.p.stage_idx[s]);
-            if (J.keys) __stcs(&J.keys[g], key);
+#pragma unroll
+        for (int q = 0; q < kChunk; ++q) {
+            if (kk[q] == 0xFFFFFFFFu) continue;
+            const uint32_t s = (uint32_t)(r0 + q) * kThreads + tid;
+            const uint32_t key = kk[q];
+            const uint32_t d = PASS == 0 ? (key & 255u) : (key >> 8);
+            const uint32_t g = sm.u.p.gofs[d] + s;
+            if (g >= J.n) {   // only reachable if counts disagree: record, do not write
+                raise_error(err, kErrBounds, item);
+                continue;
+            }
+            if (PASS == 0) {
+                J.key_b[g] = (uint16_t)key;
+                J.idx_b[g] = ix[q];
+            } else {
+                __stcs(&J.order[g], ix[q]);
+                if (J.keys) __stcs(&J.keys[g], key);
+            }
         }
     }
 }
