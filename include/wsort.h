@@ -272,8 +272,8 @@ int ws_sort_noalloc(const ws_cloud* cloud, const ws_view* view, uint32_t* order,
 /*
  * Kernel parameters. tile: splats one work item of the key and digit passes
  * covers (1024, 2048 or 4096). ctas_per_sm: the kernel variant's resident
- * CTAs per SM (2, 3 or 4; 0 picks 3), which bounds its registers per
- * thread. spin_limit: polls a device-side wait makes before it gives up
+ * CTAs per SM (2, 3 or 4, or 6 with tile 1024; 0 picks 3), which bounds its
+ * registers per thread. spin_limit: polls a device-side wait makes before it gives up
  * with WS_ERR_TIMEOUT.
  */
 typedef struct ws_params {

@@ -202,14 +202,24 @@ def test_batch_equals_each_job_alone(ctx):
         sp.destroy()
 
 
-@pytest.mark.parametrize("tile", [1024, 2048, 4096])
-def test_tile_parameters_do_not_change_the_result(ctx, tile):
+@pytest.mark.parametrize("tile,ctas", [(1024, 2), (1024, 3), (1024, 4), (1024, 6), (2048, 2), (2048, 3), (2048, 4),
+                                       (4096, 2), (4096, 3), (4096, 4)])
+def test_kernel_variants_do_not_change_the_result(ctx, tile, ctas):
     old = ctx.params
     try:
-        ctx.set_params(tile=tile)
+        ctx.set_params(tile=tile, ctas_per_sm=ctas)
         check_job(ctx, W.clusters_1m(seed=41, n=120_001))
     finally:
-        ctx.set_params(tile=old.tile)
+        ctx.set_params(tile=old.tile, ctas_per_sm=old.ctas_per_sm)
+
+
+def test_missing_kernel_variant_is_refused(ctx):
+    old = ctx.params
+    for tile, ctas in [(2048, 6), (4096, 6), (1024, 5), (1024, 1), (3000, 3)]:
+        with pytest.raises(WsError, match="tile|ctas_per_sm"):
+            ctx.set_params(tile=tile, ctas_per_sm=ctas)
+    p = ctx.params
+    assert (p.tile, p.ctas_per_sm) == (old.tile, old.ctas_per_sm)
 
 
 def test_full_size_slab_properties(ctx):

@@ -1,7 +1,8 @@
 """The sort's autotuner: tile size and kernel variant per launch size.
 
 For a workload (or synthetic clouds of given sizes), every candidate
-(tile 1024 / 2048 / 4096 x 2 / 3 / 4 resident CTAs per SM) is timed with the
+(tile 1024 / 2048 / 4096 x 2 / 3 / 4 resident CTAs per SM, and tile 1024 x 6)
+is timed with the
 library's own CUDA-event kernel timing (ws_timing) over a few launches, and
 the fastest is installed in the context's tuning table for that launch size
 (floor(log2(total splats)), ws_set_tuning). Results persist in a JSON cache
@@ -18,6 +19,7 @@ from . import _lib
 
 TILES = (1024, 2048, 4096)
 CTAS = (2, 3, 4)
+CANDIDATES = tuple((t, c) for t in TILES for c in CTAS) + ((1024, 6),)
 
 
 def bucket(splats: int) -> int:
@@ -63,10 +65,9 @@ def measure(ctx, jobs, reps: int = 5) -> list[tuple[float, int, int]]:
     ctx.check(ctx.lib.ws_set_tuning(ctx.handle, table_off, 0))
     out = []
     try:
-        for tile in TILES:
-            for ctas in CTAS:
-                ctx.set_params(tile=tile, ctas_per_sm=ctas)
-                out.append((_time_jobs(ctx, jobs, reps), tile, ctas))
+        for tile, ctas in CANDIDATES:
+            ctx.set_params(tile=tile, ctas_per_sm=ctas)
+            out.append((_time_jobs(ctx, jobs, reps), tile, ctas))
     finally:
         ctx.set_params(tile=saved.tile, ctas_per_sm=saved.ctas_per_sm)
     return sorted(out)

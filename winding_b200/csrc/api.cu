@@ -227,12 +227,15 @@ void build_items(std::vector<uint2>& items, const JobDesc* jobs, int njobs) {
 }
 
 // Resident CTAs per SM the kernel variant is built for: ctas_per_sm, or 3.
-int variant_minb(const ws_params& p) { return p.ctas_per_sm >= 2 && p.ctas_per_sm <= 4 ? (int)p.ctas_per_sm : 3; }
+int variant_minb(const ws_params& p) {
+    if (p.ctas_per_sm == 6 && p.tile == 1024) return 6;
+    return p.ctas_per_sm >= 2 && p.ctas_per_sm <= 4 ? (int)p.ctas_per_sm : 3;
+}
 
 int grid_for(ws_ctx* ctx, size_t n_items) {
     const int minb = variant_minb(ctx->params);
     const int ti = ctx->params.tile == 1024 ? 0 : ctx->params.tile == 2048 ? 1 : 2;
-    int& cached = ctx->occupancy[ti][minb - 2];
+    int& cached = ctx->occupancy[ti][minb - 2];   // minb is 2..6
     if (cached == 0) cached = sort_occupancy(ctx->params.tile, minb);
     int per_sm = cached < 1 ? 1 : cached;
     size_t g = (size_t)ctx->sms * per_sm;
@@ -469,13 +472,20 @@ extern "C" int ws_get_params(const ws_ctx* ctx, ws_params* out) {
     return WS_OK;
 }
 
+// The kernel variants that exist: tile 1024, 2048 or 4096 with 2, 3 or 4
+// resident CTAs per SM (0 picks 3), and tile 1024 with 6.
+static const char* params_problem(const ws_params* p) {
+    if (p->tile != 1024 && p->tile != 2048 && p->tile != 4096) return "tile must be 1024, 2048 or 4096";
+    if (p->spin_limit == 0) return "spin_limit must be positive";
+    const bool ok = p->ctas_per_sm == 0 || (p->ctas_per_sm >= 2 && p->ctas_per_sm <= 4) ||
+                    (p->ctas_per_sm == 6 && p->tile == 1024);
+    if (!ok) return "ctas_per_sm must be 0, 2, 3 or 4 (or 6 with tile 1024)";
+    return nullptr;
+}
+
 static int valid_params(ws_ctx* ctx, const ws_params* p) {
-    if (p->tile != 1024 && p->tile != 2048 && p->tile != 4096)
-        return set_error(ctx, WS_ERR_ARG, "tile must be 1024, 2048 or 4096");
-    if (p->spin_limit == 0) return set_error(ctx, WS_ERR_ARG, "spin_limit must be positive");
-    if (p->ctas_per_sm != 0 && (p->ctas_per_sm < 2 || p->ctas_per_sm > 4))
-        return set_error(ctx, WS_ERR_ARG, "ctas_per_sm must be 0, 2, 3 or 4");
-    return WS_OK;
+    const char* why = params_problem(p);
+    return why ? set_error(ctx, WS_ERR_ARG, "%s", why) : WS_OK;
 }
 
 extern "C" int ws_set_tuning(ws_ctx* ctx, const ws_params* table, int n) {
@@ -493,11 +503,7 @@ extern "C" int ws_set_tuning(ws_ctx* ctx, const ws_params* table, int n) {
 
 extern "C" int ws_set_params(ws_ctx* ctx, const ws_params* p) {
     if (!ctx || !p) return WS_ERR_ARG;
-    if (p->tile != 1024 && p->tile != 2048 && p->tile != 4096)
-        return set_error(ctx, WS_ERR_ARG, "ws_set_params: tile must be 1024, 2048 or 4096");
-    if (p->spin_limit == 0) return set_error(ctx, WS_ERR_ARG, "ws_set_params: spin_limit must be positive");
-    if (p->ctas_per_sm != 0 && (p->ctas_per_sm < 2 || p->ctas_per_sm > 4))
-        return set_error(ctx, WS_ERR_ARG, "ws_set_params: ctas_per_sm must be 0, 2, 3 or 4");
+    if (const char* why = params_problem(p)) return set_error(ctx, WS_ERR_ARG, "ws_set_params: %s", why);
     ctx->params = *p;
     ctx->items_valid = false;
     return WS_OK;

@@ -175,13 +175,6 @@ __device__ __forceinline__ uint32_t match_digit8(uint32_t d, bool on) {
     return m;
 }
 
-// Warp-aggregated increment of hist[d] by the lanes whose `on` is set; for
-// digits that repeat within a warp (a skewed depth distribution).
-__device__ __forceinline__ void count_digit(uint32_t* hist, uint32_t d, bool on) {
-    const uint32_t peers = match_digit8(d, on);
-    if (on && lane_id() == (uint32_t)(__ffs(peers) - 1)) atomicAdd(&hist[d], (uint32_t)__popc(peers));
-}
-
 // Keys: keys, survivor bits and low-digit counts for one tile of splats.
 // The tile's centres are copied to shared memory at once. A first sweep
 // applies the frustum and faintness tests and the footprint shortcut; the
@@ -363,22 +356,34 @@ __device__ void count_hi_item(const JobDesc& J, int job, uint32_t g, SortSmem<IP
     }
     cp_async_wait_all();
     __syncthreads();
-#pragma unroll
+    // Per-warp counters, two 16-bit digit counts to a word (a warp counts at
+    // most 32 x IPT keys of a tile), bumped with shared-memory atomics: one
+    // atomic per key, no ballots.
+    uint32_t* wc = reinterpret_cast<uint32_t*>(&sm.u.p.wcnt[0][0]);   // [kWarps][128]
+    const uint32_t warp = tid >> 5;
+#pragma unroll 1
     for (uint32_t q = 0; q < kCountSpan; ++q) {
         const uint32_t tile = g * kCountSpan + q;
         if (tile >= J.tiles) break;
-        sm.hist[tid] = 0;
+        for (int k = tid; k < kWarps * 128; k += kThreads) wc[k] = 0;
         __syncthreads();
         const uint32_t base = tile * T;
         if (base < s_total) {
-#pragma unroll 4
+#pragma unroll
             for (int r = 0; r < IPT; ++r) {
-                const uint32_t at = r * kThreads + tid;
-                count_digit(sm.hist, area[q][at] >> 8, base + at < s_total);
+                const uint32_t at = warp * 32u * IPT + r * 32u + (tid & 31);
+                if (base + at < s_total) {
+                    const uint32_t d = (q ? sm.u.p.in_key[1][at] : sm.u.p.in_key[0][at]) >> 8;
+                    atomicAdd(&wc[warp * 128 + (d >> 1)], 1u << ((d & 1u) * 16));
+                }
             }
         }
         __syncthreads();
-        J.cnt_hi[(size_t)tid * J.tiles + tile] = sm.hist[tid];
+        uint32_t total = 0;
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) total += (wc[w * 128 + (tid >> 1)] >> ((tid & 1) * 16)) & 0xFFFFu;
+        J.cnt_hi[(size_t)tid * J.tiles + tile] = total;
+        __syncthreads();   // the counters are cleared for the next tile
     }
 }
 
@@ -416,24 +421,26 @@ __device__ void scan_digit(uint32_t* cnt, uint32_t tiles, uint32_t d, uint32_t* 
 }
 
 // ScanLo / ScanHi of a job of at most kSmallScanTiles tiles, in one item:
-// thread d scans its digit's row serially.
+// thread d scans its digit's row serially, 16 loads in flight at a time (a
+// whole row in registers would spill the kernel's other phases).
 __device__ void scan_small(uint32_t* cnt, uint32_t tiles, uint32_t* tot) {
+    constexpr uint32_t V = 16;
     uint32_t* row = cnt + (size_t)threadIdx.x * tiles;
-    uint32_t v[kSmallScanTiles];
-#pragma unroll
-    for (uint32_t r = 0; r < kSmallScanTiles; ++r) v[r] = r < tiles ? __ldcg(&row[r]) : 0u;
     uint32_t run = 0;
+#pragma unroll 1
+    for (uint32_t c0 = 0; c0 < tiles; c0 += V) {
+        uint32_t v[V];
 #pragma unroll
-    for (uint32_t r = 0; r < kSmallScanTiles; ++r) {
-        if (r < tiles) row[r] = run;
-        run += v[r];
+        for (uint32_t r = 0; r < V; ++r) v[r] = c0 + r < tiles ? __ldcg(&row[c0 + r]) : 0u;
+#pragma unroll
+        for (uint32_t r = 0; r < V; ++r) {
+            if (c0 + r < tiles) row[c0 + r] = run;
+            run += v[r];
+        }
     }
     tot[threadIdx.x] = run;
 }
 
-// Low / High: one stable counting pass over 8 key bits for one tile. The
-// tile's input is copied to shared memory first (cp.async, all at once);
-// each warp ranks its 32 x IPT consecutive elements in rounds of 32, stably.
 // Low / High: one stable counting pass over 8 key bits for one tile. The
 // tile's input is copied to shared memory first (cp.async, all at once);
 // each warp ranks its 32 x IPT consecutive elements in rounds of 32, stably.
@@ -691,6 +698,8 @@ static cudaError_t launch_variant(const JobDesc* jobs, const uint2* items, uint3
 template <int IPT>
 static cudaError_t launch_ipt(int minb, const JobDesc* jobs, const uint2* items, uint32_t n_items, LaunchCtl* lctl,
                               uint32_t* err, uint32_t spin_limit, int grid, cudaStream_t stream, TraceRec* trace) {
+    if constexpr (IPT == 4)
+        if (minb == 6) return launch_variant<IPT, 6>(jobs, items, n_items, lctl, err, spin_limit, grid, stream, trace);
     switch (minb) {
         case 2: return launch_variant<IPT, 2>(jobs, items, n_items, lctl, err, spin_limit, grid, stream, trace);
         case 4: return launch_variant<IPT, 4>(jobs, items, n_items, lctl, err, spin_limit, grid, stream, trace);
@@ -699,7 +708,8 @@ static cudaError_t launch_ipt(int minb, const JobDesc* jobs, const uint2* items,
 }
 
 // Host-side launcher: the variant for a tile of `tile` elements and `minb`
-// resident CTAs per SM (2, 3 or 4).
+// resident CTAs per SM (2, 3 or 4; also 6 for tiles of 1024, whose shared
+// memory allows six).
 cudaError_t launch_sort(const JobDesc* jobs, const uint2* items, uint32_t n_items, LaunchCtl* lctl,
                         uint32_t* err, uint32_t tile, int minb, uint32_t spin_limit, int grid, cudaStream_t stream,
                         TraceRec* trace) {
@@ -720,6 +730,8 @@ static int occupancy_variant() {
 
 template <int IPT>
 static int occupancy_ipt(int minb) {
+    if constexpr (IPT == 4)
+        if (minb == 6) return occupancy_variant<IPT, 6>();
     switch (minb) {
         case 2: return occupancy_variant<IPT, 2>();
         case 4: return occupancy_variant<IPT, 4>();

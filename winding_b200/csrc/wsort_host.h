@@ -50,7 +50,7 @@ struct ws_ctx {
     std::vector<uint32_t> last_ns;
     uint32_t last_tile = 0;
     bool items_valid = false;
-    int occupancy[3][3] = {};         // resident sort CTAs per SM, by tile and variant
+    int occupancy[3][5] = {};         // resident sort CTAs per SM, by tile and variant (2..6)
     uint64_t launches = 0;
     // kernel timing (ws_timing): event pairs recorded around each launch
     bool timing = false;
