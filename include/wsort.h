@@ -188,6 +188,42 @@ int ws_device_free(ws_ctx* ctx, void* ptr);
  * queued work (and `stream`'s, if given) has finished. */
 int ws_device_download(ws_ctx* ctx, const void* device_src, void* host_dst, size_t bytes, void* stream);
 
+/* ------------------------------------------------------------ particles */
+
+/*
+ * The particle sort of an alpha emitter: the live slots of its ring in the
+ * particle pool, far to near. Replaces makeKeys / scanCounts / place of
+ * src/render/particles.js:197-243 (one dispatch triple per emitter,
+ * _encodeSort :824-850) with the same persistent sort as ws_sort_batch.
+ * A slot is live unless age >= lifetime (:202); its key is
+ * 4095 - bucket (:203-205), bucket = u32(clamp((log2(depth) + 10) * 4095 / 30,
+ * 0, 4095)) of depth = max(dot(position - eye, forward), 1e-6), with log2
+ * the f32 nearest the real log2. Slots of equal key keep slot order (the
+ * reference's atomics leave them in any order).
+ */
+#define WS_PARTICLE_BUCKETS 4096u
+typedef struct ws_emitter {
+    const void* pool;    /* device, 16-byte aligned: 32-byte particles (render/particles.js:51-56):
+                            position xyz f32, age f32, velocity xyz f32, lifetime f32 */
+    uint32_t offset;     /* the ring's first slot in the pool (Emitter.offset) */
+    uint32_t capacity;   /* slots in the ring (Emitter.capacity) */
+    float eye[3];        /* camera position (View.eye, filled at :688-693) */
+    float forward[3];    /* -view[2], -view[6], -view[10] (View.forward) */
+    uint32_t* order;     /* device, >= capacity: the live slots (pool indices), far to near */
+    uint32_t* keys;      /* device or NULL: their keys */
+    uint32_t* count;     /* device: live slots (args.instanceCount) */
+} ws_emitter;
+
+/* Sorts n emitters in one launch on `stream` (NULL: the context's stream);
+ * returns once queued. WS_ERR_ARG: a null pointer, an unaligned pool, a ring
+ * past slot 2^32 - 1; WS_ERR_CAPACITY: a ring of more than WS_MAX_SPLATS. */
+int ws_sort_particles(ws_ctx* ctx, int n, const ws_emitter* emitters, void* stream);
+
+/* The WS_PARTICLE_BUCKETS depth thresholds the kernel compares with:
+ * out[b] is the least f32 depth whose bucket is b or more (out[0] = 0).
+ * Host only; needs no device. */
+int ws_particle_thresholds(float* out);
+
 /* ------------------------------------------------------------ serving */
 
 /*

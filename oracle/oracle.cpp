@@ -349,3 +349,24 @@ extern "C" uint32_t or_sort_view(const float* centers, const float* cov, uint32_
     for (auto& th : pool) th.join();
     return total;
 }
+
+extern "C" uint32_t or_particle_key(const float* particle, const float eye[3], const float forward[3]) {
+    const float age = particle[3], lifetime = particle[7];
+    if (age >= lifetime) return OR_CULLED;                                   // particles.js:202
+    const float dx = particle[0] - eye[0], dy = particle[1] - eye[1], dz = particle[2] - eye[2];
+    const float dot = (dx * forward[0] + dy * forward[1]) + dz * forward[2];
+    const float depth = std::fmax(dot, 1e-6f);                              // :203
+    const float l = (float)log2l((long double)depth);
+    const float v = ((l - -10.0f) * 4095.0f) / 30.0f;                        // :204
+    const uint32_t bucket = (uint32_t)clampf(v, 0.0f, 4095.0f);
+    return OR_PARTICLE_BUCKETS - 1u - bucket;                                // :205
+}
+
+extern "C" uint32_t or_particle_sort(const float* pool, uint32_t offset, uint32_t capacity, const float eye[3],
+                                     const float forward[3], uint32_t* order, uint32_t* sorted_keys) {
+    std::vector<uint32_t> keys(capacity);
+    for (uint32_t i = 0; i < capacity; ++i) keys[i] = or_particle_key(pool + 8 * (size_t)(offset + i), eye, forward);
+    const uint32_t live = or_counting_sort(keys.data(), capacity, order, sorted_keys);
+    for (uint32_t j = 0; j < live; ++j) order[j] += offset;
+    return live;
+}

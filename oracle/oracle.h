@@ -11,6 +11,7 @@
  *   - the per-cloud depth range (FP64):          src/render/splats.js:559-587
  *   - makeKeys and footprint (f32):              src/render/splats.js:102-124, :155-186
  *   - the stable order of survivors:             src/render/drawlist.js:186-229
+ *   - an alpha emitter's particle keys:          src/render/particles.js:197-209
  *
  * Pinned evaluation order. WGSL lets a driver fuse and reorder f32 work, so
  * the oracle fixes one order and the CUDA kernels follow it bit for bit:
@@ -106,6 +107,29 @@ uint32_t or_sort_view(const float* centers, const float* cov, uint32_t n,
                       const float model_view[16], const float projection[16],
                       const float viewport[2], float cull,
                       uint32_t* order, uint32_t* sorted_keys, int threads);
+
+/* Depth buckets of an alpha emitter's sort: render/particles.js:44-48. */
+#define OR_PARTICLE_BUCKETS 4096u
+
+/*
+ * Particle p's key (render/particles.js:197-205), or OR_CULLED for a dead
+ * slot (age >= lifetime, :202). particle: its 8 f32 (position xyz, age,
+ * velocity xyz, lifetime). depth = max(dot(position - eye, forward), 1e-6):
+ * the dot product summed x, y, z in order; max returns the non-NaN operand.
+ * bucket = u32(clamp(((log2(depth) - -10) * 4095) / 30, 0, 4095)), each f32
+ * operation separately rounded and log2 the f32 nearest the real log2
+ * (log2l rounded once to f32; WGSL leaves its accuracy open). Key
+ * 4095 - bucket.
+ */
+uint32_t or_particle_key(const float* particle, const float eye[3], const float forward[3]);
+
+/*
+ * One emitter's sort: slots [offset, offset + capacity) of the pool (8 f32 a
+ * particle), the live ones by (key, slot). order[] receives pool slot
+ * indices; returns the live count.
+ */
+uint32_t or_particle_sort(const float* pool, uint32_t offset, uint32_t capacity, const float eye[3],
+                          const float forward[3], uint32_t* order, uint32_t* sorted_keys);
 
 #ifdef __cplusplus
 }

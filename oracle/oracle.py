@@ -70,6 +70,10 @@ def _declare(L):
     L.or_counting_sort.argtypes = [_u32p, ctypes.c_uint32, _u32p, _u32p]
     L.or_drawlist_sort.restype = None
     L.or_drawlist_sort.argtypes = [_u32p, _u32p, ctypes.c_uint32, _u32p, _u32p]
+    L.or_particle_key.restype = ctypes.c_uint32
+    L.or_particle_key.argtypes = [_f32p, _f32p, _f32p]
+    L.or_particle_sort.restype = ctypes.c_uint32
+    L.or_particle_sort.argtypes = [_f32p, ctypes.c_uint32, ctypes.c_uint32, _f32p, _f32p, _u32p, _u32p]
     L.or_sort_view.restype = ctypes.c_uint32
     L.or_sort_view.argtypes = [_f32p, _f32p, ctypes.c_uint32, _f64p, _f64p, _f32p, _f32p, _f32p,
                                ctypes.c_float, _u32p, _u32p, ctypes.c_int]
@@ -189,4 +193,29 @@ def sort_view(parsed: Parsed, model_view, projection, viewport, cull, threads: i
                            _ptr(parsed.min, _f64p), _ptr(parsed.max, _f64p), _ptr(mv, _f32p),
                            _ptr(pr, _f32p), _ptr(vp, _f32p), float(np.float32(cull)),
                            _ptr(order, _u32p), _ptr(sk, _u32p), int(threads))
+    return order[:s].copy(), sk[:s].copy()
+
+
+PARTICLE_BUCKETS = 4096
+
+
+def particle_key(particle, eye, forward) -> int:
+    """One particle's key (8 f32), or CULLED for a dead slot."""
+    p = np.ascontiguousarray(particle, np.float32).reshape(8)
+    e = np.ascontiguousarray(eye, np.float32).reshape(3)
+    f = np.ascontiguousarray(forward, np.float32).reshape(3)
+    return int(lib().or_particle_key(_ptr(p, _f32p), _ptr(e, _f32p), _ptr(f, _f32p)))
+
+
+def particle_sort(pool: np.ndarray, offset: int, capacity: int, eye, forward):
+    """(order, sorted_keys) of one emitter: the live slots by (key, slot)."""
+    pool = np.ascontiguousarray(pool, np.float32).reshape(-1)
+    if pool.size < 8 * (offset + capacity):
+        raise ValueError("the pool is shorter than the ring")
+    order = np.zeros(max(capacity, 1), np.uint32)
+    sk = np.zeros(max(capacity, 1), np.uint32)
+    e = np.ascontiguousarray(eye, np.float32).reshape(3)
+    f = np.ascontiguousarray(forward, np.float32).reshape(3)
+    s = lib().or_particle_sort(_ptr(pool, _f32p), offset, capacity, _ptr(e, _f32p), _ptr(f, _f32p),
+                               _ptr(order, _u32p), _ptr(sk, _u32p))
     return order[:s].copy(), sk[:s].copy()

@@ -64,6 +64,19 @@ class WsJob(ctypes.Structure):
     ]
 
 
+class WsEmitter(ctypes.Structure):
+    _fields_ = [
+        ("pool", ctypes.c_void_p),
+        ("offset", ctypes.c_uint32),
+        ("capacity", ctypes.c_uint32),
+        ("eye", ctypes.c_float * 3),
+        ("forward", ctypes.c_float * 3),
+        ("order", ctypes.c_void_p),
+        ("keys", ctypes.c_void_p),
+        ("count", ctypes.c_void_p),
+    ]
+
+
 class WsParams(ctypes.Structure):
     _fields_ = [
         ("tile", ctypes.c_uint32),
@@ -145,6 +158,8 @@ SIGNATURES = {
     "ws_get_params": (ctypes.c_int, [vp, ctypes.POINTER(WsParams)]),
     "ws_set_params": (ctypes.c_int, [vp, ctypes.POINTER(WsParams)]),
     "ws_sort_noalloc": (ctypes.c_int, [vp, ctypes.POINTER(WsView), vp, vp, vp, vp]),
+    "ws_sort_particles": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(WsEmitter), vp]),
+    "ws_particle_thresholds": (ctypes.c_int, [ctypes.POINTER(ctypes.c_float)]),
     "ws_server_create": (ctypes.c_int, [vp, ctypes.POINTER(WsServerOpts), ctypes.POINTER(vp)]),
     "ws_server_submit": (ctypes.c_int, [vp, vp, ctypes.POINTER(WsView), ctypes.POINTER(ctypes.c_uint64)]),
     "ws_server_poll": (ctypes.c_int, [vp, ctypes.c_uint64, ctypes.POINTER(ctypes.c_int)]),

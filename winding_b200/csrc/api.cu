@@ -9,6 +9,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -160,6 +161,52 @@ void view_shortcuts(const ws_view& v, const ws_cloud* c, uint32_t* fast, uint32_
 }
 
 // Fills job descriptors and lays the scratch out from `scratch`.
+// A job's tiles, scan items and scratch regions (job_shape's layout), from
+// `at` on; advances `at` past them.
+static void assign_scratch(JobDesc& d, uint32_t n, const ws_params& p, char*& at) {
+    size_t bytes;
+    job_shape(n, p, &d.tiles, &bytes);
+    d.scan_items = d.tiles <= kSmallScanTiles ? 1u : kScanItems;
+    const size_t np = pad_splats(n);
+    d.k16 = reinterpret_cast<uint16_t*>(at);
+    at += align_up(np * 2, 256);
+    d.mask = reinterpret_cast<uint32_t*>(at);
+    at += align_up(np / 8, 256);
+    d.key_b = reinterpret_cast<uint16_t*>(at);
+    at += align_up(np * 2, 256);
+    d.idx_b = reinterpret_cast<uint32_t*>(at);
+    at += align_up(np * 4, 256);
+    d.cnt_lo = reinterpret_cast<uint32_t*>(at);
+    at += align_up((size_t)d.tiles * 1024, 256);
+    d.cnt_hi = reinterpret_cast<uint32_t*>(at);
+    at += align_up((size_t)d.tiles * 1024, 256);
+}
+
+// Emitter jobs (ws_sort_particles): the ring, the view and the outputs.
+static void layout_emitters(JobDesc* out, const ws_emitter* em, int njobs, const ws_params& p, char* scratch,
+                            const float* thr) {
+    char* at = scratch + align_up(sizeof(LaunchCtl) + (size_t)njobs * sizeof(JobCtl), 256);
+    JobCtl* ctls = reinterpret_cast<JobCtl*>(scratch + sizeof(LaunchCtl));
+    for (int j = 0; j < njobs; ++j) {
+        JobDesc& d = out[j];
+        std::memset(&d, 0, sizeof(d));
+        d.kind = kJobParticles;
+        d.n = em[j].capacity;
+        d.idx_base = em[j].offset;
+        d.pool = static_cast<const float4*>(em[j].pool);
+        d.thr = thr;
+        for (int k = 0; k < 3; ++k) {
+            d.eye[k] = em[j].eye[k];
+            d.fwd[k] = em[j].forward[k];
+        }
+        d.order = em[j].order;
+        d.keys = em[j].keys;
+        d.count = em[j].count;
+        assign_scratch(d, em[j].capacity, p, at);
+        d.ctl = reinterpret_cast<uint32_t*>(&ctls[j]);
+    }
+}
+
 void layout_jobs(JobDesc* out, const ws_job* jobs, int njobs, const ws_params& p, char* scratch) {
     char* at = scratch + align_up(sizeof(LaunchCtl) + (size_t)njobs * sizeof(JobCtl), 256);
     JobCtl* ctls = reinterpret_cast<JobCtl*>(scratch + sizeof(LaunchCtl));
@@ -184,22 +231,7 @@ void layout_jobs(JobDesc* out, const ws_job* jobs, int njobs, const ws_params& p
         d.keys = jobs[j].keys;
         d.count = jobs[j].count;
         view_shortcuts(jobs[j].view, c, &d.fast_transform, &d.keep_byte, &d.keep_q);
-        size_t bytes;
-        job_shape(c->n, p, &d.tiles, &bytes);
-        d.scan_items = d.tiles <= kSmallScanTiles ? 1u : kScanItems;
-        const size_t np = pad_splats(c->n);
-        d.k16 = reinterpret_cast<uint16_t*>(at);
-        at += align_up(np * 2, 256);
-        d.mask = reinterpret_cast<uint32_t*>(at);
-        at += align_up(np / 8, 256);
-        d.key_b = reinterpret_cast<uint16_t*>(at);
-        at += align_up(np * 2, 256);
-        d.idx_b = reinterpret_cast<uint32_t*>(at);
-        at += align_up(np * 4, 256);
-        d.cnt_lo = reinterpret_cast<uint32_t*>(at);
-        at += align_up((size_t)d.tiles * 1024, 256);
-        d.cnt_hi = reinterpret_cast<uint32_t*>(at);
-        at += align_up((size_t)d.tiles * 1024, 256);
+        assign_scratch(d, c->n, p, at);
         d.ctl = reinterpret_cast<uint32_t*>(&ctls[j]);
     }
 }
@@ -273,11 +305,14 @@ const ws_params& params_for(const ws_ctx* ctx, uint64_t splats) {
     return ctx->params;
 }
 
-int run_batch(ws_ctx* ctx, const ws_job* jobs, int njobs, cudaStream_t stream) {
+// One persistent launch over `njobs` jobs of ns[j] elements each; `fill`
+// writes the job table (kind-specific fields and scratch) into pinned
+// staging, given the scratch base, with ctx->params already the launch's.
+template <class Fill>
+static int launch_jobs(ws_ctx* ctx, const std::vector<uint32_t>& ns, int njobs, Fill fill, cudaStream_t stream) {
     cudaError_t e;
-    std::vector<uint32_t> ns(njobs);
     uint64_t splats = 0;
-    for (int j = 0; j < njobs; ++j) splats += ns[j] = jobs[j].cloud->n;
+    for (int j = 0; j < njobs; ++j) splats += ns[j];
     const ws_params saved = ctx->params;
     ctx->params = params_for(ctx, splats);   // restored below
     struct Restore {
@@ -298,7 +333,7 @@ int run_batch(ws_ctx* ctx, const ws_job* jobs, int njobs, cudaStream_t stream) {
     if ((e = ctx->jobs_d.ensure((size_t)njobs * sizeof(JobDesc))) != cudaSuccess)
         return cuda_error(ctx, e, "ws_sort job table");
     JobDesc* hj = static_cast<JobDesc*>(ctx->jobs_h.p);
-    layout_jobs(hj, jobs, njobs, ctx->params, static_cast<char*>(ctx->scratch.p));
+    fill(hj, static_cast<char*>(ctx->scratch.p));
 
     // Items depend only on the job sizes and the tiles: reuse the last upload
     // when they are unchanged.
@@ -359,6 +394,14 @@ int run_batch(ws_ctx* ctx, const ws_job* jobs, int njobs, cudaStream_t stream) {
     ++ctx->launches;
     ++ctx->timing_launches;
     return WS_OK;
+}
+
+int run_batch(ws_ctx* ctx, const ws_job* jobs, int njobs, cudaStream_t stream) {
+    std::vector<uint32_t> ns(njobs);
+    for (int j = 0; j < njobs; ++j) ns[j] = jobs[j].cloud->n;
+    return launch_jobs(
+        ctx, ns, njobs, [&](JobDesc* hj, char* scratch) { layout_jobs(hj, jobs, njobs, ctx->params, scratch); },
+        stream);
 }
 
 // Reads and clears the sticky device error words. Call after a sync.
@@ -440,6 +483,7 @@ extern "C" int ws_destroy(ws_ctx* ctx) {
     ctx->jobs_d.release();
     ctx->items_d.release();
     ctx->out_d.release();
+    ctx->thr_d.release();
     ctx->jobs_h.release();
     ctx->items_h.release();
     ctx->count_h.release();
@@ -747,6 +791,95 @@ extern "C" int ws_sort_batch(ws_ctx* ctx, int njobs, const ws_job* jobs, void* s
     }
     cudaSetDevice(ctx->device);
     return run_batch(ctx, jobs, njobs, stream_p ? static_cast<cudaStream_t>(stream_p) : ctx->stream);
+}
+
+// -------------------------------------------------------------- particles
+
+// The pinned bucket of a particle depth d >= 1e-6 (render/particles.js:204):
+// u32(clamp((log2(d) - -10) * 4095 / 30, 0, 4095)), each f32 operation
+// separately rounded and log2 the f32 nearest the real log2 (log2l, with a
+// 64-bit significand, rounded once to f32). WGSL leaves log2's accuracy to
+// the implementation; this is the choice that every conforming one
+// approximates.
+static uint32_t particle_bucket(float d) {
+    const float l = (float)log2l((long double)d);
+    const float t = l - -10.0f;
+    const float u = t * 4095.0f;
+    const float v = u / 30.0f;
+    const float c = std::fmin(std::fmax(v, 0.0f), 4095.0f);
+    return (uint32_t)c;
+}
+
+// thr[b]: the least f32 depth whose bucket is b or more (thr[0] = 0). The
+// bucket never decreases as the depth grows, so a depth d is in bucket b
+// exactly when thr[b] <= d < thr[b + 1]; the kernel finds b by comparisons.
+static const std::vector<float>& particle_thresholds() {
+    static std::vector<float> thr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        thr.assign(kParticleBuckets, 0.0f);
+        uint32_t lo_bits, hi_bits;
+        const float lo = 1e-6f, hi = INFINITY;
+        std::memcpy(&lo_bits, &lo, 4);
+        std::memcpy(&hi_bits, &hi, 4);
+        for (uint32_t b = 1; b < kParticleBuckets; ++b) {
+            uint32_t a = lo_bits, z = hi_bits;   // bucket(a) < b <= bucket(z)
+            while (z - a > 1) {
+                const uint32_t m = a + (z - a) / 2;
+                float f;
+                std::memcpy(&f, &m, 4);
+                if (particle_bucket(f) >= b)
+                    z = m;
+                else
+                    a = m;
+            }
+            std::memcpy(&thr[b], &z, 4);
+        }
+    });
+    return thr;
+}
+
+extern "C" int ws_particle_thresholds(float* out) {
+    if (!out) return WS_ERR_ARG;
+    const std::vector<float>& thr = particle_thresholds();
+    std::memcpy(out, thr.data(), thr.size() * sizeof(float));
+    return WS_OK;
+}
+
+extern "C" int ws_sort_particles(ws_ctx* ctx, int n, const ws_emitter* emitters, void* stream_p) {
+    if (!ctx) return WS_ERR_ARG;
+    if (n < 0 || (n && !emitters)) return set_error(ctx, WS_ERR_ARG, "ws_sort_particles: bad emitter list");
+    if (n == 0) return WS_OK;
+    if (n > (1 << 20)) return set_error(ctx, WS_ERR_ARG, "ws_sort_particles: too many emitters");
+    for (int j = 0; j < n; ++j) {
+        const ws_emitter& e = emitters[j];
+        if (!e.pool || !e.order || !e.count)
+            return set_error(ctx, WS_ERR_ARG, "ws_sort_particles: emitter %d needs a pool, an order and a count", j);
+        if (reinterpret_cast<uintptr_t>(e.pool) % 16)
+            return set_error(ctx, WS_ERR_ARG, "ws_sort_particles: emitter %d's pool is not 16-byte aligned", j);
+        if (e.capacity > WS_MAX_SPLATS)
+            return set_error(ctx, WS_ERR_CAPACITY, "ws_sort_particles: emitter %d has %u slots, more than %u", j,
+                             e.capacity, WS_MAX_SPLATS);
+        if ((uint64_t)e.offset + e.capacity > 0xFFFFFFFFull)
+            return set_error(ctx, WS_ERR_ARG, "ws_sort_particles: emitter %d's ring runs past slot 2^32 - 1", j);
+    }
+    cudaSetDevice(ctx->device);
+    cudaError_t e;
+    if (!ctx->thr_d.p) {
+        const std::vector<float>& thr = particle_thresholds();
+        if ((e = ctx->thr_d.ensure(thr.size() * sizeof(float))) != cudaSuccess)
+            return cuda_error(ctx, e, "ws_sort_particles thresholds");
+        if ((e = cudaMemcpy(ctx->thr_d.p, thr.data(), thr.size() * sizeof(float), cudaMemcpyHostToDevice)) !=
+            cudaSuccess)
+            return cuda_error(ctx, e, "ws_sort_particles thresholds");
+    }
+    std::vector<uint32_t> ns(n);
+    for (int j = 0; j < n; ++j) ns[j] = emitters[j].capacity;
+    const float* thr = static_cast<const float*>(ctx->thr_d.p);
+    return launch_jobs(
+        ctx, ns, n,
+        [&](JobDesc* hj, char* scratch) { layout_emitters(hj, emitters, n, ctx->params, scratch, thr); },
+        stream_p ? static_cast<cudaStream_t>(stream_p) : ctx->stream);
 }
 
 // ------------------------------------------------------------------ plans

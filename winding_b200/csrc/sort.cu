@@ -197,7 +197,6 @@ __device__ __forceinline__ uint32_t match_digit8(uint32_t d, bool on) {
 // 2D entry is at most G (1 + 8.2u), so the area is at most
 // 2 pi (1.00001 G + 0.3)(1 + 5u); a splat with alpha times that below cull
 // is culled, again without its footprint.
-constexpr uint32_t kPending = 0xFFFFFFFEu;
 
 template <int IPT>
 __device__ void keys_tile(const JobDesc& J, int job, uint32_t tile, SortSmem<IPT>& sm) {
@@ -316,6 +315,58 @@ __device__ void keys_tile(const JobDesc& J, int job, uint32_t tile, SortSmem<IPT
     }
     __syncthreads();
     if (tid == 0) sm.mark[2] = global_ns();
+    for (uint32_t w = tid; w < T / 32; w += kThreads)
+        if (base + w * 32 < n) J.mask[(base >> 5) + w] = sm.u.k.maskw[w];
+    J.cnt_lo[(size_t)tid * J.tiles + tile] = sm.hist[tid];
+}
+
+// Keys of one tile of an alpha emitter's ring (render/particles.js:197-209):
+// a slot is live unless age >= lifetime; its depth is
+// max(dot(position - eye, forward), 1e-6) (the dot product summed x, y, z in
+// order, each product and sum separately rounded; max returns the non-NaN
+// operand); its bucket is the one of 4096 log2-depth buckets the pinned
+// bucket function of the host puts it in, found here by comparing the depth
+// with that function's thresholds (thr[b] = the least depth of bucket b or
+// above), starting from an estimate by log2f and correcting it; the key is
+// 4095 - bucket, far first.
+template <int IPT>
+__device__ void particle_keys_tile(const JobDesc& J, uint32_t tile, SortSmem<IPT>& sm) {
+    constexpr uint32_t T = SortSmem<IPT>::kTile;
+    const int tid = threadIdx.x;
+    const uint32_t lane = lane_id();
+    sm.hist[tid] = 0;
+    __syncthreads();
+    const uint32_t base = tile * T;
+    const uint32_t n = J.n;
+    const float ex = J.eye[0], ey = J.eye[1], ez = J.eye[2];
+    const float fx = J.fwd[0], fy = J.fwd[1], fz = J.fwd[2];
+#pragma unroll 2
+    for (uint32_t k = 0; k < T; k += kThreads) {
+        const uint32_t at = k + tid;
+        const uint32_t i = base + at;
+        uint32_t key = 0;
+        bool live = false;
+        if (i < n) {
+            const float4* rec = J.pool + 2 * ((size_t)J.idx_base + i);
+            const float4 a = __ldcs(rec);
+            const float life = __ldcs(&rec[1].w);
+            live = !(a.w >= life);
+            if (live) {
+                const float dot = fadd(fadd(fmul(fsub(a.x, ex), fx), fmul(fsub(a.y, ey), fy)), fmul(fsub(a.z, ez), fz));
+                const float d = fmaxf(dot, 1e-6f);
+                int b = (int)fclamp(fmul(fadd(log2f(d), 10.0f), 136.5f), 0.0f, 4095.0f);
+                // The estimate is within a bucket or two; the thresholds decide.
+                while (b < (int)kParticleBuckets - 1 && d >= __ldg(&J.thr[b + 1])) ++b;
+                while (b > 0 && d < __ldg(&J.thr[b])) --b;
+                key = kParticleBuckets - 1u - (uint32_t)b;
+            }
+            J.k16[i] = (uint16_t)key;
+        }
+        const uint32_t kb = __ballot_sync(0xffffffffu, live);
+        if (lane == 0) sm.u.k.maskw[at >> 5] = kb;
+        if (live) atomicAdd(&sm.hist[key & 255u], 1u);
+    }
+    __syncthreads();
     for (uint32_t w = tid; w < T / 32; w += kThreads)
         if (base + w * 32 < n) J.mask[(base >> 5) + w] = sm.u.k.maskw[w];
     J.cnt_lo[(size_t)tid * J.tiles + tile] = sm.hist[tid];
@@ -530,7 +581,7 @@ __device__ void digit_tile(const JobDesc& J, int job, uint32_t tile, SortSmem<IP
         const uint32_t slot = sm.u.p.lstart[d] + sm.u.p.wcnt[warp][d] + (packed[r] >> 16);
         const uint32_t at = wlocal + r * 32u + lane;
         sm.u.p.stage_key[slot] = (uint16_t)key;
-        sm.u.p.stage_idx[slot] = PASS == 0 ? base + at : sm.u.p.in_idx[at];
+        sm.u.p.stage_idx[slot] = PASS == 0 ? J.idx_base + base + at : sm.u.p.in_idx[at];
     }
     __syncthreads();
     if (tid == 0) sm.mark[2] = global_ns();
@@ -627,7 +678,12 @@ __global__ void __launch_bounds__(kThreads, MINB) sort_kernel(const JobDesc* __r
                 sm.mark[0] = sm.mark[1] = sm.mark[2] = 0;
             }
             switch (phase) {
-                case kPhaseKeys: keys_tile(J, job, tile, sm); break;
+                case kPhaseKeys:
+                    if (J.kind == kJobParticles)
+                        particle_keys_tile(J, tile, sm);
+                    else
+                        keys_tile(J, job, tile, sm);
+                    break;
                 case kPhaseScanLo:
                     if (J.scan_items == 1)
                         scan_small(J.cnt_lo, J.tiles, ctl->tot[0]);

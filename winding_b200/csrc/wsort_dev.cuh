@@ -55,7 +55,8 @@ struct alignas(16) JobDesc {
     uint32_t keep_byte;         // alpha bytes at or above this pass the footprint cull when ...
     float keep_q;               // ... keep_q 2^sexp <= 100 d^2 (+inf: never)
     uint32_t scan_items;        // items of each scan phase: 1 (small job) or 256 (one per digit)
-    uint32_t pad1[2];
+    uint32_t kind;              // kJobSplats or kJobParticles
+    uint32_t idx_base;          // added to every element index the order holds (a ring's first slot)
     // view: the values the reference writes into its Cloud uniform
     float mv[16];
     float proj[16];
@@ -74,7 +75,17 @@ struct alignas(16) JobDesc {
     uint32_t* cnt_lo;           // 256 x tiles (digit major): low-digit counts, then prefixes over tiles
     uint32_t* cnt_hi;           // 256 x tiles: the same for the high digit
     uint32_t* ctl;              // JobCtl
+    // particles (kind == kJobParticles): one emitter's ring of the pool
+    const float4* pool;         // the pool: two float4 a particle (position, age; velocity, lifetime)
+    const float* thr;           // kParticleBuckets depth thresholds of the log-depth buckets
+    float eye[4];               // camera position (View.eye)
+    float fwd[4];               // view direction (View.forward)
 };
+
+constexpr uint32_t kJobSplats = 0, kJobParticles = 1;
+// Depth buckets of an alpha emitter's sort (render/particles.js:44-48):
+// 12 bits of log2 depth over [2^-10, 2^20].
+constexpr uint32_t kParticleBuckets = 4096u;
 
 // Per-job counters, zeroed before a launch.
 struct JobCtl {

@@ -63,6 +63,7 @@ struct ws_ctx {
     std::vector<uint2> trace_items;
     int trace_grid = 0;
     std::vector<struct ws_cloud*> freed;   // freed clouds, kept as refusable handles
+    wsort::DevBuf thr_d;              // particle depth thresholds, uploaded on first use
 };
 
 struct ws_cloud {

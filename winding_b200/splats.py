@@ -132,6 +132,22 @@ class Context:
             arr[j].count = c
         self.check(self.lib.ws_sort_batch(self.handle, len(jobs), arr, stream))
 
+    def sort_particles(self, emitters: list[tuple], stream: int | None = None) -> None:
+        """emitters: (pool_ptr, offset, capacity, eye, forward, order_ptr,
+        keys_ptr or None, count_ptr), pointers into device memory; one launch
+        for all (ws_sort_particles)."""
+        arr = (_lib.WsEmitter * max(len(emitters), 1))()
+        for j, (pool, offset, capacity, eye, forward, o, k, c) in enumerate(emitters):
+            arr[j].pool = pool
+            arr[j].offset = offset
+            arr[j].capacity = capacity
+            arr[j].eye[:] = [float(np.float32(x)) for x in eye]
+            arr[j].forward[:] = [float(np.float32(x)) for x in forward]
+            arr[j].order = o
+            arr[j].keys = k
+            arr[j].count = c
+        self.check(self.lib.ws_sort_particles(self.handle, len(emitters), arr, stream))
+
     def plan(self, jobs: list[tuple]) -> "Plan":
         return Plan(self, jobs)
 
