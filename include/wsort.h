@@ -188,6 +188,37 @@ int ws_device_free(ws_ctx* ctx, void* ptr);
  * queued work (and `stream`'s, if given) has finished. */
 int ws_device_download(ws_ctx* ctx, const void* device_src, void* host_dst, size_t bytes, void* stream);
 
+/* ------------------------------------------------------------ harmonics */
+
+/*
+ * A cloud's higher spherical harmonics (a capture whose colour changes with
+ * the view; src/render/splats.js:406-408): degree 1, 2 or 3, packed as the
+ * reference packs them (src/scene/splats.js:43-47, :306-333): per splat,
+ * ceil(3 c / 2) 32-bit words (c = 3, 8 or 15 coefficients past the
+ * constant one) of half floats, coefficient by coefficient, red, green and
+ * blue in each. Copied into device memory the cloud owns (host words, or
+ * device words when on_device). Degree 0 drops them. WS_ERR_ARG when fewer
+ * than n ceil(3 c / 2) words are given.
+ */
+int ws_cloud_set_harmonics(ws_cloud* cloud, int degree, const uint32_t* words, size_t nwords, int on_device);
+
+/* The shade pass of one job: the eye in the cloud's own space (Cloud.eye,
+ * src/render/splats.js:585-586) and the per-splat colour words it writes. */
+typedef struct ws_shade {
+    float eye[3];
+    uint32_t reserved;
+    uint32_t* shaded;    /* device, >= cloud count words; entries of survivors only are written */
+} ws_shade;
+
+/*
+ * ws_sort_batch plus the shade pass after the sort (src/render/splats.js:
+ * 691-695, shade :371-381), fused into the same launch: for every survivor
+ * i of a job whose cloud has harmonics, shaded[i] = pack4x8unorm(clamp(
+ * colour + harmonics(normalize(centre - eye)), 0, 1), alpha). Jobs whose
+ * cloud has none are sorted only.
+ */
+int ws_sort_batch_shaded(ws_ctx* ctx, int njobs, const ws_job* jobs, const ws_shade* shades, void* stream);
+
 /* ------------------------------------------------------------ particles */
 
 /*

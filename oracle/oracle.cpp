@@ -370,3 +370,70 @@ extern "C" uint32_t or_particle_sort(const float* pool, uint32_t offset, uint32_
     for (uint32_t j = 0; j < live; ++j) order[j] += offset;
     return live;
 }
+
+namespace {
+
+// A half float's value (IEEE binary16), exactly.
+float half_value(uint32_t h) {
+    const uint32_t sign = (h >> 15) & 1u, e = (h >> 10) & 31u, m = h & 1023u;
+    float v;
+    if (e == 0)
+        v = std::ldexp((float)m, -24);
+    else if (e == 31)
+        v = m ? NAN : INFINITY;
+    else
+        v = std::ldexp((float)(m | 1024u), (int)e - 25);
+    return sign ? -v : v;
+}
+
+struct V3 {
+    float r, g, b;
+};
+V3 coef(const uint32_t* sh, uint32_t words, uint32_t i, uint32_t k) {   // splats.js:338-344
+    const size_t h = (size_t)i * words * 2 + k * 3;
+    const uint32_t w0 = sh[h >> 1], w1 = sh[(h >> 1) + 1];
+    const float a0 = half_value(w0 & 0xFFFFu), a1 = half_value(w0 >> 16);
+    const float b0 = half_value(w1 & 0xFFFFu), b1 = half_value(w1 >> 16);
+    return (h & 1) ? V3{a1, b0, b1} : V3{a0, a1, b0};
+}
+V3 mul(float s, V3 v) { return V3{s * v.r, s * v.g, s * v.b}; }
+V3 add(V3 a, V3 b) { return V3{a.r + b.r, a.g + b.g, a.b + b.b}; }
+V3 sub(V3 a, V3 b) { return V3{a.r - b.r, a.g - b.g, a.b - b.b}; }
+uint32_t unorm8(float e) { return (uint32_t)std::floor(0.5f + 255.0f * clampf(e, 0.0f, 1.0f)); }
+
+}  // namespace
+
+extern "C" uint32_t or_shade(const float* centers, const uint32_t* sh, int degree, uint32_t i, const float eye[3]) {
+    static const uint32_t coefficients[4] = {0, 3, 8, 15};
+    const uint32_t words = (coefficients[degree] * 3 + 1) / 2;
+    const float* c = centers + 4 * (size_t)i;
+    const float vx = c[0] - eye[0], vy = c[1] - eye[1], vz = c[2] - eye[2];
+    const float len = std::sqrt((vx * vx + vy * vy) + vz * vz);
+    const float x = vx / len, y = vy / len, z = vz / len;
+    V3 col = mul(0.4886025119029199f, sub(add(mul(-y, coef(sh, words, i, 0)), mul(z, coef(sh, words, i, 1))),
+                                          mul(x, coef(sh, words, i, 2))));
+    if (degree >= 2) {
+        const float xx = x * x, yy = y * y, zz = z * z;
+        V3 e = sub(mul(1.0925484305920792f * x * y, coef(sh, words, i, 3)),
+                   mul(1.0925484305920792f * y * z, coef(sh, words, i, 4)));
+        e = add(e, mul(0.31539156525252005f * (2.0f * zz - xx - yy), coef(sh, words, i, 5)));
+        e = sub(e, mul(1.0925484305920792f * x * z, coef(sh, words, i, 6)));
+        e = add(e, mul(0.5462742152960396f * (xx - yy), coef(sh, words, i, 7)));
+        col = add(col, e);
+        if (degree >= 3) {
+            V3 h = add(mul(-0.5900435899266435f * y * (3.0f * xx - yy), coef(sh, words, i, 8)),
+                       mul(2.890611442640554f * x * y * z, coef(sh, words, i, 9)));
+            h = sub(h, mul(0.4570457994644658f * y * (4.0f * zz - xx - yy), coef(sh, words, i, 10)));
+            h = add(h, mul(0.3731763325901154f * z * (2.0f * zz - 3.0f * xx - 3.0f * yy), coef(sh, words, i, 11)));
+            h = sub(h, mul(0.4570457994644658f * x * (4.0f * zz - xx - yy), coef(sh, words, i, 12)));
+            h = add(h, mul(1.445305721320277f * z * (xx - yy), coef(sh, words, i, 13)));
+            h = sub(h, mul(0.5900435899266435f * x * (xx - 3.0f * yy), coef(sh, words, i, 14)));
+            col = add(col, h);
+        }
+    }
+    uint32_t word;
+    std::memcpy(&word, &c[3], 4);
+    const float r = (float)(word & 255u) / 255.0f, g = (float)((word >> 8) & 255u) / 255.0f;
+    const float b = (float)((word >> 16) & 255u) / 255.0f, a = (float)(word >> 24) / 255.0f;
+    return unorm8(r + col.r) | (unorm8(g + col.g) << 8) | (unorm8(b + col.b) << 16) | (unorm8(a) << 24);
+}

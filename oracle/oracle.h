@@ -12,6 +12,7 @@
  *   - makeKeys and footprint (f32):              src/render/splats.js:102-124, :155-186
  *   - the stable order of survivors:             src/render/drawlist.js:186-229
  *   - an alpha emitter's particle keys:          src/render/particles.js:197-209
+ *   - the shade pass (harmonics):                src/render/splats.js:333-381
  *
  * Pinned evaluation order. WGSL lets a driver fuse and reorder f32 work, so
  * the oracle fixes one order and the CUDA kernels follow it bit for bit:
@@ -107,6 +108,18 @@ uint32_t or_sort_view(const float* centers, const float* cov, uint32_t n,
                       const float model_view[16], const float projection[16],
                       const float viewport[2], float cull,
                       uint32_t* order, uint32_t* sorted_keys, int threads);
+
+/*
+ * The shade pass for splat i (render/splats.js:371-381): its colour word as
+ * seen from `eye` (the cloud's space), from its centre (4 f32, the 4th the
+ * colour word's bits) and its harmonics of `degree` (1-3) in `sh`, packed as
+ * scene/splats.js:306-333 packs them. Pinned order: normalize(v) is
+ * v / sqrt((x x + y y) + z z); harmonics() (:347-368) is evaluated left to
+ * right as written, each scalar chain (K x y) before it scales a
+ * coefficient; unpack4x8unorm is byte / 255, pack4x8unorm
+ * floor(0.5 + 255 clamp(e, 0, 1)), clamp giving the bound for NaN.
+ */
+uint32_t or_shade(const float* centers, const uint32_t* sh, int degree, uint32_t i, const float eye[3]);
 
 /* Depth buckets of an alpha emitter's sort: render/particles.js:44-48. */
 #define OR_PARTICLE_BUCKETS 4096u

@@ -70,6 +70,8 @@ def _declare(L):
     L.or_counting_sort.argtypes = [_u32p, ctypes.c_uint32, _u32p, _u32p]
     L.or_drawlist_sort.restype = None
     L.or_drawlist_sort.argtypes = [_u32p, _u32p, ctypes.c_uint32, _u32p, _u32p]
+    L.or_shade.restype = ctypes.c_uint32
+    L.or_shade.argtypes = [_f32p, _u32p, ctypes.c_int, ctypes.c_uint32, _f32p]
     L.or_particle_key.restype = ctypes.c_uint32
     L.or_particle_key.argtypes = [_f32p, _f32p, _f32p]
     L.or_particle_sort.restype = ctypes.c_uint32
@@ -219,3 +221,13 @@ def particle_sort(pool: np.ndarray, offset: int, capacity: int, eye, forward):
     s = lib().or_particle_sort(_ptr(pool, _f32p), offset, capacity, _ptr(e, _f32p), _ptr(f, _f32p),
                                _ptr(order, _u32p), _ptr(sk, _u32p))
     return order[:s].copy(), sk[:s].copy()
+
+
+def shade(centers: np.ndarray, sh: np.ndarray, degree: int, indices, eye) -> np.ndarray:
+    """The shade pass's colour word for each splat index given."""
+    c = np.ascontiguousarray(centers, np.float32).reshape(-1)
+    w = np.ascontiguousarray(sh, np.uint32).reshape(-1)
+    e = np.ascontiguousarray(eye, np.float32).reshape(3)
+    L = lib()
+    cp, wp, ep = _ptr(c, _f32p), _ptr(w, _u32p), _ptr(e, _f32p)
+    return np.array([L.or_shade(cp, wp, degree, int(i), ep) for i in indices], np.uint32)

@@ -77,6 +77,14 @@ class WsEmitter(ctypes.Structure):
     ]
 
 
+class WsShade(ctypes.Structure):
+    _fields_ = [
+        ("eye", ctypes.c_float * 3),
+        ("reserved", ctypes.c_uint32),
+        ("shaded", ctypes.c_void_p),
+    ]
+
+
 class WsParams(ctypes.Structure):
     _fields_ = [
         ("tile", ctypes.c_uint32),
@@ -159,6 +167,8 @@ SIGNATURES = {
     "ws_set_params": (ctypes.c_int, [vp, ctypes.POINTER(WsParams)]),
     "ws_sort_noalloc": (ctypes.c_int, [vp, ctypes.POINTER(WsView), vp, vp, vp, vp]),
     "ws_sort_particles": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(WsEmitter), vp]),
+    "ws_cloud_set_harmonics": (ctypes.c_int, [vp, ctypes.c_int, vp, ctypes.c_size_t, ctypes.c_int]),
+    "ws_sort_batch_shaded": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(WsJob), ctypes.POINTER(WsShade), vp]),
     "ws_particle_thresholds": (ctypes.c_int, [ctypes.POINTER(ctypes.c_float)]),
     "ws_server_create": (ctypes.c_int, [vp, ctypes.POINTER(WsServerOpts), ctypes.POINTER(vp)]),
     "ws_server_submit": (ctypes.c_int, [vp, vp, ctypes.POINTER(WsView), ctypes.POINTER(ctypes.c_uint64)]),

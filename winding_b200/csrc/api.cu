@@ -702,6 +702,7 @@ extern "C" int ws_cloud_free(ws_cloud* c) {
         if (c->centers) cudaFree(c->centers);
         if (c->cov) cudaFree(c->cov);
         if (c->sexp) cudaFree(c->sexp);
+        if (c->sh) cudaFree(c->sh);
         delete c;
         return WS_OK;
     }
@@ -712,9 +713,12 @@ extern "C" int ws_cloud_free(ws_cloud* c) {
     if (c->centers) cudaFree(c->centers);
     if (c->cov) cudaFree(c->cov);
     if (c->sexp) cudaFree(c->sexp);
+    if (c->sh) cudaFree(c->sh);
     c->centers = nullptr;
     c->cov = nullptr;
     c->sexp = nullptr;
+    c->sh = nullptr;
+    c->sh_degree = 0;
     // The handle stays valid (and refused by every call) until its context
     // is destroyed, so a sort of a freed cloud is an error, not a crash.
     c->alive = false;
@@ -791,6 +795,84 @@ extern "C" int ws_sort_batch(ws_ctx* ctx, int njobs, const ws_job* jobs, void* s
     }
     cudaSetDevice(ctx->device);
     return run_batch(ctx, jobs, njobs, stream_p ? static_cast<cudaStream_t>(stream_p) : ctx->stream);
+}
+
+// -------------------------------------------------------------- harmonics
+
+// 32-bit words one splat's harmonics of `degree` take (scene/splats.js:43-47).
+static uint32_t sh_words_of(int degree) {
+    static const uint32_t coefficients[4] = {0, 3, 8, 15};
+    return (coefficients[degree] * 3 + 1) / 2;
+}
+
+extern "C" int ws_cloud_set_harmonics(ws_cloud* c, int degree, const uint32_t* words, size_t nwords, int on_device) {
+    if (!c || c->magic != kCloudMagic) return WS_ERR_ARG;
+    ws_ctx* ctx = c->ctx;
+    if (!c->alive) return set_error(ctx, WS_ERR_UNLOADED, "these splats were unloaded");
+    if (degree < 0 || degree > 3)
+        return set_error(ctx, WS_ERR_ARG, "ws_cloud_set_harmonics: degree must be 0 to 3, got %d", degree);
+    cudaSetDevice(ctx->device);
+    cudaError_t e;
+    if (c->sh) {
+        if ((e = cudaDeviceSynchronize()) != cudaSuccess) return cuda_error(ctx, e, "ws_cloud_set_harmonics");
+        cudaFree(c->sh);
+        c->sh = nullptr;
+        c->sh_degree = c->sh_words = 0;
+    }
+    if (degree == 0) return WS_OK;
+    const uint32_t per = sh_words_of(degree);
+    const size_t need = (size_t)c->n * per;
+    if (!words || nwords < need)
+        return set_error(ctx, WS_ERR_ARG, "ws_cloud_set_harmonics: %zu words for %u splats of degree %d; %zu needed",
+                         nwords, c->n, degree, need);
+    void* p = nullptr;
+    if ((e = cudaMalloc(&p, (need + 1) * 4)) != cudaSuccess) return cuda_error(ctx, e, "ws_cloud_set_harmonics");
+    // One word over, so the two-word read of the last coefficient stays inside.
+    if ((e = cudaMemset(static_cast<uint32_t*>(p) + need, 0, 4)) != cudaSuccess ||
+        (e = cudaMemcpy(p, words, need * 4, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice)) !=
+            cudaSuccess) {
+        cudaFree(p);
+        return cuda_error(ctx, e, "ws_cloud_set_harmonics");
+    }
+    c->sh = static_cast<uint32_t*>(p);
+    c->sh_degree = (uint32_t)degree;
+    c->sh_words = per;
+    return WS_OK;
+}
+
+extern "C" int ws_sort_batch_shaded(ws_ctx* ctx, int njobs, const ws_job* jobs, const ws_shade* shades,
+                                    void* stream_p) {
+    if (!ctx) return WS_ERR_ARG;
+    if (njobs < 0 || (njobs && (!jobs || !shades)))
+        return set_error(ctx, WS_ERR_ARG, "ws_sort_batch_shaded: bad job list");
+    if (njobs == 0) return WS_OK;
+    if (njobs > (1 << 20)) return set_error(ctx, WS_ERR_ARG, "ws_sort_batch_shaded: too many jobs");
+    for (int j = 0; j < njobs; ++j) {
+        int rc;
+        if ((rc = check_cloud(ctx, jobs[j].cloud)) || (rc = check_view(ctx, &jobs[j].view))) return rc;
+        if (!jobs[j].order || !jobs[j].count)
+            return set_error(ctx, WS_ERR_ARG, "ws_sort_batch_shaded: job %d has no output", j);
+        if (jobs[j].cloud->sh && !shades[j].shaded)
+            return set_error(ctx, WS_ERR_ARG, "ws_sort_batch_shaded: job %d has harmonics but no shaded output", j);
+    }
+    cudaSetDevice(ctx->device);
+    std::vector<uint32_t> ns(njobs);
+    for (int j = 0; j < njobs; ++j) ns[j] = jobs[j].cloud->n;
+    return launch_jobs(
+        ctx, ns, njobs,
+        [&](JobDesc* hj, char* scratch) {
+            layout_jobs(hj, jobs, njobs, ctx->params, scratch);
+            for (int j = 0; j < njobs; ++j) {
+                const ws_cloud* c = jobs[j].cloud;
+                if (!c->sh) continue;
+                hj[j].sh = c->sh;
+                hj[j].sh_degree = c->sh_degree;
+                hj[j].sh_words = c->sh_words;
+                hj[j].shaded = shades[j].shaded;
+                for (int k = 0; k < 3; ++k) hj[j].eye[k] = shades[j].eye[k];
+            }
+        },
+        stream_p ? static_cast<cudaStream_t>(stream_p) : ctx->stream);
 }
 
 // -------------------------------------------------------------- particles

@@ -318,6 +318,17 @@ __device__ void keys_tile(const JobDesc& J, int job, uint32_t tile, SortSmem<IPT
     for (uint32_t w = tid; w < T / 32; w += kThreads)
         if (base + w * 32 < n) J.mask[(base >> 5) + w] = sm.u.k.maskw[w];
     J.cnt_lo[(size_t)tid * J.tiles + tile] = sm.hist[tid];
+    // The shade pass, fused: every survivor of the tile (its survivor bit is
+    // final here, its centre still in shared memory) gets its colour as seen
+    // from the eye.
+    if (J.sh) {
+        for (uint32_t at = tid; at < T; at += kThreads) {
+            if (!((sm.u.k.maskw[at >> 5] >> (at & 31u)) & 1u)) continue;
+            const float4 p = sm.u.k.centers[at];
+            J.shaded[base + at] = shade_splat(J.sh, J.sh_words, J.sh_degree, base + at, p.x, p.y, p.z,
+                                              __float_as_uint(p.w), J.eye);
+        }
+    }
 }
 
 // Keys of one tile of an alpha emitter's ring (render/particles.js:197-209):

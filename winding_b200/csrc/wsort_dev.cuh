@@ -12,6 +12,7 @@
 #pragma once
 
 #include <cstdint>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 namespace wsort {
@@ -78,8 +79,14 @@ struct alignas(16) JobDesc {
     // particles (kind == kJobParticles): one emitter's ring of the pool
     const float4* pool;         // the pool: two float4 a particle (position, age; velocity, lifetime)
     const float* thr;           // kParticleBuckets depth thresholds of the log-depth buckets
-    float eye[4];               // camera position (View.eye)
+    float eye[4];               // particles: camera position (View.eye); splats: the eye in the
+                                // cloud's space (Cloud.eye), for the harmonics
     float fwd[4];               // view direction (View.forward)
+    // splats with harmonics: the shade pass, fused into the keys phase
+    const uint32_t* sh;         // packed half-float coefficients, sh_words a splat; null: no shading
+    uint32_t* shaded;           // per splat: its colour word as seen from the eye (survivors only)
+    uint32_t sh_degree;         // 1, 2 or 3
+    uint32_t sh_words;          // 32-bit words a splat: ceil(3 x coefficients / 2)
 };
 
 constexpr uint32_t kJobSplats = 0, kJobParticles = 1;
@@ -122,6 +129,88 @@ __device__ __forceinline__ float fdiv(float a, float b) { return __fdiv_rn(a, b)
 // WGSL clamp(e, low, high) = min(max(e, low), high); fmaxf/fminf return the
 // non-NaN operand.
 __device__ __forceinline__ float fclamp(float e, float lo, float hi) { return fminf(fmaxf(e, lo), hi); }
+
+// ------------------------------------------------------------- harmonics
+//
+// The shade pass (src/render/splats.js:315-382): a survivor's colour seen
+// along d = normalize(centre - eye), the constant term (its colour bytes)
+// plus the higher harmonics, clamped to [0, 1] and packed as four bytes. The
+// pinned order: normalize is v / sqrt((x x + y y) + z z); every product and
+// sum of harmonics() is separately rounded, left to right as written, each
+// scalar factor chain (K x y, say) formed before it scales a coefficient;
+// unpack4x8unorm is byte / 255 and pack4x8unorm floor(0.5 + 255 e), both
+// correctly rounded f32; clamp returns the bound for NaN.
+
+// Splat i's coefficient k as (r, g, b): three half floats from the two
+// words they lie across (coefficient(), :338-344).
+__device__ __forceinline__ float3 sh_coef(const uint32_t* sh, uint32_t words, uint32_t i, uint32_t k) {
+    const size_t h = (size_t)i * words * 2 + k * 3;
+    const uint32_t w0 = __ldg(&sh[h >> 1]), w1 = __ldg(&sh[(h >> 1) + 1]);
+    const float a0 = __half2float(__ushort_as_half((unsigned short)(w0 & 0xFFFFu)));
+    const float a1 = __half2float(__ushort_as_half((unsigned short)(w0 >> 16)));
+    const float b0 = __half2float(__ushort_as_half((unsigned short)(w1 & 0xFFFFu)));
+    const float b1 = __half2float(__ushort_as_half((unsigned short)(w1 >> 16)));
+    return (h & 1) ? make_float3(a1, b0, b1) : make_float3(a0, a1, b0);
+}
+
+// s * v and the elementwise sum / difference, each separately rounded.
+__device__ __forceinline__ float3 sv(float s, float3 v) { return make_float3(__fmul_rn(s, v.x), __fmul_rn(s, v.y), __fmul_rn(s, v.z)); }
+__device__ __forceinline__ float3 vadd(float3 a, float3 b) { return make_float3(__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y), __fadd_rn(a.z, b.z)); }
+__device__ __forceinline__ float3 vsub(float3 a, float3 b) { return make_float3(__fsub_rn(a.x, b.x), __fsub_rn(a.y, b.y), __fsub_rn(a.z, b.z)); }
+
+__device__ __forceinline__ uint32_t pack_unorm8(float e) {
+    const float c = fminf(fmaxf(e, 0.0f), 1.0f);
+    return (uint32_t)floorf(__fadd_rn(0.5f, __fmul_rn(255.0f, c)));
+}
+
+// The shaded colour word of splat i with centre (cx, cy, cz) and colour
+// word `colour`, seen from `eye` (shade(), :371-381).
+__device__ __forceinline__ uint32_t shade_splat(const uint32_t* sh, uint32_t words, uint32_t degree, uint32_t i,
+                                                float cx, float cy, float cz, uint32_t colour, const float* eye) {
+    const float vx = __fsub_rn(cx, eye[0]), vy = __fsub_rn(cy, eye[1]), vz = __fsub_rn(cz, eye[2]);
+    const float len = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(vx, vx), __fmul_rn(vy, vy)), __fmul_rn(vz, vz)));
+    const float x = __fdiv_rn(vx, len), y = __fdiv_rn(vy, len), z = __fdiv_rn(vz, len);
+    // degree 1
+    float3 c = sv(0.4886025119029199f, vsub(vadd(sv(-y, sh_coef(sh, words, i, 0)), sv(z, sh_coef(sh, words, i, 1))),
+                                            sv(x, sh_coef(sh, words, i, 2))));
+    if (degree >= 2) {
+        const float xx = __fmul_rn(x, x), yy = __fmul_rn(y, y), zz = __fmul_rn(z, z);
+        const float t1 = __fmul_rn(__fmul_rn(1.0925484305920792f, x), y);
+        const float t2 = __fmul_rn(__fmul_rn(1.0925484305920792f, y), z);
+        const float t3 = __fmul_rn(0.31539156525252005f, __fsub_rn(__fsub_rn(__fmul_rn(2.0f, zz), xx), yy));
+        const float t4 = __fmul_rn(__fmul_rn(1.0925484305920792f, x), z);
+        const float t5 = __fmul_rn(0.5462742152960396f, __fsub_rn(xx, yy));
+        float3 e = vsub(sv(t1, sh_coef(sh, words, i, 3)), sv(t2, sh_coef(sh, words, i, 4)));
+        e = vadd(e, sv(t3, sh_coef(sh, words, i, 5)));
+        e = vsub(e, sv(t4, sh_coef(sh, words, i, 6)));
+        e = vadd(e, sv(t5, sh_coef(sh, words, i, 7)));
+        c = vadd(c, e);
+        if (degree >= 3) {
+            const float q = __fsub_rn(__fsub_rn(__fmul_rn(4.0f, zz), xx), yy);
+            const float a = __fmul_rn(__fmul_rn(-0.5900435899266435f, y), __fsub_rn(__fmul_rn(3.0f, xx), yy));
+            const float b = __fmul_rn(__fmul_rn(__fmul_rn(2.890611442640554f, x), y), z);
+            const float cc = __fmul_rn(__fmul_rn(0.4570457994644658f, y), q);
+            const float d = __fmul_rn(__fmul_rn(0.3731763325901154f, z),
+                                      __fsub_rn(__fsub_rn(__fmul_rn(2.0f, zz), __fmul_rn(3.0f, xx)), __fmul_rn(3.0f, yy)));
+            const float ee = __fmul_rn(__fmul_rn(0.4570457994644658f, x), q);
+            const float f = __fmul_rn(__fmul_rn(1.445305721320277f, z), __fsub_rn(xx, yy));
+            const float g = __fmul_rn(__fmul_rn(0.5900435899266435f, x), __fsub_rn(xx, __fmul_rn(3.0f, yy)));
+            float3 h = vadd(sv(a, sh_coef(sh, words, i, 8)), sv(b, sh_coef(sh, words, i, 9)));
+            h = vsub(h, sv(cc, sh_coef(sh, words, i, 10)));
+            h = vadd(h, sv(d, sh_coef(sh, words, i, 11)));
+            h = vsub(h, sv(ee, sh_coef(sh, words, i, 12)));
+            h = vadd(h, sv(f, sh_coef(sh, words, i, 13)));
+            h = vsub(h, sv(g, sh_coef(sh, words, i, 14)));
+            c = vadd(c, h);
+        }
+    }
+    const float r = __fdiv_rn((float)(colour & 255u), 255.0f);
+    const float gr = __fdiv_rn((float)((colour >> 8) & 255u), 255.0f);
+    const float bl = __fdiv_rn((float)((colour >> 16) & 255u), 255.0f);
+    const float al = __fdiv_rn((float)(colour >> 24), 255.0f);
+    return pack_unorm8(__fadd_rn(r, c.x)) | (pack_unorm8(__fadd_rn(gr, c.y)) << 8) |
+           (pack_unorm8(__fadd_rn(bl, c.z)) << 16) | (pack_unorm8(al) << 24);
+}
 
 // Per-view constants of one job, computed once per work item. Each is the
 // same IEEE operation on the same operands the per-splat WGSL evaluates, so

@@ -132,6 +132,23 @@ class Context:
             arr[j].count = c
         self.check(self.lib.ws_sort_batch(self.handle, len(jobs), arr, stream))
 
+    def sort_batch_shaded(self, jobs: list[tuple], shades: list[tuple], stream: int | None = None) -> None:
+        """jobs as sort_batch; shades: per job (eye, shaded_ptr), the eye in
+        the cloud's space and a device array of its cloud's count words that
+        receives the survivors' shaded colours (ws_sort_batch_shaded)."""
+        arr = (WsJob * len(jobs))()
+        sh = (_lib.WsShade * len(jobs))()
+        for j, ((sp, view, o, k, c), (eye, shaded)) in enumerate(zip(jobs, shades)):
+            sp._check_alive()
+            arr[j].cloud = sp.handle
+            arr[j].view = view
+            arr[j].order = o
+            arr[j].keys = k
+            arr[j].count = c
+            sh[j].eye[:] = [float(np.float32(x)) for x in eye]
+            sh[j].shaded = shaded
+        self.check(self.lib.ws_sort_batch_shaded(self.handle, len(jobs), arr, sh, stream))
+
     def sort_particles(self, emitters: list[tuple], stream: int | None = None) -> None:
         """emitters: (pool_ptr, offset, capacity, eye, forward, order_ptr,
         keys_ptr or None, count_ptr), pointers into device memory; one launch
@@ -239,6 +256,7 @@ class Splats:
         self.min = [lo[0], lo[1], lo[2]]
         self.max = [hi[0], hi[1], hi[2]]
         self.unloaded = False
+        self.degree = 0
 
     def _check_alive(self):
         if self.unloaded:
@@ -261,12 +279,38 @@ class Splats:
                                                    ctypes.byref(dmin), ctypes.byref(dscale)))
         return bool(vis.value), dmin.value, dscale.value
 
+    def set_harmonics(self, degree: int, words) -> None:
+        """Attaches higher harmonics of `degree` (1-3): uint32 words packed as
+        the reference packs them (sh_words(degree) a splat, see SH_WORDS), or
+        degree 0 to drop them."""
+        self._check_alive()
+        if degree == 0:
+            self.ctx.check(self.ctx.lib.ws_cloud_set_harmonics(self.handle, 0, None, 0, 0))
+            self.degree = 0
+            return
+        w = np.ascontiguousarray(words, np.uint32).reshape(-1)
+        self.ctx.check(self.ctx.lib.ws_cloud_set_harmonics(self.handle, int(degree), w.ctypes.data, w.size, 0))
+        self.degree = int(degree)
+
     def destroy(self) -> None:
         """Frees the device arrays. The handle stays refusable: a later sort of
         it raises the reference's 'unloaded' error."""
         if not self.unloaded:
             self.ctx.check(self.ctx.lib.ws_cloud_free(self.handle))
             self.unloaded = True
+
+
+# 32-bit words a splat's harmonics take, by degree (scene/splats.js:43-47).
+SH_WORDS = (0, 5, 12, 23)
+
+
+def eye_in_cloud(model_view) -> np.ndarray:
+    """The eye in a cloud's own space, as the reference fills Cloud.eye
+    (render/splats.js:585-586): where the inverse of the f32 model-view
+    takes the view's origin, in doubles, stored as f32."""
+    m = np.asarray(model_view, np.float32).astype(np.float64).reshape(4, 4).T   # column-major
+    inv = np.linalg.inv(m)
+    return inv[:3, 3].astype(np.float32)
 
 
 def parse_splats(data, ctx: Context | None = None) -> Splats:
