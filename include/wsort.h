@@ -103,6 +103,20 @@ int ws_sync(ws_ctx* ctx);
  * that is not finite, or more than WS_MAX_SPLATS splats.
  */
 int ws_cloud_from_splat(ws_ctx* ctx, const uint8_t* bytes, size_t nbytes, ws_cloud** out);
+/*
+ * readSplats (src/scene/splats.js:78-90): a capture in any format the
+ * reference reads without help -- a binary .ply as training writes it
+ * (parsePly :398-468), a gzipped .spz of version 1 to 3 (parseSpz
+ * :227-303, gunzipped here on the host) or .splat records -- decoded on the
+ * device into a resident cloud, with the higher harmonics a .ply or .spz
+ * carries (ws_cloud_harmonics). Refused with the reference's messages:
+ * a .sog (it needs an image decoder for its WebP images), a zstd .spz of
+ * version 4, and every malformed header the reference refuses.
+ */
+int ws_cloud_load(ws_ctx* ctx, const uint8_t* bytes, size_t nbytes, ws_cloud** out);
+/* The cloud's harmonics degree (0-3) and, when words is not NULL, its
+ * count x ceil(3 c / 2) packed words (the layout of ws_cloud_set_harmonics). */
+int ws_cloud_harmonics(const ws_cloud* cloud, int* degree, uint32_t* words);
 /* As ws_cloud_from_splat for records already in device memory. */
 int ws_cloud_from_device(ws_ctx* ctx, const void* device_bytes, size_t nbytes, ws_cloud** out);
 /* Splats.count / .min / .max (src/render/splats.js:401-403). min/max may be NULL. */

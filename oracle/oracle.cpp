@@ -26,6 +26,10 @@ namespace {
 // +0 when every argument is zero (the caller's `|| 1` then applies).
 double v8_hypot4(double a, double b, double c, double d) {
     const double v[4] = {std::fabs(a), std::fabs(b), std::fabs(c), std::fabs(d)};
+    for (double x : v)   // ECMAScript: an infinite argument wins over NaN
+        if (std::isinf(x)) return INFINITY;
+    for (double x : v)
+        if (std::isnan(x)) return NAN;
     double max = 0.0;
     for (double x : v)
         if (x > max) max = x;
@@ -436,4 +440,273 @@ extern "C" uint32_t or_shade(const float* centers, const uint32_t* sh, int degre
     const float r = (float)(word & 255u) / 255.0f, g = (float)((word >> 8) & 255u) / 255.0f;
     const float b = (float)((word >> 16) & 255u) / 255.0f, a = (float)(word >> 24) / 255.0f;
     return unorm8(r + col.r) | (unorm8(g + col.g) << 8) | (unorm8(b + col.b) << 16) | (unorm8(a) << 24);
+}
+
+// ------------------------------------------------------------ capture readers
+
+namespace {
+
+// Double-double helpers (Knuth's two-sum, Dekker's split and product).
+struct DD {
+    double h, l;
+};
+DD dd_from_sum(double a, double b) {
+    const double s = a + b, v = s - a;
+    return {s, (a - (s - v)) + (b - v)};
+}
+DD dd_norm(double a, double b) {
+    const double s = a + b;
+    return {s, b - (s - a)};
+}
+DD dd_prod(double a, double b) {
+    const double p = a * b;
+    const double ca = 134217729.0 * a, ah = ca - (ca - a), al = a - ah;
+    const double cb = 134217729.0 * b, bh = cb - (cb - b), bl = b - bh;
+    return {p, (((ah * bh - p) + ah * bl) + al * bh) + al * bl};
+}
+DD operator+(DD a, DD b) {
+    DD s = dd_from_sum(a.h, b.h);
+    const DD t = dd_from_sum(a.l, b.l);
+    s = dd_norm(s.h, s.l + t.h);
+    return dd_norm(s.h, s.l + t.l);
+}
+DD operator*(DD a, DD b) {
+    const DD p = dd_prod(a.h, b.h);
+    return dd_norm(p.h, p.l + (a.h * b.l + a.l * b.h));
+}
+DD dd_over(DD a, double b) {
+    const double q = a.h / b;
+    const DD p = dd_prod(q, b);
+    const DD r = dd_from_sum(a.h, -p.h);
+    return dd_norm(q, ((r.h + (r.l - p.l)) + a.l) / b);
+}
+
+}  // namespace
+
+// exp(x) = 2^k exp(r / 1024)^1024, r = x - k ln 2: a 13-term series for the
+// small argument, ten squarings, all in double-double; then rounded once.
+extern "C" double or_exp(double x) {
+    if (std::isnan(x)) return x;
+    if (x > 1000.0) return INFINITY;
+    if (x < -1000.0) return 0.0;
+    const double k = std::nearbyint(x / 0.6931471805599453);
+    const DD ln2{6.93147180559945286227e-01, 2.31904681384629955842e-17};
+    const DD kl = DD{k, 0.0} * ln2;
+    const DD r = dd_over(DD{x, 0.0} + DD{-kl.h, -kl.l}, 1024.0);
+    DD term{1.0, 0.0}, sum{1.0, 0.0};
+    for (int n = 1; n <= 13; ++n) {
+        term = dd_over(term * r, (double)n);
+        sum = sum + term;
+    }
+    for (int s = 0; s < 10; ++s) sum = sum * sum;
+    double y = sum.h;
+    return std::ldexp(y, (int)k);
+}
+
+namespace {
+double js_round(double x) {
+    if (std::isnan(x) || std::isinf(x)) return x;
+    const double f = std::floor(x);
+    return (x - f >= 0.5) ? f + 1.0 : f;
+}
+uint32_t half_bits(double value) {   // render/hdr.js:152-163
+    if (!(value > 0)) return 0;
+    if (value >= 65504.0) return 0x7bff;
+    if (value < std::ldexp(1.0, -24)) return 0;
+    if (value < std::ldexp(1.0, -14)) return (uint32_t)js_round(value / std::ldexp(1.0, -24));
+    int exponent = std::ilogb(value);
+    uint32_t mantissa = (uint32_t)js_round((value / std::ldexp(1.0, exponent) - 1.0) * 1024.0);
+    if (mantissa == 1024) {
+        mantissa = 0;
+        ++exponent;
+    }
+    return ((uint32_t)(exponent + 15) << 10) | mantissa;
+}
+}  // namespace
+
+extern "C" uint32_t or_byte(double v) {
+    const double r = std::fmax(0.0, std::fmin(255.0, js_round(v * 255.0)));
+    return std::isnan(js_round(v * 255.0)) ? 0u : (uint32_t)r;
+}
+
+extern "C" uint32_t or_signed_half(double v) { return v < 0 ? (0x8000u | half_bits(-v)) : half_bits(v); }
+
+namespace {
+
+const uint32_t kCoefs[5] = {0, 3, 8, 15, 24};
+const double kC0 = 0.28209479177387814;
+
+// put() (scene/splats.js:335-369) with FP64 inputs; false for a bad position.
+bool put_d(uint32_t i, double x, double y, double z, uint32_t colour, double sx, double sy, double sz, double qw,
+           double qx, double qy, double qz, float* centers, float* cov, double bmin[3], double bmax[3]) {
+    if (!(std::isfinite(x) && std::isfinite(y) && std::isfinite(z))) return false;
+    float* c = centers + 4 * (size_t)i;
+    c[0] = (float)x;
+    c[1] = (float)y;
+    c[2] = (float)z;
+    std::memcpy(&c[3], &colour, 4);
+    const double p[3] = {x + 0.0, y + 0.0, z + 0.0};
+    for (int k = 0; k < 3; ++k) {
+        if (p[k] < bmin[k]) bmin[k] = p[k];
+        if (p[k] > bmax[k]) bmax[k] = p[k];
+    }
+    double length = v8_hypot4(qw, qx, qy, qz);
+    if (!(length != 0.0)) length = 1.0;
+    const double w = qw / length, u = qx / length, v = qy / length, t = qz / length;
+    const double r00 = 1 - 2 * (v * v + t * t), r01 = 2 * (u * v - w * t), r02 = 2 * (u * t + w * v);
+    const double r10 = 2 * (u * v + w * t), r11 = 1 - 2 * (u * u + t * t), r12 = 2 * (v * t - w * u);
+    const double r20 = 2 * (u * t - w * v), r21 = 2 * (v * t + w * u), r22 = 1 - 2 * (u * u + v * v);
+    const double m00 = r00 * sx, m01 = r01 * sy, m02 = r02 * sz;
+    const double m10 = r10 * sx, m11 = r11 * sy, m12 = r12 * sz;
+    const double m20 = r20 * sx, m21 = r21 * sy, m22 = r22 * sz;
+    float* o = cov + 6 * (size_t)i;
+    o[0] = (float)(m00 * m00 + m01 * m01 + m02 * m02);
+    o[1] = (float)(m00 * m10 + m01 * m11 + m02 * m12);
+    o[2] = (float)(m00 * m20 + m01 * m21 + m02 * m22);
+    o[3] = (float)(m10 * m10 + m11 * m11 + m12 * m12);
+    o[4] = (float)(m10 * m20 + m11 * m21 + m12 * m22);
+    o[5] = (float)(m20 * m20 + m21 * m21 + m22 * m22);
+    return true;
+}
+
+void put_sh(uint32_t* sh, uint32_t words, uint32_t i, uint32_t k, double r, double g, double b) {   // putSH
+    uint16_t* halves = reinterpret_cast<uint16_t*>(sh);
+    const size_t h = (size_t)i * words * 2 + k * 3;
+    halves[h] = (uint16_t)or_signed_half(r);
+    halves[h + 1] = (uint16_t)or_signed_half(g);
+    halves[h + 2] = (uint16_t)or_signed_half(b);
+}
+
+double ply_value(const uint8_t* p, uint32_t type) {
+    switch (type) {
+        case 1: return (double)(int8_t)p[0];
+        case 2: return (double)p[0];
+        case 3: { int16_t v; std::memcpy(&v, p, 2); return v; }
+        case 4: { uint16_t v; std::memcpy(&v, p, 2); return v; }
+        case 5: { int32_t v; std::memcpy(&v, p, 4); return v; }
+        case 6: { uint32_t v; std::memcpy(&v, p, 4); return v; }
+        case 7: { float v; std::memcpy(&v, p, 4); return v; }
+        case 8: { double v; std::memcpy(&v, p, 8); return v; }
+        default: return 0.0;
+    }
+}
+
+}  // namespace
+
+extern "C" int or_decode_ply(const uint8_t* payload, uint32_t n, uint32_t stride, const uint32_t* types,
+                             const uint32_t* offsets, uint32_t rest, float* centers, float* cov, uint32_t* sh,
+                             double bmin[3], double bmax[3], uint32_t* bad) {
+    for (int k = 0; k < 3; ++k) {
+        bmin[k] = INFINITY;
+        bmax[k] = -INFINITY;
+    }
+    const uint32_t per = rest / 3;
+    const uint32_t words = (per * 3 + 1) / 2;
+    for (uint32_t i = 0; i < n; ++i) {
+        const uint8_t* rec = payload + (size_t)i * stride;
+        auto f = [&](int k) { return ply_value(rec + offsets[k], types[k]); };
+        const uint32_t colour = or_byte(0.5 + kC0 * f(3)) | (or_byte(0.5 + kC0 * f(4)) << 8) |
+                                (or_byte(0.5 + kC0 * f(5)) << 16) |
+                                (or_byte(1.0 / (1.0 + or_exp(-f(6)))) << 24);
+        if (!put_d(i, f(0), f(1), f(2), colour, or_exp(f(7)), or_exp(f(8)), or_exp(f(9)), f(10), f(11), f(12),
+                   f(13), centers, cov, bmin, bmax)) {
+            *bad = i;
+            return -4;
+        }
+        for (uint32_t k = 0; k < per; ++k) put_sh(sh, words, i, k, f(14 + k), f(14 + k + per), f(14 + k + 2 * per));
+    }
+    return 0;
+}
+
+extern "C" int or_decode_spz(const uint8_t* data, size_t len, uint32_t* count, uint32_t* degree, float* centers,
+                             float* cov, uint32_t* sh, double bmin[3], double bmax[3], uint32_t* bad, char* err,
+                             size_t errlen) {
+    auto u32 = [&](size_t o) { uint32_t v; std::memcpy(&v, data + o, 4); return v; };
+    if (len < 16 || u32(0) != 0x5053474eu) {
+        std::snprintf(err, errlen, "splats: gzipped, but not a .spz");
+        return -7;
+    }
+    const uint32_t version = u32(4);
+    if (version < 1 || version > 3) {
+        std::snprintf(err, errlen, "splats: a .spz of version %u; versions 1 to 3 are read", version);
+        return -8;
+    }
+    const uint32_t n = u32(8), file_degree = data[12], fraction = data[13];
+    if (file_degree > 4) {
+        std::snprintf(err, errlen, "splats: a .spz with harmonics of degree %u", file_degree);
+        return -9;
+    }
+    const uint32_t deg = std::min<uint32_t>(file_degree, 3), file_coefs = kCoefs[file_degree];
+    const size_t pb = version == 1 ? 6 : 9, rb = version >= 3 ? 4 : 3;
+    const size_t positions = 16, alphas = positions + n * pb, colours = alphas + n, scales = colours + n * 3;
+    const size_t rotations = scales + n * 3, shs = rotations + n * rb, end = shs + (size_t)n * file_coefs * 3;
+    if (n == 0) {
+        std::snprintf(err, errlen, "splats: a .spz with no splats");
+        return -10;
+    }
+    if (end > len) {
+        std::snprintf(err, errlen, "splats: the .spz is cut short: %u splats need %zu bytes, it has %zu", n, end, len);
+        return -11;
+    }
+    *count = n;
+    *degree = deg;
+    if (!centers) return 0;
+    for (int k = 0; k < 3; ++k) {
+        bmin[k] = INFINITY;
+        bmax[k] = -INFINITY;
+    }
+    const double fixed = 1.0 / (double)(int32_t)(1u << (fraction & 31));
+    const uint32_t words = (kCoefs[deg] * 3 + 1) / 2;
+    static const double flip[15] = {-1, -1, 1, -1, 1, 1, -1, 1, -1, 1, -1, -1, 1, -1, 1};
+    for (uint32_t i = 0; i < n; ++i) {
+        double pos[3];
+        for (int a = 0; a < 3; ++a) {
+            if (version == 1) {
+                uint16_t h;
+                std::memcpy(&h, data + positions + i * 6 + a * 2, 2);
+                const double sign = (h & 0x8000) ? -1.0 : 1.0;
+                const int e = (h >> 10) & 31, m = h & 1023;
+                pos[a] = e == 31 ? (m ? NAN : sign * INFINITY)
+                                 : sign * (e == 0 ? m * std::ldexp(1.0, -24) : (1 + m / 1024.0) * std::ldexp(1.0, e - 15));
+            } else {
+                const uint8_t* p = data + positions + i * 9 + a * 3;
+                int32_t v = (int32_t)(p[0] | (p[1] << 8) | (p[2] << 16));
+                if (v & 0x800000) v -= 0x1000000;
+                pos[a] = v * fixed;
+            }
+        }
+        double q[4];
+        if (rb == 3) {
+            for (int a = 0; a < 3; ++a) q[a] = data[rotations + i * 3 + a] / 127.5 - 1;
+            q[3] = std::sqrt(std::fmax(0.0, 1 - (q[0] * q[0] + q[1] * q[1] + q[2] * q[2])));
+        } else {
+            uint32_t packed = u32(rotations + i * 4);
+            const uint32_t largest = packed >> 30;
+            double sum = 0;
+            for (int a = 3; a >= 0; --a) {
+                if ((uint32_t)a == largest) continue;
+                const uint32_t magnitude = packed & 511, negative = (packed >> 9) & 1;
+                packed >>= 10;
+                q[a] = 0.7071067811865476 * magnitude / 511 * (negative ? -1 : 1);
+                sum += q[a] * q[a];
+            }
+            q[largest] = std::sqrt(std::fmax(0.0, 1 - sum));
+        }
+        uint32_t colour = (uint32_t)data[alphas + i] << 24;
+        for (int k = 0; k < 3; ++k)
+            colour |= or_byte(0.5 + kC0 * ((data[colours + i * 3 + k] / 255.0 - 0.5) / 0.15)) << (8 * k);
+        double s3[3];
+        for (int k = 0; k < 3; ++k) s3[k] = or_exp(data[scales + i * 3 + k] / 16.0 - 10);
+        if (!put_d(i, pos[0], -pos[1], -pos[2], colour, s3[0], s3[1], s3[2], q[3], q[0], -q[1], -q[2], centers, cov,
+                   bmin, bmax)) {
+            *bad = i;
+            return -4;
+        }
+        for (uint32_t k = 0; k < kCoefs[deg]; ++k) {
+            const uint8_t* h = data + shs + (size_t)i * file_coefs * 3 + k * 3;
+            put_sh(sh, words, i, k, (h[0] - 128) / 128.0 * flip[k], (h[1] - 128) / 128.0 * flip[k],
+                   (h[2] - 128) / 128.0 * flip[k]);
+        }
+    }
+    return 0;
 }

@@ -13,6 +13,7 @@
  *   - the stable order of survivors:             src/render/drawlist.js:186-229
  *   - an alpha emitter's particle keys:          src/render/particles.js:197-209
  *   - the shade pass (harmonics):                src/render/splats.js:333-381
+ *   - the .ply and .spz readers' per-splat math: src/scene/splats.js:227-303, :398-468
  *
  * Pinned evaluation order. WGSL lets a driver fuse and reorder f32 work, so
  * the oracle fixes one order and the CUDA kernels follow it bit for bit:
@@ -120,6 +121,41 @@ uint32_t or_sort_view(const float* centers, const float* cov, uint32_t n,
  * floor(0.5 + 255 clamp(e, 0, 1)), clamp giving the bound for NaN.
  */
 uint32_t or_shade(const float* centers, const uint32_t* sh, int degree, uint32_t i, const float eye[3]);
+
+/*
+ * The capture readers' JavaScript arithmetic, pinned: Math.exp as the double
+ * nearest the real value (the engines are within an ulp of it; a result
+ * below 2^-1022 is rounded to a double, then to the subnormal grid), Math.round
+ * with halves up, byte() = max(0, min(255, round(v 255))) with NaN as 0,
+ * halfBits (render/hdr.js:152-163) and signedHalf (scene/splats.js:50-52).
+ */
+double or_exp(double x);
+uint32_t or_byte(double v);
+uint32_t or_signed_half(double v);
+
+/*
+ * parsePly's per-vertex loop (scene/splats.js:456-468) over `n` vertices of
+ * `stride` bytes: fields[k] = (type, offset) of x y z f_dc_0..2 opacity
+ * scale_0..2 rot_0..3 then f_rest_0.. (`rest` of them; types 1 int8, 2 uint8,
+ * 3 int16, 4 uint16, 5 int32, 6 uint32, 7 float32, 8 float64). Writes 4 f32
+ * a centre, 6 a covariance, and (rest > 0) shWords(degree) words a splat of
+ * harmonics, degree the one with rest / 3 coefficients. Returns 0, or -4
+ * with *bad the first vertex whose position is not finite. bmin / bmax: the
+ * box, as the reader's doubles.
+ */
+int or_decode_ply(const uint8_t* payload, uint32_t n, uint32_t stride, const uint32_t* types,
+                  const uint32_t* offsets, uint32_t rest, float* centers, float* cov, uint32_t* sh,
+                  double bmin[3], double bmax[3], uint32_t* bad);
+
+/*
+ * parseSpz on gunzipped bytes (scene/splats.js:227-303): the header checks
+ * (returns -7 not a .spz, -8 version, -9 degree, -10 no splats, -11 cut
+ * short; message in err), then every splat. *count and *degree are set
+ * first (call with centers NULL to learn them); sh gets shWords(degree)
+ * words a splat. -4 with *bad as for .ply.
+ */
+int or_decode_spz(const uint8_t* data, size_t len, uint32_t* count, uint32_t* degree, float* centers, float* cov,
+                  uint32_t* sh, double bmin[3], double bmax[3], uint32_t* bad, char* err, size_t errlen);
 
 /* Depth buckets of an alpha emitter's sort: render/particles.js:44-48. */
 #define OR_PARTICLE_BUCKETS 4096u

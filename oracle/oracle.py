@@ -70,6 +70,18 @@ def _declare(L):
     L.or_counting_sort.argtypes = [_u32p, ctypes.c_uint32, _u32p, _u32p]
     L.or_drawlist_sort.restype = None
     L.or_drawlist_sort.argtypes = [_u32p, _u32p, ctypes.c_uint32, _u32p, _u32p]
+    L.or_exp.restype = ctypes.c_double
+    L.or_exp.argtypes = [ctypes.c_double]
+    L.or_byte.restype = ctypes.c_uint32
+    L.or_byte.argtypes = [ctypes.c_double]
+    L.or_signed_half.restype = ctypes.c_uint32
+    L.or_signed_half.argtypes = [ctypes.c_double]
+    L.or_decode_ply.restype = ctypes.c_int
+    L.or_decode_ply.argtypes = [_u8p, ctypes.c_uint32, ctypes.c_uint32, _u32p, _u32p, ctypes.c_uint32, _f32p,
+                                _f32p, _u32p, _f64p, _f64p, _u32p]
+    L.or_decode_spz.restype = ctypes.c_int
+    L.or_decode_spz.argtypes = [_u8p, ctypes.c_size_t, _u32p, _u32p, _f32p, _f32p, _u32p, _f64p, _f64p, _u32p,
+                                ctypes.c_char_p, ctypes.c_size_t]
     L.or_shade.restype = ctypes.c_uint32
     L.or_shade.argtypes = [_f32p, _u32p, ctypes.c_int, ctypes.c_uint32, _f32p]
     L.or_particle_key.restype = ctypes.c_uint32
@@ -231,3 +243,168 @@ def shade(centers: np.ndarray, sh: np.ndarray, degree: int, indices, eye) -> np.
     L = lib()
     cp, wp, ep = _ptr(c, _f32p), _ptr(w, _u32p), _ptr(e, _f32p)
     return np.array([L.or_shade(cp, wp, degree, int(i), ep) for i in indices], np.uint32)
+
+
+# ------------------------------------------------------------ capture readers
+
+SH_COEFFICIENTS = (0, 3, 8, 15)
+PLY_TYPES = {   # scene/splats.js:391-396: name -> (type code, bytes)
+    "char": (1, 1), "int8": (1, 1), "uchar": (2, 1), "uint8": (2, 1),
+    "short": (3, 2), "int16": (3, 2), "ushort": (4, 2), "uint16": (4, 2),
+    "int": (5, 4), "int32": (5, 4), "uint": (6, 4), "uint32": (6, 4),
+    "float": (7, 4), "float32": (7, 4), "double": (8, 8), "float64": (8, 8),
+}
+PLY_NEEDS = ["x", "y", "z", "f_dc_0", "f_dc_1", "f_dc_2", "opacity", "scale_0", "scale_1", "scale_2",
+             "rot_0", "rot_1", "rot_2", "rot_3"]
+
+
+def sh_words(degree: int) -> int:
+    return (SH_COEFFICIENTS[degree] * 3 + 1) // 2
+
+
+class Capture(Parsed):
+    """A decoded capture with its harmonics: degree and sh (uint32 words)."""
+
+    def __init__(self, count, centers, covariances, bmin, bmax, degree=0, sh=None):
+        super().__init__(count, centers, covariances, bmin, bmax)
+        self.degree = degree
+        self.sh = sh if sh is not None else np.zeros(1, np.uint32)
+
+
+def _js_number_text(v: float) -> str:
+    if v != v:
+        return "NaN"
+    if v == int(v) and abs(v) < 1e21:
+        return str(int(v))
+    return repr(v)
+
+
+def _to_number(word):
+    if word is None:
+        return float("nan")
+    t = word.strip()
+    if t == "":
+        return 0.0
+    try:
+        if t[:2].lower() in ("0x", "0o", "0b"):
+            return float(int(t, 0))
+        if t in ("Infinity", "+Infinity", "-Infinity"):
+            return float(t.replace("Infinity", "inf"))
+        if any(ch not in "0123456789+-.eE" for ch in t):
+            return float("nan")
+        return float(t)
+    except ValueError:
+        return float("nan")
+
+
+def parse_ply(data: bytes) -> Capture:
+    """parsePly (scene/splats.js:398-468): the header restated here, the
+    per-vertex arithmetic in oracle.cpp."""
+    data = bytes(data)
+    marker = b"end_header"
+    end = -1
+    for i in range(min(len(data), 65536) - len(marker)):
+        if data[i:i + len(marker)] == marker:
+            end = i + len(marker)
+            break
+    if end < 0:
+        raise OracleError(-5, "splats: a .ply with no end_header")
+    if end < len(data) and data[end] == 0x0D:
+        end += 1
+    end += 1
+    header = data[:end].decode("utf-8", "replace").replace("\r\n", "\n").split("\n")
+    fmt = "null"
+    vertices = None
+    for line in header:
+        words = line.strip().split() or [""]
+        w = lambda k: words[k] if k < len(words) else None
+        if words[0] == "format":
+            fmt = w(1) if w(1) is not None else "undefined"
+        elif words[0] == "element":
+            kind = w(1) if w(1) is not None else "undefined"
+            if vertices is None and kind == "chunk":
+                raise OracleError(-5, "splats: a compressed .ply (from SuperSplat) is not read; export an "
+                                      "uncompressed .ply or a .splat")
+            if vertices is None and kind != "vertex":
+                raise OracleError(-5, f"splats: a .ply whose first element is '{kind}', not 'vertex'")
+            if vertices is not None:
+                break
+            vertices = {"count": _to_number(w(2)), "props": {}, "stride": 0}
+        elif words[0] == "property" and vertices is not None:
+            t = w(1) if w(1) is not None else "undefined"
+            if t == "list":
+                raise OracleError(-5, "splats: a .ply with list properties on its vertices is not a splat capture")
+            if t not in PLY_TYPES:
+                raise OracleError(-5, f"splats: unknown .ply property type '{t}'")
+            name = w(2) if w(2) is not None else "undefined"
+            vertices["props"][name] = (PLY_TYPES[t][0], vertices["stride"])
+            vertices["stride"] += PLY_TYPES[t][1]
+    if vertices is None:
+        raise OracleError(-5, "splats: a .ply with no vertices")
+    if fmt != "binary_little_endian":
+        raise OracleError(-5, f"splats: a .ply in '{fmt}' format; only binary_little_endian is read")
+    count = vertices["count"]
+    if not (count == count and count != float("inf") and count == int(count) and count > 0):
+        raise OracleError(-5, f"splats: a .ply with {_js_number_text(count)} vertices")
+    props = vertices["props"]
+    missing = [n for n in PLY_NEEDS if n not in props]
+    if missing:
+        raise OracleError(-5, f"splats: this .ply is not a splat capture: no {', '.join(missing)}")
+    stride = vertices["stride"]
+    n = int(count)
+    if end + n * stride > len(data):
+        raise OracleError(-5, f"splats: the .ply is cut short: {n} vertices need {n * stride} bytes, "
+                              f"it has {len(data) - end}")
+    rest = 0
+    while f"f_rest_{rest}" in props:
+        rest += 1
+    degree = SH_COEFFICIENTS.index(rest // 3) if rest % 3 == 0 and rest // 3 in SH_COEFFICIENTS else -1
+    if rest > 0 and degree < 1:
+        raise OracleError(-5, f"splats: a .ply with {rest} f_rest_ properties; harmonics of degree 1, 2 or 3 "
+                              "have 9, 24 or 45")
+    degree = max(degree, 0)
+    names = PLY_NEEDS + [f"f_rest_{k}" for k in range(rest)]
+    types = np.array([props[nm][0] for nm in names], np.uint32)
+    offsets = np.array([props[nm][1] for nm in names], np.uint32)
+    payload = np.frombuffer(data, np.uint8, count=n * stride, offset=end).copy()
+    centers = np.zeros((n, 4), np.float32)
+    cov = np.zeros((n, 6), np.float32)
+    sh = np.zeros(n * sh_words(degree) + 1 if degree else 1, np.uint32)
+    bmin = np.zeros(3, np.float64)
+    bmax = np.zeros(3, np.float64)
+    bad = ctypes.c_uint32(0)
+    rc = lib().or_decode_ply(_ptr(payload, _u8p), n, stride, _ptr(types, _u32p), _ptr(offsets, _u32p), rest,
+                             _ptr(centers, _f32p), _ptr(cov, _f32p), _ptr(sh, _u32p), _ptr(bmin, _f64p),
+                             _ptr(bmax, _f64p), ctypes.byref(bad))
+    if rc == -4:
+        raise OracleError(-4, f"splats: splat {bad.value} has a position that is not a number", bad.value)
+    return Capture(n, centers, cov, bmin, bmax, degree, sh)
+
+
+def parse_spz(gz: bytes) -> Capture:
+    """parseSpz (scene/splats.js:227-303) after gunzip (the reference's
+    DecompressionStream)."""
+    import zlib
+    data = np.frombuffer(zlib.decompress(bytes(gz), 16 + zlib.MAX_WBITS), np.uint8).copy()
+    count = ctypes.c_uint32(0)
+    degree = ctypes.c_uint32(0)
+    err = ctypes.create_string_buffer(256)
+    bad = ctypes.c_uint32(0)
+    z3 = np.zeros(3, np.float64)
+    L = lib()
+    rc = L.or_decode_spz(_ptr(data, _u8p), data.size, ctypes.byref(count), ctypes.byref(degree), None, None, None,
+                         _ptr(z3, _f64p), _ptr(z3, _f64p), ctypes.byref(bad), err, 256)
+    if rc:
+        raise OracleError(rc, err.value.decode())
+    n, d = count.value, degree.value
+    centers = np.zeros((n, 4), np.float32)
+    cov = np.zeros((n, 6), np.float32)
+    sh = np.zeros(n * sh_words(d) + 1 if d else 1, np.uint32)
+    bmin = np.zeros(3, np.float64)
+    bmax = np.zeros(3, np.float64)
+    rc = L.or_decode_spz(_ptr(data, _u8p), data.size, ctypes.byref(count), ctypes.byref(degree), _ptr(centers, _f32p),
+                         _ptr(cov, _f32p), _ptr(sh, _u32p), _ptr(bmin, _f64p), _ptr(bmax, _f64p), ctypes.byref(bad),
+                         err, 256)
+    if rc == -4:
+        raise OracleError(-4, f"splats: splat {bad.value} has a position that is not a number", bad.value)
+    return Capture(n, centers, cov, bmin, bmax, d, sh)

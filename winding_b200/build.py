@@ -17,7 +17,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libwsort.so")
-SOURCES = ["api.cu", "sort.cu", "decode.cu", "noalloc.cu", "server.cu"]
+SOURCES = ["api.cu", "sort.cu", "decode.cu", "formats.cu", "noalloc.cu", "server.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -44,7 +44,7 @@ def build(verbose: bool = False, force: bool = False) -> str:
         return LIB
     cmd = [nvcc(), *ARCH, "-lineinfo", "-O3", "-std=c++17", "-fmad=false",
            "-Xcompiler", "-fPIC,-ffp-contract=off,-O2", "-I", os.path.join(ROOT, "include"),
-           "-shared", "-o", LIB + ".tmp", *sources(), "-lpthread"]
+           "-shared", "-o", LIB + ".tmp", *sources(), "-lpthread", "-lz"]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
         print(" ".join(cmd), flush=True)

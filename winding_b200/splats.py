@@ -279,6 +279,18 @@ class Splats:
                                                    ctypes.byref(dmin), ctypes.byref(dscale)))
         return bool(vis.value), dmin.value, dscale.value
 
+    def harmonics(self):
+        """(degree, words): the higher harmonics the cloud holds, words as
+        uint32 (SH_WORDS[degree] a splat), or (0, None)."""
+        self._check_alive()
+        d = ctypes.c_int(0)
+        self.ctx.check(self.ctx.lib.ws_cloud_harmonics(self.handle, ctypes.byref(d), None))
+        if d.value == 0:
+            return 0, None
+        words = np.empty(self.count * SH_WORDS[d.value], np.uint32)
+        self.ctx.check(self.ctx.lib.ws_cloud_harmonics(self.handle, ctypes.byref(d), words.ctypes.data))
+        return d.value, words
+
     def set_harmonics(self, degree: int, words) -> None:
         """Attaches higher harmonics of `degree` (1-3): uint32 words packed as
         the reference packs them (sh_words(degree) a splat, see SH_WORDS), or
@@ -311,6 +323,22 @@ def eye_in_cloud(model_view) -> np.ndarray:
     m = np.asarray(model_view, np.float32).astype(np.float64).reshape(4, 4).T   # column-major
     inv = np.linalg.inv(m)
     return inv[:3, 3].astype(np.float32)
+
+
+def load_splats(data, ctx: Context | None = None) -> Splats:
+    """readSplats + upload (src/scene/splats.js:78-90): a binary .ply, a
+    gzipped .spz (versions 1-3) or .splat records, decoded on the device with
+    their harmonics. Raises WsError with the reference's messages."""
+    ctx = ctx or Context(0)
+    buf = np.frombuffer(bytes(data), np.uint8) if not isinstance(data, np.ndarray) else \
+        np.ascontiguousarray(data).view(np.uint8).reshape(-1)
+    h = ctypes.c_void_p()
+    ctx.check(ctx.lib.ws_cloud_load(ctx.handle, buf.ctypes.data, buf.size, ctypes.byref(h)))
+    sp = Splats(ctx, h)
+    d = ctypes.c_int(0)
+    ctx.check(ctx.lib.ws_cloud_harmonics(h, ctypes.byref(d), None))
+    sp.degree = d.value
+    return sp
 
 
 def parse_splats(data, ctx: Context | None = None) -> Splats:
