@@ -472,6 +472,109 @@ def suite(ctx, torch, flush, args):
         out["served-16"] = served(ctx, args)
     except Exception as exc:
         out["served-16"] = {"error": f"{type(exc).__name__}: {exc}"}
+    for name, fn in (("particles-64", particles_suite), ("shade-1M", shade_suite), ("decode", decode_suite)):
+        try:
+            out[name] = fn(ctx, torch, flush, peak)
+        except Exception as exc:
+            out[name] = {"error": f"{type(exc).__name__}: {exc}"}
+    return out
+
+
+def particles_suite(ctx, torch, flush, peak):
+    """64 alpha emitters of 1k-200k particles in one pool: one batched launch
+    (ws_sort_particles over all) against one launch per emitter, as the
+    reference dispatches them (render/particles.js:838-850)."""
+    from winding_b200 import particles as P, workloads as W
+    rings = W.emitter_rings()
+    n = sum(c for _, c in rings)
+    pool = torch.from_numpy(W.particle_pool(n).reshape(-1)).cuda()
+    eye = np.array([0.0, 5.0, 80.0], np.float32)
+    fwd = np.array([0.0, -0.0624, -0.998], np.float32)
+    outs = [(torch.empty(max(c, 1), dtype=torch.int32, device="cuda"), torch.empty(max(c, 1), dtype=torch.int32,
+             device="cuda"), torch.zeros(1, dtype=torch.int32, device="cuda")) for _, c in rings]
+    ptrs = [(o.data_ptr(), k.data_ptr(), c.data_ptr()) for o, k, c in outs]
+    stream = torch.cuda.current_stream().cuda_stream
+
+    def batched():
+        P.sort_emitters(ctx, pool.data_ptr(), rings, eye, fwd, ptrs, stream)
+
+    def plain():
+        for ring, out in zip(rings, ptrs):
+            P.sort_emitters(ctx, pool.data_ptr(), [ring], eye, fwd, [out], stream)
+
+    for _ in range(3):
+        batched()
+        plain()
+    ctx.timing(True)
+    b_ms = timed_sorts(ctx, torch, 10, flush, batched)
+    kms, launches = ctx.timing_read()
+    ctx.timing(False)
+    p_ms = timed_sorts(ctx, torch, 10, flush, plain)
+    live = sum(int(c.item()) for _, _, c in outs)
+    kernel_s = kms / max(launches, 1) / 1e3
+    algo = 32 * n + 8 * live
+    return {"emitters": len(rings), "particles": n, "live": live,
+            "batched_mparticles_s": n * 10 / (b_ms / 1e3) / 1e6, "plain_mparticles_s": n * 10 / (p_ms / 1e3) / 1e6,
+            "batched_vs_plain": p_ms / b_ms, "kernel_us": kernel_s * 1e6,
+            "achieved_gbs": algo / kernel_s / 1e9, "frac": algo / kernel_s / 1e9 / peak,
+            "algorithmic_bytes": "32 per slot + 8 per live particle"}
+
+
+def shade_suite(ctx, torch, flush, peak):
+    """clusters-1M with degree-3 harmonics: the sort alone against the sort
+    with the shade pass fused into it (ws_sort_batch_shaded)."""
+    from winding_b200 import parse_splats, workloads as W
+    from winding_b200.splats import eye_in_cloud
+    job = W.clusters_1m(seed=1, cull=0.5)
+    sp = parse_splats(job.records, ctx)
+    sp.set_harmonics(3, W.harmonics_words(sp.count, 3))
+    from winding_b200 import make_view
+    view = make_view(job.view.model_view, job.view.projection, job.view.viewport, 0.5)
+    o = torch.empty(sp.count, dtype=torch.int32, device="cuda")
+    k = torch.empty_like(o)
+    c = torch.zeros(1, dtype=torch.int32, device="cuda")
+    shaded = torch.empty_like(o)
+    spec = [(sp, view, o.data_ptr(), k.data_ptr(), c.data_ptr())]
+    shade = [(eye_in_cloud(job.view.model_view), shaded.data_ptr())]
+    stream = torch.cuda.current_stream().cuda_stream
+    res = {}
+    for name, fn in (("sort", lambda: ctx.sort_batch(spec, stream)),
+                     ("sort_and_shade", lambda: ctx.sort_batch_shaded(spec, shade, stream))):
+        for _ in range(3):
+            fn()
+        ctx.timing(True)
+        timed_sorts(ctx, torch, 10, flush, fn)
+        kms, launches = ctx.timing_read()
+        ctx.timing(False)
+        res[name + "_kernel_us"] = kms / max(launches, 1) * 1e3
+    s = int(c.item())
+    extra_s = (res["sort_and_shade_kernel_us"] - res["sort_kernel_us"]) / 1e6
+    res.update({"splats": sp.count, "survivors": s, "degree": 3,
+                "shade_bytes": s * (23 * 4 + 4), "shade_extra_us": extra_s * 1e6,
+                "shade_gbs": s * 96 / extra_s / 1e9 if extra_s > 0 else None})
+    sp.destroy()
+    return res
+
+
+def decode_suite(ctx, torch, flush, peak):
+    """Loading a capture through the public call (ws_cloud_load): a 1M-splat
+    .ply with degree-3 harmonics and 1M .splat records, host bytes to a
+    resident cloud (header parse, upload, device decode)."""
+    from winding_b200 import load_splats, workloads as W
+    out = {}
+    ply = W.ply_bytes(1_000_000, 3)
+    rec = W.clusters(1_000_000, 1).tobytes()
+    for name, data in (("ply_deg3", ply), ("splat", rec)):
+        load_splats(data, ctx).destroy()
+        times = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            sp = load_splats(data, ctx)
+            times.append(time.perf_counter() - t0)
+            sp.destroy()
+        t = min(times)
+        out[name] = {"splats": 1_000_000, "bytes": len(data), "ms": t * 1e3, "msplats_s": 1.0 / t,
+                     "gb_s": len(data) / t / 1e9}
     return out
 
 

@@ -269,6 +269,27 @@ int ws_sort_particles(ws_ctx* ctx, int n, const ws_emitter* emitters, void* stre
  * Host only; needs no device. */
 int ws_particle_thresholds(float* out);
 
+/* ------------------------------------------------------------ drawing */
+
+/*
+ * The splat draw (vs / fs, src/render/splats.js:252-312) into a headless
+ * image: the first *count splats of `order` (a sort's device output, far
+ * first) blended, premultiplied, over `image` (device, width x height RGBA
+ * f32, row 0 at the top, 16-byte aligned; its contents are the background).
+ * shaded (device, or NULL): the shade pass's colour words, read in place of
+ * the splats' own (the reference's SHADED pipeline). The view is the one
+ * sorted for; its viewport must be width x height (1 to 4096 a side). No fog
+ * and no depth test. Rasterisation and the shader's exp / log / pow are
+ * pinned (the library's notes on the draw say how). Synchronises `stream`
+ * once (the number of (tile, splat) pairs sizes the binning).
+ */
+int ws_draw(ws_ctx* ctx, const ws_cloud* cloud, const ws_view* view, const uint32_t* order, const uint32_t* count,
+            const uint32_t* shaded, float* image, uint32_t width, uint32_t height, void* stream);
+
+/* The draw's two 256-entry tables: decodeSRGB(byte / 255) and
+ * log(255 (byte / 255)), as the f32 the draw uses. Host only. */
+int ws_draw_tables(float* srgb, float* reach);
+
 /* ------------------------------------------------------------ serving */
 
 /*

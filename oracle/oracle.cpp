@@ -710,3 +710,116 @@ extern "C" int or_decode_spz(const uint8_t* data, size_t len, uint32_t* count, u
     }
     return 0;
 }
+
+// ------------------------------------------------------------------ draw
+
+extern "C" void or_draw_tables(float srgb[256], float reach[256]) {
+    for (int b = 0; b < 256; ++b) {
+        const float c = (float)b / 255.0f;   // unpack4x8unorm
+        if (c <= 0.04045f)
+            srgb[b] = c / 12.92f;
+        else
+            srgb[b] = (float)powl((long double)((c + 0.055f) / 1.055f), 2.4L);
+        reach[b] = (float)logl((long double)(255.0f * c));
+    }
+}
+
+namespace {
+
+// Cody and Waite's reduction, the Taylor polynomial to r^7 / 7!, 2^k.
+float exp_pinned(float x) {
+    if (std::isnan(x)) return x;
+    if (x < -104.0f) return 0.0f;
+    if (x > 88.0f) return INFINITY;
+    const float k = rintf(x * 1.44269504f);
+    const float r = (x - k * 0.693359375f) - k * -2.12194440e-4f;
+    float p = 1.98412698e-4f;
+    p = p * r + 1.38888889e-3f;
+    p = p * r + 8.33333333e-3f;
+    p = p * r + 4.16666667e-2f;
+    p = p * r + 1.66666667e-1f;
+    p = p * r + 0.5f;
+    p = p * r + 1.0f;
+    p = p * r + 1.0f;
+    int ki = (int)k;
+    if (ki < -126) {
+        p = p * std::ldexp(1.0f, ki + 126);
+        ki = -126;
+    }
+    return p * std::ldexp(1.0f, ki);
+}
+
+}  // namespace
+
+extern "C" void or_draw(const float* centers, const float* cov, const uint32_t* order, uint32_t count,
+                        const uint32_t* shaded, const float mv[16], const float P[16], uint32_t width,
+                        uint32_t height, float* image) {
+    float srgb[256], reach_t[256];
+    or_draw_tables(srgb, reach_t);
+    or_cloud c;
+    std::memcpy(c.model_view, mv, sizeof(c.model_view));
+    std::memcpy(c.projection, P, sizeof(c.projection));
+    c.viewport[0] = (float)width;
+    c.viewport[1] = (float)height;
+    const float half_w = 0.5f * (float)width, half_h = 0.5f * (float)height;
+    for (uint32_t j = 0; j < count; ++j) {
+        const uint32_t i = order[j];
+        const float* p = centers + 4 * (size_t)i;
+        float view[4], clip[4];
+        for (int k = 0; k < 4; ++k)   // modelView * (x, y, z, 1), column sums
+            view[k] = ((mv[k] * p[0] + mv[4 + k] * p[1]) + mv[8 + k] * p[2]) + mv[12 + k] * 1.0f;
+        for (int k = 0; k < 4; ++k)
+            clip[k] = ((P[k] * view[0] + P[4 + k] * view[1]) + P[8 + k] * view[2]) + P[12 + k] * view[3];
+        float f[3];
+        or_footprint(&c, cov, i, view, f);
+        const float a = f[0] + 0.3f, b = f[1], cc = f[2] + 0.3f;
+        const float mid = 0.5f * (a + cc), hd = 0.5f * (a - cc);
+        const float radius = std::sqrt(hd * hd + b * b);
+        const float major = mid + radius, minor = mid - radius;
+        uint32_t word;
+        if (shaded)
+            word = shaded[i];
+        else
+            std::memcpy(&word, &p[3], 4);
+        const float reach = reach_t[word >> 24];
+        if (!(minor > 0.0f) || !(reach > 0.0f)) continue;
+        float ax = 1.0f, ay = 0.0f;
+        if (std::fabs(b) > 1e-12f) {
+            const float ey = major - a;
+            const float len = std::sqrt(b * b + ey * ey);
+            ax = b / len;
+            ay = ey / len;
+        } else if (cc > a) {
+            ax = 0.0f;
+            ay = 1.0f;
+        }
+        const float la = std::fmin(std::sqrt(2.0f * major), 1024.0f);
+        const float lc = std::fmin(std::sqrt(2.0f * minor), 1024.0f);
+        const float qm = std::sqrt(std::fmin(reach, 4.0f));
+        const float cx = (clip[0] / clip[3] + 1.0f) * half_w;
+        const float cy = (1.0f - clip[1] / clip[3]) * half_h;
+        const float hx = qm * (la * std::fabs(ax) + lc * std::fabs(ay));
+        const float hy = qm * (la * std::fabs(ay) + lc * std::fabs(ax));
+        if (!(std::isfinite(cx) && std::isfinite(cy) && std::isfinite(hx) && std::isfinite(hy))) continue;
+        const float fx0 = std::fmax(std::floor((cx - hx) - 1.5f), 0.0f);
+        const float fx1 = std::fmin(std::ceil((cx + hx) + 0.5f), (float)(width - 1));
+        const float fy0 = std::fmax(std::floor((cy - hy) - 1.5f), 0.0f);
+        const float fy1 = std::fmin(std::ceil((cy + hy) + 0.5f), (float)(height - 1));
+        if (!(fx0 <= fx1 && fy0 <= fy1)) continue;
+        const float alpha0 = (float)(word >> 24) / 255.0f;
+        const float rgb[3] = {srgb[word & 255u], srgb[(word >> 8) & 255u], srgb[(word >> 16) & 255u]};
+        for (int py = (int)fy0; py <= (int)fy1; ++py)
+            for (int px = (int)fx0; px <= (int)fx1; ++px) {
+                const float ex = ((float)px + 0.5f) - cx, ey = cy - ((float)py + 0.5f);
+                const float ox = (ex * ax + ey * ay) / la;
+                const float oy = (ex * ay - ey * ax) / lc;
+                if (!(std::fabs(ox) <= qm && std::fabs(oy) <= qm)) continue;
+                const float alpha = std::fmin(0.99f, exp_pinned(-(ox * ox + oy * oy)) * alpha0);
+                if (alpha < 1.0f / 255.0f) continue;
+                float* d = image + 4 * ((size_t)py * width + px);
+                const float om = 1.0f - alpha;
+                for (int k = 0; k < 3; ++k) d[k] = rgb[k] * alpha + d[k] * om;
+                d[3] = alpha + d[3] * om;
+            }
+    }
+}

@@ -14,6 +14,7 @@
  *   - an alpha emitter's particle keys:          src/render/particles.js:197-209
  *   - the shade pass (harmonics):                src/render/splats.js:333-381
  *   - the .ply and .spz readers' per-splat math: src/scene/splats.js:227-303, :398-468
+ *   - the splat draw (vs / fs):                  src/render/splats.js:252-312
  *
  * Pinned evaluation order. WGSL lets a driver fuse and reorder f32 work, so
  * the oracle fixes one order and the CUDA kernels follow it bit for bit:
@@ -156,6 +157,20 @@ int or_decode_ply(const uint8_t* payload, uint32_t n, uint32_t stride, const uin
  */
 int or_decode_spz(const uint8_t* data, size_t len, uint32_t* count, uint32_t* degree, float* centers, float* cov,
                   uint32_t* sh, double bmin[3], double bmax[3], uint32_t* bad, char* err, size_t errlen);
+
+/*
+ * The splat draw (render/splats.js:252-312) as the library pins it: for each
+ * of the first `count` splats of `order`, in order, the quad the vertex
+ * shader builds and the fragments of the pixels whose centres its inverse
+ * maps into [-e, e]^2, blended premultiplied over `image` (width x height
+ * RGBA f32, row 0 at the top). shaded: colour words in place of the splats'
+ * own, or NULL. srgb / reach: the 256-entry decodeSRGB and log tables this
+ * oracle computes (or_draw_tables). See the library's draw for the pinned
+ * rules; this restates them.
+ */
+void or_draw_tables(float srgb[256], float reach[256]);
+void or_draw(const float* centers, const float* cov, const uint32_t* order, uint32_t count, const uint32_t* shaded,
+             const float model_view[16], const float projection[16], uint32_t width, uint32_t height, float* image);
 
 /* Depth buckets of an alpha emitter's sort: render/particles.js:44-48. */
 #define OR_PARTICLE_BUCKETS 4096u

@@ -82,6 +82,11 @@ def _declare(L):
     L.or_decode_spz.restype = ctypes.c_int
     L.or_decode_spz.argtypes = [_u8p, ctypes.c_size_t, _u32p, _u32p, _f32p, _f32p, _u32p, _f64p, _f64p, _u32p,
                                 ctypes.c_char_p, ctypes.c_size_t]
+    L.or_draw_tables.restype = None
+    L.or_draw_tables.argtypes = [_f32p, _f32p]
+    L.or_draw.restype = None
+    L.or_draw.argtypes = [_f32p, _f32p, _u32p, ctypes.c_uint32, _u32p, _f32p, _f32p, ctypes.c_uint32,
+                          ctypes.c_uint32, _f32p]
     L.or_shade.restype = ctypes.c_uint32
     L.or_shade.argtypes = [_f32p, _u32p, ctypes.c_int, ctypes.c_uint32, _f32p]
     L.or_particle_key.restype = ctypes.c_uint32
@@ -408,3 +413,24 @@ def parse_spz(gz: bytes) -> Capture:
     if rc == -4:
         raise OracleError(-4, f"splats: splat {bad.value} has a position that is not a number", bad.value)
     return Capture(n, centers, cov, bmin, bmax, d, sh)
+
+
+def draw_tables():
+    srgb = np.zeros(256, np.float32)
+    reach = np.zeros(256, np.float32)
+    lib().or_draw_tables(_ptr(srgb, _f32p), _ptr(reach, _f32p))
+    return srgb, reach
+
+
+def draw(parsed, order, model_view, projection, width: int, height: int, background=None, shaded=None):
+    """The pinned splat draw: an RGBA f32 image (height, width, 4)."""
+    img = np.zeros((height, width, 4), np.float32) if background is None else \
+        np.array(background, np.float32).reshape(height, width, 4).copy()
+    o = np.ascontiguousarray(order, np.uint32)
+    sh = None if shaded is None else np.ascontiguousarray(shaded, np.uint32)
+    mv = np.ascontiguousarray(model_view, np.float32).reshape(16)
+    pr = np.ascontiguousarray(projection, np.float32).reshape(16)
+    lib().or_draw(_ptr(parsed.centers, _f32p), _ptr(parsed.covariances, _f32p), _ptr(o, _u32p), o.size,
+                  None if sh is None else _ptr(sh, _u32p), _ptr(mv, _f32p), _ptr(pr, _f32p), width, height,
+                  _ptr(img, _f32p))
+    return img

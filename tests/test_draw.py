@@ -1,0 +1,139 @@
+"""The splat draw (render/splats.js:252-312) into a headless RGBA f32 image.
+
+CPU: the library's decodeSRGB and log tables against the oracle's (computed
+independently, in long double), and the oracle's draw on hand-checked cases.
+GPU: sort then ws_draw against the oracle's draw of the oracle's order, bit
+for bit, over a background, with shaded colours, an empty order and the
+refusals.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from winding_b200 import camera, workloads as W
+from winding_b200.splats import draw_tables
+
+
+def test_tables_match_the_oracle():
+    srgb, reach = draw_tables()
+    o_srgb, o_reach = O.draw_tables()
+    assert np.array_equal(srgb.view(np.uint32), o_srgb.view(np.uint32))
+    assert np.array_equal(reach.view(np.uint32), o_reach.view(np.uint32))
+    assert srgb[0] == 0 and srgb[255] == 1.0
+    assert reach[1] == 0 and np.isneginf(reach[0])
+
+
+def _one_splat(alpha_byte=255, scale=0.05):
+    rec = np.zeros(1, W.RECORD)
+    rec["scale"] = scale
+    rec["rgba"] = [255, 128, 0, alpha_byte]
+    rec["rot"] = [255, 128, 128, 128]
+    return rec
+
+
+def test_oracle_draws_one_splat_at_the_centre():
+    rec = _one_splat(scale=0.3)   # about 3 pixels across its sigma
+    parsed = O.parse_splat(rec.tobytes())
+    mv = camera.look_at((0, 0, 5), (0, 0, 0))
+    proj = camera.perspective(np.pi / 3, 1.0, 0.1)
+    img = O.draw(parsed, [0], mv, proj, 64, 64)
+    a = img[..., 3]
+    cy, cx = np.unravel_index(np.argmax(a), a.shape)
+    assert (cy, cx) in [(31, 31), (31, 32), (32, 31), (32, 32)]
+    assert 0.9 < a.max() <= 0.99
+    assert np.allclose(img[..., 0], a * 1.0) and np.all(img[..., 2] == 0)   # red 255, blue 0: premultiplied
+    assert np.all(a[0, :] == 0)                                               # a small splat: edges untouched
+    faint = O.draw(O.parse_splat(_one_splat(alpha_byte=1, scale=0.3).tobytes()), [0], mv, proj, 64, 64)
+    assert not faint.any()                                                    # reach <= 0: not drawn
+
+
+def _sorted(ctx, job, cull=0.5):
+    import torch
+    from winding_b200 import make_view, parse_splats
+    sp = parse_splats(job.records, ctx)
+    view = make_view(job.view.model_view, job.view.projection, job.view.viewport, cull)
+    o = torch.empty(sp.count, dtype=torch.int32, device="cuda")
+    k = torch.empty_like(o)
+    c = torch.zeros(1, dtype=torch.int32, device="cuda")
+    ctx.sort_device(sp, view, o.data_ptr(), k.data_ptr(), c.data_ptr())
+    return sp, view, o, c
+
+
+def _job(n, seed, w, h):
+    job = W.clusters_1m(seed=seed, n=n)
+    proj = camera.perspective(W.FOV_Y, w / h, W.NEAR)
+    job.view = W.View(job.view.model_view, proj, (float(w), float(h)), 0.5)
+    return job
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("w,h", [(480, 270), (333, 197)])
+def test_draw_matches_oracle(ctx, w, h):
+    import torch
+    job = _job(150_000, 5, w, h)
+    sp, view, o, c = _sorted(ctx, job)
+    try:
+        rng = np.random.default_rng(1)
+        bg = rng.uniform(0, 1, size=(h, w, 4)).astype(np.float32)
+        img = torch.from_numpy(bg.copy()).cuda()
+        ctx.draw(sp, view, o.data_ptr(), c.data_ptr(), img.data_ptr(), w, h)
+        ctx.sync()
+        got = img.cpu().numpy()
+        order = o[: int(c.item())].cpu().numpy().view(np.uint32)
+        want = O.draw(O.parse_splat(job.bytes()), order, job.view.model_view, job.view.projection, w, h,
+                      background=bg)
+        assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+        assert (got != bg).mean() > 0.05
+    finally:
+        sp.destroy()
+
+
+@pytest.mark.gpu
+def test_draw_with_shaded_colours(ctx):
+    import torch
+    from winding_b200.splats import eye_in_cloud
+    w, h = 320, 180
+    job = _job(60_000, 6, w, h)
+    from winding_b200 import make_view, parse_splats
+    sp = parse_splats(job.records, ctx)
+    try:
+        sp.set_harmonics(2, W.harmonics_words(sp.count, 2))
+        view = make_view(job.view.model_view, job.view.projection, job.view.viewport, 0.5)
+        o = torch.empty(sp.count, dtype=torch.int32, device="cuda")
+        k = torch.empty_like(o)
+        c = torch.zeros(1, dtype=torch.int32, device="cuda")
+        shaded = torch.zeros(sp.count, dtype=torch.int32, device="cuda")
+        ctx.sort_batch_shaded([(sp, view, o.data_ptr(), k.data_ptr(), c.data_ptr())],
+                              [(eye_in_cloud(job.view.model_view), shaded.data_ptr())])
+        img = torch.zeros((h, w, 4), dtype=torch.float32, device="cuda")
+        ctx.draw(sp, view, o.data_ptr(), c.data_ptr(), img.data_ptr(), w, h, shaded.data_ptr())
+        ctx.sync()
+        order = o[: int(c.item())].cpu().numpy().view(np.uint32)
+        want = O.draw(O.parse_splat(job.bytes()), order, job.view.model_view, job.view.projection, w, h,
+                      shaded=shaded.cpu().numpy().view(np.uint32))
+        assert np.array_equal(img.cpu().numpy().view(np.uint32), want.view(np.uint32))
+    finally:
+        sp.destroy()
+
+
+@pytest.mark.gpu
+def test_draw_nothing_and_refusals(ctx):
+    import torch
+    from winding_b200 import WsError
+    w, h = 128, 96
+    job = _job(20_000, 7, w, h)
+    sp, view, o, c = _sorted(ctx, job)
+    try:
+        img = torch.full((h, w, 4), 0.25, dtype=torch.float32, device="cuda")
+        zero = torch.zeros(1, dtype=torch.int32, device="cuda")
+        ctx.draw(sp, view, o.data_ptr(), zero.data_ptr(), img.data_ptr(), w, h)
+        ctx.sync()
+        assert torch.all(img == 0.25)
+        with pytest.raises(WsError, match="viewport"):
+            ctx.draw(sp, view, o.data_ptr(), c.data_ptr(), img.data_ptr(), w + 1, h)
+        with pytest.raises(WsError, match="16-byte aligned"):
+            ctx.draw(sp, view, o.data_ptr(), c.data_ptr(), img.data_ptr() + 4, w, h)
+        with pytest.raises(WsError, match="1 to 4096"):
+            ctx.draw(sp, view, o.data_ptr(), c.data_ptr(), img.data_ptr(), 0, h)
+    finally:
+        sp.destroy()

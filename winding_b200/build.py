@@ -17,7 +17,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libwsort.so")
-SOURCES = ["api.cu", "sort.cu", "decode.cu", "formats.cu", "noalloc.cu", "server.cu"]
+SOURCES = ["api.cu", "sort.cu", "decode.cu", "formats.cu", "raster.cu", "noalloc.cu", "server.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -396,6 +396,29 @@ static int launch_jobs(ws_ctx* ctx, const std::vector<uint32_t>& ns, int njobs, 
     return WS_OK;
 }
 
+// A stable sort of n given 16-bit keys (every element kept) in one launch:
+// order[] receives element indices by (key, index), sorted[] the keys.
+int run_given_keys(ws_ctx* ctx, const uint16_t* keys, uint32_t n, uint32_t* order, uint32_t* sorted, uint32_t* count,
+                   cudaStream_t stream) {
+    std::vector<uint32_t> ns(1, n);
+    return launch_jobs(
+        ctx, ns, 1,
+        [&](JobDesc* hj, char* scratch) {
+            char* at = scratch + align_up(sizeof(LaunchCtl) + sizeof(JobCtl), 256);
+            JobDesc& d = hj[0];
+            std::memset(&d, 0, sizeof(d));
+            d.kind = kJobKeys;
+            d.n = n;
+            d.keys_in = keys;
+            d.order = order;
+            d.keys = sorted;
+            d.count = count;
+            assign_scratch(d, n, ctx->params, at);
+            d.ctl = reinterpret_cast<uint32_t*>(scratch + sizeof(LaunchCtl));
+        },
+        stream);
+}
+
 int run_batch(ws_ctx* ctx, const ws_job* jobs, int njobs, cudaStream_t stream) {
     std::vector<uint32_t> ns(njobs);
     for (int j = 0; j < njobs; ++j) ns[j] = jobs[j].cloud->n;
@@ -484,6 +507,8 @@ extern "C" int ws_destroy(ws_ctx* ctx) {
     ctx->items_d.release();
     ctx->out_d.release();
     ctx->thr_d.release();
+    ctx->draw_d.release();
+    ctx->pairs_d.release();
     ctx->jobs_h.release();
     ctx->items_h.release();
     ctx->count_h.release();

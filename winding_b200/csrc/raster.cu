@@ -1,0 +1,466 @@
+// Drawing sorted splats into a headless image: the reference's splat draw
+// (vs / fs, src/render/splats.js:252-312) as CUDA, writing an RGBA f32
+// buffer in device memory instead of a WebGPU colour target.
+//
+// What is drawn, pinned (the reference leaves rasterisation, varyings and
+// transcendental precision to the GPU; this fixes one answer, and the CPU
+// oracle computes the same one):
+//   - per splat i = order[j], in order (far first): view and clip as the
+//     keys phase computes them; the footprint (xx, xy, yy) + 0.3 on the
+//     diagonal; the ellipse's axes from its eigen-decomposition as the vertex
+//     shader writes it (mid, radius, major, minor; the axis normalised as
+//     v / sqrt(x x + y y)); half-lengths min(sqrt(2 major), 1024) and
+//     min(sqrt(2 minor), 1024); reach = log(255 a) from a table (the f32
+//     nearest the real logarithm of each of the 256 possible 255 a); the
+//     quad's extent sqrt(min(reach, 4)) in units of the axes. A splat with
+//     minor <= 0 or reach <= 0 is not drawn, as the vertex shader leaves it
+//     off screen.
+//   - the quad covers the pixels whose centre (px + 0.5, py + 0.5) maps into
+//     [-e, e]^2 under the quad's own inverse: offset = (d . axis / la,
+//     d . perp / lc), d the centre's offset from the splat's centre in
+//     pixels (y up, as clip space). That offset is the fragment's varying
+//     (it varies linearly over the quad, as the reference interpolates it).
+//     Pixels are only considered within the quad's bounding box widened by a
+//     pixel, the same box on both sides.
+//   - the fragment: alpha = min(0.99, exp(-dot(offset, offset)) a), dropped
+//     below 1/255; colour = decodeSRGB(rgb bytes) from a table (the f32
+//     nearest ((c + 0.055) / 1.055)^2.4 above 0.04045, c / 12.92 below, c
+//     = byte / 255); blended premultiplied over what the image holds:
+//     dst = src + dst (1 - alpha) for colour and alpha, as the reference's
+//     blend state (one, one-minus-src-alpha). exp is exp_pinned below.
+//   - no fog and no depth test (a headless image has no opaque scene).
+// Every f32 operation is separately rounded (-fmad=false).
+//
+// The B200 shape: a prepare kernel (one thread per drawn splat) writes each
+// splat's quad and the 16 x 16-pixel tiles its box touches; an exclusive
+// scan gives each splat its run of (tile, splat) pairs, emitted in splat
+// order; the library's own stable sort orders the pairs by tile (a 16-bit
+// key; same-tile pairs keep splat order); one CTA per tile then blends its
+// splats in order, 256 pixels a CTA, splat records staged in shared memory.
+#include "wsort.h"
+#include "wsort_dev.cuh"
+#include "wsort_host.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+namespace wsort {
+
+int run_given_keys(ws_ctx* ctx, const uint16_t* keys, uint32_t n, uint32_t* order, uint32_t* sorted, uint32_t* count,
+                   cudaStream_t stream);
+
+namespace {
+
+constexpr int kTilePx = 16;
+constexpr uint32_t kMaxSide = 4096;   // tiles of one image fit the 16-bit sort key
+constexpr int kScanBlock = 1024;
+constexpr int kScanItems = 4;         // elements a scan thread covers
+constexpr int kScanTile = kScanBlock * kScanItems;
+
+// One drawn splat's quad, in pixels (x right, y down for the centre and the
+// pixel box; the axes are in clip space's y-up pixel units).
+struct alignas(16) Quad {
+    float cx, cy;          // centre
+    float ax, ay;          // unit major axis
+    float la, lc;          // half-lengths along the major and minor axes
+    float qm;              // extent in units of the axes
+    float a;               // alpha
+    float r, g, b;         // decoded colour
+    int x0, x1, y0, y1;    // candidate pixels (x0 > x1: nothing)
+    float pad;
+};
+
+// exp for the fragment's falloff: Cody and Waite's reduction (ln 2 split as
+// 355/512 - 2.12194440e-4, Software Manual for the Elementary Functions,
+// 1980), exp(r) by its Taylor polynomial to r^7 / 7! in Horner form, and 2^k
+// from the exponent bits; every operation separately rounded.
+__device__ __forceinline__ float exp_pinned(float x) {
+    if (x != x) return x;
+    if (x < -104.0f) return 0.0f;
+    if (x > 88.0f) return INFINITY;
+    const float k = rintf(fmul(x, 1.44269504f));
+    const float r = fsub(fsub(x, fmul(k, 0.693359375f)), fmul(k, -2.12194440e-4f));
+    float p = 1.98412698e-4f;
+    p = fadd(fmul(p, r), 1.38888889e-3f);
+    p = fadd(fmul(p, r), 8.33333333e-3f);
+    p = fadd(fmul(p, r), 4.16666667e-2f);
+    p = fadd(fmul(p, r), 1.66666667e-1f);
+    p = fadd(fmul(p, r), 0.5f);
+    p = fadd(fmul(p, r), 1.0f);
+    p = fadd(fmul(p, r), 1.0f);
+    int ki = (int)k;
+    if (ki < -126) {
+        p = fmul(p, __int_as_float((ki + 126 + 127) << 23));
+        ki = -126;
+    }
+    return fmul(p, __int_as_float((ki + 127) << 23));
+}
+
+// The quad of instance j (order[j]), or an empty one. tables: srgb[256]
+// then reach[256].
+__global__ void __launch_bounds__(256) prepare_kernel(const JobDesc* __restrict__ jd, const uint32_t* __restrict__ order,
+                                                      const uint32_t* __restrict__ count,
+                                                      const uint32_t* __restrict__ shaded,
+                                                      const float* __restrict__ tables, uint32_t n, uint32_t width,
+                                                      uint32_t height, Quad* __restrict__ quads,
+                                                      uint32_t* __restrict__ ntiles) {
+    __shared__ ViewConsts c;
+    if (threadIdx.x == 0) make_consts(*jd, c);
+    __syncthreads();
+    const JobDesc& J = *jd;
+    const uint32_t drawn = min(*count, n);
+    const float half_w = fmul(0.5f, (float)width), half_h = fmul(0.5f, (float)height);
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        Quad q;
+        q.x0 = 1;
+        q.x1 = 0;
+        q.y0 = 1;
+        q.y1 = 0;
+        uint32_t tiles = 0;
+        if (j < drawn) {
+            const uint32_t i = order[j];
+            const float4 p = J.centers[i];
+            float view[4];
+            view_of(c, p.x, p.y, p.z, view);
+            const float* P = c.proj;
+            float clip[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                clip[k] = fadd(fadd(fadd(fmul(P[k], view[0]), fmul(P[4 + k], view[1])), fmul(P[8 + k], view[2])),
+                               fmul(P[12 + k], view[3]));
+            const float2 s0 = J.cov[3 * (size_t)i], s1 = J.cov[3 * (size_t)i + 1], s2 = J.cov[3 * (size_t)i + 2];
+            const float s[6] = {s0.x, s0.y, s1.x, s1.y, s2.x, s2.y};
+            float fxx, fxy, fyy;
+            footprint2d(c, view, s, &fxx, &fxy, &fyy);
+            const float a = fadd(fxx, 0.3f), b = fxy, cc = fadd(fyy, 0.3f);
+            const float mid = fmul(0.5f, fadd(a, cc));
+            const float hd = fmul(0.5f, fsub(a, cc));
+            const float radius = __fsqrt_rn(fadd(fmul(hd, hd), fmul(b, b)));
+            const float major = fadd(mid, radius), minor = fsub(mid, radius);
+            const uint32_t word = shaded ? shaded[i] : __float_as_uint(p.w);
+            const float reach = tables[256 + (word >> 24)];
+            if (minor > 0.0f && reach > 0.0f) {
+                float ax = 1.0f, ay = 0.0f;
+                if (fabsf(b) > 1e-12f) {
+                    const float ey = fsub(major, a);
+                    const float len = __fsqrt_rn(fadd(fmul(b, b), fmul(ey, ey)));
+                    ax = fdiv(b, len);
+                    ay = fdiv(ey, len);
+                } else if (cc > a) {
+                    ax = 0.0f;
+                    ay = 1.0f;
+                }
+                q.ax = ax;
+                q.ay = ay;
+                q.la = fminf(__fsqrt_rn(fmul(2.0f, major)), 1024.0f);
+                q.lc = fminf(__fsqrt_rn(fmul(2.0f, minor)), 1024.0f);
+                q.qm = __fsqrt_rn(fminf(reach, 4.0f));
+                q.cx = fmul(fadd(fdiv(clip[0], clip[3]), 1.0f), half_w);
+                q.cy = fmul(fsub(1.0f, fdiv(clip[1], clip[3])), half_h);
+                const float hx = fmul(q.qm, fadd(fmul(q.la, fabsf(ax)), fmul(q.lc, fabsf(ay))));
+                const float hy = fmul(q.qm, fadd(fmul(q.la, fabsf(ay)), fmul(q.lc, fabsf(ax))));
+                q.a = fdiv((float)(word >> 24), 255.0f);
+                q.r = tables[word & 255u];
+                q.g = tables[(word >> 8) & 255u];
+                q.b = tables[(word >> 16) & 255u];
+                if (isfinite(q.cx) && isfinite(q.cy) && isfinite(hx) && isfinite(hy)) {
+                    const float fx0 = fmaxf(floorf(fsub(fsub(q.cx, hx), 1.5f)), 0.0f);
+                    const float fx1 = fminf(ceilf(fadd(fadd(q.cx, hx), 0.5f)), (float)(width - 1));
+                    const float fy0 = fmaxf(floorf(fsub(fsub(q.cy, hy), 1.5f)), 0.0f);
+                    const float fy1 = fminf(ceilf(fadd(fadd(q.cy, hy), 0.5f)), (float)(height - 1));
+                    if (fx0 <= fx1 && fy0 <= fy1) {
+                        q.x0 = (int)fx0;
+                        q.x1 = (int)fx1;
+                        q.y0 = (int)fy0;
+                        q.y1 = (int)fy1;
+                        tiles = (uint32_t)((q.x1 / kTilePx - q.x0 / kTilePx + 1) * (q.y1 / kTilePx - q.y0 / kTilePx + 1));
+                    }
+                }
+            }
+        }
+        quads[j] = q;
+        ntiles[j] = tiles;
+    }
+}
+
+// Exclusive scan of n words in three steps: per-4096 block scan with its
+// block sum, a scan of the block sums (one CTA; also their 64-bit total),
+// and the block offsets added.
+__global__ void __launch_bounds__(kScanBlock) scan_blocks_kernel(const uint32_t* in, uint32_t* out, uint32_t n,
+                                                                 uint32_t* sums) {
+    __shared__ uint32_t warp_sums[kScanBlock / 32];
+    const uint32_t base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+    uint32_t v[kScanItems], local = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        v[k] = base + k < n ? in[base + k] : 0u;
+        local += v[k];
+    }
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t x = local;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= (uint32_t)o) x += y;
+    }
+    if (lane == 31) warp_sums[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = warp_sums[lane];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= (uint32_t)o) w += y;
+        }
+        warp_sums[lane] = w;
+    }
+    __syncthreads();
+    uint32_t run = (warp ? warp_sums[warp - 1] : 0u) + x - local;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        if (base + k < n) out[base + k] = run;
+        run += v[k];
+    }
+    if (threadIdx.x == kScanBlock - 1) sums[blockIdx.x] = warp_sums[31];
+}
+
+__global__ void __launch_bounds__(kScanBlock) scan_sums_kernel(uint32_t* sums, uint32_t nb, unsigned long long* total) {
+    __shared__ uint32_t warp_sums[kScanBlock / 32];
+    __shared__ unsigned long long carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (uint32_t c0 = 0; c0 < nb; c0 += kScanBlock) {
+        const uint32_t k = c0 + threadIdx.x;
+        const uint32_t v = k < nb ? sums[k] : 0u;
+        uint32_t x = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= (uint32_t)o) x += y;
+        }
+        if (lane == 31) warp_sums[warp] = x;
+        __syncthreads();
+        if (warp == 0) {
+            uint32_t w = warp_sums[lane];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+                if (lane >= (uint32_t)o) w += y;
+            }
+            warp_sums[lane] = w;
+        }
+        __syncthreads();
+        const unsigned long long before = carry;
+        if (k < nb) sums[k] = (uint32_t)(before + (warp ? warp_sums[warp - 1] : 0u) + x - v);
+        __syncthreads();
+        if (threadIdx.x == 0) carry = before + warp_sums[31];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *total = carry;
+}
+
+__global__ void __launch_bounds__(256) add_offsets_kernel(uint32_t* out, uint32_t n, const uint32_t* sums) {
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+        out[k] += sums[k / kScanTile];
+}
+
+// The (tile, splat) pairs of every drawn splat, in splat order.
+__global__ void __launch_bounds__(256) emit_kernel(const Quad* __restrict__ quads, const uint32_t* __restrict__ ntiles,
+                                                   const uint32_t* __restrict__ offsets, uint32_t n,
+                                                   uint32_t tiles_x, uint16_t* __restrict__ keys,
+                                                   uint32_t* __restrict__ owner) {
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        if (!ntiles[j]) continue;
+        const Quad q = quads[j];
+        uint32_t at = offsets[j];
+        for (int ty = q.y0 / kTilePx; ty <= q.y1 / kTilePx; ++ty)
+            for (int tx = q.x0 / kTilePx; tx <= q.x1 / kTilePx; ++tx) {
+                keys[at] = (uint16_t)(ty * tiles_x + tx);
+                owner[at] = j;
+                ++at;
+            }
+    }
+}
+
+// Each tile's run [start, end) in the pairs sorted by tile.
+__global__ void __launch_bounds__(256) ranges_kernel(const uint32_t* __restrict__ skeys, uint32_t npairs,
+                                                     uint2* __restrict__ range) {
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < npairs; k += gridDim.x * blockDim.x) {
+        const uint32_t t = skeys[k];
+        if (k == 0 || skeys[k - 1] != t) range[t].x = k;
+        if (k == npairs - 1 || skeys[k + 1] != t) range[t].y = k + 1;
+    }
+}
+
+// One CTA a tile, one thread a pixel: the tile's splats in order, staged in
+// shared memory 256 at a time, blended over the image.
+__global__ void __launch_bounds__(256) blend_kernel(const Quad* __restrict__ quads, const uint32_t* __restrict__ owner,
+                                                    const uint32_t* __restrict__ sorted, const uint2* __restrict__ range,
+                                                    uint32_t width, uint32_t height, uint32_t tiles_x,
+                                                    float4* __restrict__ image) {
+    __shared__ Quad staged[256];
+    const uint32_t tile = blockIdx.x;
+    const int px = (int)((tile % tiles_x) * kTilePx + (threadIdx.x & 15));
+    const int py = (int)((tile / tiles_x) * kTilePx + (threadIdx.x >> 4));
+    const bool inside = px < (int)width && py < (int)height;
+    float4 dst = inside ? image[(size_t)py * width + px] : make_float4(0, 0, 0, 0);
+    const float fx = fadd((float)px, 0.5f), fy = fadd((float)py, 0.5f);
+    const uint2 rg = range[tile];
+    for (uint32_t c0 = rg.x; c0 < rg.y; c0 += 256) {
+        const uint32_t k = c0 + threadIdx.x;
+        __syncthreads();
+        if (k < rg.y) staged[threadIdx.x] = quads[owner[sorted[k]]];
+        __syncthreads();
+        const uint32_t m = min(256u, rg.y - c0);
+        for (uint32_t e = 0; e < m; ++e) {
+            const Quad& q = staged[e];
+            if (px < q.x0 || px > q.x1 || py < q.y0 || py > q.y1) continue;
+            const float ex = fsub(fx, q.cx), ey = fsub(q.cy, fy);
+            const float ox = fdiv(fadd(fmul(ex, q.ax), fmul(ey, q.ay)), q.la);
+            const float oy = fdiv(fsub(fmul(ex, q.ay), fmul(ey, q.ax)), q.lc);
+            if (!(fabsf(ox) <= q.qm && fabsf(oy) <= q.qm)) continue;
+            const float d2 = fadd(fmul(ox, ox), fmul(oy, oy));
+            const float alpha = fminf(0.99f, fmul(exp_pinned(-d2), q.a));
+            if (alpha < 1.0f / 255.0f) continue;
+            const float om = fsub(1.0f, alpha);
+            dst.x = fadd(fmul(q.r, alpha), fmul(dst.x, om));
+            dst.y = fadd(fmul(q.g, alpha), fmul(dst.y, om));
+            dst.z = fadd(fmul(q.b, alpha), fmul(dst.z, om));
+            dst.w = fadd(alpha, fmul(dst.w, om));
+        }
+    }
+    if (inside) image[(size_t)py * width + px] = dst;
+}
+
+// decodeSRGB of byte / 255 and log(255 byte / 255), as f32 (see the head).
+const std::vector<float>& draw_tables() {
+    static std::vector<float> t;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        t.assign(512, 0.0f);
+        for (int b = 0; b < 256; ++b) {
+            const float c = (float)b / 255.0f;
+            if (c <= 0.04045f) {
+                t[b] = c / 12.92f;
+            } else {
+                const float base = (c + 0.055f) / 1.055f;
+                t[b] = (float)std::pow((double)base, 2.4);
+            }
+            const float x = 255.0f * c;
+            t[256 + b] = (float)std::log((double)x);
+        }
+    });
+    return t;
+}
+
+}  // namespace
+}  // namespace wsort
+
+using namespace wsort;
+
+extern "C" int ws_draw_tables(float* srgb, float* reach) {
+    if (!srgb || !reach) return WS_ERR_ARG;
+    const std::vector<float>& t = draw_tables();
+    std::memcpy(srgb, t.data(), 256 * sizeof(float));
+    std::memcpy(reach, t.data() + 256, 256 * sizeof(float));
+    return WS_OK;
+}
+
+extern "C" int ws_draw(ws_ctx* ctx, const ws_cloud* cloud, const ws_view* view, const uint32_t* order,
+                       const uint32_t* count, const uint32_t* shaded, float* image, uint32_t width, uint32_t height,
+                       void* stream_p) {
+    if (!ctx) return WS_ERR_ARG;
+    if (!cloud || cloud->magic != kCloudMagic) return set_error(ctx, WS_ERR_ARG, "ws_draw: not a cloud");
+    if (!cloud->alive) return set_error(ctx, WS_ERR_UNLOADED, "addSplats: these splats were unloaded; remove the node first");
+    if (!view || !order || !count || !image) return set_error(ctx, WS_ERR_ARG, "ws_draw: null argument");
+    if (width == 0 || height == 0 || width > kMaxSide || height > kMaxSide)
+        return set_error(ctx, WS_ERR_ARG, "ws_draw: an image of %u x %u; 1 to %u pixels a side", width, height, kMaxSide);
+    if (view->viewport[0] != (float)width || view->viewport[1] != (float)height)
+        return set_error(ctx, WS_ERR_ARG, "ws_draw: the view's viewport is %g x %g, the image %u x %u",
+                         (double)view->viewport[0], (double)view->viewport[1], width, height);
+    if (reinterpret_cast<uintptr_t>(image) % 16)
+        return set_error(ctx, WS_ERR_ARG, "ws_draw: the image is not 16-byte aligned");
+    cudaSetDevice(ctx->device);
+    cudaStream_t stream = stream_p ? static_cast<cudaStream_t>(stream_p) : ctx->stream;
+    const uint32_t n = cloud->n;
+    const uint32_t tiles_x = (width + kTilePx - 1) / kTilePx, tiles_y = (height + kTilePx - 1) / kTilePx;
+    const uint32_t tiles = tiles_x * tiles_y;
+    const uint32_t nb = (n + kScanTile - 1) / kScanTile;
+    cudaError_t e;
+    // Scratch: the job table, tables, quads, per-splat tile counts and offsets,
+    // block sums, 64-bit total, tile ranges.
+    auto up = [](size_t v) { return (v + 255) / 256 * 256; };
+    const size_t o_job = 0, o_tab = up(sizeof(JobDesc)), o_quad = o_tab + up(512 * 4);
+    const size_t o_cnt = o_quad + up((size_t)n * sizeof(Quad)), o_off = o_cnt + up((size_t)n * 4);
+    const size_t o_sums = o_off + up((size_t)n * 4), o_tot = o_sums + up((size_t)nb * 4 + 4);
+    const size_t o_rng = o_tot + 256, fixed = o_rng + up((size_t)tiles * 8);
+    if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return cuda_error(ctx, e, "ws_draw");
+    if ((e = ctx->draw_d.ensure(fixed)) != cudaSuccess) return cuda_error(ctx, e, "ws_draw scratch");
+    char* base = static_cast<char*>(ctx->draw_d.p);
+    JobDesc jd;
+    std::memset(&jd, 0, sizeof(jd));
+    jd.centers = cloud->centers;
+    jd.cov = cloud->cov;
+    for (int k = 0; k < 3; ++k) {
+        jd.bmin[k] = cloud->bmin[k];
+        jd.bmax[k] = cloud->bmax[k];
+    }
+    jd.n = n;
+    std::memcpy(jd.mv, view->model_view, sizeof(jd.mv));
+    std::memcpy(jd.proj, view->projection, sizeof(jd.proj));
+    jd.viewport[0] = view->viewport[0];
+    jd.viewport[1] = view->viewport[1];
+    jd.cull = view->cull;
+    const std::vector<float>& tab = draw_tables();
+    if ((e = cudaMemcpyAsync(base + o_job, &jd, sizeof(jd), cudaMemcpyHostToDevice, stream)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(base + o_tab, tab.data(), 512 * 4, cudaMemcpyHostToDevice, stream)) != cudaSuccess ||
+        (e = cudaMemsetAsync(base + o_rng, 0, (size_t)tiles * 8, stream)) != cudaSuccess)
+        return cuda_error(ctx, e, "ws_draw");
+    Quad* quads = reinterpret_cast<Quad*>(base + o_quad);
+    uint32_t* cnt = reinterpret_cast<uint32_t*>(base + o_cnt);
+    uint32_t* off = reinterpret_cast<uint32_t*>(base + o_off);
+    uint32_t* sums = reinterpret_cast<uint32_t*>(base + o_sums);
+    unsigned long long* total = reinterpret_cast<unsigned long long*>(base + o_tot);
+    uint2* range = reinterpret_cast<uint2*>(base + o_rng);
+    const uint32_t g = std::max(1u, std::min((n + 255) / 256, (uint32_t)ctx->sms * 8));
+    prepare_kernel<<<g, 256, 0, stream>>>(reinterpret_cast<const JobDesc*>(base + o_job), order, count, shaded,
+                                          reinterpret_cast<const float*>(base + o_tab), n, width, height, quads, cnt);
+    scan_blocks_kernel<<<std::max(nb, 1u), kScanBlock, 0, stream>>>(cnt, off, n, sums);
+    scan_sums_kernel<<<1, kScanBlock, 0, stream>>>(sums, std::max(nb, 1u), total);
+    add_offsets_kernel<<<g, 256, 0, stream>>>(off, n, sums);
+    unsigned long long pairs64 = 0;
+    if ((e = cudaGetLastError()) != cudaSuccess ||
+        (e = cudaMemcpyAsync(&pairs64, total, 8, cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(stream)) != cudaSuccess)
+        return cuda_error(ctx, e, "ws_draw");
+    if (pairs64 == 0) return WS_OK;
+    if (pairs64 > WS_MAX_SPLATS)
+        return set_error(ctx, WS_ERR_CAPACITY, "ws_draw: %llu (tile, splat) pairs, more than %u", pairs64,
+                         WS_MAX_SPLATS);
+    const uint32_t pairs = (uint32_t)pairs64;
+    // The pair arrays, in a buffer of their own (growing it keeps the first):
+    // keys, owners, sorted order, sorted keys, count.
+    const size_t o_keys = 0, o_own = o_keys + up((size_t)pairs * 2), o_sorted = o_own + up((size_t)pairs * 4);
+    const size_t o_skeys = o_sorted + up((size_t)pairs * 4), o_pc = o_skeys + up((size_t)pairs * 4);
+    if ((e = ctx->pairs_d.ensure(o_pc + 256)) != cudaSuccess) return cuda_error(ctx, e, "ws_draw scratch");
+    char* pb = static_cast<char*>(ctx->pairs_d.p);
+    uint16_t* keys = reinterpret_cast<uint16_t*>(pb + o_keys);
+    uint32_t* owner = reinterpret_cast<uint32_t*>(pb + o_own);
+    uint32_t* sorted = reinterpret_cast<uint32_t*>(pb + o_sorted);
+    uint32_t* skeys = reinterpret_cast<uint32_t*>(pb + o_skeys);
+    uint32_t* pcount = reinterpret_cast<uint32_t*>(pb + o_pc);
+    emit_kernel<<<g, 256, 0, stream>>>(quads, cnt, off, n, tiles_x, keys, owner);
+    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_error(ctx, e, "ws_draw");
+    int rc = run_given_keys(ctx, keys, pairs, sorted, skeys, pcount, stream);
+    if (rc) return rc;
+    const uint32_t gp = std::max(1u, std::min((pairs + 255) / 256, (uint32_t)ctx->sms * 8));
+    ranges_kernel<<<gp, 256, 0, stream>>>(skeys, pairs, range);
+    blend_kernel<<<tiles, 256, 0, stream>>>(quads, owner, sorted, range, width, height, tiles_x,
+                                            reinterpret_cast<float4*>(image));
+    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_error(ctx, e, "ws_draw");
+    return WS_OK;
+}

@@ -383,6 +383,31 @@ __device__ void particle_keys_tile(const JobDesc& J, uint32_t tile, SortSmem<IPT
     J.cnt_lo[(size_t)tid * J.tiles + tile] = sm.hist[tid];
 }
 
+// Keys of one tile of a job whose keys are given (kind kJobKeys): every
+// element survives, its key as given.
+template <int IPT>
+__device__ void given_keys_tile(const JobDesc& J, uint32_t tile, SortSmem<IPT>& sm) {
+    constexpr uint32_t T = SortSmem<IPT>::kTile;
+    const int tid = threadIdx.x;
+    const uint32_t lane = lane_id();
+    sm.hist[tid] = 0;
+    __syncthreads();
+    const uint32_t base = tile * T;
+    const uint32_t n = J.n;
+#pragma unroll 4
+    for (uint32_t k = 0; k < T; k += kThreads) {
+        const uint32_t i = base + k + tid;
+        const bool on = i < n;
+        const uint32_t key = on ? J.keys_in[i] : 0u;
+        if (on) J.k16[i] = (uint16_t)key;
+        const uint32_t b = __ballot_sync(0xffffffffu, on);
+        if (lane == 0 && on) J.mask[i >> 5] = b;
+        if (on) atomicAdd(&sm.hist[key & 255u], 1u);
+    }
+    __syncthreads();
+    J.cnt_lo[(size_t)tid * J.tiles + tile] = sm.hist[tid];
+}
+
 // The start of each digit in a pass's output (an exclusive scan of the
 // pass's digit totals), cached per (job, pass) for the CTA's next items.
 template <int IPT>
@@ -692,6 +717,8 @@ __global__ void __launch_bounds__(kThreads, MINB) sort_kernel(const JobDesc* __r
                 case kPhaseKeys:
                     if (J.kind == kJobParticles)
                         particle_keys_tile(J, tile, sm);
+                    else if (J.kind == kJobKeys)
+                        given_keys_tile(J, tile, sm);
                     else
                         keys_tile(J, job, tile, sm);
                     break;

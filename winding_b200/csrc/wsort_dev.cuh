@@ -87,9 +87,11 @@ struct alignas(16) JobDesc {
     uint32_t* shaded;           // per splat: its colour word as seen from the eye (survivors only)
     uint32_t sh_degree;         // 1, 2 or 3
     uint32_t sh_words;          // 32-bit words a splat: ceil(3 x coefficients / 2)
+    // given keys (kind == kJobKeys): n 16-bit keys, every element a survivor
+    const uint16_t* keys_in;
 };
 
-constexpr uint32_t kJobSplats = 0, kJobParticles = 1;
+constexpr uint32_t kJobSplats = 0, kJobParticles = 1, kJobKeys = 2;
 // Depth buckets of an alpha emitter's sort (render/particles.js:44-48):
 // 12 bits of log2 depth over [2^-10, 2^20].
 constexpr uint32_t kParticleBuckets = 4096u;
@@ -310,12 +312,13 @@ __device__ __forceinline__ bool in_frustum(const ViewConsts& c, const float view
     return !(view[2] >= 0.0f || clip[2] > w || fabsf(clip[0]) > fmul(1.3f, w) || fabsf(clip[1]) > fmul(1.3f, w));
 }
 
-// The footprint cull (render/splats.js:172-178 with footprint :102-124).
-// Returns true when the splat is kept. s[6] is its covariance. J's entries
-// J[0][1] and J[1][0] are zero in both of its forms, so their products with
-// the (finite) model-view are zeros and are left out of T = J W.
-__device__ __forceinline__ bool footprint_keeps(const ViewConsts& c, const float view[4], const float s[6],
-                                                float alpha) {
+// footprint (render/splats.js:102-124): the 2D covariance (xx, xy, yy) in
+// pixels, before the third of a pixel the draw adds. s[6] is the splat's
+// covariance. J's entries J[0][1] and J[1][0] are zero in both of its forms,
+// so their products with the (finite) model-view are zeros and are left out
+// of T = J W.
+__device__ __forceinline__ void footprint2d(const ViewConsts& c, const float view[4], const float s[6], float* pxx,
+                                            float* pxy, float* pyy) {
     float J00 = c.fx, J11 = c.fy, J02 = 0.0f, J12 = 0.0f;
     if (c.persp) {
         const float d = -view[2];
@@ -343,6 +346,16 @@ __device__ __forceinline__ bool footprint_keeps(const ViewConsts& c, const float
     const float fxx = fadd(fadd(fmul(U[0][0], T[0][0]), fmul(U[0][1], T[0][1])), fmul(U[0][2], T[0][2]));
     const float fxy = fadd(fadd(fmul(U[1][0], T[0][0]), fmul(U[1][1], T[0][1])), fmul(U[1][2], T[0][2]));
     const float fyy = fadd(fadd(fmul(U[1][0], T[1][0]), fmul(U[1][1], T[1][1])), fmul(U[1][2], T[1][2]));
+    *pxx = fxx;
+    *pxy = fxy;
+    *pyy = fyy;
+}
+
+// The footprint cull (render/splats.js:172-178): true when the splat is kept.
+__device__ __forceinline__ bool footprint_keeps(const ViewConsts& c, const float view[4], const float s[6],
+                                                float alpha) {
+    float fxx, fxy, fyy;
+    footprint2d(c, view, s, &fxx, &fxy, &fyy);
     const float det = fsub(fmul(fadd(fxx, 0.3f), fadd(fyy, 0.3f)), fmul(fxy, fxy));
     const float area = fmul(6.2831853f, __fsqrt_rn(fmaxf(det, 0.0f)));
     return !(fmul(alpha, area) < c.cull);

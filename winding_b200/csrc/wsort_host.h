@@ -64,6 +64,7 @@ struct ws_ctx {
     int trace_grid = 0;
     std::vector<struct ws_cloud*> freed;   // freed clouds, kept as refusable handles
     wsort::DevBuf thr_d;              // particle depth thresholds, uploaded on first use
+    wsort::DevBuf draw_d, pairs_d;    // ws_draw: per-splat quads and scans; (tile, splat) pairs
 };
 
 struct ws_cloud {

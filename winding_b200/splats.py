@@ -149,6 +149,14 @@ class Context:
             sh[j].shaded = shaded
         self.check(self.lib.ws_sort_batch_shaded(self.handle, len(jobs), arr, sh, stream))
 
+    def draw(self, splats: "Splats", view: WsView, order_ptr: int, count_ptr: int, image_ptr: int, width: int,
+             height: int, shaded_ptr: int | None = None, stream: int | None = None) -> None:
+        """Blends the first *count splats of a sort's order (device pointers)
+        over an RGBA f32 device image of width x height (ws_draw)."""
+        splats._check_alive()
+        self.check(self.lib.ws_draw(self.handle, splats.handle, ctypes.byref(view), order_ptr, count_ptr,
+                                    shaded_ptr, image_ptr, int(width), int(height), stream))
+
     def sort_particles(self, emitters: list[tuple], stream: int | None = None) -> None:
         """emitters: (pool_ptr, offset, capacity, eye, forward, order_ptr,
         keys_ptr or None, count_ptr), pointers into device memory; one launch
@@ -310,6 +318,14 @@ class Splats:
         if not self.unloaded:
             self.ctx.check(self.ctx.lib.ws_cloud_free(self.handle))
             self.unloaded = True
+
+
+def draw_tables():
+    """(srgb, reach): the draw's decodeSRGB and log tables, 256 f32 each."""
+    srgb = np.zeros(256, np.float32)
+    reach = np.zeros(256, np.float32)
+    check(_lib.load().ws_draw_tables(srgb.ctypes.data_as(_lib.f32p), reach.ctypes.data_as(_lib.f32p)))
+    return srgb, reach
 
 
 # 32-bit words a splat's harmonics take, by degree (scene/splats.js:43-47).

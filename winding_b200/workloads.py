@@ -200,3 +200,65 @@ def poisson_arrivals(rate_hz: float, duration_s: float, seed: int = 5) -> np.nda
     n = int(rate_hz * duration_s * 1.5) + 16
     t = np.cumsum(rng.exponential(1.0 / rate_hz, size=n))
     return t[t < duration_s]
+
+
+# ----------------------------------------------------------------- particles
+
+def particle_pool(n: int, seed: int = 7, spread: float = 20.0, dead: float = 0.15) -> np.ndarray:
+    """A pool of n 32-byte particles (position, age, velocity, lifetime as
+    f32; render/particles.js:51-56): positions N(0, spread), lifetimes
+    U[0.5, 4] s, a `dead` share past their lifetime and some never used."""
+    rng = np.random.default_rng(seed)
+    pool = np.zeros((n, 8), np.float32)
+    pool[:, 0:3] = rng.normal(size=(n, 3)) * spread
+    pool[:, 4:7] = rng.normal(size=(n, 3))
+    pool[:, 7] = rng.uniform(0.5, 4.0, size=n)
+    pool[:, 3] = pool[:, 7] * rng.uniform(0.0, 1.0, size=n)
+    gone = rng.random(n) < dead
+    pool[gone, 3] = pool[gone, 7] + 0.1
+    return pool
+
+
+def emitter_rings(emitters: int = 64, lo: int = 1_000, hi: int = 200_000, seed: int = 8) -> list[tuple[int, int]]:
+    """(offset, capacity) of `emitters` rings laid end to end in one pool,
+    capacities log-uniform in [lo, hi]."""
+    rng = np.random.default_rng(seed)
+    caps = np.exp(rng.uniform(math.log(lo), math.log(hi), size=emitters)).astype(np.int64)
+    offs = np.concatenate([[0], np.cumsum(caps)[:-1]])
+    return [(int(o), int(c)) for o, c in zip(offs, caps)]
+
+
+# ----------------------------------------------------------------- harmonics and .ply
+
+SH_COEFFICIENTS = (0, 3, 8, 15)
+
+
+def harmonics_words(n: int, degree: int, seed: int = 9, scale: float = 0.3) -> np.ndarray:
+    """Random harmonics of `degree` for n splats, packed as the reference
+    packs them (ceil(3 c / 2) words a splat of half floats, scene/splats.js:306-333)."""
+    rng = np.random.default_rng(seed)
+    c = SH_COEFFICIENTS[degree]
+    per = (3 * c + 1) // 2
+    halves = np.zeros((n, per * 2), np.float16)
+    halves[:, :3 * c] = rng.uniform(-scale, scale, size=(n, 3 * c)).astype(np.float16)
+    return halves.view(np.uint16).reshape(-1).view(np.uint32).copy()
+
+
+def ply_bytes(n: int, degree: int = 0, seed: int = 10) -> bytes:
+    """A binary .ply as training writes it (scene/splats.js:6-13): x y z,
+    normals, f_dc_0..2, opacity, scale_0..2, rot_0..3 and 9, 24 or 45
+    f_rest_ properties, all float."""
+    rng = np.random.default_rng(seed)
+    rest = 3 * SH_COEFFICIENTS[degree]
+    names = ["x", "y", "z", "nx", "ny", "nz", "f_dc_0", "f_dc_1", "f_dc_2", "opacity",
+             "scale_0", "scale_1", "scale_2", "rot_0", "rot_1", "rot_2", "rot_3"] + [f"f_rest_{k}" for k in range(rest)]
+    cols = np.zeros((n, len(names)), np.float32)
+    cols[:, 0:3] = rng.normal(0, 10, (n, 3))
+    cols[:, 6:9] = rng.normal(0, 1.5, (n, 3))
+    cols[:, 9] = rng.normal(0, 4, n)
+    cols[:, 10:13] = rng.normal(-4, 1, (n, 3))
+    cols[:, 13:17] = rng.normal(size=(n, 4))
+    cols[:, 17:] = rng.normal(0, 0.3, (n, rest))
+    head = ("ply\nformat binary_little_endian 1.0\nelement vertex %d\n" % n
+            + "".join(f"property float {p}\n" for p in names) + "end_header\n").encode()
+    return head + cols.astype("<f4").tobytes()
