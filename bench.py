@@ -472,7 +472,8 @@ def suite(ctx, torch, flush, args):
         out["served-16"] = served(ctx, args)
     except Exception as exc:
         out["served-16"] = {"error": f"{type(exc).__name__}: {exc}"}
-    for name, fn in (("particles-64", particles_suite), ("shade-1M", shade_suite), ("decode", decode_suite)):
+    for name, fn in (("particles-64", particles_suite), ("shade-1M", shade_suite), ("decode", decode_suite),
+                     ("draw-1M", draw_suite)):
         try:
             out[name] = fn(ctx, torch, flush, peak)
         except Exception as exc:
@@ -554,6 +555,36 @@ def shade_suite(ctx, torch, flush, peak):
                 "shade_gbs": s * 96 / extra_s / 1e9 if extra_s > 0 else None})
     sp.destroy()
     return res
+
+
+def draw_suite(ctx, torch, flush, peak):
+    """clusters-1M sorted and drawn into a 1920 x 1080 RGBA f32 image
+    (ws_draw): the draw alone, timed with CUDA events around the call (it
+    synchronises its stream once, to size the binning)."""
+    from winding_b200 import make_view, parse_splats, workloads as W
+    job = W.clusters_1m(seed=1, cull=0.5)
+    sp = parse_splats(job.records, ctx)
+    view = make_view(job.view.model_view, job.view.projection, job.view.viewport, 0.5)
+    o = torch.empty(sp.count, dtype=torch.int32, device="cuda")
+    k = torch.empty_like(o)
+    c = torch.zeros(1, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    ctx.sort_device(sp, view, o.data_ptr(), k.data_ptr(), c.data_ptr(), stream)
+    img = torch.zeros((1080, 1920, 4), dtype=torch.float32, device="cuda")
+
+    def draw():
+        img.zero_()
+        ctx.draw(sp, view, o.data_ptr(), c.data_ptr(), img.data_ptr(), 1920, 1080, None, stream)
+
+    for _ in range(3):
+        draw()
+    ms = timed_sorts(ctx, torch, 10, flush, draw) / 10
+    drawn = int(c.item())
+    covered = float((img[..., 3] > 0).float().mean().item())
+    sp.destroy()
+    return {"splats": 1_000_000, "drawn": drawn, "width": 1920, "height": 1080, "ms": ms,
+            "msplats_s": drawn / (ms / 1e3) / 1e6, "covered_fraction": covered,
+            "note": "includes clearing the 33 MB image and the call's one stream sync"}
 
 
 def decode_suite(ctx, torch, flush, peak):

@@ -369,6 +369,18 @@ int ws_server_destroy(ws_server* server);
 int ws_sort_noalloc(const ws_cloud* cloud, const ws_view* view, uint32_t* order, uint32_t* keys, uint32_t* count,
                     void* stream);
 
+/* ------------------------------------------------------------ self-test */
+
+/*
+ * Failure detection, exercised: queues one job whose first phase is left out,
+ * so its next phase's wait can never be satisfied, and launches it with
+ * `spin_limit` polls (1 to 2^20). The wait gives up, the kernel records the
+ * error and drains, and this returns WS_ERR_TIMEOUT with the message every
+ * real timeout gets; the context stays usable. No counterpart in the
+ * reference (its WebGPU queue has no bounded waits).
+ */
+int ws_selftest_wait(ws_ctx* ctx, uint32_t spin_limit);
+
 /* ------------------------------------------------------------ tuning */
 
 /*

@@ -295,3 +295,14 @@ def test_tuning_table_changes_no_result(ctx):
     assert ctx.lib.ws_set_tuning(ctx.handle, bad, 1) == _lib.WS_ERR_ARG
     autotune.install(ctx, {})
     splats.destroy()
+
+
+def test_a_wait_that_runs_out_is_reported_and_the_context_recovers(ctx):
+    """Failure detection without a fault: a queued phase whose dependency
+    never completes; its bounded wait gives up, the launch reports
+    WS_ERR_TIMEOUT, and the next sort on the same context is exact."""
+    from winding_b200 import _lib
+    rc = ctx.lib.ws_selftest_wait(ctx.handle, 2000)
+    assert rc == _lib.WS_ERR_TIMEOUT
+    assert "device-side wait gave up" in ctx.lib.ws_last_error(ctx.handle).decode()
+    check_job(ctx, W.uniform_100k(seed=77, n=50_000))

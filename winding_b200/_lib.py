@@ -171,6 +171,7 @@ SIGNATURES = {
     "ws_cloud_load": (ctypes.c_int, [vp, vp, ctypes.c_size_t, ctypes.POINTER(ctypes.c_void_p)]),
     "ws_draw": (ctypes.c_int, [vp, vp, ctypes.POINTER(WsView), vp, vp, vp, vp, ctypes.c_uint32, ctypes.c_uint32, vp]),
     "ws_draw_tables": (ctypes.c_int, [ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]),
+    "ws_selftest_wait": (ctypes.c_int, [vp, ctypes.c_uint32]),
     "ws_cloud_harmonics": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_int), vp]),
     "ws_sort_batch_shaded": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(WsJob), ctypes.POINTER(WsShade), vp]),
     "ws_particle_thresholds": (ctypes.c_int, [ctypes.POINTER(ctypes.c_float)]),

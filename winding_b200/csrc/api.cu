@@ -822,6 +822,56 @@ extern "C" int ws_sort_batch(ws_ctx* ctx, int njobs, const ws_job* jobs, void* s
     return run_batch(ctx, jobs, njobs, stream_p ? static_cast<cudaStream_t>(stream_p) : ctx->stream);
 }
 
+// -------------------------------------------------------------- self-test
+
+extern "C" int ws_selftest_wait(ws_ctx* ctx, uint32_t spin_limit) {
+    if (!ctx) return WS_ERR_ARG;
+    if (spin_limit == 0 || spin_limit > (1u << 20))
+        return set_error(ctx, WS_ERR_ARG, "ws_selftest_wait: spin_limit must be 1 to 2^20");
+    cudaSetDevice(ctx->device);
+    cudaError_t e;
+    if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return cuda_error(ctx, e, "ws_selftest_wait");
+    // One job of 4096 given keys whose keys items are not queued: its scan
+    // items wait for a count that nothing raises.
+    const uint32_t n = 4096;
+    const size_t keys_bytes = 16384, out_bytes = 3 * 4 * (size_t)n + 256;
+    const size_t sort_bytes = launch_scratch_bytes(&n, 1, ctx->params);
+    if ((e = ctx->scratch.ensure(sort_bytes + keys_bytes + out_bytes)) != cudaSuccess)
+        return cuda_error(ctx, e, "ws_selftest_wait scratch");
+    char* base = static_cast<char*>(ctx->scratch.p);
+    uint16_t* keys = reinterpret_cast<uint16_t*>(base + sort_bytes);
+    uint32_t* outs = reinterpret_cast<uint32_t*>(base + sort_bytes + keys_bytes);
+    JobDesc d;
+    std::memset(&d, 0, sizeof(d));
+    d.kind = kJobKeys;
+    d.n = n;
+    d.keys_in = keys;
+    d.order = outs;
+    d.keys = outs + n;
+    d.count = outs + 2 * n;
+    char* at = base + align_up(sizeof(LaunchCtl) + sizeof(JobCtl), 256);
+    assign_scratch(d, n, ctx->params, at);
+    d.ctl = reinterpret_cast<uint32_t*>(base + sizeof(LaunchCtl));
+    std::vector<uint2> items;
+    for (uint32_t t = 0; t < d.scan_items; ++t) items.push_back(make_uint2(0u, (kPhaseScanLo << kPhaseShift) | t));
+    if ((e = ctx->jobs_d.ensure(sizeof(JobDesc))) != cudaSuccess ||
+        (e = ctx->items_d.ensure(items.size() * sizeof(uint2))) != cudaSuccess)
+        return cuda_error(ctx, e, "ws_selftest_wait");
+    ctx->items_valid = false;   // the item upload below replaces the cached list
+    if ((e = cudaMemcpy(ctx->jobs_d.p, &d, sizeof(d), cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(ctx->items_d.p, items.data(), items.size() * sizeof(uint2), cudaMemcpyHostToDevice)) !=
+            cudaSuccess ||
+        (e = cudaMemset(base, 0, sizeof(LaunchCtl) + sizeof(JobCtl))) != cudaSuccess ||
+        (e = cudaMemset(keys, 0, keys_bytes)) != cudaSuccess)
+        return cuda_error(ctx, e, "ws_selftest_wait");
+    e = launch_sort(static_cast<JobDesc*>(ctx->jobs_d.p), static_cast<uint2*>(ctx->items_d.p), (uint32_t)items.size(),
+                    static_cast<LaunchCtl*>(ctx->scratch.p), ctx->err_d, ctx->params.tile, variant_minb(ctx->params),
+                    spin_limit, 2, ctx->stream, nullptr);
+    if (e != cudaSuccess) return cuda_error(ctx, e, "ws_selftest_wait launch");
+    if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return cuda_error(ctx, e, "ws_selftest_wait");
+    return take_device_error(ctx);
+}
+
 // -------------------------------------------------------------- harmonics
 
 // 32-bit words one splat's harmonics of `degree` take (scene/splats.js:43-47).
