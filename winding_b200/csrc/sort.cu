@@ -40,8 +40,6 @@ struct SortSmem {
     uint32_t next;                  // the ticket this CTA works on next
     uint32_t drain;
     uint32_t abort;
-    int pend_job;                   // items done but not yet published: their job,
-    uint32_t pend_phase, pend_n;    // phase and number
     int ready_job;                  // (job, phase) whose dependency this CTA has seen met
     uint32_t ready_phase;
     uint64_t mark[4];               // tracing: timestamps inside an item
@@ -83,6 +81,10 @@ __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
 __device__ __forceinline__ void cp_async_wait_all() {
     asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
 }
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+// Waits until at most one of this thread's committed copy groups is pending.
+__device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_none() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
 // Copies `bytes` (a multiple of 16, both ends 16-byte aligned) with the whole
 // CTA; the caller waits and synchronises.
@@ -144,24 +146,6 @@ __device__ bool wait_phase(const uint32_t* done, uint32_t need, SortSmem<IPT>& s
     return sm.abort == 0;
 }
 
-// Publishes the CTA's finished items of one (job, phase): the CTA barrier
-// orders every thread's writes before thread 0's release, whose acquire by a
-// waiting CTA (wait_phase) makes them visible there. Items are published in
-// bulk when the CTA moves on to another (job, phase) or leaves, never while
-// it waits, so the queue still drains.
-template <int IPT>
-__device__ void flush_pending(const JobDesc* jobs, SortSmem<IPT>& sm) {
-    if (sm.pend_job < 0) return;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        JobCtl* ctl = reinterpret_cast<JobCtl*>(jobs[sm.pend_job].ctl);
-        red_release_add(&ctl->done[sm.pend_phase], sm.pend_n);
-        sm.pend_job = -1;
-        sm.pend_n = 0;
-    }
-    __syncthreads();
-}
-
 // The lanes of the warp whose `on` is set and whose 8-bit digit equals this
 // lane's: one ballot per digit bit (faster than __match_any_sync here).
 __device__ __forceinline__ uint32_t match_digit8(uint32_t d, bool on) {
@@ -217,13 +201,21 @@ __device__ void keys_tile(const JobDesc& J, int job, uint32_t tile, SortSmem<IPT
     const bool any = c.visible != 0;
     const bool fp = c.cull > 0.0f;
     const uint32_t n = J.n;
-    // Every centre of the tile in flight at once: this thread copies the ones
-    // it will read (the cloud is padded to a whole number of tiles).
+    // Every centre of the tile in flight at once, in two groups: this thread
+    // copies the ones it will read (the cloud is padded to a whole number of
+    // tiles), the first half with the exponents, then the second half, which
+    // is still arriving while the first is swept.
     if (any) {
 #pragma unroll
-        for (int r = 0; r < IPT; ++r) cp_async16(&sm.u.k.centers[r * kThreads + tid], &J.centers[base + r * kThreads + tid]);
+        for (int r = 0; r < IPT / 2; ++r)
+            cp_async16(&sm.u.k.centers[r * kThreads + tid], &J.centers[base + r * kThreads + tid]);
         if (fp) cta_copy(sm.u.k.sexp, J.sexp + base, T);
-        cp_async_wait_all();
+        cp_async_commit();
+#pragma unroll
+        for (int r = IPT / 2; r < IPT; ++r)
+            cp_async16(&sm.u.k.centers[r * kThreads + tid], &J.centers[base + r * kThreads + tid]);
+        cp_async_commit();
+        cp_async_wait_one();
     }
     __syncthreads();   // the exponents were copied by other threads
     if (tid == 0) sm.mark[0] = global_ns();
@@ -231,8 +223,9 @@ __device__ void keys_tile(const JobDesc& J, int job, uint32_t tile, SortSmem<IPT
     // is written now (the passes read only the slots whose survivor bit is
     // set), with the survivor bits and digit counts of the splats already
     // decided; the ones whose footprint must still be evaluated go to a queue.
-#pragma unroll 1
+#pragma unroll 2
     for (uint32_t k = 0; k < T; k += kThreads) {
+        if (k == T / 2 && any) cp_async_wait_none();   // this thread's second-half centres
         const uint32_t at = k + tid;
         uint32_t key = 0;
         bool kept = false, pending = false;
@@ -679,8 +672,6 @@ __global__ void __launch_bounds__(kThreads, MINB) sort_kernel(const JobDesc* __r
     if (tid == 0) {
         sm.next = atomicAdd(&lctl->ticket, 1u);
         sm.drain = *(volatile uint32_t*)err;
-        sm.pend_job = -1;
-        sm.pend_n = 0;
         sm.ready_job = -1;
     }
     uint64_t t_claim = 0, t_start = 0;
@@ -694,7 +685,6 @@ __global__ void __launch_bounds__(kThreads, MINB) sort_kernel(const JobDesc* __r
         const int job = (int)item.x;
         const JobDesc& J = jobs[job];
         JobCtl* ctl = reinterpret_cast<JobCtl*>(J.ctl);
-        if (job != sm.pend_job || phase != sm.pend_phase) flush_pending(jobs, sm);
         bool work = !sm.drain;   // after an error: claim the remaining items, do no work
         if (work && phase != kPhaseKeys && !(sm.ready_job == job && sm.ready_phase == phase)) {
             // Items the phase before this one has: tiles, pairs of tiles, or
@@ -742,9 +732,9 @@ __global__ void __launch_bounds__(kThreads, MINB) sort_kernel(const JobDesc* __r
         }
         if (tid == 0) {
             if (work) {
-                sm.pend_job = job;
-                sm.pend_phase = phase;
-                sm.pend_n += 1;
+                // Published at once (after the barrier above, so every
+                // thread's writes of the item are ordered before it).
+                red_release_add(&ctl->done[phase], 1u);
                 if (trace) {
                     TraceRec r;
                     r.claim = t_claim;
@@ -761,7 +751,6 @@ __global__ void __launch_bounds__(kThreads, MINB) sort_kernel(const JobDesc* __r
             if (trace) t_claim = global_ns();
         }
     }
-    flush_pending(jobs, sm);
     cp_async_wait_all();   // no copy into this CTA's shared memory outlives it
     if (tid == 0) atomicAdd(&lctl->exited, 1u);
 }
