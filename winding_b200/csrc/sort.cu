@@ -469,31 +469,47 @@ __device__ void count_hi_item(const JobDesc& J, int job, uint32_t g, SortSmem<IP
 
 // ScanLo / ScanHi: for digit d, the exclusive prefix over tiles of its
 // per-tile counts (a contiguous row of the digit-major count matrix), in
-// place, and its total. Chunks of 256 x 16 tiles: all loads of a chunk are
-// in flight before the scan.
+// place, and its total. Chunks of 4096 tiles go through shared memory:
+// loaded and stored coalesced (word e of the chunk at e + e / 32, so a
+// thread's run of 16 is read without bank conflicts), each thread scanning
+// 16 consecutive words between.
 template <int IPT>
 __device__ void scan_digit(uint32_t* cnt, uint32_t tiles, uint32_t d, uint32_t* tot, SortSmem<IPT>& sm) {
     constexpr int V = 16;
+    constexpr uint32_t kChunk = kThreads * V;
+    static_assert(sizeof(sm.u) >= (kChunk + kChunk / 32) * 4, "chunk fits the phase union");
+    uint32_t* buf = reinterpret_cast<uint32_t*>(&sm.u);
     const int tid = threadIdx.x;
     uint32_t* row = cnt + (size_t)d * tiles;
     uint32_t carry = 0;
-    for (uint32_t c0 = 0; c0 < tiles; c0 += kThreads * V) {
-        uint32_t v[V];
+    for (uint32_t c0 = 0; c0 < tiles; c0 += kChunk) {
+        __syncthreads();   // the previous chunk's stores have read buf
+#pragma unroll
+        for (int q = 0; q < V; ++q) {
+            const uint32_t e = q * kThreads + tid;
+            buf[e + e / 32] = c0 + e < tiles ? __ldcg(&row[c0 + e]) : 0u;
+        }
+        __syncthreads();
         uint32_t local = 0;
 #pragma unroll
         for (int q = 0; q < V; ++q) {
-            const uint32_t r = c0 + tid * V + q;
-            v[q] = r < tiles ? __ldcg(&row[r]) : 0u;
+            const uint32_t e = tid * V + q;
+            local += buf[e + e / 32];
         }
-#pragma unroll
-        for (int q = 0; q < V; ++q) local += v[q];
         uint32_t chunk_total;
         uint32_t run = carry + block_exclusive_scan(local, sm.scan, &chunk_total);
 #pragma unroll
+        for (int q = 0; q < V; ++q) {   // only this thread touches its run of 16
+            const uint32_t e = tid * V + q;
+            const uint32_t x = buf[e + e / 32];
+            buf[e + e / 32] = run;
+            run += x;
+        }
+        __syncthreads();
+#pragma unroll
         for (int q = 0; q < V; ++q) {
-            const uint32_t r = c0 + tid * V + q;
-            if (r < tiles) row[r] = run;
-            run += v[q];
+            const uint32_t e = q * kThreads + tid;
+            if (c0 + e < tiles) row[c0 + e] = buf[e + e / 32];
         }
         carry += chunk_total;
     }
