@@ -426,8 +426,9 @@ template <int IPT>
 __device__ void count_hi_item(const JobDesc& J, int job, uint32_t g, SortSmem<IPT>& sm) {
     constexpr uint32_t T = SortSmem<IPT>::kTile;
     const int tid = threadIdx.x;
-    digit_starts(J, job, 0, sm);
-    const uint32_t s_total = sm.gtotal;
+    // The survivor count, which the low pass's first tile stored (the whole
+    // low pass is done before this phase starts).
+    const uint32_t s_total = __ldcg(J.count);
     uint16_t* area[kCountSpan] = {sm.u.p.in_key[0], sm.u.p.in_key[1]};
 #pragma unroll
     for (uint32_t q = 0; q < kCountSpan; ++q) {
@@ -436,34 +437,42 @@ __device__ void count_hi_item(const JobDesc& J, int job, uint32_t g, SortSmem<IP
     }
     cp_async_wait_all();
     __syncthreads();
-    // Per-warp counters, two 16-bit digit counts to a word (a warp counts at
-    // most 32 x IPT keys of a tile), bumped with shared-memory atomics: one
-    // atomic per key, no ballots.
-    uint32_t* wc = reinterpret_cast<uint32_t*>(&sm.u.p.wcnt[0][0]);   // [kWarps][128]
-    const uint32_t warp = tid >> 5;
+    if (tid == 0) sm.mark[0] = global_ns();
+    // Counters: four per warp (one per 8 lanes, so at most 8 lanes of a warp
+    // meet on one counter however few digits the tile holds), two 16-bit
+    // digit counts to a word (a counter sees at most 8 x IPT keys), bumped
+    // with shared-memory atomics; counter w's word for digit pair p is at
+    // w * 128 + (p ^ w), so one digit's counters are in different banks.
+    // They live past the two key buffers.
+    constexpr int kSubs = kWarps * 4;
+    static_assert(sizeof(sm.u) >= 4 * (size_t)T + kSubs * 128 * 4, "counters fit the phase union");
+    uint32_t* wc = reinterpret_cast<uint32_t*>(reinterpret_cast<unsigned char*>(&sm.u) + 4 * (size_t)T);
+    const uint32_t warp = tid >> 5, lane = tid & 31;
+    const uint32_t sub = warp * 4 + (lane >> 3);
 #pragma unroll 1
     for (uint32_t q = 0; q < kCountSpan; ++q) {
         const uint32_t tile = g * kCountSpan + q;
         if (tile >= J.tiles) break;
-        for (int k = tid; k < kWarps * 128; k += kThreads) wc[k] = 0;
+        for (int k = tid; k < kSubs * 128; k += kThreads) wc[k] = 0;
         __syncthreads();
         const uint32_t base = tile * T;
         if (base < s_total) {
 #pragma unroll
             for (int r = 0; r < IPT; ++r) {
-                const uint32_t at = warp * 32u * IPT + r * 32u + (tid & 31);
+                const uint32_t at = warp * 32u * IPT + r * 32u + lane;
                 if (base + at < s_total) {
                     const uint32_t d = (q ? sm.u.p.in_key[1][at] : sm.u.p.in_key[0][at]) >> 8;
-                    atomicAdd(&wc[warp * 128 + (d >> 1)], 1u << ((d & 1u) * 16));
+                    atomicAdd(&wc[sub * 128 + ((d >> 1) ^ sub)], 1u << ((d & 1u) * 16));
                 }
             }
         }
         __syncthreads();
         uint32_t total = 0;
-#pragma unroll
-        for (int w = 0; w < kWarps; ++w) total += (wc[w * 128 + (tid >> 1)] >> ((tid & 1) * 16)) & 0xFFFFu;
+#pragma unroll 8
+        for (int w = 0; w < kSubs; ++w) total += (wc[w * 128 + ((tid >> 1) ^ w)] >> ((tid & 1) * 16)) & 0xFFFFu;
         J.cnt_hi[(size_t)tid * J.tiles + tile] = total;
         __syncthreads();   // the counters are cleared for the next tile
+        if (tid == 0) sm.mark[1 + q] = global_ns();
     }
 }
 
