@@ -201,6 +201,7 @@ __device__ void keys_tile(const JobDesc& J, int job, uint32_t tile, SortSmem<IPT
     const bool any = c.visible != 0;
     const bool fp = c.cull > 0.0f;
     const uint32_t n = J.n;
+    uint16_t* const k16 = J.k16;
     // Every centre of the tile in flight at once, in two groups: this thread
     // copies the ones it will read (the cloud is padded to a whole number of
     // tiles), the first half with the exponents, then the second half, which
@@ -273,7 +274,7 @@ __device__ void keys_tile(const JobDesc& J, int job, uint32_t tile, SortSmem<IPT
             }
         }
         const uint32_t i = base + at;
-        if (i < n) J.k16[i] = (uint16_t)key;
+        if (i < n) k16[i] = (uint16_t)key;
         const uint32_t kb = __ballot_sync(0xffffffffu, kept);
         if (lane == 0) sm.u.k.maskw[at >> 5] = kb;
         if (kept) atomicAdd(&sm.hist[key & 255u], 1u);
@@ -640,8 +641,14 @@ __device__ void digit_tile(const JobDesc& J, int job, uint32_t tile, SortSmem<IP
     __syncthreads();
     if (tid == 0) sm.mark[2] = global_ns();
     // Write-out in chunks of four slots per thread: the chunk's staged
-    // entries are read first, so their shared-memory loads overlap.
+    // entries are read first, so their shared-memory loads overlap. The job's
+    // output pointers and size are read once, into registers.
     constexpr int kChunk = 4;
+    const uint32_t n_out = J.n;
+    uint16_t* const key_b = J.key_b;
+    uint32_t* const idx_b = J.idx_b;
+    uint32_t* const order = J.order;
+    uint32_t* const keys_out = J.keys;
 #pragma unroll 1
     for (int r0 = 0; r0 < IPT && (uint32_t)r0 * kThreads < tile_total; r0 += kChunk) {
         uint32_t kk[kChunk], ix[kChunk];
@@ -659,16 +666,16 @@ __device__ void digit_tile(const JobDesc& J, int job, uint32_t tile, SortSmem<IP
             const uint32_t key = kk[q];
             const uint32_t d = PASS == 0 ? (key & 255u) : (key >> 8);
             const uint32_t g = sm.u.p.gofs[d] + s;
-            if (g >= J.n) {   // only reachable if counts disagree: record, do not write
+            if (g >= n_out) {   // only reachable if counts disagree: record, do not write
                 raise_error(err, kErrBounds, item);
                 continue;
             }
             if (PASS == 0) {
-                J.key_b[g] = (uint16_t)key;
-                J.idx_b[g] = ix[q];
+                key_b[g] = (uint16_t)key;
+                idx_b[g] = ix[q];
             } else {
-                __stcs(&J.order[g], ix[q]);
-                if (J.keys) __stcs(&J.keys[g], key);
+                __stcs(&order[g], ix[q]);
+                if (keys_out) __stcs(&keys_out[g], key);
             }
         }
     }
