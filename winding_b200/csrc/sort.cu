@@ -182,6 +182,97 @@ __device__ __forceinline__ uint32_t match_digit8(uint32_t d, bool on) {
 // 2 pi (1.00001 G + 0.3)(1 + 5u); a splat with alpha times that below cull
 // is culled, again without its footprint.
 
+// Sweep 1 of the keys tile (see keys_tile). kFast: the fast transform, with
+// the view's constants in registers (FastView) for the whole tile.
+template <bool kFast, int IPT>
+__device__ __forceinline__ void keys_sweep(const ViewConsts& c, SortSmem<IPT>& sm, uint32_t base, uint32_t n, bool any,
+                                           bool fp, uint16_t* k16) {
+    constexpr uint32_t T = SortSmem<IPT>::kTile;
+    const int tid = threadIdx.x;
+    const uint32_t lane = lane_id();
+    FastView fv;
+    if constexpr (kFast) fv = fast_view_of(c);
+    const bool persp = c.persp;
+    const float keep_q = c.keep_q, cull = c.cull;
+    const uint32_t keep_byte = c.keep_byte;
+    // Sweep 1: tests, keys and the footprint shortcut. Every splat's key slot
+    // is written now (the passes read only the slots whose survivor bit is
+    // set), with the survivor bits and digit counts of the splats already
+    // decided; the ones whose footprint must still be evaluated go to a queue.
+#pragma unroll 2
+    for (uint32_t k = 0; k < T; k += kThreads) {
+        if (k == T / 2 && any) cp_async_wait_none();   // this thread's second-half centres
+        const uint32_t at = k + tid;
+        uint32_t key = 0;
+        bool kept = false, pending = false;
+        if (any && base + at < n) {
+            const float4 p = sm.u.k.centers[at];
+            float view[4];
+            bool inside;
+            if constexpr (kFast) {
+                fast_view(fv, p.x, p.y, p.z, view);
+                inside = fast_in_frustum(fv, view);
+            } else {
+                view_of(c, p.x, p.y, p.z, view);
+                inside = in_frustum(c, view);
+            }
+            if (inside) {
+                const uint32_t byte = __float_as_uint(p.w) >> 24;
+                const float alpha = sm.alpha[byte];
+                if (!(fmul(alpha, 255.0f) <= 1.0f)) {   // else too faint to reach 1/255
+                    if constexpr (kFast)
+                        key = fast_depth_key(fv, view);
+                    else
+                        key = depth_key(c, view);
+                    kept = true;
+                    if (fp) {
+                        // Decided without the footprint when the bounds allow
+                        // (see above); else queued.
+                        bool decided = false;
+                        if (persp) {
+                            const float d = -view[2];
+                            // keep_q 2^sexp, exactly: sexp is in [-100, 127] and
+                            // keep_q >= 2^-20, so the product is a normal float
+                            // (or +inf).
+                            const float pow2 = __int_as_float((int(sm.u.k.sexp[at]) + 127) << 23);
+                            const float q = fmul(keep_q, pow2);
+                            const float dd = fmul(d, d);
+                            if (byte >= keep_byte && q <= fmul(100.0f, dd)) {
+                                decided = true;   // kept
+                            } else if (dd > 1e-30f && dd < 1e30f && q < 1e30f) {
+                                // An upper bound of G: the approximate quotient is
+                                // within a few ulps, far inside the 1.002 margin.
+                                const float g = fmul(1.002f, __fdividef(q, dd));
+                                const float top = fmul(fmul(fmul(alpha, 6.2832f), fadd(fmul(g, 1.00001f), 0.3f)), 1.0001f);
+                                if (top < cull) {
+                                    kept = false;
+                                    decided = true;
+                                }
+                            }
+                        }
+                        if (!decided) {
+                            kept = false;
+                            pending = true;
+                        }
+                    }
+                }
+            }
+        }
+        const uint32_t i = base + at;
+        if (i < n) k16[i] = (uint16_t)key;
+        const uint32_t kb = __ballot_sync(0xffffffffu, kept);
+        if (lane == 0) sm.u.k.maskw[at >> 5] = kb;
+        if (kept) atomicAdd(&sm.hist[key & 255u], 1u);
+        const uint32_t pend = __ballot_sync(0xffffffffu, pending);
+        if (pend) {
+            uint32_t first = 0;
+            if (lane == (uint32_t)(__ffs(pend) - 1)) first = atomicAdd(&sm.u.k.qn, (uint32_t)__popc(pend));
+            first = __shfl_sync(0xffffffffu, first, __ffs(pend) - 1);
+            if (pending) sm.u.k.queue[first + __popc(pend & lanemask_lt())] = (uint16_t)at;
+        }
+    }
+}
+
 template <int IPT>
 __device__ void keys_tile(const JobDesc& J, int job, uint32_t tile, SortSmem<IPT>& sm) {
     constexpr uint32_t T = SortSmem<IPT>::kTile;
@@ -220,72 +311,10 @@ __device__ void keys_tile(const JobDesc& J, int job, uint32_t tile, SortSmem<IPT
     }
     __syncthreads();   // the exponents were copied by other threads
     if (tid == 0) sm.mark[0] = global_ns();
-    // Sweep 1: tests, keys and the footprint shortcut. Every splat's key slot
-    // is written now (the passes read only the slots whose survivor bit is
-    // set), with the survivor bits and digit counts of the splats already
-    // decided; the ones whose footprint must still be evaluated go to a queue.
-#pragma unroll 2
-    for (uint32_t k = 0; k < T; k += kThreads) {
-        if (k == T / 2 && any) cp_async_wait_none();   // this thread's second-half centres
-        const uint32_t at = k + tid;
-        uint32_t key = 0;
-        bool kept = false, pending = false;
-        if (any && base + at < n) {
-            const float4 p = sm.u.k.centers[at];
-            float view[4];
-            view_of(c, p.x, p.y, p.z, view);
-            if (in_frustum(c, view)) {
-                const uint32_t byte = __float_as_uint(p.w) >> 24;
-                const float alpha = sm.alpha[byte];
-                if (!(fmul(alpha, 255.0f) <= 1.0f)) {   // else too faint to reach 1/255
-                    key = depth_key(c, view);
-                    kept = true;
-                    if (fp) {
-                        // Decided without the footprint when the bounds allow
-                        // (see above); else queued.
-                        bool decided = false;
-                        if (c.persp) {
-                            const float d = -view[2];
-                            // keep_q 2^sexp, exactly: sexp is in [-100, 127] and
-                            // keep_q >= 2^-20, so the product is a normal float
-                            // (or +inf).
-                            const float pow2 = __int_as_float((int(sm.u.k.sexp[at]) + 127) << 23);
-                            const float q = fmul(c.keep_q, pow2);
-                            const float dd = fmul(d, d);
-                            if (byte >= c.keep_byte && q <= fmul(100.0f, dd)) {
-                                decided = true;   // kept
-                            } else if (dd > 1e-30f && dd < 1e30f && q < 1e30f) {
-                                // An upper bound of G: the approximate quotient is
-                                // within a few ulps, far inside the 1.002 margin.
-                                const float g = fmul(1.002f, __fdividef(q, dd));
-                                const float top = fmul(fmul(fmul(alpha, 6.2832f), fadd(fmul(g, 1.00001f), 0.3f)), 1.0001f);
-                                if (top < c.cull) {
-                                    kept = false;
-                                    decided = true;
-                                }
-                            }
-                        }
-                        if (!decided) {
-                            kept = false;
-                            pending = true;
-                        }
-                    }
-                }
-            }
-        }
-        const uint32_t i = base + at;
-        if (i < n) k16[i] = (uint16_t)key;
-        const uint32_t kb = __ballot_sync(0xffffffffu, kept);
-        if (lane == 0) sm.u.k.maskw[at >> 5] = kb;
-        if (kept) atomicAdd(&sm.hist[key & 255u], 1u);
-        const uint32_t pend = __ballot_sync(0xffffffffu, pending);
-        if (pend) {
-            uint32_t first = 0;
-            if (lane == (uint32_t)(__ffs(pend) - 1)) first = atomicAdd(&sm.u.k.qn, (uint32_t)__popc(pend));
-            first = __shfl_sync(0xffffffffu, first, __ffs(pend) - 1);
-            if (pending) sm.u.k.queue[first + __popc(pend & lanemask_lt())] = (uint16_t)at;
-        }
-    }
+    if (c.fast)
+        keys_sweep<true>(c, sm, base, n, any, fp, k16);
+    else
+        keys_sweep<false>(c, sm, base, n, any, fp, k16);
     __syncthreads();
     if (tid == 0) sm.mark[1] = global_ns();
     // Sweep 2: the queued footprints, densely; a kept splat sets its bit and

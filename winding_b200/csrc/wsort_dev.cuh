@@ -351,6 +351,54 @@ __device__ __forceinline__ void footprint2d(const ViewConsts& c, const float vie
     *pyy = fyy;
 }
 
+// The per-view constants the keys sweep needs on the fast transform, held in
+// registers for a whole tile (the same values as ViewConsts; the functions
+// below are view_of, in_frustum and depth_key's fast branches, op for op).
+struct FastView {
+    float m[12];                   // model-view entries 0-2, 4-6, 8-10, 12-14 (columns, rows 0-2)
+    float p0, p5, p8, p9, p10, p11, p14;
+    float depth_min, depth_scale;
+};
+
+__device__ __forceinline__ FastView fast_view_of(const ViewConsts& c) {
+    FastView f;
+#pragma unroll
+    for (int col = 0; col < 4; ++col)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) f.m[col * 3 + j] = c.mv[col * 4 + j];
+    f.p0 = c.proj[0];
+    f.p5 = c.proj[5];
+    f.p8 = c.proj[8];
+    f.p9 = c.proj[9];
+    f.p10 = c.proj[10];
+    f.p11 = c.proj[11];
+    f.p14 = c.proj[14];
+    f.depth_min = c.depth_min;
+    f.depth_scale = c.depth_scale;
+    return f;
+}
+
+__device__ __forceinline__ void fast_view(const FastView& f, float x, float y, float z, float view[4]) {
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+        view[j] = fadd(fadd(fadd(fmul(f.m[j], x), fmul(f.m[3 + j], y)), fmul(f.m[6 + j], z)), f.m[9 + j]);
+    view[3] = 1.0f;
+}
+
+__device__ __forceinline__ bool fast_in_frustum(const FastView& f, const float view[4]) {
+    const float c0 = fadd(fmul(f.p0, view[0]), fmul(f.p8, view[2]));
+    const float c1 = fadd(fmul(f.p5, view[1]), fmul(f.p9, view[2]));
+    const float c2 = fadd(fmul(f.p10, view[2]), f.p14);
+    const float w = fmul(f.p11, view[2]);
+    return !(view[2] >= 0.0f || c2 > w || fabsf(c0) > fmul(1.3f, w) || fabsf(c1) > fmul(1.3f, w));
+}
+
+__device__ __forceinline__ uint32_t fast_depth_key(const FastView& f, const float view[4]) {
+    const float scaled = fmul(fsub(-view[2], f.depth_min), f.depth_scale);
+    const uint32_t bucket = __float2uint_rz(fclamp(scaled, 0.0f, 65535.0f));
+    return kBuckets - 1u - bucket;
+}
+
 // The footprint cull (render/splats.js:172-178): true when the splat is kept.
 __device__ __forceinline__ bool footprint_keeps(const ViewConsts& c, const float view[4], const float s[6],
                                                 float alpha) {
