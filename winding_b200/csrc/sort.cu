@@ -374,17 +374,30 @@ __device__ void particle_keys_tile(const JobDesc& J, uint32_t tile, SortSmem<IPT
     const uint32_t n = J.n;
     const float ex = J.eye[0], ey = J.eye[1], ez = J.eye[2];
     const float fx = J.fwd[0], fy = J.fwd[1], fz = J.fwd[2];
-#pragma unroll 2
-    for (uint32_t k = 0; k < T; k += kThreads) {
-        const uint32_t at = k + tid;
+    // Every particle of the tile in flight at once: position and age (a
+    // record's first 16 bytes) into shared memory, lifetimes into registers;
+    // each thread reads back only its own.
+    const float4* pool = J.pool + 2 * ((size_t)J.idx_base + base);
+    float life[IPT];
+#pragma unroll
+    for (int r = 0; r < IPT; ++r) {
+        const uint32_t at = r * kThreads + tid;
+        if (base + at < n) {
+            cp_async16(&sm.u.k.centers[at], &pool[2 * (size_t)at]);
+            life[r] = __ldcs(&pool[2 * (size_t)at + 1].w);
+        }
+    }
+    cp_async_wait_all();
+    uint16_t* const k16 = J.k16;
+#pragma unroll
+    for (int r = 0; r < IPT; ++r) {
+        const uint32_t at = r * kThreads + tid;
         const uint32_t i = base + at;
         uint32_t key = 0;
         bool live = false;
         if (i < n) {
-            const float4* rec = J.pool + 2 * ((size_t)J.idx_base + i);
-            const float4 a = __ldcs(rec);
-            const float life = __ldcs(&rec[1].w);
-            live = !(a.w >= life);
+            const float4 a = sm.u.k.centers[at];
+            live = !(a.w >= life[r]);
             if (live) {
                 const float dot = fadd(fadd(fmul(fsub(a.x, ex), fx), fmul(fsub(a.y, ey), fy)), fmul(fsub(a.z, ez), fz));
                 const float d = fmaxf(dot, 1e-6f);
@@ -394,7 +407,7 @@ __device__ void particle_keys_tile(const JobDesc& J, uint32_t tile, SortSmem<IPT
                 while (b > 0 && d < __ldg(&J.thr[b])) --b;
                 key = kParticleBuckets - 1u - (uint32_t)b;
             }
-            J.k16[i] = (uint16_t)key;
+            k16[i] = (uint16_t)key;
         }
         const uint32_t kb = __ballot_sync(0xffffffffu, live);
         if (lane == 0) sm.u.k.maskw[at >> 5] = kb;
