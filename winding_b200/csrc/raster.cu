@@ -296,43 +296,111 @@ __global__ void __launch_bounds__(256) ranges_kernel(const uint32_t* __restrict_
     }
 }
 
+// The splat of each pair, in tile order: one indirection less for the blend.
+__global__ void __launch_bounds__(256) gather_kernel(const uint32_t* __restrict__ owner,
+                                                     const uint32_t* __restrict__ sorted, uint32_t npairs,
+                                                     uint32_t* __restrict__ splat_of) {
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < npairs; k += gridDim.x * blockDim.x)
+        splat_of[k] = owner[sorted[k]];
+}
+
+// Splat q's fragment at pixel centre (fx, fy) of pixel (px, py): its alpha,
+// or 0 when the quad does not cover the pixel or the fragment is dropped.
+__device__ __forceinline__ float fragment_alpha(const Quad& q, int px, int py, float fx, float fy) {
+    if (px < q.x0 || px > q.x1 || py < q.y0 || py > q.y1) return 0.0f;
+    const float ex = fsub(fx, q.cx), ey = fsub(q.cy, fy);
+    const float ox = fdiv(fadd(fmul(ex, q.ax), fmul(ey, q.ay)), q.la);
+    const float oy = fdiv(fsub(fmul(ex, q.ay), fmul(ey, q.ax)), q.lc);
+    if (!(fabsf(ox) <= q.qm && fabsf(oy) <= q.qm)) return 0.0f;
+    const float d2 = fadd(fmul(ox, ox), fmul(oy, oy));
+    const float alpha = fminf(0.99f, fmul(exp_pinned(-d2), q.a));
+    return alpha < 1.0f / 255.0f ? 0.0f : alpha;
+}
+
 // One CTA a tile, one thread a pixel: the tile's splats in order, staged in
-// shared memory 256 at a time, blended over the image.
-__global__ void __launch_bounds__(256) blend_kernel(const Quad* __restrict__ quads, const uint32_t* __restrict__ owner,
-                                                    const uint32_t* __restrict__ sorted, const uint2* __restrict__ range,
-                                                    uint32_t width, uint32_t height, uint32_t tiles_x,
-                                                    float4* __restrict__ image) {
-    __shared__ Quad staged[256];
+// shared memory 256 at a time (the next chunk copied with cp.async while
+// this one is blended), blended over the image. Warp w holds the tile's
+// pixel rows 2w and 2w + 1; for each chunk it marks (one ballot per 32
+// splats) the splats whose pixel box reaches those rows and walks only the
+// marked ones, four at a time: their fragments are evaluated independently,
+// then blended in order. A pixel meets exactly the splats whose box holds
+// it, in order, and a splat that leaves it untouched is skipped, as when
+// every splat is tried one by one.
+__global__ void __launch_bounds__(256) blend_kernel(const Quad* __restrict__ quads,
+                                                    const uint32_t* __restrict__ splat_of,
+                                                    const uint2* __restrict__ range, uint32_t width, uint32_t height,
+                                                    uint32_t tiles_x, float4* __restrict__ image) {
+    __shared__ Quad staged[2][256];
     const uint32_t tile = blockIdx.x;
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int px = (int)((tile % tiles_x) * kTilePx + (threadIdx.x & 15));
     const int py = (int)((tile / tiles_x) * kTilePx + (threadIdx.x >> 4));
+    const int row0 = (int)((tile / tiles_x) * kTilePx + 2 * warp), row1 = row0 + 1;
     const bool inside = px < (int)width && py < (int)height;
     float4 dst = inside ? image[(size_t)py * width + px] : make_float4(0, 0, 0, 0);
     const float fx = fadd((float)px, 0.5f), fy = fadd((float)py, 0.5f);
     const uint2 rg = range[tile];
-    for (uint32_t c0 = rg.x; c0 < rg.y; c0 += 256) {
+    auto stage = [&](uint32_t c0, int b) {   // this thread's quad of the chunk at c0 into buffer b
         const uint32_t k = c0 + threadIdx.x;
-        __syncthreads();
-        if (k < rg.y) staged[threadIdx.x] = quads[owner[sorted[k]]];
-        __syncthreads();
+        if (k < rg.y) {
+            const Quad* src = &quads[splat_of[k]];
+#pragma unroll
+            for (int w = 0; w < 4; ++w) cp_async16(reinterpret_cast<float4*>(&staged[b][threadIdx.x]) + w,
+                                                   reinterpret_cast<const float4*>(src) + w);
+        }
+        cp_async_commit();
+    };
+    if (rg.x < rg.y) stage(rg.x, 0);
+    int b = 0;
+    for (uint32_t c0 = rg.x; c0 < rg.y; c0 += 256, b ^= 1) {
+        cp_async_wait_none();
+        __syncthreads();   // chunk c0 is in staged[b]; staged[b ^ 1] is no longer read
+        if (c0 + 256 < rg.y) stage(c0 + 256, b ^ 1);
         const uint32_t m = min(256u, rg.y - c0);
-        for (uint32_t e = 0; e < m; ++e) {
-            const Quad& q = staged[e];
-            if (px < q.x0 || px > q.x1 || py < q.y0 || py > q.y1) continue;
-            const float ex = fsub(fx, q.cx), ey = fsub(q.cy, fy);
-            const float ox = fdiv(fadd(fmul(ex, q.ax), fmul(ey, q.ay)), q.la);
-            const float oy = fdiv(fsub(fmul(ex, q.ay), fmul(ey, q.ax)), q.lc);
-            if (!(fabsf(ox) <= q.qm && fabsf(oy) <= q.qm)) continue;
-            const float d2 = fadd(fmul(ox, ox), fmul(oy, oy));
-            const float alpha = fminf(0.99f, fmul(exp_pinned(-d2), q.a));
-            if (alpha < 1.0f / 255.0f) continue;
-            const float om = fsub(1.0f, alpha);
-            dst.x = fadd(fmul(q.r, alpha), fmul(dst.x, om));
-            dst.y = fadd(fmul(q.g, alpha), fmul(dst.y, om));
-            dst.z = fadd(fmul(q.b, alpha), fmul(dst.z, om));
-            dst.w = fadd(alpha, fmul(dst.w, om));
+        uint32_t marks[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const uint32_t e = j * 32 + lane;
+            bool hit = false;
+            if (e < m) {
+                const Quad& q = staged[b][e];
+                hit = q.y0 <= row1 && q.y1 >= row0;
+            }
+            marks[j] = __ballot_sync(0xffffffffu, hit);
+        }
+#pragma unroll 1
+        for (int j = 0; j < 8; ++j) {
+            uint32_t word = marks[j];
+            while (word) {
+                uint32_t e[4];
+                int cnt = 0;
+#pragma unroll
+                for (int t = 0; t < 4; ++t) {
+                    e[t] = 0;
+                    if (word) {
+                        e[t] = j * 32 + (__ffs(word) - 1);
+                        word &= word - 1;
+                        cnt = t + 1;
+                    }
+                }
+                float al[4];
+#pragma unroll
+                for (int t = 0; t < 4; ++t) al[t] = t < cnt ? fragment_alpha(staged[b][e[t]], px, py, fx, fy) : 0.0f;
+#pragma unroll
+                for (int t = 0; t < 4; ++t) {
+                    const float alpha = al[t];
+                    if (alpha == 0.0f) continue;
+                    const Quad& q = staged[b][e[t]];
+                    const float om = fsub(1.0f, alpha);
+                    dst.x = fadd(fmul(q.r, alpha), fmul(dst.x, om));
+                    dst.y = fadd(fmul(q.g, alpha), fmul(dst.y, om));
+                    dst.z = fadd(fmul(q.b, alpha), fmul(dst.z, om));
+                    dst.w = fadd(alpha, fmul(dst.w, om));
+                }
+            }
         }
     }
+    cp_async_wait_none();
     if (inside) image[(size_t)py * width + px] = dst;
 }
 
@@ -443,9 +511,10 @@ extern "C" int ws_draw(ws_ctx* ctx, const ws_cloud* cloud, const ws_view* view, 
                          WS_MAX_SPLATS);
     const uint32_t pairs = (uint32_t)pairs64;
     // The pair arrays, in a buffer of their own (growing it keeps the first):
-    // keys, owners, sorted order, sorted keys, count.
+    // keys, owners, sorted order, sorted keys, splats in tile order, count.
     const size_t o_keys = 0, o_own = o_keys + up((size_t)pairs * 2), o_sorted = o_own + up((size_t)pairs * 4);
-    const size_t o_skeys = o_sorted + up((size_t)pairs * 4), o_pc = o_skeys + up((size_t)pairs * 4);
+    const size_t o_skeys = o_sorted + up((size_t)pairs * 4), o_spl = o_skeys + up((size_t)pairs * 4);
+    const size_t o_pc = o_spl + up((size_t)pairs * 4);
     if ((e = ctx->pairs_d.ensure(o_pc + 256)) != cudaSuccess) return cuda_error(ctx, e, "ws_draw scratch");
     char* pb = static_cast<char*>(ctx->pairs_d.p);
     uint16_t* keys = reinterpret_cast<uint16_t*>(pb + o_keys);
@@ -453,13 +522,15 @@ extern "C" int ws_draw(ws_ctx* ctx, const ws_cloud* cloud, const ws_view* view, 
     uint32_t* sorted = reinterpret_cast<uint32_t*>(pb + o_sorted);
     uint32_t* skeys = reinterpret_cast<uint32_t*>(pb + o_skeys);
     uint32_t* pcount = reinterpret_cast<uint32_t*>(pb + o_pc);
+    uint32_t* splat_of = reinterpret_cast<uint32_t*>(pb + o_spl);
     emit_kernel<<<g, 256, 0, stream>>>(quads, cnt, off, n, tiles_x, keys, owner);
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_error(ctx, e, "ws_draw");
     int rc = run_given_keys(ctx, keys, pairs, sorted, skeys, pcount, stream);
     if (rc) return rc;
     const uint32_t gp = std::max(1u, std::min((pairs + 255) / 256, (uint32_t)ctx->sms * 8));
     ranges_kernel<<<gp, 256, 0, stream>>>(skeys, pairs, range);
-    blend_kernel<<<tiles, 256, 0, stream>>>(quads, owner, sorted, range, width, height, tiles_x,
+    gather_kernel<<<gp, 256, 0, stream>>>(owner, sorted, pairs, splat_of);
+    blend_kernel<<<tiles, 256, 0, stream>>>(quads, splat_of, range, width, height, tiles_x,
                                             reinterpret_cast<float4*>(image));
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_error(ctx, e, "ws_draw");
     return WS_OK;

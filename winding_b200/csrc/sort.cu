@@ -72,20 +72,6 @@ __device__ __forceinline__ uint64_t global_ns() {
     return t;
 }
 
-// 16-byte asynchronous copies global -> shared (cp.async, cached in L2
-// only), and the wait for all of this thread's copies.
-__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
-    const uint32_t dst = (uint32_t)__cvta_generic_to_shared(smem_dst);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(gsrc) : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() {
-    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-// Waits until at most one of this thread's committed copy groups is pending.
-__device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_none() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
-
 // Copies `bytes` (a multiple of 16, both ends 16-byte aligned) with the whole
 // CTA; the caller waits and synchronises.
 __device__ __forceinline__ void cta_copy(void* smem_dst, const void* gsrc, uint32_t bytes) {
