@@ -795,6 +795,7 @@ extern "C" void or_draw(const float* centers, const float* cov, const uint32_t* 
         }
         const float la = std::fmin(std::sqrt(2.0f * major), 1024.0f);
         const float lc = std::fmin(std::sqrt(2.0f * minor), 1024.0f);
+        const float ila = 1.0f / la, ilc = 1.0f / lc;
         const float qm = std::sqrt(std::fmin(reach, 4.0f));
         const float cx = (clip[0] / clip[3] + 1.0f) * half_w;
         const float cy = (1.0f - clip[1] / clip[3]) * half_h;
@@ -811,8 +812,8 @@ extern "C" void or_draw(const float* centers, const float* cov, const uint32_t* 
         for (int py = (int)fy0; py <= (int)fy1; ++py)
             for (int px = (int)fx0; px <= (int)fx1; ++px) {
                 const float ex = ((float)px + 0.5f) - cx, ey = cy - ((float)py + 0.5f);
-                const float ox = (ex * ax + ey * ay) / la;
-                const float oy = (ex * ay - ey * ax) / lc;
+                const float ox = (ex * ax + ey * ay) * ila;
+                const float oy = (ex * ay - ey * ax) * ilc;
                 if (!(std::fabs(ox) <= qm && std::fabs(oy) <= qm)) continue;
                 const float alpha = std::fmin(0.99f, exp_pinned(-(ox * ox + oy * oy)) * alpha0);
                 if (alpha < 1.0f / 255.0f) continue;

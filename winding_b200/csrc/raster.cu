@@ -16,9 +16,10 @@
 //     minor <= 0 or reach <= 0 is not drawn, as the vertex shader leaves it
 //     off screen.
 //   - the quad covers the pixels whose centre (px + 0.5, py + 0.5) maps into
-//     [-e, e]^2 under the quad's own inverse: offset = (d . axis / la,
-//     d . perp / lc), d the centre's offset from the splat's centre in
-//     pixels (y up, as clip space). That offset is the fragment's varying
+//     [-e, e]^2 under the quad's own inverse: offset = ((d . axis) (1 / la),
+//     (d . perp) (1 / lc)), the reciprocals rounded once per splat, d the
+//     centre's offset from the splat's centre in pixels (y up, as clip
+//     space). That offset is the fragment's varying
 //     (it varies linearly over the quad, as the reference interpolates it).
 //     Pixels are only considered within the quad's bounding box widened by a
 //     pixel, the same box on both sides.
@@ -27,7 +28,11 @@
 //     nearest ((c + 0.055) / 1.055)^2.4 above 0.04045, c / 12.92 below, c
 //     = byte / 255); blended premultiplied over what the image holds:
 //     dst = src + dst (1 - alpha) for colour and alpha, as the reference's
-//     blend state (one, one-minus-src-alpha). exp is exp_pinned below.
+//     blend state (one, one-minus-src-alpha). exp is the one in
+//     fragment_alpha: Cody and Waite's reduction (ln 2 split as 355/512 -
+//     2.12194440e-4, Software Manual for the Elementary Functions, 1980),
+//     exp(r) by its Taylor polynomial to r^7 / 7! in Horner form, 2^k from
+//     the exponent bits (in two steps below 2^-126).
 //   - no fog and no depth test (a headless image has no opaque scene).
 // Every f32 operation is separately rounded (-fmad=false).
 //
@@ -65,39 +70,13 @@ constexpr int kScanTile = kScanBlock * kScanItems;
 struct alignas(16) Quad {
     float cx, cy;          // centre
     float ax, ay;          // unit major axis
-    float la, lc;          // half-lengths along the major and minor axes
+    float ila, ilc;        // 1 / the half-lengths along the major and minor axes
     float qm;              // extent in units of the axes
     float a;               // alpha
     float r, g, b;         // decoded colour
     int x0, x1, y0, y1;    // candidate pixels (x0 > x1: nothing)
     float pad;
 };
-
-// exp for the fragment's falloff: Cody and Waite's reduction (ln 2 split as
-// 355/512 - 2.12194440e-4, Software Manual for the Elementary Functions,
-// 1980), exp(r) by its Taylor polynomial to r^7 / 7! in Horner form, and 2^k
-// from the exponent bits; every operation separately rounded.
-__device__ __forceinline__ float exp_pinned(float x) {
-    if (x != x) return x;
-    if (x < -104.0f) return 0.0f;
-    if (x > 88.0f) return INFINITY;
-    const float k = rintf(fmul(x, 1.44269504f));
-    const float r = fsub(fsub(x, fmul(k, 0.693359375f)), fmul(k, -2.12194440e-4f));
-    float p = 1.98412698e-4f;
-    p = fadd(fmul(p, r), 1.38888889e-3f);
-    p = fadd(fmul(p, r), 8.33333333e-3f);
-    p = fadd(fmul(p, r), 4.16666667e-2f);
-    p = fadd(fmul(p, r), 1.66666667e-1f);
-    p = fadd(fmul(p, r), 0.5f);
-    p = fadd(fmul(p, r), 1.0f);
-    p = fadd(fmul(p, r), 1.0f);
-    int ki = (int)k;
-    if (ki < -126) {
-        p = fmul(p, __int_as_float((ki + 126 + 127) << 23));
-        ki = -126;
-    }
-    return fmul(p, __int_as_float((ki + 127) << 23));
-}
 
 // The quad of instance j (order[j]), or an empty one. tables: srgb[256]
 // then reach[256].
@@ -155,13 +134,15 @@ __global__ void __launch_bounds__(256) prepare_kernel(const JobDesc* __restrict_
                 }
                 q.ax = ax;
                 q.ay = ay;
-                q.la = fminf(__fsqrt_rn(fmul(2.0f, major)), 1024.0f);
-                q.lc = fminf(__fsqrt_rn(fmul(2.0f, minor)), 1024.0f);
+                const float la = fminf(__fsqrt_rn(fmul(2.0f, major)), 1024.0f);
+                const float lc = fminf(__fsqrt_rn(fmul(2.0f, minor)), 1024.0f);
+                q.ila = fdiv(1.0f, la);
+                q.ilc = fdiv(1.0f, lc);
                 q.qm = __fsqrt_rn(fminf(reach, 4.0f));
                 q.cx = fmul(fadd(fdiv(clip[0], clip[3]), 1.0f), half_w);
                 q.cy = fmul(fsub(1.0f, fdiv(clip[1], clip[3])), half_h);
-                const float hx = fmul(q.qm, fadd(fmul(q.la, fabsf(ax)), fmul(q.lc, fabsf(ay))));
-                const float hy = fmul(q.qm, fadd(fmul(q.la, fabsf(ay)), fmul(q.lc, fabsf(ax))));
+                const float hx = fmul(q.qm, fadd(fmul(la, fabsf(ax)), fmul(lc, fabsf(ay))));
+                const float hy = fmul(q.qm, fadd(fmul(la, fabsf(ay)), fmul(lc, fabsf(ax))));
                 q.a = fdiv((float)(word >> 24), 255.0f);
                 q.r = tables[word & 255u];
                 q.g = tables[(word >> 8) & 255u];
@@ -304,17 +285,55 @@ __global__ void __launch_bounds__(256) gather_kernel(const uint32_t* __restrict_
         splat_of[k] = owner[sorted[k]];
 }
 
-// Splat q's fragment at pixel centre (fx, fy) of pixel (px, py): its alpha,
-// or 0 when the quad does not cover the pixel or the fragment is dropped.
-__device__ __forceinline__ float fragment_alpha(const Quad& q, int px, int py, float fx, float fy) {
-    if (px < q.x0 || px > q.x1 || py < q.y0 || py > q.y1) return 0.0f;
-    const float ex = fsub(fx, q.cx), ey = fsub(q.cy, fy);
-    const float ox = fdiv(fadd(fmul(ex, q.ax), fmul(ey, q.ay)), q.la);
-    const float oy = fdiv(fsub(fmul(ex, q.ay), fmul(ey, q.ax)), q.lc);
-    if (!(fabsf(ox) <= q.qm && fabsf(oy) <= q.qm)) return 0.0f;
-    const float d2 = fadd(fmul(ox, ox), fmul(oy, oy));
-    const float alpha = fminf(0.99f, fmul(exp_pinned(-d2), q.a));
-    return alpha < 1.0f / 255.0f ? 0.0f : alpha;
+// The fragments of splats q[0..N) at pixel centre (fx, fy) of pixel
+// (px, py): each one's alpha, or 0 when its quad does not cover the pixel or
+// the fragment is dropped. Evaluated in lock-step, every stage for all N
+// splats before the next, so the N independent chains overlap; without
+// branches (every value computed, the answer selected). For x = -d2 <= 0 exp
+// is 0 below -104, else 2^k p(r) as the head describes (the two-step
+// scaling multiplies by 2^0 when one step suffices, which is exact).
+template <int N>
+__device__ __forceinline__ void fragment_alphas(const Quad* const* q, int px, int py, float fx, float fy, float* out) {
+    float x[N], k[N], r[N], p[N];
+    bool covered[N];
+#pragma unroll
+    for (int t = 0; t < N; ++t) {
+        const bool in_box = px >= q[t]->x0 && px <= q[t]->x1 && py >= q[t]->y0 && py <= q[t]->y1;
+        const float ex = fsub(fx, q[t]->cx), ey = fsub(q[t]->cy, fy);
+        const float ox = fmul(fadd(fmul(ex, q[t]->ax), fmul(ey, q[t]->ay)), q[t]->ila);
+        const float oy = fmul(fsub(fmul(ex, q[t]->ay), fmul(ey, q[t]->ax)), q[t]->ilc);
+        covered[t] = in_box && fabsf(ox) <= q[t]->qm && fabsf(oy) <= q[t]->qm;
+        x[t] = -fadd(fmul(ox, ox), fmul(oy, oy));
+    }
+#pragma unroll
+    for (int t = 0; t < N; ++t) {
+        k[t] = rintf(fmul(x[t], 1.44269504f));
+        r[t] = fsub(fsub(x[t], fmul(k[t], 0.693359375f)), fmul(k[t], -2.12194440e-4f));
+        p[t] = 1.98412698e-4f;
+    }
+#pragma unroll
+    for (int t = 0; t < N; ++t) p[t] = fadd(fmul(p[t], r[t]), 1.38888889e-3f);
+#pragma unroll
+    for (int t = 0; t < N; ++t) p[t] = fadd(fmul(p[t], r[t]), 8.33333333e-3f);
+#pragma unroll
+    for (int t = 0; t < N; ++t) p[t] = fadd(fmul(p[t], r[t]), 4.16666667e-2f);
+#pragma unroll
+    for (int t = 0; t < N; ++t) p[t] = fadd(fmul(p[t], r[t]), 1.66666667e-1f);
+#pragma unroll
+    for (int t = 0; t < N; ++t) p[t] = fadd(fmul(p[t], r[t]), 0.5f);
+#pragma unroll
+    for (int t = 0; t < N; ++t) p[t] = fadd(fmul(p[t], r[t]), 1.0f);
+#pragma unroll
+    for (int t = 0; t < N; ++t) p[t] = fadd(fmul(p[t], r[t]), 1.0f);
+#pragma unroll
+    for (int t = 0; t < N; ++t) {
+        const int ki = max((int)fmaxf(k[t], -200.0f), -200);
+        const int k1 = ki < -126 ? ki + 126 : 0, k2 = ki < -126 ? -126 : ki;
+        const float e0 = fmul(fmul(p[t], __int_as_float((k1 + 127) << 23)), __int_as_float((k2 + 127) << 23));
+        const float e = (x[t] != x[t]) ? x[t] : (x[t] < -104.0f ? 0.0f : e0);
+        const float alpha = fminf(0.99f, fmul(e, q[t]->a));
+        out[t] = (covered[t] && !(alpha < 1.0f / 255.0f)) ? alpha : 0.0f;
+    }
 }
 
 // One CTA a tile, one thread a pixel: the tile's splats in order, staged in
@@ -384,8 +403,13 @@ __global__ void __launch_bounds__(256) blend_kernel(const Quad* __restrict__ qua
                     }
                 }
                 float al[4];
+                const Quad* qs[4];
 #pragma unroll
-                for (int t = 0; t < 4; ++t) al[t] = t < cnt ? fragment_alpha(staged[b][e[t]], px, py, fx, fy) : 0.0f;
+                for (int t = 0; t < 4; ++t) qs[t] = &staged[b][e[t]];
+                fragment_alphas<4>(qs, px, py, fx, fy, al);
+#pragma unroll
+                for (int t = 0; t < 4; ++t)
+                    if (t >= cnt) al[t] = 0.0f;
 #pragma unroll
                 for (int t = 0; t < 4; ++t) {
                     const float alpha = al[t];
