@@ -673,9 +673,30 @@ def served(ctx, args, rate_hz: float = 2000.0, seconds: float = 2.0):
         ctx.check(ctx.lib.ws_device_download(ctx.handle, c.data_ptr(), _ct.byref(cnt), 4, None))
 
     plain_wall, plain_lat = run(plain, lambda res: None)
+
+    # Saturated: every request queued at once (a closed queue), so the server
+    # batches as many as it admits; against one plain sort per request.
+    burst = reqs[:1024]
+    burst_splats = sum(scenes[k].count for k, _ in burst)
+    with Server(ctx, memory_budget=8 << 30, max_batch=64, streams=2) as srv:
+        t0 = time.perf_counter()
+        tickets = [srv.submit(scenes[sc], v) for sc, v in burst]
+        for tk in tickets:
+            collect(srv, tk)
+        sat_wall = time.perf_counter() - t0
+        sat = srv.stats()
+    t0 = time.perf_counter()
+    for sc, v in burst:
+        plain(scenes[sc], v)
+    sat_plain_wall = time.perf_counter() - t0
     for sp in scenes:
         sp.destroy()
     return {
+        "saturated": {"requests": len(burst), "splats": burst_splats,
+                      "served_msplats_s": burst_splats / sat_wall / 1e6,
+                      "plain_msplats_s": burst_splats / sat_plain_wall / 1e6,
+                      "served_vs_plain": sat_plain_wall / sat_wall, "mean_batch": sat["mean_batch"],
+                      "batches": sat["batches"]},
         "requests": len(reqs), "rate_hz": rate_hz, "scenes": len(scenes), "resident_bytes": resident,
         "splats": splats,
         "served_msplats_s": splats / wall / 1e6, "served_p50_ms": float(np.percentile(lat, 50)),
