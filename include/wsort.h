@@ -150,7 +150,10 @@ int ws_depth_range(const ws_cloud* cloud, const float model_view[16], int* visib
  * (binding 7), here `count`. order and keys (keys may be NULL) must hold the
  * cloud's count of u32; entries [0, *count) are written: order[j] is a splat
  * index, keys[j] its key (65535 - depth bucket, so the farthest first).
- * A cloud wholly behind the camera yields *count == 0.
+ * A cloud wholly behind the camera yields *count == 0. With WS_HOST_OUTPUT
+ * into pinned host memory (cudaHostAlloc / cudaMallocHost, or registered),
+ * the survivors are written into it by the device and the call synchronises
+ * once; other host memory is filled by copies after the count is known.
  * Errors: WS_ERR_ARG for a cull that is negative or not finite, with the
  * reference's message "splatCull must be 0 or more, got <cull>"
  * (src/render/renderer.js:1529); WS_ERR_UNLOADED for a freed cloud

@@ -306,3 +306,33 @@ def test_a_wait_that_runs_out_is_reported_and_the_context_recovers(ctx):
     assert rc == _lib.WS_ERR_TIMEOUT
     assert "device-side wait gave up" in ctx.lib.ws_last_error(ctx.handle).decode()
     check_job(ctx, W.uniform_100k(seed=77, n=50_000))
+
+
+def test_host_output_into_pinned_buffers(ctx):
+    """ws_sort with pinned host outputs takes the direct path (the survivors
+    written into the host buffers by a kernel, one synchronisation); the
+    result is the pageable path's, with and without keys, twice in a row."""
+    import ctypes
+
+    import torch
+
+    from winding_b200 import _lib
+    job = W.clusters_1m(seed=91, n=200_000)
+    splats = parse_splats(job.records, ctx)
+    view = make_view(job.view.model_view, job.view.projection, job.view.viewport, 0.5)
+    try:
+        want_o, want_k = ctx.sort(splats, view)
+        order = torch.full((splats.count,), -1, dtype=torch.int32).pin_memory()
+        keys = torch.full((splats.count,), -1, dtype=torch.int32).pin_memory()
+        cnt = ctypes.c_uint32()
+        for with_keys in (True, False, True):
+            ctx.check(ctx.lib.ws_sort(ctx.handle, splats.handle, ctypes.byref(view), order.data_ptr(),
+                                      keys.data_ptr() if with_keys else None, ctypes.byref(cnt),
+                                      _lib.WS_HOST_OUTPUT, None))
+            s = cnt.value
+            assert s == len(want_o)
+            assert np.array_equal(order[:s].numpy().view(np.uint32), want_o)
+            if with_keys:
+                assert np.array_equal(keys[:s].numpy().view(np.uint32), want_k)
+    finally:
+        splats.destroy()

@@ -618,7 +618,7 @@ static int decode_cloud(ws_ctx* ctx, const void* dev_records, uint32_t n, ws_clo
         ws_cloud_free(c);
         return cuda_error(ctx, e, "ws_cloud");
     }
-    uint32_t* words = nullptr;   // bounds[6], max |covariance|, bad
+    uint32_t* words = nullptr;   // bounds[6], unused, bad
     if ((e = cudaMalloc(&words, 8 * sizeof(uint32_t))) != cudaSuccess) {
         ws_cloud_free(c);
         return cuda_error(ctx, e, "ws_cloud");
@@ -640,13 +640,6 @@ static int decode_cloud(ws_ctx* ctx, const void* dev_records, uint32_t n, ws_clo
     if (back[7] != 0xFFFFFFFFu) {
         ws_cloud_free(c);
         return set_error(ctx, WS_ERR_NAN, "splats: splat %u has a position that is not a number", back[7]);
-    }
-    {
-        const uint32_t o = back[6];
-        const uint32_t u = (o & 0x80000000u) ? (o & 0x7FFFFFFFu) : ~o;
-        float f;
-        std::memcpy(&f, &u, 4);
-        c->smax = o ? f : 0.0f;   // NaN if any entry is NaN (then no shortcut applies)
     }
     for (int k = 0; k < 3; ++k) {
         uint32_t lo = back[k], hi = back[3 + k];
@@ -760,6 +753,39 @@ extern "C" int ws_depth_range(const ws_cloud* c, const float mv[16], int* visibl
 
 // ------------------------------------------------------------------ sorting
 
+// The device address of pinned host memory (mapped under unified
+// addressing), or null for any other pointer.
+static uint32_t* mapped_alias(uint32_t* p) {
+    cudaPointerAttributes a;
+    if (!p || cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    if (a.type != cudaMemoryTypeHost || !a.devicePointer) return nullptr;
+    return static_cast<uint32_t*>(a.devicePointer);
+}
+
+// The survivors' order (and keys) into mapped host memory, and the count and
+// the error words into `words`: consecutive threads write consecutive words,
+// so each warp's stores leave as whole 128-byte writes.
+__global__ void __launch_bounds__(256) copy_out_kernel(const uint32_t* __restrict__ order,
+                                                       const uint32_t* __restrict__ keys,
+                                                       const uint32_t* __restrict__ count,
+                                                       const uint32_t* __restrict__ err, uint32_t* horder,
+                                                       uint32_t* hkeys, uint32_t* words, uint32_t cap) {
+    const uint32_t c = *count;
+    const uint32_t s = c < cap ? c : cap;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        words[0] = c;
+        words[1] = err[0];
+        words[2] = err[1];
+    }
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < s; i += gridDim.x * blockDim.x) {
+        horder[i] = order[i];
+        if (hkeys) hkeys[i] = keys[i];
+    }
+}
+
 extern "C" int ws_sort(ws_ctx* ctx, const ws_cloud* cloud, const ws_view* view, uint32_t* order, uint32_t* keys,
                        uint32_t* count, int flags, void* stream_p) {
     if (!ctx) return WS_ERR_ARG;
@@ -782,6 +808,14 @@ extern "C" int ws_sort(ws_ctx* ctx, const ws_cloud* cloud, const ws_view* view, 
     // the survivors only.
     const size_t n = cloud->n;
     cudaError_t e;
+    // Pinned (device-mapped) host outputs: a small kernel after the sort
+    // reads the count on the device and writes the survivors straight into
+    // them, and the count and error words into the context's pinned words;
+    // one synchronisation instead of a count read-back and a second copy.
+    uint32_t* order_dev = mapped_alias(order);
+    uint32_t* keys_dev = keys ? mapped_alias(keys) : nullptr;
+    uint32_t* words_dev = mapped_alias(static_cast<uint32_t*>(ctx->count_h.p));
+    const bool direct = order_dev && words_dev && (!keys || keys_dev);
     if ((e = cudaEventSynchronize(ctx->launched)) != cudaSuccess) return cuda_error(ctx, e, "ws_sort");
     if ((e = ctx->out_d.ensure(align_up((2 * n + 1) * sizeof(uint32_t), 256))) != cudaSuccess)
         return cuda_error(ctx, e, "ws_sort output");
@@ -791,6 +825,16 @@ extern "C" int ws_sort(ws_ctx* ctx, const ws_cloud* cloud, const ws_view* view, 
     job.count = d + 2 * n;
     if ((rc = run_batch(ctx, &job, 1, stream))) return rc;
     uint32_t* hc = static_cast<uint32_t*>(ctx->count_h.p);
+    if (direct) {
+        const uint32_t blocks = std::max(1u, std::min((uint32_t)((n + 1023) / 1024), (uint32_t)ctx->sms * 4));
+        copy_out_kernel<<<blocks, 256, 0, stream>>>(job.order, job.keys, job.count, ctx->err_d, order_dev, keys_dev,
+                                                    words_dev, (uint32_t)n);
+        if ((e = cudaGetLastError()) != cudaSuccess || (e = cudaStreamSynchronize(stream)) != cudaSuccess)
+            return cuda_error(ctx, e, "ws_sort");
+        if (hc[1]) return take_device_error(ctx);
+        *count = hc[0];
+        return WS_OK;
+    }
     if ((e = cudaMemcpyAsync(hc, job.count, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
         (e = cudaMemcpyAsync(hc + 1, ctx->err_d, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
         (e = cudaStreamSynchronize(stream)) != cudaSuccess)

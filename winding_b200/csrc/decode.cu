@@ -28,16 +28,13 @@ __device__ __forceinline__ void covariance(float fsx, float fsy, float fsz, uint
 }
 
 // bounds: 3 ordered minima then 3 ordered maxima (initialised by the host to
-// 0xFFFFFFFF and 0), then the ordered maximum of |covariance entry| over the
-// cloud (initialised to 0); bad: first non-finite index (initialised to
-// 0xFFFFFFFF).
+// 0xFFFFFFFF and 0); bad: first non-finite index (initialised to 0xFFFFFFFF).
 __global__ void __launch_bounds__(256) decode_kernel(const uint4* __restrict__ rec, uint32_t n,
                                                      float4* __restrict__ centers, float2* __restrict__ cov,
                                                      int8_t* __restrict__ sexp, uint32_t* __restrict__ bounds,
                                                      uint32_t* __restrict__ bad) {
     uint32_t lo[3] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu};
     uint32_t hi[3] = {0u, 0u, 0u};
-    uint32_t smax = 0u;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint4 a = __ldcs(&rec[2 * (size_t)i]);
         const uint4 b = __ldcs(&rec[2 * (size_t)i + 1]);
@@ -68,8 +65,6 @@ __global__ void __launch_bounds__(256) decode_kernel(const uint4* __restrict__ r
             e = e < -100 ? -100 : (e > 127 ? 127 : e);
         }
         sexp[i] = (int8_t)e;
-#pragma unroll
-        for (int k = 0; k < 6; ++k) smax = max(smax, ordered(fabsf(c[k])));
         const uint32_t o[3] = {ordered(x), ordered(y), ordered(z)};
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
@@ -85,15 +80,12 @@ __global__ void __launch_bounds__(256) decode_kernel(const uint4* __restrict__ r
             hi[k] = max(hi[k], __shfl_xor_sync(0xffffffffu, hi[k], off));
         }
     }
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) smax = max(smax, __shfl_xor_sync(0xffffffffu, smax, off));
     if ((threadIdx.x & 31) == 0) {
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
             if (lo[k] != 0xFFFFFFFFu) atomicMin(&bounds[k], lo[k]);
             if (hi[k] != 0u) atomicMax(&bounds[3 + k], hi[k]);
         }
-        if (smax != 0u) atomicMax(&bounds[6], smax);
     }
 }
 

@@ -76,7 +76,6 @@ struct ws_cloud {
     float2* cov = nullptr;
     int8_t* sexp = nullptr;         // per splat: max |covariance entry| <= 2^sexp
     double bmin[3] = {0, 0, 0}, bmax[3] = {0, 0, 0};
-    float smax = 0.0f;              // largest |covariance entry| of the cloud
     uint32_t* sh = nullptr;         // harmonics: sh_words packed half-float words a splat, + 1
     uint32_t sh_degree = 0;         // 0: none
     uint32_t sh_words = 0;
