@@ -296,8 +296,8 @@ int ws_draw_tables(float* srgb, float* reach);
 /* ------------------------------------------------------------ serving */
 
 /*
- * A request loop over resident clouds (no counterpart in
- * the reference, which sorts once per frame on its own thread). Requests
+ * A request loop over resident clouds (no counterpart in the reference,
+ * which sorts once per frame on its own thread). Requests
  * (cloud, view) are submitted from any thread; a dispatcher thread batches
  * whatever has arrived into one persistent launch (continuous batching),
  * admitting requests in arrival order while their device memory (outputs
@@ -323,6 +323,7 @@ typedef struct ws_server_stats {
     double mean_batch;
     uint64_t max_batch_seen;
     uint64_t overlapped_batches; /* batches launched while another was still running */
+    uint64_t cancelled;         /* requests withdrawn by ws_server_cancel */
 } ws_server_stats;
 
 int ws_server_create(ws_ctx* ctx, const ws_server_opts* opts, ws_server** out);
@@ -344,6 +345,12 @@ int ws_server_wait(ws_server* server, uint64_t ticket, uint32_t* order, uint32_t
 int ws_server_result(ws_server* server, uint64_t ticket, const uint32_t** order, const uint32_t** keys,
                      uint32_t* count, int timeout_ms);
 int ws_server_release(ws_server* server, uint64_t ticket);
+/* Withdraws a request that is still queued (not yet in a batch): its ticket
+ * is forgotten and nothing is computed for it. WS_ERR_BUSY once it has been
+ * dispatched (collect it with ws_server_wait / result + release);
+ * WS_ERR_ARG for an unknown ticket. No counterpart in the reference (a frame
+ * there is never withdrawn). */
+int ws_server_cancel(ws_server* server, uint64_t ticket);
 int ws_server_get_stats(ws_server* server, ws_server_stats* out);
 /* Finishes the requests in flight, drops the queued ones, stops the threads. */
 int ws_server_destroy(ws_server* server);
@@ -373,6 +380,14 @@ int ws_sort_noalloc(const ws_cloud* cloud, const ws_view* view, uint32_t* order,
                     void* stream);
 
 /* ------------------------------------------------------------ self-test */
+
+/*
+ * Failure injection for tests: the next `count` growths of the library's
+ * device buffers (a context's sort scratch, job and item tables, outputs)
+ * fail as if the device were out of memory, across the process. The call
+ * that meets one returns WS_ERR_NOMEM and the context stays usable.
+ */
+int ws_inject_alloc_failures(int count);
 
 /*
  * Failure detection, exercised: queues one job whose first phase is left out,

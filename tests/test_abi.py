@@ -40,3 +40,9 @@ def test_view_struct_layout_matches_the_header():
     # float model_view[16], projection[16], viewport[2], cull
     assert ctypes.sizeof(_lib.WsView) == 35 * 4
     assert _lib.WsJob.view.offset == 8
+
+
+def test_alloc_failure_hook_takes_counts_only():
+    L = _lib.load()
+    assert L.ws_inject_alloc_failures(-1) == _lib.WS_ERR_ARG
+    assert L.ws_inject_alloc_failures(0) == _lib.WS_OK

@@ -121,6 +121,7 @@ class WsServerStats(ctypes.Structure):
         ("mean_batch", ctypes.c_double),
         ("max_batch_seen", ctypes.c_uint64),
         ("overlapped_batches", ctypes.c_uint64),
+        ("cancelled", ctypes.c_uint64),
     ]
 
 
@@ -172,6 +173,8 @@ SIGNATURES = {
     "ws_draw": (ctypes.c_int, [vp, vp, ctypes.POINTER(WsView), vp, vp, vp, vp, ctypes.c_uint32, ctypes.c_uint32, vp]),
     "ws_draw_tables": (ctypes.c_int, [ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]),
     "ws_selftest_wait": (ctypes.c_int, [vp, ctypes.c_uint32]),
+    "ws_inject_alloc_failures": (ctypes.c_int, [ctypes.c_int]),
+    "ws_server_cancel": (ctypes.c_int, [vp, ctypes.c_uint64]),
     "ws_cloud_harmonics": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_int), vp]),
     "ws_sort_batch_shaded": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(WsJob), ctypes.POINTER(WsShade), vp]),
     "ws_particle_thresholds": (ctypes.c_int, [ctypes.POINTER(ctypes.c_float)]),

@@ -5,6 +5,7 @@
 #include "wsort_host.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -38,9 +39,23 @@ int cuda_error(ws_ctx* ctx, cudaError_t e, const char* what) {
     return set_error(ctx, WS_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
 }
 
+// Device allocations that are to fail as if the device were out of memory
+// (ws_inject_alloc_failures): a test hook for the allocation-failure paths.
+static std::atomic<int> g_alloc_failures{0};
+
+extern "C" int ws_inject_alloc_failures(int count) {
+    if (count < 0) return WS_ERR_ARG;
+    g_alloc_failures.store(count);
+    return WS_OK;
+}
+
 cudaError_t DevBuf::ensure(size_t n) {
     if (n <= bytes) return cudaSuccess;
     release();
+    int pending = g_alloc_failures.load();
+    while (pending > 0 && !g_alloc_failures.compare_exchange_weak(pending, pending - 1)) {
+    }
+    if (pending > 0) return cudaErrorMemoryAllocation;
     const cudaError_t e = cudaMalloc(&p, n);
     if (e != cudaSuccess) {
         p = nullptr;

@@ -534,6 +534,24 @@ extern "C" int ws_server_result(ws_server* S, uint64_t ticket, const uint32_t** 
     return WS_OK;
 }
 
+extern "C" int ws_server_cancel(ws_server* S, uint64_t ticket) {
+    if (!S) return WS_ERR_ARG;
+    std::lock_guard<std::mutex> lock(S->mu);
+    auto it = S->reqs.find(ticket);
+    if (it == S->reqs.end()) return WS_ERR_ARG;
+    Request* r = it->second;
+    if (r->state != 0) return WS_ERR_BUSY;   // dispatched: collect it instead
+    for (auto q = S->queue.begin(); q != S->queue.end(); ++q)
+        if (*q == r) {
+            S->queue.erase(q);
+            break;
+        }
+    S->reqs.erase(it);
+    delete r;
+    ++S->stats.cancelled;
+    return WS_OK;
+}
+
 extern "C" int ws_server_release(ws_server* S, uint64_t ticket) {
     if (!S) return WS_ERR_ARG;
     std::unique_lock<std::mutex> lock(S->mu);

@@ -72,6 +72,14 @@ class Server:
             raise WsError(rc, f"ws_server_result: {_lib.ERROR_NAMES.get(rc, rc)}")
         return o.value, k.value, count.value
 
+    def cancel(self, ticket: int) -> bool:
+        """Withdraws a request still queued; False once it has been dispatched."""
+        rc = self.lib.ws_server_cancel(self.handle, ticket)
+        if rc == _lib.WS_ERR_BUSY:
+            return False
+        _lib.check(rc)
+        return True
+
     def release(self, ticket: int) -> None:
         rc = self.lib.ws_server_release(self.handle, ticket)
         if rc != _lib.WS_OK:
