@@ -178,10 +178,13 @@ void view_shortcuts(const ws_view& v, const ws_cloud* c, uint32_t* fast, uint32_
 // Fills job descriptors and lays the scratch out from `scratch`.
 // A job's tiles, scan items and scratch regions (job_shape's layout), from
 // `at` on; advances `at` past them.
-static void assign_scratch(JobDesc& d, uint32_t n, const ws_params& p, char*& at) {
+// `alone`: the job is its launch's only one (see kRedHiTiles).
+static void assign_scratch(JobDesc& d, uint32_t n, const ws_params& p, char*& at, bool alone) {
     size_t bytes;
     job_shape(n, p, &d.tiles, &bytes);
     d.scan_items = d.tiles <= kSmallScanTiles ? 1u : kScanItems;
+    d.red_hi = alone && d.tiles <= kRedHiTiles ? 1u : 0u;
+    d.hi_items = d.red_hi ? d.tiles : (d.tiles + kCountSpan - 1) / kCountSpan;
     const size_t np = pad_splats(n);
     d.k16 = reinterpret_cast<uint16_t*>(at);
     at += align_up(np * 2, 256);
@@ -217,7 +220,7 @@ static void layout_emitters(JobDesc* out, const ws_emitter* em, int njobs, const
         d.order = em[j].order;
         d.keys = em[j].keys;
         d.count = em[j].count;
-        assign_scratch(d, em[j].capacity, p, at);
+        assign_scratch(d, em[j].capacity, p, at, njobs == 1);
         d.ctl = reinterpret_cast<uint32_t*>(&ctls[j]);
     }
 }
@@ -246,7 +249,7 @@ void layout_jobs(JobDesc* out, const ws_job* jobs, int njobs, const ws_params& p
         d.keys = jobs[j].keys;
         d.count = jobs[j].count;
         view_shortcuts(jobs[j].view, c, &d.fast_transform, &d.keep_byte, &d.keep_q);
-        assign_scratch(d, c->n, p, at);
+        assign_scratch(d, c->n, p, at, njobs == 1);
         d.ctl = reinterpret_cast<uint32_t*>(&ctls[j]);
     }
 }
@@ -254,7 +257,7 @@ void layout_jobs(JobDesc* out, const ws_job* jobs, int njobs, const ws_params& p
 // Items of one phase of one job.
 static void push_phase(std::vector<uint2>& items, const JobDesc& d, uint32_t job, uint32_t phase) {
     const uint32_t count = (phase == kPhaseScanLo || phase == kPhaseScanHi) ? d.scan_items
-                           : phase == kPhaseCountHi ? (d.tiles + kCountSpan - 1) / kCountSpan
+                           : phase == kPhaseCountHi ? (d.red_hi ? 0u : d.hi_items)
                                                     : d.tiles;
     for (uint32_t t = 0; t < count; ++t) items.push_back(make_uint2(job, (phase << kPhaseShift) | t));
 }
@@ -428,7 +431,7 @@ int run_given_keys(ws_ctx* ctx, const uint16_t* keys, uint32_t n, uint32_t* orde
             d.order = order;
             d.keys = sorted;
             d.count = count;
-            assign_scratch(d, n, ctx->params, at);
+            assign_scratch(d, n, ctx->params, at, true);
             d.ctl = reinterpret_cast<uint32_t*>(scratch + sizeof(LaunchCtl));
         },
         stream);
@@ -909,7 +912,7 @@ extern "C" int ws_selftest_wait(ws_ctx* ctx, uint32_t spin_limit) {
     d.keys = outs + n;
     d.count = outs + 2 * n;
     char* at = base + align_up(sizeof(LaunchCtl) + sizeof(JobCtl), 256);
-    assign_scratch(d, n, ctx->params, at);
+    assign_scratch(d, n, ctx->params, at, true);
     d.ctl = reinterpret_cast<uint32_t*>(base + sizeof(LaunchCtl));
     std::vector<uint2> items;
     for (uint32_t t = 0; t < d.scan_items; ++t) items.push_back(make_uint2(0u, (kPhaseScanLo << kPhaseShift) | t));

@@ -46,7 +46,8 @@ constexpr uint32_t kSpinLimit = 1u << 22;
 
 // Tiles of the largest cloud, and the work items of one job of that size:
 // keys, low pass and high pass one per tile, high-digit counts one per two
-// tiles, and the two scans one per digit value.
+// tiles (none when the low pass counts them), and the two scans one per
+// digit value.
 constexpr uint32_t kMaxTiles = (WS_NOALLOC_MAX_SPLATS + kTile - 1) / kTile;
 constexpr uint32_t kMaxItems = 3 * kMaxTiles + (kMaxTiles + kCountSpan - 1) / kCountSpan + 2 * kScanItems;
 
@@ -79,7 +80,8 @@ __global__ void noalloc_setup_kernel(JobDesc desc, uint32_t tiles, uint32_t clea
     // The phases in order: keys, low scan, low pass, high counts, high scan,
     // high pass (the order ws_sort's work list has for a single job).
     const uint32_t scans = desc.scan_items;
-    const uint32_t counts[kPhases] = {tiles, scans, tiles, (tiles + kCountSpan - 1) / kCountSpan, scans, tiles};
+    const uint32_t hi_counts = desc.red_hi ? 0u : desc.hi_items;
+    const uint32_t counts[kPhases] = {tiles, scans, tiles, hi_counts, scans, tiles};
     uint32_t first = 0;
     for (uint32_t ph = 0; ph < kPhases; ++ph) {
         for (uint32_t t = tid; t < counts[ph]; t += stride) items[first + t] = make_uint2(0u, (ph << kPhaseShift) | t);
@@ -148,7 +150,7 @@ extern "C" int ws_sort_noalloc(const ws_cloud* cloud, const ws_view* view, uint3
     layout_jobs(&desc, &job, 1, p, base);
 
     const uint32_t tiles = desc.tiles;
-    const uint32_t n_items = 3 * tiles + (tiles + kCountSpan - 1) / kCountSpan + 2 * desc.scan_items;
+    const uint32_t n_items = 3 * tiles + (desc.red_hi ? 0u : desc.hi_items) + 2 * desc.scan_items;
     const uint32_t clear_bytes = (uint32_t)(((sizeof(LaunchCtl) + sizeof(JobCtl)) + 3) / 4 * 4);
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);

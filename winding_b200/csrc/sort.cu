@@ -13,8 +13,11 @@
 // Each digit pass is reduce-then-scan: per-tile digit counts (stored digit
 // major), a scan over tiles for each digit (ScanLo / ScanHi) that turns them
 // into each tile's starting offset per digit, then a stable warp-ranked
-// scatter. The low pass's counts
-// come out of the key phase for free. There is no serial chain between
+// scatter. The low pass's counts come out of the key phase for free. A job
+// alone in its launch, of up to kRedHiTiles tiles, gets the high pass's
+// counts from the low pass's scatter as well (atomic adds into the count of
+// the tile each element lands in), which takes the CountHi phase off its
+// critical path. There is no serial chain between
 // tiles, so a pass whose tiles all start at once (they do: each pass waits
 // for the whole of the one before) costs no look-back latency.
 //
@@ -592,7 +595,11 @@ __device__ void digit_tile(const JobDesc& J, int job, uint32_t tile, SortSmem<IP
     if (PASS == 0 && tile == 0 && tid == 0) *J.count = total;
     const uint32_t n_in = PASS == 0 ? J.n : total;
     const uint32_t base = tile * T;
-    if (base >= n_in) return;
+    if (base >= n_in) {   // an empty job's one tile: nothing to move, but counted
+        if (PASS == 0 && J.red_hi && tid == 0)
+            red_release_add(&reinterpret_cast<JobCtl*>(J.ctl)->done[kPhaseCountHi], 1u);
+        return;
+    }
     const uint32_t* cnt = PASS == 0 ? J.cnt_lo : J.cnt_hi;
     const uint32_t excl = __ldcg(&cnt[(size_t)tid * J.tiles + tile]);
     const uint32_t b = 0;
@@ -670,11 +677,19 @@ __device__ void digit_tile(const JobDesc& J, int job, uint32_t tile, SortSmem<IP
     if (tid == 0) sm.mark[2] = global_ns();
     // Write-out in chunks of four slots per thread: the chunk's staged
     // entries are read first, so their shared-memory loads overlap. The job's
-    // output pointers and size are read once, into registers.
+    // output pointers and size are read once, into registers. A low pass
+    // that counts the high digits adds each element to the count of its
+    // digit in the high pass's tile it lands in (tile g / T of its output);
+    // the keys phase zeroed those counts.
     constexpr int kChunk = 4;
+    constexpr uint32_t kTileShift = __builtin_ctz(T);
+    static_assert((1u << kTileShift) == T, "tiles are powers of two");
     const uint32_t n_out = J.n;
     uint16_t* const key_b = J.key_b;
     uint32_t* const idx_b = J.idx_b;
+    uint32_t* const cnt_hi = J.cnt_hi;
+    const size_t hi_row = J.tiles;
+    const bool red_hi = PASS == 0 && J.red_hi;
     uint32_t* const order = J.order;
     uint32_t* const keys_out = J.keys;
 #pragma unroll 1
@@ -706,6 +721,34 @@ __device__ void digit_tile(const JobDesc& J, int job, uint32_t tile, SortSmem<IP
                 if (keys_out) __stcs(&keys_out[g], key);
             }
         }
+        if (red_hi) {
+            // Lanes hold consecutive staged slots, so neighbours often land
+            // in the same tile with the same high digit: the first lane of
+            // each such run adds the run's length. (The job's choice is
+            // uniform, so every lane of the warp is here.)
+#pragma unroll
+            for (int q = 0; q < kChunk; ++q) {
+                const uint32_t s = (uint32_t)(r0 + q) * kThreads + tid;
+                const uint32_t key = kk[q];
+                const uint32_t g = key != 0xFFFFFFFFu ? sm.u.p.gofs[key & 255u] + s : n_out;
+                const bool put = g < n_out;
+                const uint32_t cell = put ? ((key >> 8) << 21) | (g >> kTileShift) : 0xFFFFFFFFu;
+                const uint32_t before = __shfl_up_sync(0xffffffffu, cell, 1);
+                const bool head = lane == 0 || cell != before;
+                const uint32_t heads = __ballot_sync(0xffffffffu, head);
+                if (put && head) {
+                    const uint32_t later = heads & ~((2u << lane) - 1u);
+                    const uint32_t end = later ? (uint32_t)__ffs(later) - 1u : 32u;
+                    atomicAdd(&cnt_hi[(key >> 8) * hi_row + (g >> kTileShift)], end - lane);
+                }
+            }
+        }
+    }
+    if (red_hi) {
+        // Published as a CountHi item (the job has none), for ScanHi; the
+        // item's own publication as a low-pass item follows as usual.
+        __syncthreads();
+        if (tid == 0) red_release_add(&reinterpret_cast<JobCtl*>(J.ctl)->done[kPhaseCountHi], 1u);
     }
 }
 
@@ -747,10 +790,11 @@ __global__ void __launch_bounds__(kThreads, MINB) sort_kernel(const JobDesc* __r
         JobCtl* ctl = reinterpret_cast<JobCtl*>(J.ctl);
         bool work = !sm.drain;   // after an error: claim the remaining items, do no work
         if (work && phase != kPhaseKeys && !(sm.ready_job == job && sm.ready_phase == phase)) {
-            // Items the phase before this one has: tiles, pairs of tiles, or
-            // one per digit.
+            // Items the phase before this one has: tiles, one per digit, or
+            // for ScanHi the items that count the high digits (CountHi's, or
+            // the low pass's when it counts them and publishes as CountHi).
             const uint32_t need = (phase == kPhaseLow || phase == kPhaseHigh) ? J.scan_items
-                                  : phase == kPhaseScanHi ? (J.tiles + kCountSpan - 1) / kCountSpan
+                                  : phase == kPhaseScanHi ? J.hi_items
                                                           : J.tiles;
             work = wait_phase(&ctl->done[phase - 1], need, sm, err, it, spin_limit);
             if (work && tid == 0) {
@@ -771,6 +815,9 @@ __global__ void __launch_bounds__(kThreads, MINB) sort_kernel(const JobDesc* __r
                         given_keys_tile(J, tile, sm);
                     else
                         keys_tile(J, job, tile, sm);
+                    // This tile's column of the high-digit counts, which a
+                    // red_hi job's low pass adds to.
+                    if (J.red_hi) J.cnt_hi[(size_t)tid * J.tiles + tile] = 0;
                     break;
                 case kPhaseScanLo:
                     if (J.scan_items == 1)

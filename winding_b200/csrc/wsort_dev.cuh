@@ -31,14 +31,23 @@ constexpr uint32_t kErrBounds = 3;        // a scatter position fell outside the
 // one before it.
 //   Keys     per tile of splats: cull, key, survivor bit, low-digit counts
 //   ScanLo   per digit: scan over tiles of the low-digit counts
-//   Low      per tile of splats: stable rank by the low key byte, scatter
+//   Low      per tile of splats: stable rank by the low key byte, scatter;
+//            in a job that counts its high digits here (red_hi) also adds
+//            each element to the count of its high digit in the output tile
+//            it lands in (one atomic add per run of equal cells in a warp)
 //   CountHi  per two tiles of the low pass's output: high-digit counts
+//            (none in a red_hi job)
 //   ScanHi   per digit: scan over tiles of the high-digit counts
 //   High     per tile of the low pass's output: stable rank by the high
 //            byte, scatter the final order and keys
 constexpr uint32_t kPhaseKeys = 0, kPhaseScanLo = 1, kPhaseLow = 2, kPhaseCountHi = 3, kPhaseScanHi = 4,
                    kPhaseHigh = 5, kPhases = 6;
 constexpr uint32_t kCountSpan = 2;        // tiles one CountHi item covers
+// A job alone in its launch with at most this many tiles counts its high
+// digits in the low pass (red_hi): a phase fewer on the critical path. In a
+// batch, CountHi items overlap other jobs' work and cost less than the atomic
+// adds; in a larger job of concentrated keys the adds meet on few counts.
+constexpr uint32_t kRedHiTiles = 1024;
 constexpr uint32_t kScanItems = 256;      // scan items per pass of a large job: one per digit value
 constexpr uint32_t kSmallScanTiles = 64;  // a job of at most this many tiles scans in one item
 
@@ -63,7 +72,7 @@ struct alignas(16) JobDesc {
     float proj[16];
     float viewport[2];
     float cull;
-    uint32_t pad0;
+    uint32_t red_hi;            // 1: the low pass counts the high digits (no CountHi items)
     // outputs
     uint32_t* order;            // >= n
     uint32_t* keys;             // >= n, or null
@@ -89,6 +98,8 @@ struct alignas(16) JobDesc {
     uint32_t sh_words;          // 32-bit words a splat: ceil(3 x coefficients / 2)
     // given keys (kind == kJobKeys): n 16-bit keys, every element a survivor
     const uint16_t* keys_in;
+    uint32_t hi_items;          // items that publish as CountHi: its own, or the low pass's (red_hi)
+    uint32_t pad1[3];
 };
 
 constexpr uint32_t kJobSplats = 0, kJobParticles = 1, kJobKeys = 2;
