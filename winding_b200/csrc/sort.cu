@@ -558,24 +558,45 @@ __device__ void scan_digit(uint32_t* cnt, uint32_t tiles, uint32_t d, uint32_t* 
 }
 
 // ScanLo / ScanHi of a job of at most kSmallScanTiles tiles, in one item:
-// thread d scans its digit's row serially, 16 loads in flight at a time (a
-// whole row in registers would spill the kernel's other phases).
-__device__ void scan_small(uint32_t* cnt, uint32_t tiles, uint32_t* tot) {
-    constexpr uint32_t V = 16;
-    uint32_t* row = cnt + (size_t)threadIdx.x * tiles;
+// thread d scans its digit's row. The count matrix is digit major, so a row
+// per thread would make every load and store of a warp touch 32 rows; the
+// rows go through shared memory instead, 16 tiles at a time: thread t moves
+// column t % 16 of rows t / 16, t / 16 + 16, ..., so each warp reads and
+// writes two runs of 64 contiguous bytes.
+template <int IPT>
+__device__ void scan_small(uint32_t* cnt, uint32_t tiles, uint32_t* tot, SortSmem<IPT>& sm) {
+    constexpr uint32_t V = 16, P = V + 1;   // chunk width; padded row stride (no bank conflicts)
+    static_assert(sizeof(sm.u) >= 256 * P * 4, "the chunk fits the phase union");
+    static_assert(kThreads == 256, "one row per thread, sixteen rows per pass of the CTA");
+    uint32_t* buf = reinterpret_cast<uint32_t*>(&sm.u);
+    const uint32_t tid = threadIdx.x, col = tid % V, row0 = tid / V;
+    const size_t gstride = (size_t)V * tiles;   // sixteen rows on
     uint32_t run = 0;
 #pragma unroll 1
     for (uint32_t c0 = 0; c0 < tiles; c0 += V) {
+        const bool in = c0 + col < tiles;
+        const uint32_t* src = cnt + (size_t)row0 * tiles + c0 + col;
         uint32_t v[V];
 #pragma unroll
-        for (uint32_t r = 0; r < V; ++r) v[r] = c0 + r < tiles ? __ldcg(&row[c0 + r]) : 0u;
+        for (uint32_t r = 0; r < V; ++r) v[r] = in ? __ldcg(src + r * gstride) : 0u;
 #pragma unroll
-        for (uint32_t r = 0; r < V; ++r) {
-            if (c0 + r < tiles) row[c0 + r] = run;
-            run += v[r];
+        for (uint32_t r = 0; r < V; ++r) buf[(row0 + r * V) * P + col] = v[r];
+        __syncthreads();
+#pragma unroll
+        for (uint32_t c = 0; c < V; ++c) {
+            const uint32_t x = buf[tid * P + c];
+            buf[tid * P + c] = run;
+            run += x;
         }
+        __syncthreads();
+        if (in) {
+            uint32_t* dst = cnt + (size_t)row0 * tiles + c0 + col;
+#pragma unroll
+            for (uint32_t r = 0; r < V; ++r) dst[r * gstride] = buf[(row0 + r * V) * P + col];
+        }
+        __syncthreads();   // the buffer is refilled for the next chunk
     }
-    tot[threadIdx.x] = run;
+    tot[tid] = run;
 }
 
 // Low / High: one stable counting pass over 8 key bits for one tile. The
@@ -821,7 +842,7 @@ __global__ void __launch_bounds__(kThreads, MINB) sort_kernel(const JobDesc* __r
                     break;
                 case kPhaseScanLo:
                     if (J.scan_items == 1)
-                        scan_small(J.cnt_lo, J.tiles, ctl->tot[0]);
+                        scan_small(J.cnt_lo, J.tiles, ctl->tot[0], sm);
                     else
                         scan_digit(J.cnt_lo, J.tiles, tile, ctl->tot[0], sm);
                     break;
@@ -829,7 +850,7 @@ __global__ void __launch_bounds__(kThreads, MINB) sort_kernel(const JobDesc* __r
                 case kPhaseCountHi: count_hi_item(J, job, tile, sm); break;
                 case kPhaseScanHi:
                     if (J.scan_items == 1)
-                        scan_small(J.cnt_hi, J.tiles, ctl->tot[1]);
+                        scan_small(J.cnt_hi, J.tiles, ctl->tot[1], sm);
                     else
                         scan_digit(J.cnt_hi, J.tiles, tile, ctl->tot[1], sm);
                     break;
