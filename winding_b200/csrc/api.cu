@@ -182,7 +182,7 @@ void view_shortcuts(const ws_view& v, const ws_cloud* c, uint32_t* fast, uint32_
 static void assign_scratch(JobDesc& d, uint32_t n, const ws_params& p, char*& at, bool alone) {
     size_t bytes;
     job_shape(n, p, &d.tiles, &bytes);
-    d.scan_items = d.tiles <= kSmallScanTiles ? 1u : kScanItems;
+    d.scan_items = d.tiles <= kSmallScanTiles ? kSmallScanItems : kScanItems;
     d.red_hi = alone && d.tiles <= kRedHiTiles ? 1u : 0u;
     d.hi_items = d.red_hi ? d.tiles : (d.tiles + kCountSpan - 1) / kCountSpan;
     const size_t np = pad_splats(n);

@@ -557,46 +557,37 @@ __device__ void scan_digit(uint32_t* cnt, uint32_t tiles, uint32_t d, uint32_t* 
     if (tid == 0) tot[d] = carry;
 }
 
-// ScanLo / ScanHi of a job of at most kSmallScanTiles tiles, in one item:
-// thread d scans its digit's row. The count matrix is digit major, so a row
-// per thread would make every load and store of a warp touch 32 rows; the
-// rows go through shared memory instead, 16 tiles at a time: thread t moves
-// column t % 16 of rows t / 16, t / 16 + 16, ..., so each warp reads and
-// writes two runs of 64 contiguous bytes.
+// ScanLo / ScanHi of a job of at most kSmallScanTiles tiles: item g scans the
+// rows of digits 32g .. 32g + 31, which are one contiguous block of the
+// digit-major count matrix (32 x tiles words). The block is read into shared
+// memory with coalesced loads, each of warp 0's lanes scans one row there,
+// and the block is written back the same way.
 template <int IPT>
-__device__ void scan_small(uint32_t* cnt, uint32_t tiles, uint32_t* tot, SortSmem<IPT>& sm) {
-    constexpr uint32_t V = 16, P = V + 1;   // chunk width; padded row stride (no bank conflicts)
-    static_assert(sizeof(sm.u) >= 256 * P * 4, "the chunk fits the phase union");
-    static_assert(kThreads == 256, "one row per thread, sixteen rows per pass of the CTA");
+__device__ void scan_rows(uint32_t* cnt, uint32_t tiles, uint32_t* tot, uint32_t g, SortSmem<IPT>& sm) {
+    constexpr uint32_t R = 256 / kSmallScanItems;   // rows an item scans
+    static_assert(sizeof(sm.u) >= R * (kSmallScanTiles + 1) * 4, "the block fits the phase union");
     uint32_t* buf = reinterpret_cast<uint32_t*>(&sm.u);
-    const uint32_t tid = threadIdx.x, col = tid % V, row0 = tid / V;
-    const size_t gstride = (size_t)V * tiles;   // sixteen rows on
-    uint32_t run = 0;
-#pragma unroll 1
-    for (uint32_t c0 = 0; c0 < tiles; c0 += V) {
-        const bool in = c0 + col < tiles;
-        const uint32_t* src = cnt + (size_t)row0 * tiles + c0 + col;
-        uint32_t v[V];
-#pragma unroll
-        for (uint32_t r = 0; r < V; ++r) v[r] = in ? __ldcg(src + r * gstride) : 0u;
-#pragma unroll
-        for (uint32_t r = 0; r < V; ++r) buf[(row0 + r * V) * P + col] = v[r];
-        __syncthreads();
-#pragma unroll
-        for (uint32_t c = 0; c < V; ++c) {
-            const uint32_t x = buf[tid * P + c];
-            buf[tid * P + c] = run;
+    const uint32_t tid = threadIdx.x;
+    const uint32_t P = tiles | 1u;                  // odd row stride: the row scans meet no bank conflict
+    uint32_t* block = cnt + (size_t)g * R * tiles;
+    const uint32_t words = R * tiles;
+#pragma unroll 4
+    for (uint32_t e = tid; e < words; e += kThreads) buf[(e / tiles) * P + e % tiles] = __ldcg(&block[e]);
+    __syncthreads();
+    if (tid < R) {
+        uint32_t run = 0;
+        uint32_t* row = buf + tid * P;
+#pragma unroll 4
+        for (uint32_t c = 0; c < tiles; ++c) {
+            const uint32_t x = row[c];
+            row[c] = run;
             run += x;
         }
-        __syncthreads();
-        if (in) {
-            uint32_t* dst = cnt + (size_t)row0 * tiles + c0 + col;
-#pragma unroll
-            for (uint32_t r = 0; r < V; ++r) dst[r * gstride] = buf[(row0 + r * V) * P + col];
-        }
-        __syncthreads();   // the buffer is refilled for the next chunk
+        tot[g * R + tid] = run;
     }
-    tot[tid] = run;
+    __syncthreads();
+#pragma unroll 4
+    for (uint32_t e = tid; e < words; e += kThreads) block[e] = buf[(e / tiles) * P + e % tiles];
 }
 
 // Low / High: one stable counting pass over 8 key bits for one tile. The
@@ -841,16 +832,16 @@ __global__ void __launch_bounds__(kThreads, MINB) sort_kernel(const JobDesc* __r
                     if (J.red_hi) J.cnt_hi[(size_t)tid * J.tiles + tile] = 0;
                     break;
                 case kPhaseScanLo:
-                    if (J.scan_items == 1)
-                        scan_small(J.cnt_lo, J.tiles, ctl->tot[0], sm);
+                    if (J.scan_items == kSmallScanItems)
+                        scan_rows(J.cnt_lo, J.tiles, ctl->tot[0], tile, sm);
                     else
                         scan_digit(J.cnt_lo, J.tiles, tile, ctl->tot[0], sm);
                     break;
                 case kPhaseLow: digit_tile<0>(J, job, tile, sm, err, it); break;
                 case kPhaseCountHi: count_hi_item(J, job, tile, sm); break;
                 case kPhaseScanHi:
-                    if (J.scan_items == 1)
-                        scan_small(J.cnt_hi, J.tiles, ctl->tot[1], sm);
+                    if (J.scan_items == kSmallScanItems)
+                        scan_rows(J.cnt_hi, J.tiles, ctl->tot[1], tile, sm);
                     else
                         scan_digit(J.cnt_hi, J.tiles, tile, ctl->tot[1], sm);
                     break;

@@ -49,7 +49,8 @@ constexpr uint32_t kCountSpan = 2;        // tiles one CountHi item covers
 // adds; in a larger job of concentrated keys the adds meet on few counts.
 constexpr uint32_t kRedHiTiles = 1024;
 constexpr uint32_t kScanItems = 256;      // scan items per pass of a large job: one per digit value
-constexpr uint32_t kSmallScanTiles = 64;  // a job of at most this many tiles scans in one item
+constexpr uint32_t kSmallScanTiles = 64;  // a job of at most this many tiles scans in ...
+constexpr uint32_t kSmallScanItems = 8;   // ... this many items per pass, 32 digit values each
 
 // One (cloud, view) to sort, as the persistent kernel reads it.
 struct alignas(16) JobDesc {
@@ -64,7 +65,7 @@ struct alignas(16) JobDesc {
     uint32_t fast_transform;    // affine model-view, reverse-Z perspective, no overflow possible
     uint32_t keep_byte;         // alpha bytes at or above this pass the footprint cull when ...
     float keep_q;               // ... keep_q 2^sexp <= 100 d^2 (+inf: never)
-    uint32_t scan_items;        // items of each scan phase: 1 (small job) or 256 (one per digit)
+    uint32_t scan_items;        // items of each scan phase: kSmallScanItems (small job) or 256 (one per digit)
     uint32_t kind;              // kJobSplats or kJobParticles
     uint32_t idx_base;          // added to every element index the order holds (a ring's first slot)
     // view: the values the reference writes into its Cloud uniform
