@@ -114,6 +114,33 @@ int ws_cloud_from_splat(ws_ctx* ctx, const uint8_t* bytes, size_t nbytes, ws_clo
  * version 4, and every malformed header the reference refuses.
  */
 int ws_cloud_load(ws_ctx* ctx, const uint8_t* bytes, size_t nbytes, ws_cloud** out);
+
+/* A decoded image: width x height pixels of 4 bytes (red, green, blue,
+ * alpha), row by row, exactly as stored -- never premultiplied, never
+ * colour-managed -- what the reference's decodeImage returns. */
+typedef struct ws_image {
+    uint32_t width, height;
+    const uint8_t* rgba;   /* width x height x 4 bytes */
+} ws_image;
+/* The caller's image decoder (decodeImage(bytes) -> {width, height, rgba},
+ * src/scene/splats.js:81-84): decodes one image file of a bundle (a .sog's
+ * lossless WebP) into *out and returns 0, or returns nonzero if it cannot.
+ * The pixels must stay readable until the next call or until ws_cloud_read
+ * returns. */
+typedef int (*ws_decode_image)(void* user, const uint8_t* bytes, size_t nbytes, ws_image* out);
+/*
+ * readSplats(bytes, {decodeImage}) (src/scene/splats.js:85-92): as
+ * ws_cloud_load, and a .sog -- a zip (stored or deflated entries, not zip64)
+ * of meta.json (version 2) and images, readSog :127-200 -- is unzipped and
+ * read on the host, its images decoded by `decode` (called with `user`),
+ * and its splats decoded on the device: log-encoded positions, smallest-three
+ * rotations, colour and scale codebooks, and the harmonics palette. With
+ * decode NULL a .sog is refused as the reference refuses it. Every refusal
+ * of readSog carries its message; where the reference would throw a
+ * TypeError (a meta.json member missing), the message names the member.
+ */
+int ws_cloud_read(ws_ctx* ctx, const uint8_t* bytes, size_t nbytes, ws_decode_image decode, void* user,
+                  ws_cloud** out);
 /* The cloud's harmonics degree (0-3) and, when words is not NULL, its
  * count x ceil(3 c / 2) packed words (the layout of ws_cloud_set_harmonics). */
 int ws_cloud_harmonics(const ws_cloud* cloud, int* degree, uint32_t* words);

@@ -711,6 +711,67 @@ extern "C" int or_decode_spz(const uint8_t* data, size_t len, uint32_t* count, u
     return 0;
 }
 
+// readSog's loop (scene/splats.js:167-199). Positions were stored as
+// sign(x) ln(|x| + 1) in 16 bits over the means' range; rotations as the
+// three smallest components of w x y z, the largest named by the alpha
+// byte (252 + its index); colours, scales and harmonics through codebooks.
+extern "C" int or_decode_sog(uint32_t n, uint32_t degree, const uint8_t* low, const uint8_t* high,
+                             const uint8_t* quats, const uint8_t* scales, const uint8_t* sh0, const uint8_t* labels,
+                             const uint8_t* palette, uint32_t palette_width, size_t palette_bytes,
+                             const double mins[3], const double maxs[3], const double scale_book[256],
+                             const double colour_book[256], const double sh_book[256], double sh_count,
+                             float* centers, float* cov, uint32_t* sh, double bmin[3], double bmax[3], uint32_t* bad) {
+    for (int k = 0; k < 3; ++k) {
+        bmin[k] = INFINITY;
+        bmax[k] = -INFINITY;
+    }
+    const uint32_t per = kCoefs[degree], words = (per * 3 + 1) / 2;
+    for (uint32_t i = 0; i < n; ++i) {
+        const size_t o = (size_t)i * 4;
+        double m[3];
+        for (int a = 0; a < 3; ++a) {
+            const double v = (double)(low[o + a] | (high[o + a] << 8));
+            double range = maxs[a] - mins[a];
+            if (!(range != 0.0)) range = 1.0;   // (maxs - mins) || 1
+            const double t = mins[a] + range * v / 65535.0;
+            const double e = or_exp(std::fabs(t)) - 1.0;
+            m[a] = t < 0 ? -e : e;
+        }
+        double q[4] = {1, 0, 0, 0};
+        const uint32_t tag = quats[o + 3];
+        if (tag >= 252) {
+            const uint32_t largest = tag - 252;
+            uint32_t k = 0;
+            double sum = 0;
+            for (uint32_t c = 0; c < 4; ++c) {
+                if (c == largest) continue;
+                q[c] = ((quats[o + k++] / 255.0) * 2.0 - 1.0) / 1.4142135623730951;
+                sum += q[c] * q[c];
+            }
+            q[largest] = std::sqrt(std::fmax(0.0, 1.0 - sum));
+        }
+        uint32_t colour = (uint32_t)sh0[o + 3] << 24;
+        for (int k = 0; k < 3; ++k) colour |= or_byte(0.5 + kC0 * colour_book[sh0[o + k]]) << (8 * k);
+        const double sx = or_exp(scale_book[scales[o]]), sy = or_exp(scale_book[scales[o + 1]]),
+                     sz = or_exp(scale_book[scales[o + 2]]);
+        if (!put_d(i, m[0], m[1], m[2], colour, sx, sy, sz, q[0], q[1], q[2], q[3], centers, cov, bmin, bmax)) {
+            *bad = i;
+            return -4;
+        }
+        if (degree == 0) continue;
+        const double label = (double)(labels[o] | (labels[o + 1] << 8));
+        if (label >= sh_count) continue;
+        const uint32_t lab = (uint32_t)label;
+        const size_t row = (size_t)(lab / 64) * palette_width + (size_t)(lab % 64) * per;
+        for (uint32_t k = 0; k < per; ++k) {
+            const size_t c = (row + k) * 4;
+            if (c + 2 >= palette_bytes) break;
+            put_sh(sh, words, i, k, sh_book[palette[c]], sh_book[palette[c + 1]], sh_book[palette[c + 2]]);
+        }
+    }
+    return 0;
+}
+
 // ------------------------------------------------------------------ draw
 
 extern "C" void or_draw_tables(float srgb[256], float reach[256]) {

@@ -159,6 +159,21 @@ int or_decode_spz(const uint8_t* data, size_t len, uint32_t* count, uint32_t* de
                   uint32_t* sh, double bmin[3], double bmax[3], uint32_t* bad, char* err, size_t errlen);
 
 /*
+ * readSog's per-splat loop (scene/splats.js:167-199) on images already
+ * decoded and meta.json's numbers already read: pixel i of each image is its
+ * bytes 4i .. 4i + 3 (labels and the palette only when degree > 0). mins,
+ * maxs: the means' ranges; the codebooks hold 256 numbers each (NaN where
+ * the reference's array has no entry); sh_count is shN.count as a number.
+ * Returns 0, or -4 with *bad the first splat whose position is not finite.
+ */
+int or_decode_sog(uint32_t n, uint32_t degree, const uint8_t* low, const uint8_t* high, const uint8_t* quats,
+                  const uint8_t* scales, const uint8_t* sh0, const uint8_t* labels, const uint8_t* palette,
+                  uint32_t palette_width, size_t palette_bytes, const double mins[3], const double maxs[3],
+                  const double scale_book[256], const double colour_book[256], const double sh_book[256],
+                  double sh_count, float* centers, float* cov, uint32_t* sh, double bmin[3], double bmax[3],
+                  uint32_t* bad);
+
+/*
  * The splat draw (render/splats.js:252-312) as the library pins it: for each
  * of the first `count` splats of `order`, in order, the quad the vertex
  * shader builds and the fragments of the pixels whose centres its inverse

@@ -82,6 +82,10 @@ def _declare(L):
     L.or_decode_spz.restype = ctypes.c_int
     L.or_decode_spz.argtypes = [_u8p, ctypes.c_size_t, _u32p, _u32p, _f32p, _f32p, _u32p, _f64p, _f64p, _u32p,
                                 ctypes.c_char_p, ctypes.c_size_t]
+    L.or_decode_sog.restype = ctypes.c_int
+    L.or_decode_sog.argtypes = [ctypes.c_uint32, ctypes.c_uint32] + [_u8p] * 7 + [
+        ctypes.c_uint32, ctypes.c_size_t, _f64p, _f64p, _f64p, _f64p, _f64p, ctypes.c_double, _f32p, _f32p, _u32p,
+        _f64p, _f64p, _u32p]
     L.or_draw_tables.restype = None
     L.or_draw_tables.argtypes = [_f32p, _f32p]
     L.or_draw.restype = None
@@ -413,6 +417,259 @@ def parse_spz(gz: bytes) -> Capture:
     if rc == -4:
         raise OracleError(-4, f"splats: splat {bad.value} has a position that is not a number", bad.value)
     return Capture(n, centers, cov, bmin, bmax, d, sh)
+
+
+# ------------------------------------------------------------------ .sog
+
+class _Undefined:
+    """JavaScript's undefined: a property the parsed meta.json does not have."""
+
+    def __repr__(self):
+        return "undefined"
+
+
+UNDEFINED = _Undefined()
+
+
+def js_string(v) -> str:
+    """String(v) for a value JSON.parse can give (or undefined)."""
+    if v is UNDEFINED:
+        return "undefined"
+    if v is None:
+        return "null"
+    if v is True or v is False:
+        return "true" if v else "false"
+    if isinstance(v, (int, float)):
+        return js_number_string(float(v))
+    if isinstance(v, str):
+        return v
+    if isinstance(v, list):   # Array.prototype.join: null and undefined as ""
+        return ",".join("" if (x is None or x is UNDEFINED) else js_string(x) for x in v)
+    return "[object Object]"
+
+
+def js_number_string(v: float) -> str:
+    """Number::toString (ECMA-262 6.1.6.1.20) from the shortest round-trip digits."""
+    if v != v:
+        return "NaN"
+    if v == 0:
+        return "0"
+    if v in (float("inf"), float("-inf")):
+        return "Infinity" if v > 0 else "-Infinity"
+    if v < 0:
+        return "-" + js_number_string(-v)
+    mant, _, exp = repr(v).partition("e")
+    ip, _, fp = mant.partition(".")
+    digits = (ip + fp).lstrip("0")
+    lead = len(ip + fp) - len((ip + fp).lstrip("0"))
+    n = len(ip) - lead + (int(exp) if exp else 0)   # value = 0.digits x 10^n
+    digits = digits.rstrip("0")
+    k = len(digits)
+    if k <= n <= 21:
+        return digits + "0" * (n - k)
+    if 0 < n <= 21:
+        return digits[:n] + "." + digits[n:]
+    if -6 < n <= 0:
+        return "0." + "0" * (-n) + digits
+    e = n - 1
+    return digits[0] + ("." + digits[1:] if k > 1 else "") + "e" + ("+" if e >= 0 else "-") + str(abs(e))
+
+
+def js_to_number(v) -> float:
+    """ToNumber(v) for a value JSON.parse can give (or undefined)."""
+    if v is UNDEFINED:
+        return float("nan")
+    if v is None or v is False:
+        return 0.0
+    if v is True:
+        return 1.0
+    if isinstance(v, (int, float)):
+        return float(v)
+    if isinstance(v, str):
+        return _to_number(v)
+    return _to_number(js_string(v))   # ToPrimitive of an array or object is its string
+
+
+def _get(v, key):
+    """v[key] in JavaScript for JSON values; None when that would throw (v
+    null or undefined)."""
+    if v is None or v is UNDEFINED:
+        return None
+    if isinstance(v, dict):
+        return v.get(str(key), UNDEFINED)
+    if isinstance(v, list):
+        return v[key] if isinstance(key, int) and 0 <= key < len(v) else UNDEFINED
+    if isinstance(v, str):
+        return v[key] if isinstance(key, int) and 0 <= key < len(v) else UNDEFINED
+    return UNDEFINED
+
+
+def _truthy(v) -> bool:
+    if v is None or v is UNDEFINED or v is False:
+        return False
+    if isinstance(v, (int, float)) and not isinstance(v, bool):
+        return not (v == 0 or v != v)
+    if isinstance(v, str):
+        return v != ""
+    return True
+
+
+def _unzip(data: bytes) -> dict:
+    """The zip directory walk of readSplats (scene/splats.js:95-125): name ->
+    entry bytes (deflated entries inflated), stored and deflate only."""
+    import zlib
+    n = len(data)
+    u16 = lambda o: int.from_bytes(data[o:o + 2], "little")
+    u32 = lambda o: int.from_bytes(data[o:o + 4], "little")
+    end = -1
+    for i in range(n - 22, max(0, n - 22 - 65535) - 1, -1):
+        if i >= 0 and u32(i) == 0x06054B50:
+            end = i
+            break
+    if end < 0:
+        raise OracleError(-20, "splats: a zip with no end record: cut short?")
+    files = {}
+    at = u32(end + 16)
+    for _ in range(u16(end + 10)):
+        if at + 46 > n or u32(at) != 0x02014B50:
+            raise OracleError(-21, "splats: a zip whose directory is damaged")
+        method, size, name_len, local = u16(at + 10), u32(at + 20), u16(at + 28), u32(at + 42)
+        name = data[at + 46:at + 46 + name_len].decode("utf-8", "replace")
+        if name.startswith("\ufeff"):
+            name = name[1:]
+        if size == 0xFFFFFFFF or local == 0xFFFFFFFF:
+            raise OracleError(-22, "splats: a zip64 .sog is not read")
+        at += 46 + name_len + u16(at + 30) + u16(at + 32)
+        start = local + 30 + u16(local + 26) + u16(local + 28)
+        if start + size > n:
+            raise OracleError(-23, f"splats: the zip is cut short in {name}")
+        stored = data[start:start + size]
+        if method not in (0, 8):
+            raise OracleError(-24, f"splats: {name} is compressed with method {method}; stored and deflate are read")
+        files[name] = (method, stored)
+    return files
+
+
+def _inflate(entry) -> bytes:
+    import zlib
+    method, stored = entry
+    return bytes(stored) if method == 0 else zlib.decompress(bytes(stored), -15)
+
+
+def parse_sog(data: bytes, decode_image=None) -> Capture:
+    """readSog (scene/splats.js:127-200): the container, meta.json and the
+    checks restated here with the reference's messages, in its order; the
+    per-splat loop in oracle.cpp. decode_image(bytes) -> (width, height,
+    rgba) plays the reference's decodeImage."""
+    import json
+    if decode_image is None:
+        raise OracleError(-25, "splats: a .sog needs decodeImage, for its WebP images")
+    data = bytes(data)
+    files = _unzip(data)
+
+    def file(name):
+        if not isinstance(name, str) or name not in files:
+            raise OracleError(-26, f"splats: the .sog has no {js_string(name)}")
+        return _inflate(files[name])
+
+    text = file("meta.json").decode("utf-8", "replace")
+    if text.startswith("\ufeff"):
+        text = text[1:]
+    try:
+        meta = json.loads(text)
+    except ValueError:
+        raise OracleError(-27, "splats: the .sog's meta.json is not JSON")
+    version = _get(meta, "version")
+    if version is None:
+        raise OracleError(-28, "splats: the .sog's meta.json has no version")
+    if not (isinstance(version, (int, float)) and not isinstance(version, bool) and version == 2):
+        shown = "1" if version is UNDEFINED or version is None else js_string(version)
+        raise OracleError(-29, f"splats: a .sog of version {shown}; version 2 is read (re-save it with splat-transform)")
+    count = _get(meta, "count")
+    if not (isinstance(count, (int, float)) and not isinstance(count, bool) and count == count
+            and float(count).is_integer() and count > 0):
+        raise OracleError(-30, f"splats: a .sog of {js_string(count)} splats")
+    count = int(count)
+
+    def member(path):
+        """meta.path; reading a property of null or undefined (JavaScript's
+        TypeError) names the member that is missing."""
+        v, shown = meta, []
+        for key in path:
+            if v is None or v is UNDEFINED:
+                raise OracleError(-31, "splats: the .sog's meta.json has no " + ".".join(shown))
+            v = _get(v, key)
+            shown.append(str(key))
+        return v
+
+    def decoded(name):
+        w, h, rgba = decode_image(file(name))
+        return int(w), int(h), np.frombuffer(bytes(rgba), np.uint8)
+
+    names = [member(("means", "files", 0)), member(("means", "files", 1)), member(("quats", "files", 0)),
+             member(("scales", "files", 0)), member(("sh0", "files", 0))]
+    for nm in names:
+        file(nm)
+    images = []
+    for nm in names:
+        w, h, rgba = decoded(nm)
+        if w * h < count:
+            raise OracleError(-32, f"splats: {js_string(nm)} has {w * h} pixels, for {count} splats")
+        images.append(rgba)
+    shn = _get(meta, "shN")
+    bands = _get(shn, "bands") if _truthy(shn) else 0
+    if bands is None:
+        bands = UNDEFINED
+    key = js_string(bands) if isinstance(bands, str) else (js_number_string(float(bands))
+                                                              if isinstance(bands, (int, float)) and not isinstance(bands, bool) else None)
+    degree = int(key) if key in ("1", "2", "3") else 0
+    per = SH_COEFFICIENTS[degree]
+    labels = np.zeros(4, np.uint8)
+    palette = np.zeros(4, np.uint8)
+    pw = 0
+    if degree > 0:
+        pw, _, palette = decoded(member(("shN", "files", 0)))
+        lname = member(("shN", "files", 1))
+        lw, lh, labels = decoded(lname)
+        if lw * lh < count:
+            raise OracleError(-32, f"splats: {js_string(lname)} has {lw * lh} pixels, for {count} splats")
+        if pw != 64 * per:
+            raise OracleError(-33, f"splats: the .sog's harmonic palette is {pw} wide; {64 * per} for degree {degree}")
+
+    def book(path):
+        b = member(path)
+        if b is None or b is UNDEFINED:
+            raise OracleError(-31, "splats: the .sog's meta.json has no " + ".".join(path))
+        return np.array([js_to_number(_get(b, k)) for k in range(256)], np.float64)
+
+    def triple(path):
+        b = member(path)
+        if b is None or b is UNDEFINED:
+            raise OracleError(-31, "splats: the .sog's meta.json has no " + ".".join(path))
+        return np.array([js_to_number(_get(b, k)) for k in range(3)], np.float64)
+
+    mins, maxs = triple(("means", "mins")), triple(("means", "maxs"))
+    colour_book = book(("sh0", "codebook"))
+    scale_book = book(("scales", "codebook"))
+    sh_book = book(("shN", "codebook")) if degree > 0 else np.zeros(256, np.float64)
+    sh_count = js_to_number(_get(shn, "count")) if degree > 0 else 0.0
+    pix = [np.ascontiguousarray(im[:count * 4]) for im in images]
+    lab = np.ascontiguousarray(labels[:count * 4]) if degree > 0 else np.zeros(4, np.uint8)
+    pal = np.ascontiguousarray(palette)
+    centers = np.zeros((count, 4), np.float32)
+    cov = np.zeros((count, 6), np.float32)
+    sh = np.zeros(count * sh_words(degree) + 1 if degree else 1, np.uint32)
+    bmin = np.zeros(3, np.float64)
+    bmax = np.zeros(3, np.float64)
+    bad = ctypes.c_uint32(0)
+    rc = lib().or_decode_sog(count, degree, *[_ptr(p, _u8p) for p in pix], _ptr(lab, _u8p), _ptr(pal, _u8p), pw,
+                             pal.size, _ptr(mins, _f64p), _ptr(maxs, _f64p), _ptr(scale_book, _f64p),
+                             _ptr(colour_book, _f64p), _ptr(sh_book, _f64p), sh_count, _ptr(centers, _f32p),
+                             _ptr(cov, _f32p), _ptr(sh, _u32p), _ptr(bmin, _f64p), _ptr(bmax, _f64p),
+                             ctypes.byref(bad))
+    if rc == -4:
+        raise OracleError(-4, f"splats: splat {bad.value} has a position that is not a number", bad.value)
+    return Capture(count, centers, cov, bmin, bmax, degree, sh)
 
 
 def draw_tables():

@@ -5,6 +5,7 @@ The compute path is the CUDA library; this package is its Python host side
 (ctypes), mirroring the reference's parseSplats / Splats / SplatPass.
 """
 from ._lib import WsError
-from .splats import Context, Plan, SplatPass, Splats, load_splats, make_view, parse_splats, SPLAT_CULL
+from .splats import Context, Plan, SplatPass, Splats, load_splats, make_view, parse_splats, read_splats, SPLAT_CULL
 
-__all__ = ["WsError", "Context", "Plan", "SplatPass", "Splats", "load_splats", "make_view", "parse_splats", "SPLAT_CULL"]
+__all__ = ["WsError", "Context", "Plan", "SplatPass", "Splats", "load_splats", "make_view", "parse_splats", "read_splats",
+           "SPLAT_CULL"]

@@ -105,6 +105,15 @@ class WsServerOpts(ctypes.Structure):
     ]
 
 
+class WsImage(ctypes.Structure):
+    _fields_ = [("width", ctypes.c_uint32), ("height", ctypes.c_uint32), ("rgba", ctypes.c_void_p)]
+
+
+# int (*ws_decode_image)(void* user, const uint8_t* bytes, size_t nbytes, ws_image* out)
+DECODE_IMAGE = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint8), ctypes.c_size_t,
+                                ctypes.POINTER(WsImage))
+
+
 class WsServerStats(ctypes.Structure):
     _fields_ = [
         ("submitted", ctypes.c_uint64),
@@ -176,6 +185,7 @@ SIGNATURES = {
     "ws_inject_alloc_failures": (ctypes.c_int, [ctypes.c_int]),
     "ws_server_cancel": (ctypes.c_int, [vp, ctypes.c_uint64]),
     "ws_cloud_harmonics": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_int), vp]),
+    "ws_cloud_read": (ctypes.c_int, [vp, vp, ctypes.c_size_t, vp, vp, ctypes.POINTER(ctypes.c_void_p)]),
     "ws_sort_batch_shaded": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(WsJob), ctypes.POINTER(WsShade), vp]),
     "ws_particle_thresholds": (ctypes.c_int, [ctypes.POINTER(ctypes.c_float)]),
     "ws_server_create": (ctypes.c_int, [vp, ctypes.POINTER(WsServerOpts), ctypes.POINTER(vp)]),

@@ -1,5 +1,6 @@
 // Capture formats besides .splat, decoded on the device: the binary .ply that
-// training writes and Niantic's .spz (readSplats, src/scene/splats.js:60-90).
+// training writes, Niantic's .spz and PlayCanvas's .sog (readSplats,
+// src/scene/splats.js:60-92).
 //
 // The host does what the reference's browser does for it -- reading the
 // .ply's text header, gunzipping a .spz (the reference's DecompressionStream;
@@ -9,6 +10,8 @@
 // on the device, in the reference's double arithmetic (jsmath.cuh, put.cuh).
 //   .ply  parsePly   src/scene/splats.js:398-468
 //   .spz  parseSpz   src/scene/splats.js:227-303
+//   .sog  readSog    src/scene/splats.js:95-200 (images decoded by the caller's
+//                    decoder, as the reference's by its decodeImage)
 #include "jsmath.cuh"
 #include "put.cuh"
 #include "wsort.h"
@@ -20,6 +23,8 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <algorithm>
+#include <initializer_list>
 #include <map>
 #include <new>
 #include <sstream>
@@ -261,6 +266,79 @@ __global__ void __launch_bounds__(256) spz_kernel(const uint8_t* __restrict__ da
                         jsmath::signed_half(((double)h[k * 3 + ch] - 128.0) / 128.0 * (double)kSpzShFlip[k]);
             put_halves(o, i, halves, 3 * nc);
         }
+    }
+    finish_box(o, box);
+}
+
+// .sog (readSog, scene/splats.js:167-199): images already decoded on the
+// host, pixel i of each at bytes 4i .. 4i + 3; the codebooks as numbers.
+struct SogLayout {
+    uint32_t count, degree, per, palette_width;
+    unsigned long long palette_bytes;
+    const uint8_t *low, *high, *quats, *scales, *sh0, *labels, *palette;
+    const double* books;   // scales' codebook, then sh0's, then shN's: 256 each (NaN: no entry)
+    double mins[3], maxs[3];
+    double sh_count;       // shN.count as a number
+};
+
+__global__ void __launch_bounds__(256) sog_kernel(SogLayout L, Sink o) {
+    Box box;
+    for (int k = 0; k < 3; ++k) {
+        box.lo[k] = ~0ull;
+        box.hi[k] = 0ull;
+    }
+    const double* scale_book = L.books;
+    const double* colour_book = L.books + 256;
+    const double* sh_book = L.books + 512;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < L.count; i += gridDim.x * blockDim.x) {
+        const size_t o4 = (size_t)i * 4;
+        // Positions were stored as sign(x) ln(|x| + 1), 16 bits over the
+        // means' range ((maxs - mins) || 1).
+        double m[3];
+        for (int a = 0; a < 3; ++a) {
+            const double v = (double)(L.low[o4 + a] | (L.high[o4 + a] << 8));
+            double range = L.maxs[a] - L.mins[a];
+            if (!(range != 0.0)) range = 1.0;
+            const double t = L.mins[a] + range * v / 65535.0;
+            const double e = jsmath::exp_js(fabs(t)) - 1.0;
+            m[a] = t < 0 ? -e : e;
+        }
+        // w x y z less the largest, which the alpha byte (252 + its index)
+        // names and unit length gives back; below 252, no rotation.
+        double q[4] = {1.0, 0.0, 0.0, 0.0};
+        const uint32_t tag = L.quats[o4 + 3];
+        if (tag >= 252) {
+            const uint32_t largest = tag - 252;
+            uint32_t k = 0;
+            double sum = 0.0;
+            for (uint32_t c = 0; c < 4; ++c) {
+                if (c == largest) continue;
+                q[c] = (((double)L.quats[o4 + k++] / 255.0) * 2.0 - 1.0) / 1.4142135623730951;
+                sum = sum + q[c] * q[c];
+            }
+            q[largest] = sqrt(fmax(0.0, 1.0 - sum));
+        }
+        uint32_t colour = (uint32_t)L.sh0[o4 + 3] << 24;
+        for (int k = 0; k < 3; ++k) colour |= jsmath::js_byte(0.5 + kShC0 * colour_book[L.sh0[o4 + k]]) << (8 * k);
+        const double sx = jsmath::exp_js(scale_book[L.scales[o4]]);
+        const double sy = jsmath::exp_js(scale_book[L.scales[o4 + 1]]);
+        const double sz = jsmath::exp_js(scale_book[L.scales[o4 + 2]]);
+        if (!put_splat(o, box, i, m[0], m[1], m[2], colour, sx, sy, sz, q[0], q[1], q[2], q[3])) continue;
+        if (!o.sh) continue;
+        // The palette: label / 64 rows of 64 entries, each `per` pixels of
+        // red, green and blue codebook indices.
+        const double label = (double)(L.labels[o4] | (L.labels[o4 + 1] << 8));
+        if (label >= L.sh_count) continue;
+        const uint32_t lab = (uint32_t)label;
+        const unsigned long long row = (unsigned long long)(lab / 64) * L.palette_width + (lab % 64) * L.per;
+        uint32_t halves[45];
+        uint32_t nh = 0;
+        for (uint32_t k = 0; k < L.per; ++k) {
+            const unsigned long long c = (row + k) * 4;
+            if (c + 2 >= L.palette_bytes) break;
+            for (int ch = 0; ch < 3; ++ch) halves[nh++] = jsmath::signed_half(sh_book[L.palette[c + ch]]);
+        }
+        put_halves(o, i, halves, nh);
     }
     finish_box(o, box);
 }
@@ -635,6 +713,558 @@ int load_spz(ws_ctx* ctx, const uint8_t* gz, size_t len, ws_cloud** out) {
     return rc;
 }
 
+// ------------------------------------------------------------------- .sog
+// The container (a zip: unzip, scene/splats.js:95-125), meta.json and the
+// checks of readSog (:127-166), with the reference's messages, on the host;
+// the caller's decoder plays decodeImage.
+
+// A value JSON.parse gives, or undefined (a property that is not there).
+struct Json {
+    enum Kind : uint8_t { kUndefined, kNull, kBool, kNumber, kString, kArray, kObject };
+    Kind kind = kUndefined;
+    bool b = false;
+    double num = 0.0;
+    std::string str;
+    std::vector<Json> items;
+    std::vector<std::pair<std::string, Json>> fields;
+};
+
+// JSON.parse's grammar (RFC 8259): duplicate keys, the last wins. Nesting
+// is limited (a deeper document is refused, as V8 refuses one too deep
+// for its stack).
+class JsonParser {
+  public:
+    JsonParser(const char* p, const char* end) : p_(p), end_(end) {}
+    bool parse(Json& out) {
+        skip();
+        if (!value(out, 0)) return false;
+        skip();
+        return p_ == end_;
+    }
+
+  private:
+    const char *p_, *end_;
+    void skip() {
+        while (p_ < end_ && (*p_ == ' ' || *p_ == '\t' || *p_ == '\n' || *p_ == '\r')) ++p_;
+    }
+    bool literal(const char* w) {
+        const size_t n = std::strlen(w);
+        if ((size_t)(end_ - p_) < n || std::memcmp(p_, w, n) != 0) return false;
+        p_ += n;
+        return true;
+    }
+    static void utf8(std::string& s, uint32_t c) {
+        if (c < 0x80) {
+            s += (char)c;
+        } else if (c < 0x800) {
+            s += (char)(0xC0 | (c >> 6));
+            s += (char)(0x80 | (c & 63));
+        } else if (c < 0x10000) {
+            s += (char)(0xE0 | (c >> 12));
+            s += (char)(0x80 | ((c >> 6) & 63));
+            s += (char)(0x80 | (c & 63));
+        } else {
+            s += (char)(0xF0 | (c >> 18));
+            s += (char)(0x80 | ((c >> 12) & 63));
+            s += (char)(0x80 | ((c >> 6) & 63));
+            s += (char)(0x80 | (c & 63));
+        }
+    }
+    bool hex4(uint32_t* v) {
+        if (end_ - p_ < 4) return false;
+        uint32_t x = 0;
+        for (int k = 0; k < 4; ++k) {
+            const char c = *p_++;
+            x <<= 4;
+            if (c >= '0' && c <= '9') x |= (uint32_t)(c - '0');
+            else if (c >= 'a' && c <= 'f') x |= (uint32_t)(c - 'a' + 10);
+            else if (c >= 'A' && c <= 'F') x |= (uint32_t)(c - 'A' + 10);
+            else return false;
+        }
+        *v = x;
+        return true;
+    }
+    bool string(std::string& s) {
+        ++p_;   // the opening quote
+        while (p_ < end_) {
+            const unsigned char c = (unsigned char)*p_++;
+            if (c == '"') return true;
+            if (c < 0x20) return false;
+            if (c != '\\') {
+                s += (char)c;
+                continue;
+            }
+            if (p_ >= end_) return false;
+            const char e = *p_++;
+            switch (e) {
+                case '"': s += '"'; break;
+                case '\\': s += '\\'; break;
+                case '/': s += '/'; break;
+                case 'b': s += '\b'; break;
+                case 'f': s += '\f'; break;
+                case 'n': s += '\n'; break;
+                case 'r': s += '\r'; break;
+                case 't': s += '\t'; break;
+                case 'u': {
+                    uint32_t c1;
+                    if (!hex4(&c1)) return false;
+                    if (c1 >= 0xD800 && c1 < 0xDC00 && end_ - p_ >= 6 && p_[0] == '\\' && p_[1] == 'u') {
+                        const char* back = p_;
+                        p_ += 2;
+                        uint32_t c2;
+                        if (hex4(&c2) && c2 >= 0xDC00 && c2 < 0xE000) {
+                            c1 = 0x10000 + ((c1 - 0xD800) << 10) + (c2 - 0xDC00);
+                        } else {
+                            p_ = back;
+                        }
+                    }
+                    utf8(s, c1);
+                    break;
+                }
+                default: return false;
+            }
+        }
+        return false;
+    }
+    bool number(double* v) {
+        const char* q = p_;
+        if (q < end_ && *q == '-') ++q;
+        if (q >= end_) return false;
+        if (*q == '0') {
+            ++q;
+        } else if (*q >= '1' && *q <= '9') {
+            while (q < end_ && *q >= '0' && *q <= '9') ++q;
+        } else {
+            return false;
+        }
+        if (q < end_ && *q == '.') {
+            ++q;
+            if (q >= end_ || !(*q >= '0' && *q <= '9')) return false;
+            while (q < end_ && *q >= '0' && *q <= '9') ++q;
+        }
+        if (q < end_ && (*q == 'e' || *q == 'E')) {
+            ++q;
+            if (q < end_ && (*q == '+' || *q == '-')) ++q;
+            if (q >= end_ || !(*q >= '0' && *q <= '9')) return false;
+            while (q < end_ && *q >= '0' && *q <= '9') ++q;
+        }
+        *v = std::strtod(std::string(p_, q).c_str(), nullptr);   // correctly rounded
+        p_ = q;
+        return true;
+    }
+    bool value(Json& out, int depth) {
+        if (depth > 512 || p_ >= end_) return false;
+        const char c = *p_;
+        if (c == '{') {
+            ++p_;
+            out.kind = Json::kObject;
+            skip();
+            if (p_ < end_ && *p_ == '}') {
+                ++p_;
+                return true;
+            }
+            for (;;) {
+                skip();
+                if (p_ >= end_ || *p_ != '"') return false;
+                std::string key;
+                if (!string(key)) return false;
+                skip();
+                if (p_ >= end_ || *p_ != ':') return false;
+                ++p_;
+                skip();
+                Json v;
+                if (!value(v, depth + 1)) return false;
+                bool replaced = false;
+                for (auto& f : out.fields)
+                    if (f.first == key) {
+                        f.second = std::move(v);
+                        replaced = true;
+                        break;
+                    }
+                if (!replaced) out.fields.emplace_back(std::move(key), std::move(v));
+                skip();
+                if (p_ < end_ && *p_ == ',') {
+                    ++p_;
+                    continue;
+                }
+                if (p_ < end_ && *p_ == '}') {
+                    ++p_;
+                    return true;
+                }
+                return false;
+            }
+        }
+        if (c == '[') {
+            ++p_;
+            out.kind = Json::kArray;
+            skip();
+            if (p_ < end_ && *p_ == ']') {
+                ++p_;
+                return true;
+            }
+            for (;;) {
+                skip();
+                Json v;
+                if (!value(v, depth + 1)) return false;
+                out.items.push_back(std::move(v));
+                skip();
+                if (p_ < end_ && *p_ == ',') {
+                    ++p_;
+                    continue;
+                }
+                if (p_ < end_ && *p_ == ']') {
+                    ++p_;
+                    return true;
+                }
+                return false;
+            }
+        }
+        if (c == '"') {
+            out.kind = Json::kString;
+            return string(out.str);
+        }
+        if (literal("true")) {
+            out.kind = Json::kBool;
+            out.b = true;
+            return true;
+        }
+        if (literal("false")) {
+            out.kind = Json::kBool;
+            return true;
+        }
+        if (literal("null")) {
+            out.kind = Json::kNull;
+            return true;
+        }
+        out.kind = Json::kNumber;
+        return number(&out.num);
+    }
+};
+
+// v == null || v === undefined: reading a property of it throws.
+bool js_nullish(const Json& v) { return v.kind == Json::kUndefined || v.kind == Json::kNull; }
+
+// v[key] for a value that is not null or undefined (an index for arrays and
+// strings, a name for objects; anything else has no such property).
+Json js_get(const Json& v, const std::string& key) {
+    if (v.kind == Json::kObject) {
+        for (auto it = v.fields.rbegin(); it != v.fields.rend(); ++it)
+            if (it->first == key) return it->second;
+        return Json();
+    }
+    if (v.kind == Json::kArray || v.kind == Json::kString) {
+        if (key.empty() || key.size() > 9 || key.find_first_not_of("0123456789") != std::string::npos ||
+            (key.size() > 1 && key[0] == '0'))
+            return Json();
+        const size_t k = std::stoul(key);
+        if (v.kind == Json::kArray) return k < v.items.size() ? v.items[k] : Json();
+        Json c;   // the code unit at k, for the ASCII strings a codebook could hold
+        if (k < v.str.size()) {
+            c.kind = Json::kString;
+            c.str = v.str.substr(k, 1);
+        }
+        return c;
+    }
+    return Json();
+}
+
+std::string js_string(const Json& v) {   // String(v)
+    switch (v.kind) {
+        case Json::kUndefined: return "undefined";
+        case Json::kNull: return "null";
+        case Json::kBool: return v.b ? "true" : "false";
+        case Json::kNumber: return js_number(v.num);
+        case Json::kString: return v.str;
+        case Json::kArray: {   // Array.prototype.join: null and undefined as ""
+            std::string s;
+            for (size_t k = 0; k < v.items.size(); ++k) {
+                if (k) s += ',';
+                if (!js_nullish(v.items[k])) s += js_string(v.items[k]);
+            }
+            return s;
+        }
+        default: return "[object Object]";
+    }
+}
+
+double js_value_number(const Json& v) {   // ToNumber(v)
+    switch (v.kind) {
+        case Json::kUndefined: return std::nan("");
+        case Json::kNull: return 0.0;
+        case Json::kBool: return v.b ? 1.0 : 0.0;
+        case Json::kNumber: return v.num;
+        default: return js_to_number(js_string(v), true);
+    }
+}
+
+bool js_truthy(const Json& v) {
+    switch (v.kind) {
+        case Json::kUndefined:
+        case Json::kNull: return false;
+        case Json::kBool: return v.b;
+        case Json::kNumber: return !(v.num == 0.0 || v.num != v.num);
+        case Json::kString: return !v.str.empty();
+        default: return true;
+    }
+}
+
+std::string strip_bom(std::string s) {   // TextDecoder drops a leading byte-order mark
+    if (s.size() >= 3 && (unsigned char)s[0] == 0xEF && (unsigned char)s[1] == 0xBB && (unsigned char)s[2] == 0xBF)
+        s.erase(0, 3);
+    return s;
+}
+
+struct ZipEntry {
+    uint16_t method;
+    const uint8_t* data;
+    uint32_t size;
+};
+
+// The zip's entries by name (a later entry of a name replaces an earlier).
+int unzip(ws_ctx* ctx, const uint8_t* d, size_t n, std::map<std::string, ZipEntry>& files) {
+    auto u16 = [&](size_t o) -> uint32_t { return o + 2 <= n ? (uint32_t)(d[o] | (d[o + 1] << 8)) : 0u; };
+    auto u32 = [&](size_t o) -> uint32_t {
+        if (o + 4 > n) return 0u;
+        uint32_t v;
+        std::memcpy(&v, d + o, 4);
+        return v;
+    };
+    // The end record is the last thing in the file, before a comment of at
+    // most 65535 bytes.
+    long long end = -1;
+    if (n >= 22) {
+        const long long lo = n >= 22 + 65535 ? (long long)(n - 22 - 65535) : 0;
+        for (long long i = (long long)n - 22; i >= lo; --i)
+            if (u32((size_t)i) == 0x06054b50u) {
+                end = i;
+                break;
+            }
+    }
+    if (end < 0) return set_error(ctx, WS_ERR_FORMAT, "splats: a zip with no end record: cut short?");
+    size_t at = u32((size_t)end + 16);
+    for (uint32_t k = u16((size_t)end + 10); k > 0; --k) {
+        if (at + 46 > n || u32(at) != 0x02014b50u)
+            return set_error(ctx, WS_ERR_FORMAT, "splats: a zip whose directory is damaged");
+        const uint32_t method = u16(at + 10), size = u32(at + 20), name_len = u16(at + 28), local = u32(at + 42);
+        const size_t name_end = std::min(n, at + 46 + name_len);
+        const std::string name = strip_bom(std::string(reinterpret_cast<const char*>(d) + at + 46,
+                                                       reinterpret_cast<const char*>(d) + name_end));
+        if (size == 0xFFFFFFFFu || local == 0xFFFFFFFFu)
+            return set_error(ctx, WS_ERR_FORMAT, "splats: a zip64 .sog is not read");
+        at += 46 + name_len + u16(at + 30) + u16(at + 32);
+        if ((size_t)local + 30 > n)
+            return set_error(ctx, WS_ERR_FORMAT, "splats: the zip is cut short in %s", name.c_str());
+        const size_t start = (size_t)local + 30 + u16((size_t)local + 26) + u16((size_t)local + 28);
+        if (start + size > n) return set_error(ctx, WS_ERR_FORMAT, "splats: the zip is cut short in %s", name.c_str());
+        if (method != 0 && method != 8)
+            return set_error(ctx, WS_ERR_FORMAT, "splats: %s is compressed with method %u; stored and deflate are read",
+                             name.c_str(), method);
+        files[name] = ZipEntry{(uint16_t)method, d + start, size};
+    }
+    return WS_OK;
+}
+
+// An entry's bytes: stored, or inflated (raw deflate, the reference's
+// DecompressionStream('deflate-raw')).
+int entry_bytes(ws_ctx* ctx, const std::string& name, const ZipEntry& e, std::vector<uint8_t>& out) {
+    out.clear();
+    if (e.method == 0) {
+        out.assign(e.data, e.data + e.size);
+        return WS_OK;
+    }
+    z_stream zs;
+    std::memset(&zs, 0, sizeof(zs));
+    if (inflateInit2(&zs, -MAX_WBITS) != Z_OK) return set_error(ctx, WS_ERR_NOMEM, "splats: inflate failed");
+    zs.next_in = const_cast<Bytef*>(e.data);
+    zs.avail_in = e.size;
+    int z = Z_OK;
+    std::vector<uint8_t> chunk(1 << 20);
+    while (z != Z_STREAM_END) {
+        zs.next_out = chunk.data();
+        zs.avail_out = (uInt)chunk.size();
+        z = inflate(&zs, Z_NO_FLUSH);
+        if (z != Z_OK && z != Z_STREAM_END) break;
+        out.insert(out.end(), chunk.data(), chunk.data() + (chunk.size() - zs.avail_out));
+        if (z == Z_OK && zs.avail_in == 0 && zs.avail_out != 0) break;
+    }
+    inflateEnd(&zs);
+    if (z != Z_STREAM_END)
+        return set_error(ctx, WS_ERR_FORMAT, "splats: %s is not a whole deflate stream", name.c_str());
+    return WS_OK;
+}
+
+int load_sog(ws_ctx* ctx, const uint8_t* bytes, size_t nbytes, ws_decode_image decode, void* user, ws_cloud** out) {
+    std::map<std::string, ZipEntry> files;
+    int rc;
+    if ((rc = unzip(ctx, bytes, nbytes, files))) return rc;
+    std::vector<uint8_t> buf;
+    auto file = [&](const Json& name) -> int {   // the entry's bytes into buf
+        auto it = name.kind == Json::kString ? files.find(name.str) : files.end();
+        if (it == files.end())
+            return set_error(ctx, WS_ERR_FORMAT, "splats: the .sog has no %s", js_string(name).c_str());
+        return entry_bytes(ctx, it->first, it->second, buf);
+    };
+    Json meta_name;
+    meta_name.kind = Json::kString;
+    meta_name.str = "meta.json";
+    if ((rc = file(meta_name))) return rc;
+    const std::string text = strip_bom(std::string(buf.begin(), buf.end()));
+    Json meta;
+    if (!JsonParser(text.data(), text.data() + text.size()).parse(meta))
+        return set_error(ctx, WS_ERR_FORMAT, "splats: the .sog's meta.json is not JSON");
+    // meta.a.b...: the error JavaScript's TypeError stands for when a step
+    // reads a property of null or undefined.
+    auto member = [&](std::initializer_list<const char*> path, Json* v) -> int {
+        Json cur = meta;
+        std::string shown;
+        for (const char* key : path) {
+            if (js_nullish(cur))
+                return set_error(ctx, WS_ERR_FORMAT, "splats: the .sog's meta.json has no %s", shown.c_str());
+            cur = js_get(cur, key);
+            shown += shown.empty() ? key : std::string(".") + key;
+        }
+        *v = std::move(cur);
+        return WS_OK;
+    };
+    if (js_nullish(meta)) return set_error(ctx, WS_ERR_FORMAT, "splats: the .sog's meta.json has no version");
+    const Json version = js_get(meta, "version");
+    if (!(version.kind == Json::kNumber && version.num == 2.0))
+        return set_error(ctx, WS_ERR_FORMAT,
+                         "splats: a .sog of version %s; version 2 is read (re-save it with splat-transform)",
+                         js_nullish(version) ? "1" : js_string(version).c_str());
+    const Json count_v = js_get(meta, "count");
+    if (!(count_v.kind == Json::kNumber && std::isfinite(count_v.num) && count_v.num == std::floor(count_v.num) &&
+          count_v.num > 0))
+        return set_error(ctx, WS_ERR_FORMAT, "splats: a .sog of %s splats", js_string(count_v).c_str());
+    if (count_v.num > (double)WS_MAX_SPLATS)
+        return set_error(ctx, WS_ERR_CAPACITY, "splats: %s splats are more than this device holds in one buffer, %u",
+                         js_string(count_v).c_str(), WS_MAX_SPLATS);
+    const uint32_t count = (uint32_t)count_v.num;
+
+    // The five images every .sog has: their names (in the order the
+    // reference reads them), that each is there, then each decoded.
+    Json names[5];
+    if ((rc = member({"means", "files", "0"}, &names[0])) || (rc = member({"means", "files", "1"}, &names[1])) ||
+        (rc = member({"quats", "files", "0"}, &names[2])) || (rc = member({"scales", "files", "0"}, &names[3])) ||
+        (rc = member({"sh0", "files", "0"}, &names[4])))
+        return rc;
+    for (const Json& nm : names)
+        if (nm.kind != Json::kString || !files.count(nm.str))
+            return set_error(ctx, WS_ERR_FORMAT, "splats: the .sog has no %s", js_string(nm).c_str());
+    // Decoded pixels kept on the host: count x 4 bytes of each image (labels
+    // sixth), then the palette.
+    std::vector<uint8_t> pix;
+    auto decoded = [&](const Json& name, bool check, uint32_t* width, size_t* nbytes_out) -> int {
+        if ((rc = file(name))) return rc;
+        ws_image img{0, 0, nullptr};
+        if (decode(user, buf.data(), buf.size(), &img) != 0 || (!img.rgba && img.width && img.height))
+            return set_error(ctx, WS_ERR_FORMAT, "splats: decodeImage failed on %s", js_string(name).c_str());
+        const unsigned long long pixels = (unsigned long long)img.width * img.height;
+        if (check && pixels < count)
+            return set_error(ctx, WS_ERR_FORMAT, "splats: %s has %llu pixels, for %u splats", js_string(name).c_str(),
+                             pixels, count);
+        const size_t take = check ? (size_t)count * 4 : (size_t)pixels * 4;
+        pix.insert(pix.end(), img.rgba, img.rgba + take);
+        if (width) *width = img.width;
+        if (nbytes_out) *nbytes_out = (size_t)pixels * 4;
+        return WS_OK;
+    };
+    for (const Json& nm : names)
+        if ((rc = decoded(nm, true, nullptr, nullptr))) return rc;
+    Json shn;
+    if ((rc = member({"shN"}, &shn))) return rc;
+    Json bands;
+    if (js_truthy(shn)) bands = js_get(shn, "bands");
+    const std::string key = bands.kind == Json::kString ? bands.str
+                            : bands.kind == Json::kNumber ? js_number(bands.num) : std::string();
+    const uint32_t degree = key == "1" ? 1u : key == "2" ? 2u : key == "3" ? 3u : 0u;
+    const uint32_t per = kShCoefficients[degree];
+    uint32_t palette_width = 0;
+    size_t palette_bytes = 0;
+    if (degree) {
+        Json pname, lname;
+        if ((rc = member({"shN", "files", "0"}, &pname))) return rc;
+        if ((rc = decoded(pname, false, &palette_width, &palette_bytes))) return rc;
+        if ((rc = member({"shN", "files", "1"}, &lname))) return rc;
+        // labels go sixth: move the palette's bytes behind them
+        std::vector<uint8_t> palette(pix.end() - (ptrdiff_t)palette_bytes, pix.end());
+        pix.resize(pix.size() - palette_bytes);
+        if ((rc = decoded(lname, true, nullptr, nullptr))) return rc;
+        pix.insert(pix.end(), palette.begin(), palette.end());
+        if (palette_width != 64 * per)
+            return set_error(ctx, WS_ERR_FORMAT, "splats: the .sog's harmonic palette is %u wide; %u for degree %s",
+                             palette_width, 64 * per, key.c_str());
+    }
+    // The numbers the loop reads: the means' ranges and the codebooks (an
+    // entry past a codebook's end reads as NaN, as undefined does).
+    SogLayout L;
+    std::memset(&L, 0, sizeof(L));
+    auto numbers = [&](std::initializer_list<const char*> path, double* outv, int k) -> int {
+        Json v;
+        if ((rc = member(path, &v))) return rc;
+        if (js_nullish(v)) {
+            std::string shown;
+            for (const char* p : path) shown += shown.empty() ? p : std::string(".") + p;
+            return set_error(ctx, WS_ERR_FORMAT, "splats: the .sog's meta.json has no %s", shown.c_str());
+        }
+        for (int j = 0; j < k; ++j) outv[j] = js_value_number(js_get(v, std::to_string(j)));
+        return WS_OK;
+    };
+    std::vector<double> books(768, 0.0);
+    if ((rc = numbers({"means", "mins"}, L.mins, 3)) || (rc = numbers({"means", "maxs"}, L.maxs, 3)) ||
+        (rc = numbers({"sh0", "codebook"}, books.data() + 256, 256)) ||
+        (rc = numbers({"scales", "codebook"}, books.data(), 256)))
+        return rc;
+    if (degree) {
+        if ((rc = numbers({"shN", "codebook"}, books.data() + 512, 256))) return rc;
+        L.sh_count = js_value_number(js_get(shn, "count"));
+    }
+
+    // Up to the device: the pixels, the codebooks, then one thread a splat.
+    const size_t img_bytes = (size_t)count * 4;
+    const size_t pix_bytes = pix.size();
+    const size_t books_at = (pix_bytes + 255) / 256 * 256;
+    const size_t total = books_at + books.size() * sizeof(double);
+    cudaSetDevice(ctx->device);
+    void* staging = nullptr;
+    cudaError_t e = cudaMalloc(&staging, total);
+    if (e != cudaSuccess) return cuda_error(ctx, e, "ws_cloud_read");
+    uint8_t* dev = static_cast<uint8_t*>(staging);
+    if ((e = cudaMemcpyAsync(dev, pix.data(), pix_bytes, cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(dev + books_at, books.data(), books.size() * sizeof(double), cudaMemcpyHostToDevice,
+                             ctx->stream)) != cudaSuccess) {
+        cudaStreamSynchronize(ctx->stream);
+        cudaFree(staging);
+        return cuda_error(ctx, e, "ws_cloud_read upload");
+    }
+    L.count = count;
+    L.degree = degree;
+    L.per = per;
+    L.palette_width = palette_width;
+    L.palette_bytes = palette_bytes;
+    L.low = dev;
+    L.high = dev + img_bytes;
+    L.quats = dev + 2 * img_bytes;
+    L.scales = dev + 3 * img_bytes;
+    L.sh0 = dev + 4 * img_bytes;
+    L.labels = degree ? dev + 5 * img_bytes : dev;
+    L.palette = degree ? dev + 6 * img_bytes : dev;
+    L.books = reinterpret_cast<const double*>(dev + books_at);
+    unsigned long long* words = nullptr;
+    ws_cloud* c = new_cloud(ctx, count, degree, &words, &rc);
+    if (!c) {
+        cudaStreamSynchronize(ctx->stream);
+        cudaFree(staging);
+        return rc;
+    }
+    sog_kernel<<<grid_of(ctx, count), 256, 0, ctx->stream>>>(L, sink_of(c, words));
+    e = cudaGetLastError();
+    rc = finish_cloud(ctx, c, words, e, out);
+    cudaStreamSynchronize(ctx->stream);   // the host staging is freed on return
+    cudaFree(staging);
+    return rc;
+}
+
 }  // namespace
 }  // namespace wsort
 
@@ -658,6 +1288,17 @@ extern "C" int ws_cloud_load(ws_ctx* ctx, const uint8_t* bytes, size_t nbytes, w
     if (nbytes >= 4 && d[0] == 0x70 && d[1] == 0x6c && d[2] == 0x79 && (d[3] == 0x0a || d[3] == 0x0d))
         return load_ply(ctx, bytes, nbytes, out);
     return ws_cloud_from_splat(ctx, bytes, nbytes, out);
+}
+
+extern "C" int ws_cloud_read(ws_ctx* ctx, const uint8_t* bytes, size_t nbytes, ws_decode_image decode, void* user,
+                             ws_cloud** out) {
+    if (!ctx || !out || (!bytes && nbytes)) return set_error(ctx, WS_ERR_ARG, "ws_cloud_read: null argument");
+    *out = nullptr;
+    const uint8_t* d = bytes;
+    const bool zip = nbytes >= 4 && d[0] == 0x50 && d[1] == 0x4b && d[2] == 0x03 && d[3] == 0x04;
+    if (!zip || !decode) return ws_cloud_load(ctx, bytes, nbytes, out);
+    cudaSetDevice(ctx->device);
+    return load_sog(ctx, bytes, nbytes, decode, user, out);
 }
 
 extern "C" int ws_cloud_harmonics(const ws_cloud* c, int* degree, uint32_t* words) {

@@ -357,6 +357,47 @@ def load_splats(data, ctx: Context | None = None) -> Splats:
     return sp
 
 
+def read_splats(data, decode_image=None, ctx: Context | None = None) -> Splats:
+    """readSplats(bytes, {decodeImage}) (src/scene/splats.js:85-92): as
+    load_splats, and a .sog bundle too, its images decoded by
+    decode_image(bytes) -> (width, height, rgba), rgba width x height x 4
+    bytes as stored (the reference's decodeImage). Raises WsError with the
+    reference's messages; an exception of decode_image is raised as is."""
+    ctx = ctx or Context(0)
+    buf = np.frombuffer(bytes(data), np.uint8) if not isinstance(data, np.ndarray) else \
+        np.ascontiguousarray(data).view(np.uint8).reshape(-1)
+    keep = []        # decoded pixels, alive until the call returns
+    raised = []
+
+    def trampoline(user, ptr, n, out):
+        try:
+            width, height, rgba = decode_image(ctypes.string_at(ptr, n))
+            pixels = np.ascontiguousarray(np.frombuffer(bytes(rgba), np.uint8) if not isinstance(rgba, np.ndarray)
+                                          else rgba.view(np.uint8).reshape(-1))
+            if pixels.size < int(width) * int(height) * 4:
+                raise ValueError(f"decode_image gave {pixels.size} bytes for {width} x {height} pixels")
+            keep.append(pixels)
+            out[0].width, out[0].height = int(width), int(height)
+            out[0].rgba = pixels.ctypes.data
+            return 0
+        except BaseException as e:   # noqa: BLE001 - handed back to the caller below
+            raised.append(e)
+            return 1
+
+    callback = _lib.DECODE_IMAGE(trampoline) if decode_image is not None else None
+    h = ctypes.c_void_p()
+    rc = ctx.lib.ws_cloud_read(ctx.handle, buf.ctypes.data, buf.size,
+                               ctypes.cast(callback, ctypes.c_void_p) if callback else None, None, ctypes.byref(h))
+    if raised:
+        raise raised[0]
+    ctx.check(rc)
+    sp = Splats(ctx, h)
+    d = ctypes.c_int(0)
+    ctx.check(ctx.lib.ws_cloud_harmonics(h, ctypes.byref(d), None))
+    sp.degree = d.value
+    return sp
+
+
 def parse_splats(data, ctx: Context | None = None) -> Splats:
     """parseSplats + upload: .splat bytes (bytes, bytearray, numpy uint8 or
     structured records) to a resident cloud. Refuses what the reference refuses."""
