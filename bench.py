@@ -374,7 +374,8 @@ def _run_wsort(args, rank, world, local_rank, torch):
         "e2e": {"value": e2e_value, "unit": "Msplats/s", "h2d_bytes_per_step": view_bytes, "d2h_bytes_per_step": d2h,
                 "call": "ws_sort(WS_HOST_OUTPUT) into a pinned host buffer: the order and the survivor count, "
                         "the reference's outputs (its keys stay unsorted on the device and are never read back)"},
-        "gpu_launches": launches,
+        # each ws_sort of a lone job is two launches, the staging kernel and the sort
+        "gpu_launches": launches * (2 if len(jobs) == 1 else 1),
         "clocks": clk,
     }
     if rank == 0:

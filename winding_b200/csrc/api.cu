@@ -323,6 +323,18 @@ const ws_params& params_for(const ws_ctx* ctx, uint64_t splats) {
     return ctx->params;
 }
 
+// A lone job's staging in one launch: its description (passed by value with
+// the launch, so no host-to-device copy) into the job table, and the launch's
+// and the job's counters zeroed.
+__global__ void __launch_bounds__(256) stage_kernel(const __grid_constant__ JobDesc job, JobDesc* __restrict__ dst,
+                                                    uint32_t* __restrict__ ctl, uint32_t ctl_words) {
+    static_assert(sizeof(JobDesc) % 4 == 0, "copied in words");
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(&job);
+    uint32_t* d = reinterpret_cast<uint32_t*>(dst);
+    for (uint32_t k = threadIdx.x; k < sizeof(JobDesc) / 4; k += blockDim.x) d[k] = src[k];
+    for (uint32_t k = threadIdx.x; k < ctl_words; k += blockDim.x) ctl[k] = 0;
+}
+
 // One persistent launch over `njobs` jobs of ns[j] elements each; `fill`
 // writes the job table (kind-specific fields and scratch) into pinned
 // staging, given the scratch base, with ctx->params already the launch's.
@@ -368,9 +380,15 @@ static int launch_jobs(ws_ctx* ctx, const std::vector<uint32_t>& ns, int njobs, 
         std::memcpy(ctx->items_h.p, ctx->items.data(), ctx->items.size() * sizeof(uint2));
     }
     if (stream != ctx->stream) cudaStreamWaitEvent(stream, ctx->launched, 0);
-    if ((e = cudaMemcpyAsync(ctx->jobs_d.p, hj, (size_t)njobs * sizeof(JobDesc), cudaMemcpyHostToDevice, stream)) !=
-        cudaSuccess)
+    const size_t ctl_bytes = sizeof(LaunchCtl) + (size_t)njobs * sizeof(JobCtl);
+    if (njobs == 1) {
+        stage_kernel<<<1, 256, 0, stream>>>(*hj, static_cast<JobDesc*>(ctx->jobs_d.p),
+                                            static_cast<uint32_t*>(ctx->scratch.p), (uint32_t)(ctl_bytes / 4));
+        if ((e = cudaGetLastError()) != cudaSuccess) return cuda_error(ctx, e, "ws_sort staging");
+    } else if ((e = cudaMemcpyAsync(ctx->jobs_d.p, hj, (size_t)njobs * sizeof(JobDesc), cudaMemcpyHostToDevice,
+                                    stream)) != cudaSuccess) {
         return cuda_error(ctx, e, "ws_sort upload");
+    }
     if (!same) {
         if ((e = cudaMemcpyAsync(ctx->items_d.p, ctx->items_h.p, ctx->items.size() * sizeof(uint2),
                                  cudaMemcpyHostToDevice, stream)) != cudaSuccess)
@@ -380,8 +398,7 @@ static int launch_jobs(ws_ctx* ctx, const std::vector<uint32_t>& ns, int njobs, 
         ctx->items_valid = true;
     }
     cudaEventRecord(ctx->staged, stream);
-    const size_t ctl_bytes = sizeof(LaunchCtl) + (size_t)njobs * sizeof(JobCtl);
-    if ((e = cudaMemsetAsync(ctx->scratch.p, 0, ctl_bytes, stream)) != cudaSuccess)
+    if (njobs != 1 && (e = cudaMemsetAsync(ctx->scratch.p, 0, ctl_bytes, stream)) != cudaSuccess)
         return cuda_error(ctx, e, "ws_sort reset");
     const size_t n_items = ctx->items.size();
     cudaEvent_t t_stop = nullptr;
