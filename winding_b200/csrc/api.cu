@@ -823,6 +823,7 @@ __global__ void __launch_bounds__(256) copy_out_kernel(const uint32_t* __restric
 
 extern "C" int ws_sort(ws_ctx* ctx, const ws_cloud* cloud, const ws_view* view, uint32_t* order, uint32_t* keys,
                        uint32_t* count, int flags, void* stream_p) {
+    NvtxRange nvtx("ws_sort");
     if (!ctx) return WS_ERR_ARG;
     int rc;
     if ((rc = check_cloud(ctx, cloud)) || (rc = check_view(ctx, view))) return rc;
@@ -888,6 +889,7 @@ extern "C" int ws_sort(ws_ctx* ctx, const ws_cloud* cloud, const ws_view* view, 
 }
 
 extern "C" int ws_sort_batch(ws_ctx* ctx, int njobs, const ws_job* jobs, void* stream_p) {
+    NvtxRange nvtx("ws_sort_batch");
     if (!ctx) return WS_ERR_ARG;
     if (njobs < 0 || (njobs && !jobs)) return set_error(ctx, WS_ERR_ARG, "ws_sort_batch: bad job list");
     if (njobs == 0) return WS_OK;
@@ -996,6 +998,7 @@ extern "C" int ws_cloud_set_harmonics(ws_cloud* c, int degree, const uint32_t* w
 
 extern "C" int ws_sort_batch_shaded(ws_ctx* ctx, int njobs, const ws_job* jobs, const ws_shade* shades,
                                     void* stream_p) {
+    NvtxRange nvtx("ws_sort_batch_shaded");
     if (!ctx) return WS_ERR_ARG;
     if (njobs < 0 || (njobs && (!jobs || !shades)))
         return set_error(ctx, WS_ERR_ARG, "ws_sort_batch_shaded: bad job list");
@@ -1083,6 +1086,7 @@ extern "C" int ws_particle_thresholds(float* out) {
 }
 
 extern "C" int ws_sort_particles(ws_ctx* ctx, int n, const ws_emitter* emitters, void* stream_p) {
+    NvtxRange nvtx("ws_sort_particles");
     if (!ctx) return WS_ERR_ARG;
     if (n < 0 || (n && !emitters)) return set_error(ctx, WS_ERR_ARG, "ws_sort_particles: bad emitter list");
     if (n == 0) return WS_OK;
@@ -1227,6 +1231,7 @@ extern "C" int ws_plan_set_views(ws_plan* p, const ws_view* views) {
 }
 
 extern "C" int ws_plan_launch(ws_plan* p, void* stream_p) {
+    NvtxRange nvtx("ws_plan_launch");
     if (!p) return WS_ERR_ARG;
     for (int j = 0; j < p->njobs; ++j) {
         int rc = check_cloud(p->ctx, p->jobs[j].cloud);

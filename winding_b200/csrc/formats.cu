@@ -1271,6 +1271,7 @@ int load_sog(ws_ctx* ctx, const uint8_t* bytes, size_t nbytes, ws_decode_image d
 using namespace wsort;
 
 extern "C" int ws_cloud_load(ws_ctx* ctx, const uint8_t* bytes, size_t nbytes, ws_cloud** out) {
+    NvtxRange nvtx("ws_cloud_load");
     if (!ctx || !out || (!bytes && nbytes)) return set_error(ctx, WS_ERR_ARG, "ws_cloud_load: null argument");
     *out = nullptr;
     const uint8_t* d = bytes;
@@ -1292,6 +1293,7 @@ extern "C" int ws_cloud_load(ws_ctx* ctx, const uint8_t* bytes, size_t nbytes, w
 
 extern "C" int ws_cloud_read(ws_ctx* ctx, const uint8_t* bytes, size_t nbytes, ws_decode_image decode, void* user,
                              ws_cloud** out) {
+    NvtxRange nvtx("ws_cloud_read");
     if (!ctx || !out || (!bytes && nbytes)) return set_error(ctx, WS_ERR_ARG, "ws_cloud_read: null argument");
     *out = nullptr;
     const uint8_t* d = bytes;

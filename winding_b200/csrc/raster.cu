@@ -465,6 +465,7 @@ extern "C" int ws_draw_tables(float* srgb, float* reach) {
 extern "C" int ws_draw(ws_ctx* ctx, const ws_cloud* cloud, const ws_view* view, const uint32_t* order,
                        const uint32_t* count, const uint32_t* shaded, float* image, uint32_t width, uint32_t height,
                        void* stream_p) {
+    NvtxRange nvtx("ws_draw");
     if (!ctx) return WS_ERR_ARG;
     if (!cloud || cloud->magic != kCloudMagic) return set_error(ctx, WS_ERR_ARG, "ws_draw: not a cloud");
     if (!cloud->alive) return set_error(ctx, WS_ERR_UNLOADED, "addSplats: these splats were unloaded; remove the node first");

@@ -251,6 +251,7 @@ bool form_batch(ws_server* S, Slot& slot) {
 
 // Stages and launches a formed batch on its slot (no lock held).
 bool launch_batch(ws_server* S, Slot& slot) {
+    NvtxRange nvtx("launch_batch");
     const int nj = (int)slot.batch.size();
     std::vector<ws_job> jobs(nj);
     for (int j = 0; j < nj; ++j) {

@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <cstdint>
 #include <string>
@@ -11,6 +12,15 @@
 #include "wsort.h"
 
 namespace wsort {
+
+// A named range on the calling thread's NVTX timeline (what nsys shows
+// around each call); without a tool attached, a check and nothing more.
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 struct DevBuf {
     void* p = nullptr;
