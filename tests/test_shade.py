@@ -4,7 +4,8 @@ CPU: the oracle's shade against an independent numpy float32 restatement of
 harmonics() (every op rounded to f32, left to right), and the identity that
 all-zero harmonics leave a colour word as it is.
 GPU: ws_sort_batch_shaded against the oracle for degrees 1, 2 and 3, only the
-survivors' words written, the order and keys identical to the plain sort's.
+survivors' words written, the order and keys identical to the plain sort's;
+a lone job shaded between plain sorts of the same size.
 """
 import numpy as np
 import pytest
@@ -133,6 +134,42 @@ def test_sort_batch_shaded_matches_oracle(ctx, degree):
     finally:
         for sp in clouds:
             sp.destroy()
+
+
+@pytest.mark.gpu
+def test_lone_job_shaded_between_plain_sorts(ctx):
+    """One job alone in its launch, sorted plain, then shaded, then plain
+    again at the same size: each launch does its own work (the shade pass
+    runs exactly when asked for), and the shaded words match the oracle."""
+    import torch
+    rng = np.random.default_rng(31)
+    job = W.clusters_1m(seed=71, n=120_000)
+    sp = parse_splats(job.records, ctx)
+    try:
+        parsed = O.parse_splat(job.bytes())
+        sh = _sh_words(sp.count, 3, rng)
+        sp.set_harmonics(3, sh)
+        view = make_view(job.view.model_view, job.view.projection, job.view.viewport, 0.5)
+        eye = eye_in_cloud(job.view.model_view)
+        o = torch.empty(sp.count, dtype=torch.int32, device="cuda")
+        k = torch.empty_like(o)
+        c = torch.zeros(1, dtype=torch.int32, device="cuda")
+        shaded = torch.full((sp.count,), 0x5A5A5A5A, dtype=torch.int32, device="cuda")
+        spec = [(sp, view, o.data_ptr(), k.data_ptr(), c.data_ptr())]
+        ctx.sort_batch(spec)
+        ctx.sync()
+        assert torch.all(shaded == 0x5A5A5A5A)
+        ctx.sort_batch_shaded(spec, [(eye, shaded.data_ptr())])
+        ctx.sync()
+        order = o[:int(c.item())].cpu().numpy().view(np.uint32)
+        got = shaded.cpu().numpy().view(np.uint32)
+        assert np.array_equal(got[order], O.shade(parsed.centers, sh, 3, order, eye))
+        shaded.fill_(0x5A5A5A5A)
+        ctx.sort_batch(spec)
+        ctx.sync()
+        assert torch.all(shaded == 0x5A5A5A5A)
+    finally:
+        sp.destroy()
 
 
 @pytest.mark.gpu
