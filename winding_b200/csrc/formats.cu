@@ -1163,7 +1163,13 @@ int load_sog(ws_ctx* ctx, const uint8_t* bytes, size_t nbytes, ws_decode_image d
         if (check && pixels < count)
             return set_error(ctx, WS_ERR_FORMAT, "splats: %s has %llu pixels, for %u splats", js_string(name).c_str(),
                              pixels, count);
-        const size_t take = check ? (size_t)count * 4 : (size_t)pixels * 4;
+        // An image checked against the count is read for its first `count`
+        // pixels; the palette for its first 1024 rows, all that 16-bit labels
+        // reach (label / 64 < 1024), though its whole length stays the bound
+        // the reference's loop checks.
+        const unsigned long long keep = check ? (unsigned long long)count
+                                              : std::min<unsigned long long>(pixels, 1024ull * img.width);
+        const size_t take = (size_t)keep * 4;
         pix.insert(pix.end(), img.rgba, img.rgba + take);
         if (width) *width = img.width;
         if (nbytes_out) *nbytes_out = (size_t)pixels * 4;
@@ -1270,8 +1276,20 @@ int load_sog(ws_ctx* ctx, const uint8_t* bytes, size_t nbytes, ws_decode_image d
 
 using namespace wsort;
 
+static int cloud_load(ws_ctx* ctx, const uint8_t* bytes, size_t nbytes, ws_cloud** out);
+
+// The loaders size host buffers from the bytes they are given: a request the
+// host cannot meet is an error, never an exception across the C ABI.
 extern "C" int ws_cloud_load(ws_ctx* ctx, const uint8_t* bytes, size_t nbytes, ws_cloud** out) {
     NvtxRange nvtx("ws_cloud_load");
+    try {
+        return cloud_load(ctx, bytes, nbytes, out);
+    } catch (const std::bad_alloc&) {
+        return set_error(ctx, WS_ERR_NOMEM, "ws_cloud_load: out of host memory");
+    }
+}
+
+static int cloud_load(ws_ctx* ctx, const uint8_t* bytes, size_t nbytes, ws_cloud** out) {
     if (!ctx || !out || (!bytes && nbytes)) return set_error(ctx, WS_ERR_ARG, "ws_cloud_load: null argument");
     *out = nullptr;
     const uint8_t* d = bytes;
@@ -1300,7 +1318,11 @@ extern "C" int ws_cloud_read(ws_ctx* ctx, const uint8_t* bytes, size_t nbytes, w
     const bool zip = nbytes >= 4 && d[0] == 0x50 && d[1] == 0x4b && d[2] == 0x03 && d[3] == 0x04;
     if (!zip || !decode) return ws_cloud_load(ctx, bytes, nbytes, out);
     cudaSetDevice(ctx->device);
-    return load_sog(ctx, bytes, nbytes, decode, user, out);
+    try {
+        return load_sog(ctx, bytes, nbytes, decode, user, out);
+    } catch (const std::bad_alloc&) {
+        return set_error(ctx, WS_ERR_NOMEM, "ws_cloud_read: out of host memory");
+    }
 }
 
 extern "C" int ws_cloud_harmonics(const ws_cloud* c, int* degree, uint32_t* words) {
