@@ -60,6 +60,8 @@ def parse_args():
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU baseline sample length")
     ap.add_argument("--tile", type=int, default=0, help="fixed tile size (skips the autotuner; with --ctas)")
     ap.add_argument("--ctas", type=int, default=0, help="fixed resident CTAs per SM (with --tile)")
+    ap.add_argument("--only", default="", choices=["", "particles-64", "shade-1M", "decode", "draw-1M"],
+                    help="run one side measurement alone and print its result (no bench line)")
     return ap.parse_args()
 
 
@@ -290,6 +292,14 @@ def _run_wsort(args, rank, world, local_rank, torch):
         import torch.distributed as dist
     ctx = Context(local_rank)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device="cuda")
+    if args.only:   # one side measurement alone (for a profiler, say)
+        fns = {"particles-64": particles_suite, "shade-1M": shade_suite, "decode": decode_suite,
+               "draw-1M": draw_suite}
+        peak, _ = peak_hbm()
+        result = fns[args.only](ctx, torch, flush, peak)
+        if rank == 0:
+            print(json.dumps({"only": args.only, "result": result}), flush=True)
+        return
     jobs = make_jobs(args.workload, args.cull, seed_offset=0)
     # A batch of independent jobs is split across ranks (no collective on
     # the data path); a single cloud runs as one replica per rank.
