@@ -202,6 +202,31 @@ def test_batch_equals_each_job_alone(ctx):
         sp.destroy()
 
 
+# The bench's own workloads, whole, against the oracle: the configurations
+# the throughput figures are measured on are the ones shown exact.
+
+def test_bench_workload_clusters_1m(ctx):
+    check_job(ctx, W.clusters_1m(seed=1))
+
+
+def test_bench_workload_slab_6m(ctx):
+    check_job(ctx, W.slab_6m(seed=2), culls=(0.5,))
+
+
+def test_bench_workload_mixed_64_batched(ctx):
+    import torch
+    jobs = W.mixed_64(seed=3, cull=0.5)
+    outs, specs = _device_jobs(ctx, jobs, [j.view.cull for j in jobs])
+    try:
+        ctx.sort_batch(specs, stream=torch.cuda.current_stream().cuda_stream)
+        for (order, keys), job in zip(_results(outs), jobs):
+            want_o, want_k = oracle_sort(O.parse_splat(job.bytes()), job.view, job.view.cull)
+            assert np.array_equal(order, want_o) and np.array_equal(keys, want_k)
+    finally:
+        for sp, *_ in outs:
+            sp.destroy()
+
+
 @pytest.mark.parametrize("tile,ctas", [(1024, 2), (1024, 3), (1024, 4), (1024, 6), (2048, 2), (2048, 3), (2048, 4),
                                        (4096, 2), (4096, 3), (4096, 4)])
 def test_kernel_variants_do_not_change_the_result(ctx, tile, ctas):
