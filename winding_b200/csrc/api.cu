@@ -547,6 +547,11 @@ extern "C" int ws_destroy(ws_ctx* ctx) {
     ctx->jobs_h.release();
     ctx->items_h.release();
     ctx->count_h.release();
+    for (int b = 0; b < 2; ++b) {
+        ctx->load_h[b].release();
+        ctx->load_d[b].release();
+        if (ctx->load_done[b]) cudaEventDestroy(ctx->load_done[b]);
+    }
     if (ctx->err_d) cudaFree(ctx->err_d);
     if (ctx->staged) cudaEventDestroy(ctx->staged);
     if (ctx->launched) cudaEventDestroy(ctx->launched);

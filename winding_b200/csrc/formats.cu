@@ -29,6 +29,7 @@
 #include <new>
 #include <sstream>
 #include <string>
+#include <thread>
 #include <vector>
 
 namespace wsort {
@@ -164,15 +165,17 @@ __device__ __forceinline__ double ply_read(const uint8_t* rec, uint8_t type, uin
     }
 }
 
-__global__ void __launch_bounds__(256) ply_kernel(const uint8_t* __restrict__ data, uint32_t n, PlyLayout L,
-                                                  Sink o) {
+// Vertices first .. first + n - 1 of the file, whose records start at data.
+__global__ void __launch_bounds__(256) ply_kernel(const uint8_t* __restrict__ data, uint32_t n, uint32_t first,
+                                                  PlyLayout L, Sink o) {
     Box box;
     for (int k = 0; k < 3; ++k) {
         box.lo[k] = ~0ull;
         box.hi[k] = 0ull;
     }
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const uint8_t* rec = data + (size_t)i * L.stride;
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        const uint8_t* rec = data + (size_t)j * L.stride;
+        const uint32_t i = first + j;
         double v[kPlyNeeds];
 #pragma unroll
         for (int k = 0; k < kPlyNeeds; ++k) v[k] = ply_read(rec, L.type[k], L.offset[k]);
@@ -483,6 +486,59 @@ int finish_cloud(ws_ctx* ctx, ws_cloud* c, unsigned long long* words, cudaError_
     return WS_OK;
 }
 
+// Copies `bytes` from src to dst with the host's threads (the copy into pinned
+// memory is what bounds a streamed upload).
+void parallel_copy(void* dst, const void* src, size_t bytes) {
+    const unsigned hw = std::thread::hardware_concurrency();
+    const size_t parts = std::min<size_t>(hw ? std::min(hw, 8u) : 4u, std::max<size_t>(1, bytes >> 22));
+    if (parts <= 1) {
+        std::memcpy(dst, src, bytes);
+        return;
+    }
+    const size_t each = (bytes + parts - 1) / parts;
+    std::vector<std::thread> team;
+    for (size_t k = 1; k < parts; ++k)
+        team.emplace_back([=] {
+            const size_t lo = k * each, hi = std::min(bytes, lo + each);
+            if (lo < hi) std::memcpy(static_cast<char*>(dst) + lo, static_cast<const char*>(src) + lo, hi - lo);
+        });
+    std::memcpy(dst, src, std::min(bytes, each));
+    for (auto& t : team) t.join();
+}
+
+// Streams n fixed-size records from host memory to the device, a chunk of
+// about 32 MB at a time through the context's two pinned and two device
+// buffers: while one chunk crosses PCIe and is decoded (`decode(dev, first,
+// count)`, queued on the context's stream), the host copies the next one.
+// Returns the first CUDA error; the caller's decode launches are checked.
+template <class Decode>
+cudaError_t stream_records(ws_ctx* ctx, const uint8_t* src, uint32_t n, size_t stride, Decode decode) {
+    constexpr size_t kChunkBytes = 32u << 20;
+    const uint32_t per = (uint32_t)std::max<size_t>(1, std::min<size_t>(kChunkBytes / stride, n ? n : 1));
+    const size_t chunk = (size_t)per * stride;
+    cudaError_t e;
+    for (int b = 0; b < 2; ++b) {
+        if ((e = ctx->load_h[b].ensure(chunk)) != cudaSuccess || (e = ctx->load_d[b].ensure(chunk)) != cudaSuccess)
+            return e;
+        if (!ctx->load_done[b] && (e = cudaEventCreateWithFlags(&ctx->load_done[b], cudaEventDisableTiming)) != cudaSuccess)
+            return e;
+    }
+    for (uint32_t first = 0, k = 0; first < n; first += per, ++k) {
+        const int b = (int)(k & 1u);
+        const uint32_t count = std::min(per, n - first);
+        const size_t bytes = (size_t)count * stride;
+        if (k >= 2 && (e = cudaEventSynchronize(ctx->load_done[b])) != cudaSuccess) return e;   // buffer b is free
+        parallel_copy(ctx->load_h[b].p, src + (size_t)first * stride, bytes);
+        if ((e = cudaMemcpyAsync(ctx->load_d[b].p, ctx->load_h[b].p, bytes, cudaMemcpyHostToDevice, ctx->stream)) !=
+            cudaSuccess)
+            return e;
+        decode(static_cast<const uint8_t*>(ctx->load_d[b].p), first, count);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        if ((e = cudaEventRecord(ctx->load_done[b], ctx->stream)) != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
 uint32_t grid_of(ws_ctx* ctx, uint32_t n) {
     const uint32_t want = (n + 255) / 256;
     const uint32_t cap = (uint32_t)ctx->sms * 8u;
@@ -600,27 +656,15 @@ int load_ply(ws_ctx* ctx, const uint8_t* data, size_t len, ws_cloud** out) {
         L.offset[kPlyNeeds + k] = p.second;
     }
     cudaSetDevice(ctx->device);
-    void* staging = nullptr;
-    const size_t bytes = (size_t)n * stride;
-    cudaError_t e = cudaMalloc(&staging, bytes ? bytes : 1);
-    if (e != cudaSuccess) return cuda_error(ctx, e, "ws_cloud_load");
-    if ((e = cudaMemcpyAsync(staging, data + end, bytes, cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess) {
-        cudaFree(staging);
-        return cuda_error(ctx, e, "ws_cloud_load upload");
-    }
     unsigned long long* words = nullptr;
     int rc;
     ws_cloud* c = new_cloud(ctx, n, (uint32_t)degree, &words, &rc);
-    if (!c) {
-        cudaStreamSynchronize(ctx->stream);
-        cudaFree(staging);
-        return rc;
-    }
-    ply_kernel<<<grid_of(ctx, n), 256, 0, ctx->stream>>>(static_cast<const uint8_t*>(staging), n, L, sink_of(c, words));
-    e = cudaGetLastError();
-    rc = finish_cloud(ctx, c, words, e, out);
-    cudaFree(staging);
-    return rc;
+    if (!c) return rc;
+    const Sink sink = sink_of(c, words);
+    cudaError_t e = stream_records(ctx, data + end, n, stride, [&](const uint8_t* dev, uint32_t first, uint32_t count) {
+        ply_kernel<<<grid_of(ctx, count), 256, 0, ctx->stream>>>(dev, count, first, L, sink);
+    });
+    return finish_cloud(ctx, c, words, e, out);
 }
 
 int load_spz(ws_ctx* ctx, const uint8_t* gz, size_t len, ws_cloud** out) {

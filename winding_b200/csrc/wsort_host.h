@@ -75,6 +75,11 @@ struct ws_ctx {
     std::vector<struct ws_cloud*> freed;   // freed clouds, kept as refusable handles
     wsort::DevBuf thr_d;              // particle depth thresholds, uploaded on first use
     wsort::DevBuf draw_d, pairs_d;    // ws_draw: per-splat quads and scans; (tile, splat) pairs
+    // Capture loads: two chunks of a file on their way to the device (pinned
+    // host, device), each free again once its event has passed.
+    wsort::HostBuf load_h[2];
+    wsort::DevBuf load_d[2];
+    cudaEvent_t load_done[2] = {nullptr, nullptr};
 };
 
 struct ws_cloud {
