@@ -159,6 +159,16 @@ def test_emitter_batch_matches_oracle(ctx):
 
 
 @pytest.mark.gpu
+def test_bench_workload_particles_64(ctx):
+    """The bench's particle workload, whole: 64 rings of 1k-200k slots in one
+    pool, sorted in one launch, every ring against the oracle."""
+    from winding_b200 import workloads as W
+    rings = W.emitter_rings()
+    pool = W.particle_pool(sum(c for _, c in rings))
+    _check(ctx, pool, rings, np.array([0.0, 5.0, 80.0], np.float32), np.array([0.0, -0.0624, -0.998], np.float32))
+
+
+@pytest.mark.gpu
 def test_depths_on_bucket_thresholds(ctx):
     """Particles exactly on each threshold and one ulp below: the buckets
     the comparisons give are the oracle's."""

@@ -22,8 +22,7 @@ def _sh_words(n, degree, rng, scale=0.4):
     per = SH_WORDS[degree]
     halves = np.zeros(n * per * 2 + 2, np.uint16)
     vals = (rng.uniform(-scale, scale, size=(n, COEFS[degree] * 3))).astype(np.float16)
-    for i in range(n):
-        halves[i * per * 2: i * per * 2 + COEFS[degree] * 3] = vals[i].view(np.uint16)
+    halves[: n * per * 2].reshape(n, per * 2)[:, : COEFS[degree] * 3] = vals.view(np.uint16)
     return halves.view(np.uint32)[: n * per + 1].copy()
 
 
@@ -134,6 +133,34 @@ def test_sort_batch_shaded_matches_oracle(ctx, degree):
     finally:
         for sp in clouds:
             sp.destroy()
+
+
+@pytest.mark.gpu
+def test_bench_workload_shade_1m(ctx):
+    """The bench's shade measurement, whole: clusters-1M with degree-3
+    harmonics, sorted and shaded in one launch, every survivor's word
+    against the oracle."""
+    import torch
+    rng = np.random.default_rng(41)
+    job = W.clusters_1m(seed=1)
+    sp = parse_splats(job.records, ctx)
+    try:
+        parsed = O.parse_splat(job.bytes())
+        sh = _sh_words(sp.count, 3, rng)
+        sp.set_harmonics(3, sh)
+        view = make_view(job.view.model_view, job.view.projection, job.view.viewport, 0.5)
+        eye = eye_in_cloud(job.view.model_view)
+        o = torch.empty(sp.count, dtype=torch.int32, device="cuda")
+        k = torch.empty_like(o)
+        c = torch.zeros(1, dtype=torch.int32, device="cuda")
+        shaded = torch.zeros(sp.count, dtype=torch.int32, device="cuda")
+        ctx.sort_batch_shaded([(sp, view, o.data_ptr(), k.data_ptr(), c.data_ptr())], [(eye, shaded.data_ptr())])
+        ctx.sync()
+        order = o[:int(c.item())].cpu().numpy().view(np.uint32)
+        got = shaded.cpu().numpy().view(np.uint32)
+        assert np.array_equal(got[order], O.shade(parsed.centers, sh, 3, order, eye))
+    finally:
+        sp.destroy()
 
 
 @pytest.mark.gpu
