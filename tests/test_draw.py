@@ -89,6 +89,24 @@ def test_draw_matches_oracle(ctx, w, h):
 
 
 @pytest.mark.gpu
+def test_bench_workload_draw_1m(ctx):
+    """The bench's draw, whole: clusters-1M sorted and drawn at 1920 x 1080,
+    bit for bit against the oracle's draw of the oracle's order."""
+    import torch
+    job = W.clusters_1m(seed=1)
+    sp, view, o, c = _sorted(ctx, job)
+    try:
+        img = torch.zeros((1080, 1920, 4), dtype=torch.float32, device="cuda")
+        ctx.draw(sp, view, o.data_ptr(), c.data_ptr(), img.data_ptr(), 1920, 1080)
+        ctx.sync()
+        order = o[: int(c.item())].cpu().numpy().view(np.uint32)
+        want = O.draw(O.parse_splat(job.bytes()), order, job.view.model_view, job.view.projection, 1920, 1080)
+        assert np.array_equal(img.cpu().numpy().view(np.uint32), want.view(np.uint32))
+    finally:
+        sp.destroy()
+
+
+@pytest.mark.gpu
 def test_draw_with_shaded_colours(ctx):
     import torch
     from winding_b200.splats import eye_in_cloud
