@@ -316,6 +316,12 @@ int ws_particle_thresholds(float* out);
 int ws_draw(ws_ctx* ctx, const ws_cloud* cloud, const ws_view* view, const uint32_t* order, const uint32_t* count,
             const uint32_t* shaded, float* image, uint32_t width, uint32_t height, void* stream);
 
+/* Which tiles ws_draw blends with four warps to each pair of pixel rows
+ * instead of one: those whose splat list holds min_splats or more (a power
+ * of two; 0: none; 1: every tile with a splat; default 1024). The image is
+ * the same either way; only the time differs. */
+int ws_set_draw_crowded(ws_ctx* ctx, uint32_t min_splats);
+
 /* The draw's two 256-entry tables: decodeSRGB(byte / 255) and
  * log(255 (byte / 255)), as the f32 the draw uses. Host only. */
 int ws_draw_tables(float* srgb, float* reach);

@@ -89,6 +89,34 @@ def test_draw_matches_oracle(ctx, w, h):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("crowd_min", [0, 1, 256])
+def test_crowded_tile_kernel_matches_oracle(ctx, crowd_min):
+    """Every tile through the crowded-tile kernel (1), none (0), and a split
+    (256): the same image, bit for bit, as the oracle's."""
+    import torch
+    from winding_b200 import WsError
+    w, h = 480, 270
+    job = _job(150_000, 8, w, h)
+    sp, view, o, c = _sorted(ctx, job)
+    try:
+        ctx.set_draw_crowded(crowd_min)
+        rng = np.random.default_rng(2)
+        bg = rng.uniform(0, 1, size=(h, w, 4)).astype(np.float32)
+        img = torch.from_numpy(bg.copy()).cuda()
+        ctx.draw(sp, view, o.data_ptr(), c.data_ptr(), img.data_ptr(), w, h)
+        ctx.sync()
+        order = o[: int(c.item())].cpu().numpy().view(np.uint32)
+        want = O.draw(O.parse_splat(job.bytes()), order, job.view.model_view, job.view.projection, w, h,
+                      background=bg)
+        assert np.array_equal(img.cpu().numpy().view(np.uint32), want.view(np.uint32))
+        with pytest.raises(WsError, match="power of two"):
+            ctx.set_draw_crowded(1000)
+    finally:
+        ctx.set_draw_crowded(1024)
+        sp.destroy()
+
+
+@pytest.mark.gpu
 def test_bench_workload_draw_1m(ctx):
     """The bench's draw, whole: clusters-1M sorted and drawn at 1920 x 1080,
     bit for bit against the oracle's draw of the oracle's order."""

@@ -181,6 +181,7 @@ SIGNATURES = {
     "ws_cloud_load": (ctypes.c_int, [vp, vp, ctypes.c_size_t, ctypes.POINTER(ctypes.c_void_p)]),
     "ws_draw": (ctypes.c_int, [vp, vp, ctypes.POINTER(WsView), vp, vp, vp, vp, ctypes.c_uint32, ctypes.c_uint32, vp]),
     "ws_draw_tables": (ctypes.c_int, [ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]),
+    "ws_set_draw_crowded": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32]),
     "ws_selftest_wait": (ctypes.c_int, [vp, ctypes.c_uint32]),
     "ws_inject_alloc_failures": (ctypes.c_int, [ctypes.c_int]),
     "ws_server_cancel": (ctypes.c_int, [vp, ctypes.c_uint64]),

@@ -41,7 +41,9 @@
 // scan gives each splat its run of (tile, splat) pairs, emitted in splat
 // order; the library's own stable sort orders the pairs by tile (a 16-bit
 // key; same-tile pairs keep splat order); one CTA per tile then blends its
-// splats in order, 256 pixels a CTA, splat records staged in shared memory.
+// splats in order, 256 pixels a CTA, splat records staged in shared memory,
+// the tiles with the longest lists launched first; tiles with thousands of
+// splats are blended first, by a kernel with four warps to a row pair.
 #include "wsort.h"
 #include "wsort_dev.cuh"
 #include "wsort_host.h"
@@ -277,6 +279,46 @@ __global__ void __launch_bounds__(256) ranges_kernel(const uint32_t* __restrict_
     }
 }
 
+// The order the blend visits tiles in: longest splat lists first (by the
+// list length's top two bits: lengths within a factor of 1.5 share a class,
+// in no particular order), so that the crowded tiles start in the first
+// wave, one to an SM, instead of wherever their index falls. One CTA; any
+// order gives the same image, as each tile is blended on its own.
+// It also counts the crowded tiles, those whose list holds crowd_min splats
+// or more (a power of two, so that they are exactly the first classes; 0:
+// none), which take the first places of the order.
+constexpr int kOrderClasses = 66;   // 0: empty; then 2 classes an octave, longest last
+__device__ __forceinline__ int length_class(uint32_t len) {
+    if (len == 0) return 0;
+    const int top = 31 - __clz(len);                                             // 0..31
+    const int half = top > 0 ? (int)((len >> (top - 1)) & 1u) : 0;             // the bit below the top
+    return 2 + 2 * top + half;
+}
+
+__global__ void __launch_bounds__(1024) order_tiles_kernel(const uint2* __restrict__ range, uint32_t tiles,
+                                                           uint32_t crowd_min, uint32_t* __restrict__ tile_order,
+                                                           uint32_t* __restrict__ n_crowded) {
+    __shared__ uint32_t count[kOrderClasses], start[kOrderClasses];
+    auto class_of = [](uint2 r) -> int { return length_class(r.y - r.x); };
+    for (int c = threadIdx.x; c < kOrderClasses; c += blockDim.x) count[c] = 0;
+    __syncthreads();
+    for (uint32_t t = threadIdx.x; t < tiles; t += blockDim.x) atomicAdd(&count[class_of(range[t])], 1u);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int crowd_class = crowd_min ? length_class(crowd_min) : kOrderClasses;
+        uint32_t run = 0;
+        for (int c = kOrderClasses - 1; c >= 0; --c) {
+            start[c] = run;
+            run += count[c];
+            if (c == crowd_class) *n_crowded = run;
+        }
+        if (crowd_class >= kOrderClasses) *n_crowded = 0;
+    }
+    __syncthreads();
+    for (uint32_t t = threadIdx.x; t < tiles; t += blockDim.x)
+        tile_order[atomicAdd(&start[class_of(range[t])], 1u)] = t;
+}
+
 // The splat of each pair, in tile order: one indirection less for the blend.
 __global__ void __launch_bounds__(256) gather_kernel(const uint32_t* __restrict__ owner,
                                                      const uint32_t* __restrict__ sorted, uint32_t npairs,
@@ -289,9 +331,12 @@ __global__ void __launch_bounds__(256) gather_kernel(const uint32_t* __restrict_
 // (px, py): each one's alpha, or 0 when its quad does not cover the pixel or
 // the fragment is dropped. Evaluated in lock-step, every stage for all N
 // splats before the next, so the N independent chains overlap; without
-// branches (every value computed, the answer selected). For x = -d2 <= 0 exp
-// is 0 below -104, else 2^k p(r) as the head describes (the two-step
-// scaling multiplies by 2^0 when one step suffices, which is exact).
+// branches (every value computed, the answer selected). A covered fragment
+// has |ox|, |oy| <= qm <= 2, so x = -d2 lies in [-8, 0] and k in [-12, 0]:
+// exp is 2^k p(r) with 2^k a normal power of two, one multiply (the head's
+// two-step scaling multiplies by 2^0 first there, which is exact, and its
+// cases for x below -104 or NaN are never reached). An uncovered fragment's
+// value is discarded, whatever these steps give for it.
 template <int N>
 __device__ __forceinline__ void fragment_alphas(const Quad* const* q, int px, int py, float fx, float fy, float* out) {
     float x[N], k[N], r[N], p[N];
@@ -327,10 +372,8 @@ __device__ __forceinline__ void fragment_alphas(const Quad* const* q, int px, in
     for (int t = 0; t < N; ++t) p[t] = fadd(fmul(p[t], r[t]), 1.0f);
 #pragma unroll
     for (int t = 0; t < N; ++t) {
-        const int ki = max((int)fmaxf(k[t], -200.0f), -200);
-        const int k1 = ki < -126 ? ki + 126 : 0, k2 = ki < -126 ? -126 : ki;
-        const float e0 = fmul(fmul(p[t], __int_as_float((k1 + 127) << 23)), __int_as_float((k2 + 127) << 23));
-        const float e = (x[t] != x[t]) ? x[t] : (x[t] < -104.0f ? 0.0f : e0);
+        const uint32_t bits = ((uint32_t)__float2int_rn(k[t]) + 127u) << 23;
+        const float e = fmul(p[t], __uint_as_float(bits));
         const float alpha = fminf(0.99f, fmul(e, q[t]->a));
         out[t] = (covered[t] && !(alpha < 1.0f / 255.0f)) ? alpha : 0.0f;
     }
@@ -347,10 +390,14 @@ __device__ __forceinline__ void fragment_alphas(const Quad* const* q, int px, in
 // every splat is tried one by one.
 __global__ void __launch_bounds__(256) blend_kernel(const Quad* __restrict__ quads,
                                                     const uint32_t* __restrict__ splat_of,
-                                                    const uint2* __restrict__ range, uint32_t width, uint32_t height,
-                                                    uint32_t tiles_x, float4* __restrict__ image) {
+                                                    const uint2* __restrict__ range,
+                                                    const uint32_t* __restrict__ tile_order,
+                                                    const uint32_t* __restrict__ n_crowded, uint32_t width,
+                                                    uint32_t height, uint32_t tiles_x, float4* __restrict__ image) {
     __shared__ Quad staged[2][256];
-    const uint32_t tile = blockIdx.x;
+    const uint32_t slot = *n_crowded + blockIdx.x;   // the grid is one CTA a tile; the crowded ones are done
+    if (slot >= gridDim.x) return;
+    const uint32_t tile = tile_order[slot];
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int px = (int)((tile % tiles_x) * kTilePx + (threadIdx.x & 15));
     const int py = (int)((tile / tiles_x) * kTilePx + (threadIdx.x >> 4));
@@ -428,6 +475,142 @@ __global__ void __launch_bounds__(256) blend_kernel(const Quad* __restrict__ qua
     if (inside) image[(size_t)py * width + px] = dst;
 }
 
+// Crowded tiles: the same blend, with four warps to each pair of pixel rows
+// instead of one. A tile whose list runs to thousands of splats keeps one
+// warp of blend_kernel busy for every one of them while the SM has little
+// else to issue; here, for each chunk of 64 splats, three warps evaluate the
+// row pair's fragments (the marked splats dealt out in turn) into a
+// shared-memory table, and the fourth blends them, in order, one chunk
+// behind. The values and the order of every operation on a pixel are
+// blend_kernel's, so the image is the same to the bit. One CTA of 1024
+// threads an SM (its shared memory keeps it alone there), looping over the
+// crowded tiles, longest first.
+constexpr int kCrowdThreads = 1024;
+constexpr uint32_t kCrowdChunk = 64;     // splats a step
+constexpr uint32_t kCrowdEval = 3;       // evaluating warps a row pair
+struct CrowdSmem {
+    Quad staged[3][kCrowdChunk];                           // chunk i in staged[i % 3]
+    float alpha[2][8][kCrowdChunk][32];                    // chunk i's alphas in alpha[i % 2], by row pair, mark, lane
+    uint8_t marks[8][kCrowdEval][kCrowdChunk];             // each evaluating warp's marked splats, in order
+};
+
+__global__ void __launch_bounds__(kCrowdThreads, 1) crowd_kernel(const Quad* __restrict__ quads,
+                                                                 const uint32_t* __restrict__ splat_of,
+                                                                 const uint2* __restrict__ range,
+                                                                 const uint32_t* __restrict__ tile_order,
+                                                                 const uint32_t* __restrict__ n_crowded,
+                                                                 uint32_t width, uint32_t height, uint32_t tiles_x,
+                                                                 float4* __restrict__ image) {
+    extern __shared__ __align__(16) unsigned char crowd_raw[];
+    CrowdSmem& sm = *reinterpret_cast<CrowdSmem*>(crowd_raw);
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t pair = warp >> 2, role = warp & 3;   // role 0 blends; 1..3 evaluate
+    const uint32_t lt = (1u << lane) - 1u;
+    const uint32_t crowded = *n_crowded;
+    for (uint32_t slot = blockIdx.x; slot < crowded; slot += gridDim.x) {
+        const uint32_t tile = tile_order[slot];
+        const int px = (int)((tile % tiles_x) * kTilePx + (lane & 15));
+        const int row0 = (int)((tile / tiles_x) * kTilePx + 2 * pair), row1 = row0 + 1;
+        const int py = row0 + (int)(lane >> 4);
+        const bool inside = px < (int)width && py < (int)height;
+        float4 dst = make_float4(0, 0, 0, 0);
+        if (role == 0 && inside) dst = image[(size_t)py * width + px];
+        const float fx = fadd((float)px, 0.5f), fy = fadd((float)py, 0.5f);
+        const uint2 rg = range[tile];
+        const uint32_t chunks = (rg.y - rg.x + kCrowdChunk - 1) / kCrowdChunk;
+        // Staging: threads 0..255 copy one 16-byte quarter of a quad each;
+        // the splat index is read a chunk ahead, so its latency is hidden.
+        auto index_of = [&](uint32_t c) -> uint32_t {
+            const uint32_t k = rg.x + c * kCrowdChunk + (threadIdx.x >> 2);
+            return threadIdx.x < kCrowdChunk * 4 && c < chunks && k < rg.y ? splat_of[k] : 0xffffffffu;
+        };
+        auto stage = [&](uint32_t idx, uint32_t b) {
+            if (idx != 0xffffffffu)
+                cp_async16(reinterpret_cast<float4*>(&sm.staged[b][threadIdx.x >> 2]) + (threadIdx.x & 3),
+                           reinterpret_cast<const float4*>(&quads[idx]) + (threadIdx.x & 3));
+            cp_async_commit();
+        };
+        // The row pair's marks in chunk c: the splats whose box reaches its rows.
+        auto mark = [&](uint32_t c, uint32_t b, uint32_t* mk) {
+            const uint32_t m = min(kCrowdChunk, rg.y - rg.x - c * kCrowdChunk);
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                const uint32_t e = j * 32 + lane;
+                bool hit = false;
+                if (e < m) {
+                    const Quad& q = sm.staged[b][e];
+                    hit = q.y0 <= row1 && q.y1 >= row0;
+                }
+                mk[j] = __ballot_sync(0xffffffffu, hit);
+            }
+        };
+        __syncthreads();   // the previous tile's last reads of the tables are done
+        stage(index_of(0), 0);
+        uint32_t next = index_of(1);
+        for (uint32_t i = 0; i <= chunks; ++i) {
+            cp_async_wait_none();
+            __syncthreads();   // chunk i is staged; chunk i - 2's quads and alphas are no longer read
+            if (i + 1 < chunks) {
+                stage(next, (i + 1) % 3);
+                next = index_of(i + 2);
+            }
+            if (role == 0) {
+                if (i == 0) continue;
+                const uint32_t c = i - 1, b = c % 3;
+                uint32_t mk[2];
+                mark(c, b, mk);
+                const float* in = &sm.alpha[c & 1][pair][0][0];
+                uint32_t rank = 0;
+#pragma unroll
+                for (int j = 0; j < 2; ++j) {
+                    uint32_t word = mk[j];
+                    while (word) {
+                        const uint32_t e = j * 32 + (__ffs(word) - 1);
+                        word &= word - 1;
+                        const float alpha = in[rank * 32 + lane];
+                        ++rank;
+                        if (alpha == 0.0f) continue;
+                        const Quad& q = sm.staged[b][e];
+                        const float om = fsub(1.0f, alpha);
+                        dst.x = fadd(fmul(q.r, alpha), fmul(dst.x, om));
+                        dst.y = fadd(fmul(q.g, alpha), fmul(dst.y, om));
+                        dst.z = fadd(fmul(q.b, alpha), fmul(dst.z, om));
+                        dst.w = fadd(alpha, fmul(dst.w, om));
+                    }
+                }
+            } else if (i < chunks) {
+                const uint32_t b = i % 3;
+                uint32_t mk[2];
+                mark(i, b, mk);
+                const uint32_t total = __popc(mk[0]) + __popc(mk[1]);
+                uint8_t* list = sm.marks[pair][role - 1];
+#pragma unroll
+                for (int j = 0; j < 2; ++j)
+                    if (mk[j] & (1u << lane)) list[(j ? __popc(mk[0]) : 0u) + __popc(mk[j] & lt)] = (uint8_t)(j * 32 + lane);
+                __syncwarp();
+                float* out = &sm.alpha[i & 1][pair][0][0];
+                for (uint32_t r0 = role - 1; r0 < total; r0 += 4 * kCrowdEval) {
+                    const Quad* qs[4];
+#pragma unroll
+                    for (int t = 0; t < 4; ++t) {
+                        const uint32_t r = r0 + t * kCrowdEval;
+                        qs[t] = &sm.staged[b][list[r < total ? r : r0]];
+                    }
+                    float al[4];
+                    fragment_alphas<4>(qs, px, py, fx, fy, al);
+#pragma unroll
+                    for (int t = 0; t < 4; ++t) {
+                        const uint32_t r = r0 + t * kCrowdEval;
+                        if (r < total) out[r * 32 + lane] = al[t];
+                    }
+                }
+                __syncwarp();
+            }
+        }
+        if (role == 0 && inside) image[(size_t)py * width + px] = dst;
+    }
+}
+
 // decodeSRGB of byte / 255 and log(255 byte / 255), as f32 (see the head).
 const std::vector<float>& draw_tables() {
     static std::vector<float> t;
@@ -462,6 +645,14 @@ extern "C" int ws_draw_tables(float* srgb, float* reach) {
     return WS_OK;
 }
 
+extern "C" int ws_set_draw_crowded(ws_ctx* ctx, uint32_t min_splats) {
+    if (!ctx) return WS_ERR_ARG;
+    if (min_splats & (min_splats - 1))
+        return set_error(ctx, WS_ERR_ARG, "ws_set_draw_crowded: %u is not a power of two (or 0)", min_splats);
+    ctx->draw_crowd_min = min_splats;
+    return WS_OK;
+}
+
 extern "C" int ws_draw(ws_ctx* ctx, const ws_cloud* cloud, const ws_view* view, const uint32_t* order,
                        const uint32_t* count, const uint32_t* shaded, float* image, uint32_t width, uint32_t height,
                        void* stream_p) {
@@ -485,12 +676,14 @@ extern "C" int ws_draw(ws_ctx* ctx, const ws_cloud* cloud, const ws_view* view, 
     const uint32_t nb = (n + kScanTile - 1) / kScanTile;
     cudaError_t e;
     // Scratch: the job table, tables, quads, per-splat tile counts and offsets,
-    // block sums, 64-bit total, tile ranges.
+    // block sums, 64-bit total, tile ranges, the blend's tile order, the
+    // number of crowded tiles.
     auto up = [](size_t v) { return (v + 255) / 256 * 256; };
     const size_t o_job = 0, o_tab = up(sizeof(JobDesc)), o_quad = o_tab + up(512 * 4);
     const size_t o_cnt = o_quad + up((size_t)n * sizeof(Quad)), o_off = o_cnt + up((size_t)n * 4);
     const size_t o_sums = o_off + up((size_t)n * 4), o_tot = o_sums + up((size_t)nb * 4 + 4);
-    const size_t o_rng = o_tot + 256, fixed = o_rng + up((size_t)tiles * 8);
+    const size_t o_rng = o_tot + 256, o_tord = o_rng + up((size_t)tiles * 8), o_ncr = o_tord + up((size_t)tiles * 4);
+    const size_t fixed = o_ncr + 256;
     if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return cuda_error(ctx, e, "ws_draw");
     if ((e = ctx->draw_d.ensure(fixed)) != cudaSuccess) return cuda_error(ctx, e, "ws_draw scratch");
     char* base = static_cast<char*>(ctx->draw_d.p);
@@ -519,6 +712,8 @@ extern "C" int ws_draw(ws_ctx* ctx, const ws_cloud* cloud, const ws_view* view, 
     uint32_t* sums = reinterpret_cast<uint32_t*>(base + o_sums);
     unsigned long long* total = reinterpret_cast<unsigned long long*>(base + o_tot);
     uint2* range = reinterpret_cast<uint2*>(base + o_rng);
+    uint32_t* tile_order = reinterpret_cast<uint32_t*>(base + o_tord);
+    uint32_t* n_crowded = reinterpret_cast<uint32_t*>(base + o_ncr);
     const uint32_t g = std::max(1u, std::min((n + 255) / 256, (uint32_t)ctx->sms * 8));
     prepare_kernel<<<g, 256, 0, stream>>>(reinterpret_cast<const JobDesc*>(base + o_job), order, count, shaded,
                                           reinterpret_cast<const float*>(base + o_tab), n, width, height, quads, cnt);
@@ -555,7 +750,15 @@ extern "C" int ws_draw(ws_ctx* ctx, const ws_cloud* cloud, const ws_view* view, 
     const uint32_t gp = std::max(1u, std::min((pairs + 255) / 256, (uint32_t)ctx->sms * 8));
     ranges_kernel<<<gp, 256, 0, stream>>>(skeys, pairs, range);
     gather_kernel<<<gp, 256, 0, stream>>>(owner, sorted, pairs, splat_of);
-    blend_kernel<<<tiles, 256, 0, stream>>>(quads, splat_of, range, width, height, tiles_x,
+    order_tiles_kernel<<<1, 1024, 0, stream>>>(range, tiles, ctx->draw_crowd_min, tile_order, n_crowded);
+    if (ctx->draw_crowd_min) {
+        if ((e = cudaFuncSetAttribute(crowd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)sizeof(CrowdSmem))) != cudaSuccess)
+            return cuda_error(ctx, e, "ws_draw");
+        crowd_kernel<<<std::min(tiles, (uint32_t)ctx->sms), kCrowdThreads, sizeof(CrowdSmem), stream>>>(
+            quads, splat_of, range, tile_order, n_crowded, width, height, tiles_x, reinterpret_cast<float4*>(image));
+    }
+    blend_kernel<<<tiles, 256, 0, stream>>>(quads, splat_of, range, tile_order, n_crowded, width, height, tiles_x,
                                             reinterpret_cast<float4*>(image));
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_error(ctx, e, "ws_draw");
     return WS_OK;

@@ -157,6 +157,12 @@ class Context:
         self.check(self.lib.ws_draw(self.handle, splats.handle, ctypes.byref(view), order_ptr, count_ptr,
                                     shaded_ptr, image_ptr, int(width), int(height), stream))
 
+    def set_draw_crowded(self, min_splats: int) -> None:
+        """Tiles whose splat list holds min_splats or more (a power of two;
+        0: none) are blended with four warps to a row pair
+        (ws_set_draw_crowded); the image is the same either way."""
+        self.check(self.lib.ws_set_draw_crowded(self.handle, int(min_splats)))
+
     def sort_particles(self, emitters: list[tuple], stream: int | None = None) -> None:
         """emitters: (pool_ptr, offset, capacity, eye, forward, order_ptr,
         keys_ptr or None, count_ptr), pointers into device memory; one launch
