@@ -327,8 +327,8 @@ __global__ void __launch_bounds__(256) gather_kernel(const uint32_t* __restrict_
         splat_of[k] = owner[sorted[k]];
 }
 
-// The fragments of splats q[0..N) at pixel centre (fx, fy) of pixel
-// (px, py): each one's alpha, or 0 when its quad does not cover the pixel or
+// The fragments of splats q[0..N), splat t at pixel (px[t], py[t]) whose
+// centre is (fx[t], fy[t]): each one's alpha, or 0 when its quad does not cover the pixel or
 // the fragment is dropped. Evaluated in lock-step, every stage for all N
 // splats before the next, so the N independent chains overlap; without
 // branches (every value computed, the answer selected). A covered fragment
@@ -337,14 +337,16 @@ __global__ void __launch_bounds__(256) gather_kernel(const uint32_t* __restrict_
 // two-step scaling multiplies by 2^0 first there, which is exact, and its
 // cases for x below -104 or NaN are never reached). An uncovered fragment's
 // value is discarded, whatever these steps give for it.
-template <int N>
-__device__ __forceinline__ void fragment_alphas(const Quad* const* q, int px, int py, float fx, float fy, float* out) {
+template <int N, bool kInBox = false>   // kInBox: the caller knows every pixel lies in its splat's box
+__device__ __forceinline__ void fragment_alphas_at(const Quad* const* q, const int* px, const int* py, const float* fx,
+                                                   const float* fy, float* out) {
     float x[N], k[N], r[N], p[N];
     bool covered[N];
 #pragma unroll
     for (int t = 0; t < N; ++t) {
-        const bool in_box = px >= q[t]->x0 && px <= q[t]->x1 && py >= q[t]->y0 && py <= q[t]->y1;
-        const float ex = fsub(fx, q[t]->cx), ey = fsub(q[t]->cy, fy);
+        const bool in_box =
+            kInBox || (px[t] >= q[t]->x0 && px[t] <= q[t]->x1 && py[t] >= q[t]->y0 && py[t] <= q[t]->y1);
+        const float ex = fsub(fx[t], q[t]->cx), ey = fsub(q[t]->cy, fy[t]);
         const float ox = fmul(fadd(fmul(ex, q[t]->ax), fmul(ey, q[t]->ay)), q[t]->ila);
         const float oy = fmul(fsub(fmul(ex, q[t]->ay), fmul(ey, q[t]->ax)), q[t]->ilc);
         covered[t] = in_box && fabsf(ox) <= q[t]->qm && fabsf(oy) <= q[t]->qm;
@@ -377,6 +379,21 @@ __device__ __forceinline__ void fragment_alphas(const Quad* const* q, int px, in
         const float alpha = fminf(0.99f, fmul(e, q[t]->a));
         out[t] = (covered[t] && !(alpha < 1.0f / 255.0f)) ? alpha : 0.0f;
     }
+}
+
+// The same, every splat at the one pixel (px, py) whose centre is (fx, fy).
+template <int N>
+__device__ __forceinline__ void fragment_alphas(const Quad* const* q, int px, int py, float fx, float fy, float* out) {
+    int pxs[N], pys[N];
+    float fxs[N], fys[N];
+#pragma unroll
+    for (int t = 0; t < N; ++t) {
+        pxs[t] = px;
+        pys[t] = py;
+        fxs[t] = fx;
+        fys[t] = fy;
+    }
+    fragment_alphas_at<N>(q, pxs, pys, fxs, fys, out);
 }
 
 // One CTA a tile, one thread a pixel: the tile's splats in order, staged in
@@ -475,24 +492,40 @@ __global__ void __launch_bounds__(256) blend_kernel(const Quad* __restrict__ qua
     if (inside) image[(size_t)py * width + px] = dst;
 }
 
-// Crowded tiles: the same blend, with four warps to each pair of pixel rows
-// instead of one. A tile whose list runs to thousands of splats keeps one
-// warp of blend_kernel busy for every one of them while the SM has little
-// else to issue; here, for each chunk of 64 splats, three warps evaluate the
-// row pair's fragments (the marked splats dealt out in turn) into a
-// shared-memory table, and the fourth blends them, in order, one chunk
-// behind. The values and the order of every operation on a pixel are
-// blend_kernel's, so the image is the same to the bit. One CTA of 1024
-// threads an SM (its shared memory keeps it alone there), looping over the
+// Crowded tiles: the same blend, with the fragments evaluated by 24 warps
+// and blended by 8. A tile whose list runs to thousands of splats keeps the
+// warps of blend_kernel evaluating 32 pixels for every splat that reaches
+// their two rows, most of them outside its box, while the SM has little else
+// to issue. Here, for each chunk of 64 splats, the evaluating warps take the
+// pixels of the splats' boxes (within the tile) as one flat list of items,
+// a lane an item, and write each nonzero alpha into a splat x pixel table in
+// shared memory; one chunk behind, each pixel's own thread walks its column
+// of the table in splat order, blends the nonzero entries and clears them.
+// The values and the order of every operation on a pixel are blend_kernel's,
+// so the image is the same to the bit. One CTA of 1024 threads an SM (its
+// registers and shared memory keep it alone there), looping over the
 // crowded tiles, longest first.
 constexpr int kCrowdThreads = 1024;
-constexpr uint32_t kCrowdChunk = 64;     // splats a step
-constexpr uint32_t kCrowdEval = 3;       // evaluating warps a row pair
+constexpr uint32_t kCrowdChunk = 64;                     // splats a step
+constexpr uint32_t kCrowdBlenders = 256;                 // a thread a pixel: warps 0..7
+constexpr uint32_t kCrowdEvalWarps = (kCrowdThreads - kCrowdBlenders) / 32;
+constexpr uint32_t kCrowdBatch = 2;                      // items a lane evaluates at once
 struct CrowdSmem {
-    Quad staged[3][kCrowdChunk];                           // chunk i in staged[i % 3]
-    float alpha[2][8][kCrowdChunk][32];                    // chunk i's alphas in alpha[i % 2], by row pair, mark, lane
-    uint8_t marks[8][kCrowdEval][kCrowdChunk];             // each evaluating warp's marked splats, in order
+    Quad staged[3][kCrowdChunk];                         // chunk i in staged[i % 3]
+    float alpha[2][kCrowdChunk][kTilePx * kTilePx];      // chunk i's alphas in alpha[i % 2]; 0 where none
+    uint32_t start[kCrowdEvalWarps][kCrowdChunk + 1];    // each evaluating warp's copy of the items' starts
+    uint32_t box[kCrowdEvalWarps][kCrowdChunk];          // and of the boxes (crowd_box)
 };
+
+// A staged splat's box within its tile, packed for the item decode: first
+// column and row relative to the tile (4 bits each), width - 1 (4 bits), and
+// ceil(2^16 / width) (17 bits), with which (local * that) >> 16 is local /
+// width exactly for every local < 256 (the error, below 256 / 2^16, never
+// reaches the next multiple of 1 / width >= 1 / 16).
+__device__ __forceinline__ uint32_t crowd_box(int bx, int by, int bw) {
+    const uint32_t magic = (65536u + (uint32_t)bw - 1u) / (uint32_t)bw;
+    return (uint32_t)bx | ((uint32_t)by << 4) | ((uint32_t)(bw - 1) << 8) | (magic << 12);
+}
 
 __global__ void __launch_bounds__(kCrowdThreads, 1) crowd_kernel(const Quad* __restrict__ quads,
                                                                  const uint32_t* __restrict__ splat_of,
@@ -504,18 +537,20 @@ __global__ void __launch_bounds__(kCrowdThreads, 1) crowd_kernel(const Quad* __r
     extern __shared__ __align__(16) unsigned char crowd_raw[];
     CrowdSmem& sm = *reinterpret_cast<CrowdSmem*>(crowd_raw);
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t pair = warp >> 2, role = warp & 3;   // role 0 blends; 1..3 evaluate
-    const uint32_t lt = (1u << lane) - 1u;
+    const bool blender = threadIdx.x < kCrowdBlenders;
+    const uint32_t ew = warp - kCrowdBlenders / 32;      // evaluating warp index (blenders: unused)
+    {
+        float4* z = reinterpret_cast<float4*>(&sm.alpha[0][0][0]);
+        for (uint32_t k = threadIdx.x; k < sizeof(sm.alpha) / 16; k += kCrowdThreads) z[k] = make_float4(0, 0, 0, 0);
+    }
     const uint32_t crowded = *n_crowded;
     for (uint32_t slot = blockIdx.x; slot < crowded; slot += gridDim.x) {
         const uint32_t tile = tile_order[slot];
-        const int px = (int)((tile % tiles_x) * kTilePx + (lane & 15));
-        const int row0 = (int)((tile / tiles_x) * kTilePx + 2 * pair), row1 = row0 + 1;
-        const int py = row0 + (int)(lane >> 4);
-        const bool inside = px < (int)width && py < (int)height;
+        const int tx0 = (int)((tile % tiles_x) * kTilePx), ty0 = (int)((tile / tiles_x) * kTilePx);
+        const int px = tx0 + (int)(threadIdx.x & 15), py = ty0 + (int)((threadIdx.x >> 4) & 15);
+        const bool inside = blender && px < (int)width && py < (int)height;
         float4 dst = make_float4(0, 0, 0, 0);
-        if (role == 0 && inside) dst = image[(size_t)py * width + px];
-        const float fx = fadd((float)px, 0.5f), fy = fadd((float)py, 0.5f);
+        if (inside) dst = image[(size_t)py * width + px];
         const uint2 rg = range[tile];
         const uint32_t chunks = (rg.y - rg.x + kCrowdChunk - 1) / kCrowdChunk;
         // Staging: threads 0..255 copy one 16-byte quarter of a quad each;
@@ -530,19 +565,14 @@ __global__ void __launch_bounds__(kCrowdThreads, 1) crowd_kernel(const Quad* __r
                            reinterpret_cast<const float4*>(&quads[idx]) + (threadIdx.x & 3));
             cp_async_commit();
         };
-        // The row pair's marks in chunk c: the splats whose box reaches its rows.
-        auto mark = [&](uint32_t c, uint32_t b, uint32_t* mk) {
-            const uint32_t m = min(kCrowdChunk, rg.y - rg.x - c * kCrowdChunk);
-#pragma unroll
-            for (int j = 0; j < 2; ++j) {
-                const uint32_t e = j * 32 + lane;
-                bool hit = false;
-                if (e < m) {
-                    const Quad& q = sm.staged[b][e];
-                    hit = q.y0 <= row1 && q.y1 >= row0;
-                }
-                mk[j] = __ballot_sync(0xffffffffu, hit);
-            }
+        // A staged splat's box within the tile: first column and row, width,
+        // and its pixel count (0 past the chunk's end).
+        auto box_of = [&](const Quad& q, int& bx, int& by, int& bw) -> uint32_t {
+            bx = max(q.x0, tx0);
+            by = max(q.y0, ty0);
+            bw = min(q.x1, tx0 + kTilePx - 1) - bx + 1;
+            const int bh = min(q.y1, ty0 + kTilePx - 1) - by + 1;
+            return (uint32_t)(bw * bh);
         };
         __syncthreads();   // the previous tile's last reads of the tables are done
         stage(index_of(0), 0);
@@ -554,60 +584,90 @@ __global__ void __launch_bounds__(kCrowdThreads, 1) crowd_kernel(const Quad* __r
                 stage(next, (i + 1) % 3);
                 next = index_of(i + 2);
             }
-            if (role == 0) {
+            if (blender) {
                 if (i == 0) continue;
                 const uint32_t c = i - 1, b = c % 3;
-                uint32_t mk[2];
-                mark(c, b, mk);
-                const float* in = &sm.alpha[c & 1][pair][0][0];
-                uint32_t rank = 0;
-#pragma unroll
-                for (int j = 0; j < 2; ++j) {
-                    uint32_t word = mk[j];
-                    while (word) {
-                        const uint32_t e = j * 32 + (__ffs(word) - 1);
-                        word &= word - 1;
-                        const float alpha = in[rank * 32 + lane];
-                        ++rank;
-                        if (alpha == 0.0f) continue;
-                        const Quad& q = sm.staged[b][e];
-                        const float om = fsub(1.0f, alpha);
-                        dst.x = fadd(fmul(q.r, alpha), fmul(dst.x, om));
-                        dst.y = fadd(fmul(q.g, alpha), fmul(dst.y, om));
-                        dst.z = fadd(fmul(q.b, alpha), fmul(dst.z, om));
-                        dst.w = fadd(alpha, fmul(dst.w, om));
-                    }
+                const uint32_t m = min(kCrowdChunk, rg.y - rg.x - c * kCrowdChunk);
+                float* col = &sm.alpha[c & 1][0][threadIdx.x];
+#pragma unroll 4
+                for (uint32_t e = 0; e < m; ++e) {
+                    const float alpha = col[e * kTilePx * kTilePx];
+                    if (alpha == 0.0f) continue;
+                    col[e * kTilePx * kTilePx] = 0.0f;
+                    const Quad& q = sm.staged[b][e];
+                    const float om = fsub(1.0f, alpha);
+                    dst.x = fadd(fmul(q.r, alpha), fmul(dst.x, om));
+                    dst.y = fadd(fmul(q.g, alpha), fmul(dst.y, om));
+                    dst.z = fadd(fmul(q.b, alpha), fmul(dst.z, om));
+                    dst.w = fadd(alpha, fmul(dst.w, om));
                 }
             } else if (i < chunks) {
                 const uint32_t b = i % 3;
-                uint32_t mk[2];
-                mark(i, b, mk);
-                const uint32_t total = __popc(mk[0]) + __popc(mk[1]);
-                uint8_t* list = sm.marks[pair][role - 1];
+                const uint32_t m = min(kCrowdChunk, rg.y - rg.x - i * kCrowdChunk);
+                // The items' starts: an inclusive scan of the box sizes, this
+                // warp's copy (lane l holds splats l and 32 + l).
+                int bx, by, bw;
+                uint32_t* bt = sm.box[ew];
+                uint32_t n0 = 0, n1 = 0;
+                if (lane < m) {
+                    n0 = box_of(sm.staged[b][lane], bx, by, bw);
+                    bt[lane] = crowd_box(bx - tx0, by - ty0, bw);
+                }
+                if (lane + 32 < m) {
+                    n1 = box_of(sm.staged[b][lane + 32], bx, by, bw);
+                    bt[lane + 32] = crowd_box(bx - tx0, by - ty0, bw);
+                }
 #pragma unroll
-                for (int j = 0; j < 2; ++j)
-                    if (mk[j] & (1u << lane)) list[(j ? __popc(mk[0]) : 0u) + __popc(mk[j] & lt)] = (uint8_t)(j * 32 + lane);
-                __syncwarp();
-                float* out = &sm.alpha[i & 1][pair][0][0];
-                for (uint32_t r0 = role - 1; r0 < total; r0 += 4 * kCrowdEval) {
-                    const Quad* qs[4];
-#pragma unroll
-                    for (int t = 0; t < 4; ++t) {
-                        const uint32_t r = r0 + t * kCrowdEval;
-                        qs[t] = &sm.staged[b][list[r < total ? r : r0]];
-                    }
-                    float al[4];
-                    fragment_alphas<4>(qs, px, py, fx, fy, al);
-#pragma unroll
-                    for (int t = 0; t < 4; ++t) {
-                        const uint32_t r = r0 + t * kCrowdEval;
-                        if (r < total) out[r * 32 + lane] = al[t];
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t y0 = __shfl_up_sync(0xffffffffu, n0, o), y1 = __shfl_up_sync(0xffffffffu, n1, o);
+                    if (lane >= (uint32_t)o) {
+                        n0 += y0;
+                        n1 += y1;
                     }
                 }
+                const uint32_t half = __shfl_sync(0xffffffffu, n0, 31);
+                uint32_t* st = sm.start[ew];
+                st[lane + 1] = n0;
+                st[lane + 33] = n1 + half;
+                if (lane == 0) st[0] = 0;
+                const uint32_t total = __shfl_sync(0xffffffffu, n1, 31) + half;
                 __syncwarp();
+                float* table = &sm.alpha[i & 1][0][0];
+                for (uint32_t g0 = ew * 32 + lane; g0 < total; g0 += kCrowdEvalWarps * 32 * kCrowdBatch) {
+                    const Quad* qs[kCrowdBatch];
+                    int ipx[kCrowdBatch], ipy[kCrowdBatch];
+                    float ifx[kCrowdBatch], ify[kCrowdBatch];
+                    uint32_t cell[kCrowdBatch];
+                    bool live[kCrowdBatch];
+#pragma unroll
+                    for (int t = 0; t < (int)kCrowdBatch; ++t) {
+                        const uint32_t g = g0 + t * kCrowdEvalWarps * 32;
+                        live[t] = g < total;
+                        const uint32_t gg = live[t] ? g : g0;
+                        uint32_t e = 0;   // the splat of item gg: the last start <= gg
+#pragma unroll
+                        for (uint32_t step = 32; step; step >>= 1)
+                            e += st[e + step] <= gg ? step : 0u;
+                        const uint32_t bx = bt[e], local = gg - st[e];
+                        const uint32_t w = ((bx >> 8) & 15u) + 1u;
+                        const uint32_t dy = (local * (bx >> 12)) >> 16;
+                        const uint32_t cx = (bx & 15u) + local - dy * w, cy = ((bx >> 4) & 15u) + dy;
+                        ipx[t] = tx0 + (int)cx;
+                        ipy[t] = ty0 + (int)cy;
+                        ifx[t] = fadd((float)ipx[t], 0.5f);
+                        ify[t] = fadd((float)ipy[t], 0.5f);
+                        qs[t] = &sm.staged[b][e];
+                        cell[t] = e * (kTilePx * kTilePx) + cy * kTilePx + cx;
+                    }
+                    float al[kCrowdBatch];
+                    fragment_alphas_at<kCrowdBatch, true>(qs, ipx, ipy, ifx, ify, al);
+#pragma unroll
+                    for (int t = 0; t < (int)kCrowdBatch; ++t)
+                        if (live[t] && al[t] != 0.0f) table[cell[t]] = al[t];
+                }
             }
         }
-        if (role == 0 && inside) image[(size_t)py * width + px] = dst;
+        if (inside) image[(size_t)py * width + px] = dst;
     }
 }
 
