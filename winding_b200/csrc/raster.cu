@@ -492,29 +492,32 @@ __global__ void __launch_bounds__(256) blend_kernel(const Quad* __restrict__ qua
     if (inside) image[(size_t)py * width + px] = dst;
 }
 
-// Crowded tiles: the same blend, with the fragments evaluated by 24 warps
+// Crowded tiles: the same blend, with the fragments evaluated by 23 warps
 // and blended by 8. A tile whose list runs to thousands of splats keeps the
 // warps of blend_kernel evaluating 32 pixels for every splat that reaches
 // their two rows, most of them outside its box, while the SM has little else
-// to issue. Here, for each chunk of 64 splats, the evaluating warps take the
-// pixels of the splats' boxes (within the tile) as one flat list of items,
-// a lane an item, and write each nonzero alpha into a splat x pixel table in
-// shared memory; one chunk behind, each pixel's own thread walks its column
-// of the table in splat order, blends the nonzero entries and clears them.
-// The values and the order of every operation on a pixel are blend_kernel's,
-// so the image is the same to the bit. One CTA of 1024 threads an SM (its
-// registers and shared memory keep it alone there), looping over the
-// crowded tiles, longest first.
+// to issue. Here the tile's list goes by in chunks of 64 splats, a stage
+// each: one warp lists the boxes of chunk i + 1 (each splat's box within the
+// tile and where its pixels start in a flat list of items), the evaluating
+// warps take chunk i's items, a lane an item, and write each nonzero alpha
+// into a splat x pixel table in shared memory, and each pixel's own thread
+// walks its column of chunk i - 1's table in splat order, blends the nonzero
+// entries and clears them, while chunk i + 2 is copied in. The values and
+// the order of every operation on a pixel are blend_kernel's, so the image
+// is the same to the bit. One CTA of 1024 threads an SM (its registers keep
+// it alone there), looping over the crowded tiles, longest first.
 constexpr int kCrowdThreads = 1024;
-constexpr uint32_t kCrowdChunk = 64;                     // splats a step
+constexpr uint32_t kCrowdChunk = 64;                     // splats a stage
 constexpr uint32_t kCrowdBlenders = 256;                 // a thread a pixel: warps 0..7
-constexpr uint32_t kCrowdEvalWarps = (kCrowdThreads - kCrowdBlenders) / 32;
+constexpr uint32_t kCrowdLister = kCrowdBlenders / 32;   // warp 8 lists the boxes
+constexpr uint32_t kCrowdEvalWarps = kCrowdThreads / 32 - kCrowdLister - 1;   // warps 9..31
 constexpr uint32_t kCrowdBatch = 2;                      // items a lane evaluates at once
+constexpr uint32_t kCrowdRead = 8;                       // table entries a blending thread reads at once
 struct CrowdSmem {
-    Quad staged[3][kCrowdChunk];                         // chunk i in staged[i % 3]
+    Quad staged[4][kCrowdChunk];                         // chunk i in staged[i % 4]
     float alpha[2][kCrowdChunk][kTilePx * kTilePx];      // chunk i's alphas in alpha[i % 2]; 0 where none
-    uint32_t start[kCrowdEvalWarps][kCrowdChunk + 1];    // each evaluating warp's copy of the items' starts
-    uint32_t box[kCrowdEvalWarps][kCrowdChunk];          // and of the boxes (crowd_box)
+    uint32_t start[2][kCrowdChunk + 1];                  // chunk i's items: splat e's start in start[i % 2][e]
+    uint32_t box[2][kCrowdChunk];                        // and its box (crowd_box)
 };
 
 // A staged splat's box within its tile, packed for the item decode: first
@@ -537,8 +540,8 @@ __global__ void __launch_bounds__(kCrowdThreads, 1) crowd_kernel(const Quad* __r
     extern __shared__ __align__(16) unsigned char crowd_raw[];
     CrowdSmem& sm = *reinterpret_cast<CrowdSmem*>(crowd_raw);
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const bool blender = threadIdx.x < kCrowdBlenders;
-    const uint32_t ew = warp - kCrowdBlenders / 32;      // evaluating warp index (blenders: unused)
+    const bool blender = threadIdx.x < kCrowdBlenders, lister = warp == kCrowdLister;
+    const uint32_t ew = warp - kCrowdLister - 1;         // evaluating warp index (others: unused)
     {
         float4* z = reinterpret_cast<float4*>(&sm.alpha[0][0][0]);
         for (uint32_t k = threadIdx.x; k < sizeof(sm.alpha) / 16; k += kCrowdThreads) z[k] = make_float4(0, 0, 0, 0);
@@ -553,6 +556,7 @@ __global__ void __launch_bounds__(kCrowdThreads, 1) crowd_kernel(const Quad* __r
         if (inside) dst = image[(size_t)py * width + px];
         const uint2 rg = range[tile];
         const uint32_t chunks = (rg.y - rg.x + kCrowdChunk - 1) / kCrowdChunk;
+        auto chunk_len = [&](uint32_t c) { return min(kCrowdChunk, rg.y - rg.x - c * kCrowdChunk); };
         // Staging: threads 0..255 copy one 16-byte quarter of a quad each;
         // the splat index is read a chunk ahead, so its latency is hidden.
         auto index_of = [&](uint32_t c) -> uint32_t {
@@ -565,73 +569,83 @@ __global__ void __launch_bounds__(kCrowdThreads, 1) crowd_kernel(const Quad* __r
                            reinterpret_cast<const float4*>(&quads[idx]) + (threadIdx.x & 3));
             cp_async_commit();
         };
-        // A staged splat's box within the tile: first column and row, width,
-        // and its pixel count (0 past the chunk's end).
-        auto box_of = [&](const Quad& q, int& bx, int& by, int& bw) -> uint32_t {
-            bx = max(q.x0, tx0);
-            by = max(q.y0, ty0);
-            bw = min(q.x1, tx0 + kTilePx - 1) - bx + 1;
-            const int bh = min(q.y1, ty0 + kTilePx - 1) - by + 1;
-            return (uint32_t)(bw * bh);
+        // The lister's part: chunk c's boxes within the tile and their
+        // items' starts (an inclusive scan of the box sizes; lane l holds
+        // splats l and 32 + l).
+        auto list_boxes = [&](uint32_t c) {
+            const uint32_t m = chunk_len(c), b = c % 4;
+            uint32_t* st = sm.start[c & 1];
+            uint32_t* bt = sm.box[c & 1];
+            uint32_t n[2];
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                const uint32_t e = j * 32 + lane;
+                n[j] = 0;
+                if (e < m) {
+                    const Quad& q = sm.staged[b][e];
+                    const int bx = max(q.x0, tx0), by = max(q.y0, ty0);
+                    const int bw = min(q.x1, tx0 + kTilePx - 1) - bx + 1, bh = min(q.y1, ty0 + kTilePx - 1) - by + 1;
+                    n[j] = (uint32_t)(bw * bh);
+                    bt[e] = crowd_box(bx - tx0, by - ty0, bw);
+                }
+            }
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y0 = __shfl_up_sync(0xffffffffu, n[0], o), y1 = __shfl_up_sync(0xffffffffu, n[1], o);
+                if (lane >= (uint32_t)o) {
+                    n[0] += y0;
+                    n[1] += y1;
+                }
+            }
+            const uint32_t half = __shfl_sync(0xffffffffu, n[0], 31);
+            st[lane + 1] = n[0];
+            st[lane + 33] = n[1] + half;
+            if (lane == 0) st[0] = 0;
         };
         __syncthreads();   // the previous tile's last reads of the tables are done
         stage(index_of(0), 0);
-        uint32_t next = index_of(1);
+        stage(index_of(1), 1);
+        uint32_t next = index_of(2);
+        cp_async_wait_none();
+        __syncthreads();   // chunks 0 and 1 are staged
+        if (lister && chunks) list_boxes(0);
         for (uint32_t i = 0; i <= chunks; ++i) {
             cp_async_wait_none();
-            __syncthreads();   // chunk i is staged; chunk i - 2's quads and alphas are no longer read
-            if (i + 1 < chunks) {
-                stage(next, (i + 1) % 3);
-                next = index_of(i + 2);
+            __syncthreads();   // chunk i + 1 is staged and chunk i listed; chunk i - 2 is no longer read
+            if (i + 2 < chunks) {
+                stage(next, (i + 2) % 4);
+                next = index_of(i + 3);
             }
             if (blender) {
                 if (i == 0) continue;
-                const uint32_t c = i - 1, b = c % 3;
-                const uint32_t m = min(kCrowdChunk, rg.y - rg.x - c * kCrowdChunk);
+                const uint32_t c = i - 1, b = c % 4, m = chunk_len(c);
                 float* col = &sm.alpha[c & 1][0][threadIdx.x];
-#pragma unroll 4
-                for (uint32_t e = 0; e < m; ++e) {
-                    const float alpha = col[e * kTilePx * kTilePx];
-                    if (alpha == 0.0f) continue;
-                    col[e * kTilePx * kTilePx] = 0.0f;
-                    const Quad& q = sm.staged[b][e];
-                    const float om = fsub(1.0f, alpha);
-                    dst.x = fadd(fmul(q.r, alpha), fmul(dst.x, om));
-                    dst.y = fadd(fmul(q.g, alpha), fmul(dst.y, om));
-                    dst.z = fadd(fmul(q.b, alpha), fmul(dst.z, om));
-                    dst.w = fadd(alpha, fmul(dst.w, om));
-                }
-            } else if (i < chunks) {
-                const uint32_t b = i % 3;
-                const uint32_t m = min(kCrowdChunk, rg.y - rg.x - i * kCrowdChunk);
-                // The items' starts: an inclusive scan of the box sizes, this
-                // warp's copy (lane l holds splats l and 32 + l).
-                int bx, by, bw;
-                uint32_t* bt = sm.box[ew];
-                uint32_t n0 = 0, n1 = 0;
-                if (lane < m) {
-                    n0 = box_of(sm.staged[b][lane], bx, by, bw);
-                    bt[lane] = crowd_box(bx - tx0, by - ty0, bw);
-                }
-                if (lane + 32 < m) {
-                    n1 = box_of(sm.staged[b][lane + 32], bx, by, bw);
-                    bt[lane + 32] = crowd_box(bx - tx0, by - ty0, bw);
-                }
+                // Entries past the chunk's end are 0 (never written), so
+                // reading them in groups is harmless.
+                for (uint32_t e0 = 0; e0 < m; e0 += kCrowdRead) {
+                    float a[kCrowdRead];
 #pragma unroll
-                for (int o = 1; o < 32; o <<= 1) {
-                    const uint32_t y0 = __shfl_up_sync(0xffffffffu, n0, o), y1 = __shfl_up_sync(0xffffffffu, n1, o);
-                    if (lane >= (uint32_t)o) {
-                        n0 += y0;
-                        n1 += y1;
+                    for (uint32_t k = 0; k < kCrowdRead; ++k) a[k] = col[(e0 + k) * kTilePx * kTilePx];
+#pragma unroll
+                    for (uint32_t k = 0; k < kCrowdRead; ++k) {
+                        const float alpha = a[k];
+                        if (alpha == 0.0f) continue;
+                        col[(e0 + k) * kTilePx * kTilePx] = 0.0f;
+                        const Quad& q = sm.staged[b][e0 + k];
+                        const float om = fsub(1.0f, alpha);
+                        dst.x = fadd(fmul(q.r, alpha), fmul(dst.x, om));
+                        dst.y = fadd(fmul(q.g, alpha), fmul(dst.y, om));
+                        dst.z = fadd(fmul(q.b, alpha), fmul(dst.z, om));
+                        dst.w = fadd(alpha, fmul(dst.w, om));
                     }
                 }
-                const uint32_t half = __shfl_sync(0xffffffffu, n0, 31);
-                uint32_t* st = sm.start[ew];
-                st[lane + 1] = n0;
-                st[lane + 33] = n1 + half;
-                if (lane == 0) st[0] = 0;
-                const uint32_t total = __shfl_sync(0xffffffffu, n1, 31) + half;
-                __syncwarp();
+            } else if (lister) {
+                if (i + 1 < chunks) list_boxes(i + 1);
+            } else if (i < chunks) {
+                const uint32_t b = i % 4;
+                const uint32_t* st = sm.start[i & 1];
+                const uint32_t* bt = sm.box[i & 1];
+                const uint32_t total = st[kCrowdChunk];
                 float* table = &sm.alpha[i & 1][0][0];
                 for (uint32_t g0 = ew * 32 + lane; g0 < total; g0 += kCrowdEvalWarps * 32 * kCrowdBatch) {
                     const Quad* qs[kCrowdBatch];
@@ -644,9 +658,9 @@ __global__ void __launch_bounds__(kCrowdThreads, 1) crowd_kernel(const Quad* __r
                         const uint32_t g = g0 + t * kCrowdEvalWarps * 32;
                         live[t] = g < total;
                         const uint32_t gg = live[t] ? g : g0;
-                        uint32_t e = 0;   // the splat of item gg: the last start <= gg
+                        uint32_t e = 0;   // the splat of item gg: the last start <= gg (a splat with items)
 #pragma unroll
-                        for (uint32_t step = 32; step; step >>= 1)
+                        for (uint32_t step = kCrowdChunk / 2; step; step >>= 1)
                             e += st[e + step] <= gg ? step : 0u;
                         const uint32_t bx = bt[e], local = gg - st[e];
                         const uint32_t w = ((bx >> 8) & 15u) + 1u;
