@@ -406,9 +406,13 @@ def _run_wsort(args, rank, world, local_rank, torch):
                             "layout_frac": lay / kernel_s / 1e9 / peak}
         if world == 1:
             v, sample = cpu_baseline(jobs, args.cpu_seconds, os.cpu_count() or 1)
+            v1, sample1 = cpu_baseline(jobs, max(args.cpu_seconds / 3, 1.0), 1)
             line["cpu_baseline"] = {"value": v, "unit": "Msplats/s", "cores": os.cpu_count() or 1, "kind": "port",
                                     "sample": sample + "; C++ restatement of the reference's makeKeys + stable "
-                                                       "counting sort, all host threads"}
+                                                       "counting sort, all host threads",
+                                    "single_thread": {"value": v1, "unit": "Msplats/s", "cores": 1,
+                                                      "sample": sample1 + ", one thread (the reference's "
+                                                                          "JavaScript runs on one)"}}
         if not args.no_suite and world == 1:
             try:
                 line["suite"] = suite(ctx, torch, flush, args)

@@ -2,7 +2,10 @@
 
     python tests/golden/make_golden.py
 
-Each case is a small seeded cloud from winding_b200.workloads with one view;
+Each case is a small seeded cloud from winding_b200.workloads with one view,
+or a seeded subset of the reference's real capture (demo/cactus.splat, a
+3D Gaussian Splatting scan by Steam Studio released CC0, read from the
+reference checkout when it is present) with a framing or a posed view;
 the expected survivor order and keys come from the CPU oracle (oracle/), which
 is itself cross-checked against a second restatement (oracle/pyoracle.py) and
 the reference's known-answer tests in tests/test_oracle.py. Stored per case:
@@ -21,6 +24,28 @@ from oracle import oracle  # noqa: E402
 from winding_b200 import workloads as W  # noqa: E402
 
 CULLS = (0.0, 0.5)
+CACTUS = "/root/reference/demo/cactus.splat"
+CACTUS_SUBSET = 16384
+
+
+def cactus_cases():
+    """Two seeded subsets of the capture (records kept in file order): one
+    seen from +z at the fitted distance, one from a seeded direction."""
+    if not os.path.exists(CACTUS):
+        return
+    rec = np.fromfile(CACTUS, dtype=W.RECORD)
+    for name, seed, posed in (("cactus_front_16384", 21, False), ("cactus_posed_16384", 22, True)):
+        rng = np.random.default_rng(seed)
+        sub = rec[np.sort(rng.choice(len(rec), CACTUS_SUBSET, replace=False))]
+        view = W._framing_view(sub, 0.5)
+        if posed:
+            lo, hi = W._bounds(sub)
+            centre = (lo + hi) / 2
+            d = rng.normal(size=3)
+            d /= np.linalg.norm(d)
+            r = W.fit_distance(W.bounds_radius(lo, hi), W.FOV_Y, W.ASPECT, 1.0, W.NEAR) * rng.uniform(0.6, 1.2)
+            view = W.View(W.look_at(centre + d * r, centre), view.projection, view.viewport, view.cull)
+        yield name, W.Job(sub, view, "capture")
 
 
 def cases():
@@ -30,6 +55,7 @@ def cases():
     rng = np.random.default_rng(14)
     rec = W.scene("cluster", 2500, 15)
     yield "posed_2500", W.Job(rec, W.View(W.random_pose(rng), W.perspective(W.FOV_Y, W.ASPECT, W.NEAR)), "cluster")
+    yield from cactus_cases()
 
 
 def main():

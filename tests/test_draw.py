@@ -117,6 +117,38 @@ def test_crowded_tile_kernel_matches_oracle(ctx, crowd_min):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("crowd_min", [1, 1024])
+def test_draw_of_the_real_capture(ctx, crowd_min):
+    """16,384 splats of the reference's real capture (the cactus fixture),
+    sorted and drawn at 1920 x 1080, against the oracle's draw."""
+    import os
+    import torch
+    from winding_b200 import make_view, parse_splats
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "cactus_posed_16384.npz"))
+    w, h = (int(v) for v in g["viewport"])
+    sp = parse_splats(g["records"].tobytes(), ctx)
+    try:
+        ctx.set_draw_crowded(crowd_min)
+        view = make_view(g["model_view"], g["projection"], tuple(g["viewport"]), 0.5)
+        o = torch.empty(sp.count, dtype=torch.int32, device="cuda")
+        k = torch.empty_like(o)
+        c = torch.zeros(1, dtype=torch.int32, device="cuda")
+        ctx.sort_device(sp, view, o.data_ptr(), k.data_ptr(), c.data_ptr())
+        img = torch.zeros((h, w, 4), dtype=torch.float32, device="cuda")
+        ctx.draw(sp, view, o.data_ptr(), c.data_ptr(), img.data_ptr(), w, h)
+        ctx.sync()
+        order = o[: int(c.item())].cpu().numpy().view(np.uint32)
+        assert np.array_equal(order, g["order_0p5"])
+        want = O.draw(O.parse_splat(g["records"].tobytes()), order, g["model_view"], g["projection"], w, h)
+        got = img.cpu().numpy()
+        assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+        assert (got[..., 3] > 0).mean() > 0.01
+    finally:
+        ctx.set_draw_crowded(1024)
+        sp.destroy()
+
+
+@pytest.mark.gpu
 def test_bench_workload_draw_1m(ctx):
     """The bench's draw, whole: clusters-1M sorted and drawn at 1920 x 1080,
     bit for bit against the oracle's draw of the oracle's order."""

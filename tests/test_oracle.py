@@ -111,6 +111,22 @@ def test_oracle_matches_the_python_restatement(cull):
     assert list(o1) == o2 and list(k1) == k2
 
 
+@pytest.mark.parametrize("cull", [0.0, 0.5])
+def test_python_restatement_on_the_real_capture(cull):
+    """The two restatements agree on 1500 records of the real capture (the
+    cactus fixture: measured scales and rotations, not sampled ones)."""
+    g = np.load(os.path.join(GOLDEN, "cactus_posed_16384.npz"))
+    data = g["records"].tobytes()[: 1500 * 32]
+    parsed = O.parse_splat(data)
+    c2, cov2, lo, hi = P.decode(data)
+    assert np.array_equal(parsed.centers.view(np.uint32), c2.view(np.uint32))
+    assert np.array_equal(parsed.covariances.view(np.uint32), cov2.view(np.uint32))
+    mv, pr, vp = g["model_view"], g["projection"], tuple(g["viewport"])
+    o1, k1 = O.sort_view(parsed, mv, pr, vp, cull)
+    o2, k2 = P.sort_view(data, mv, pr, vp, cull)
+    assert len(o2) > 500 and list(o1) == o2 and list(k1) == k2
+
+
 def test_counting_sort_is_drawlist_order():
     rng = np.random.default_rng(3)
     keys = rng.integers(0, 400, size=20000).astype(np.uint32)
