@@ -812,6 +812,91 @@ float exp_pinned(float x) {
 
 }  // namespace
 
+// A property check of the library's draw: its prepare step cuts each
+// splat's pixel box to the pixels whose centre lies within the quad's
+// half-extents (hx, hy) plus a margin of 1/64 pixel and 2^-16 of the extent.
+// Over the splats of `order` this counts, out[0], the pixels in the pinned
+// box that the coverage test covers and the cut leaves out (it must be 0),
+// out[1] the covered pixels, out[2] the pinned box pixels and out[3] the cut
+// box pixels.
+extern "C" void or_draw_cut_check(const float* centers, const float* cov, const uint32_t* order, uint32_t count,
+                                  const float mv[16], const float P[16], uint32_t width, uint32_t height,
+                                  uint64_t out[4]) {
+    float srgb[256], reach_t[256];
+    or_draw_tables(srgb, reach_t);
+    or_cloud c;
+    std::memcpy(c.model_view, mv, sizeof(c.model_view));
+    std::memcpy(c.projection, P, sizeof(c.projection));
+    c.viewport[0] = (float)width;
+    c.viewport[1] = (float)height;
+    const float half_w = 0.5f * (float)width, half_h = 0.5f * (float)height;
+    for (int k = 0; k < 4; ++k) out[k] = 0;
+    for (uint32_t j = 0; j < count; ++j) {
+        const uint32_t i = order[j];
+        const float* p = centers + 4 * (size_t)i;
+        float view[4], clip[4];
+        for (int k = 0; k < 4; ++k)
+            view[k] = ((mv[k] * p[0] + mv[4 + k] * p[1]) + mv[8 + k] * p[2]) + mv[12 + k] * 1.0f;
+        for (int k = 0; k < 4; ++k)
+            clip[k] = ((P[k] * view[0] + P[4 + k] * view[1]) + P[8 + k] * view[2]) + P[12 + k] * view[3];
+        float f[3];
+        or_footprint(&c, cov, i, view, f);
+        const float a = f[0] + 0.3f, b = f[1], cc = f[2] + 0.3f;
+        const float mid = 0.5f * (a + cc), hd = 0.5f * (a - cc);
+        const float radius = std::sqrt(hd * hd + b * b);
+        const float major = mid + radius, minor = mid - radius;
+        uint32_t word;
+        std::memcpy(&word, &p[3], 4);
+        const float reach = reach_t[word >> 24];
+        if (!(minor > 0.0f) || !(reach > 0.0f)) continue;
+        float ax = 1.0f, ay = 0.0f;
+        if (std::fabs(b) > 1e-12f) {
+            const float ey = major - a;
+            const float len = std::sqrt(b * b + ey * ey);
+            ax = b / len;
+            ay = ey / len;
+        } else if (cc > a) {
+            ax = 0.0f;
+            ay = 1.0f;
+        }
+        const float la = std::fmin(std::sqrt(2.0f * major), 1024.0f);
+        const float lc = std::fmin(std::sqrt(2.0f * minor), 1024.0f);
+        const float ila = 1.0f / la, ilc = 1.0f / lc;
+        const float qm = std::sqrt(std::fmin(reach, 4.0f));
+        const float cx = (clip[0] / clip[3] + 1.0f) * half_w;
+        const float cy = (1.0f - clip[1] / clip[3]) * half_h;
+        const float hx = qm * (la * std::fabs(ax) + lc * std::fabs(ay));
+        const float hy = qm * (la * std::fabs(ay) + lc * std::fabs(ax));
+        if (!(std::isfinite(cx) && std::isfinite(cy) && std::isfinite(hx) && std::isfinite(hy))) continue;
+        const float fx0 = std::fmax(std::floor((cx - hx) - 1.5f), 0.0f);
+        const float fx1 = std::fmin(std::ceil((cx + hx) + 0.5f), (float)(width - 1));
+        const float fy0 = std::fmax(std::floor((cy - hy) - 1.5f), 0.0f);
+        const float fy1 = std::fmin(std::ceil((cy + hy) + 0.5f), (float)(height - 1));
+        if (!(fx0 <= fx1 && fy0 <= fy1)) continue;
+        // the cut, as the library's prepare step computes it
+        const float mx = (hx + 0.015625f) + hx * (1.0f / 65536.0f);
+        const float my = (hy + 0.015625f) + hy * (1.0f / 65536.0f);
+        const float gx0 = std::fmax(fx0, std::ceil((cx - mx) - 0.5f));
+        const float gx1 = std::fmin(fx1, std::floor((cx + mx) - 0.5f));
+        const float gy0 = std::fmax(fy0, std::ceil((cy - my) - 0.5f));
+        const float gy1 = std::fmin(fy1, std::floor((cy + my) - 0.5f));
+        const bool cut_empty = !(gx0 <= gx1 && gy0 <= gy1);
+        const int x0 = cut_empty ? 1 : (int)gx0, x1 = cut_empty ? 0 : (int)gx1;
+        const int y0 = cut_empty ? 1 : (int)gy0, y1 = cut_empty ? 0 : (int)gy1;
+        out[2] += (uint64_t)((int)fx1 - (int)fx0 + 1) * (uint64_t)((int)fy1 - (int)fy0 + 1);
+        if (!cut_empty) out[3] += (uint64_t)(x1 - x0 + 1) * (uint64_t)(y1 - y0 + 1);
+        for (int py = (int)fy0; py <= (int)fy1; ++py)
+            for (int px = (int)fx0; px <= (int)fx1; ++px) {
+                const float ex = ((float)px + 0.5f) - cx, ey = cy - ((float)py + 0.5f);
+                const float ox = (ex * ax + ey * ay) * ila;
+                const float oy = (ex * ay - ey * ax) * ilc;
+                if (!(std::fabs(ox) <= qm && std::fabs(oy) <= qm)) continue;
+                ++out[1];
+                if (px < x0 || px > x1 || py < y0 || py > y1) ++out[0];
+            }
+    }
+}
+
 extern "C" void or_draw(const float* centers, const float* cov, const uint32_t* order, uint32_t count,
                         const uint32_t* shaded, const float mv[16], const float P[16], uint32_t width,
                         uint32_t height, float* image) {

@@ -184,6 +184,11 @@ int or_decode_sog(uint32_t n, uint32_t degree, const uint8_t* low, const uint8_t
  * rules; this restates them.
  */
 void or_draw_tables(float srgb[256], float reach[256]);
+/* The draw's box cut against the coverage test (the library's raster.cu,
+ * prepare step): out = {covered pixels the cut leaves out, covered pixels,
+ * pinned box pixels, cut box pixels}. */
+void or_draw_cut_check(const float* centers, const float* cov, const uint32_t* order, uint32_t count,
+                       const float mv[16], const float P[16], uint32_t width, uint32_t height, uint64_t out[4]);
 void or_draw(const float* centers, const float* cov, const uint32_t* order, uint32_t count, const uint32_t* shaded,
              const float model_view[16], const float projection[16], uint32_t width, uint32_t height, float* image);
 

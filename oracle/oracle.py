@@ -91,6 +91,9 @@ def _declare(L):
     L.or_draw.restype = None
     L.or_draw.argtypes = [_f32p, _f32p, _u32p, ctypes.c_uint32, _u32p, _f32p, _f32p, ctypes.c_uint32,
                           ctypes.c_uint32, _f32p]
+    L.or_draw_cut_check.restype = None
+    L.or_draw_cut_check.argtypes = [_f32p, _f32p, _u32p, ctypes.c_uint32, _f32p, _f32p, ctypes.c_uint32,
+                                    ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint64)]
     L.or_shade.restype = ctypes.c_uint32
     L.or_shade.argtypes = [_f32p, _u32p, ctypes.c_int, ctypes.c_uint32, _f32p]
     L.or_particle_key.restype = ctypes.c_uint32
@@ -677,6 +680,20 @@ def draw_tables():
     reach = np.zeros(256, np.float32)
     lib().or_draw_tables(_ptr(srgb, _f32p), _ptr(reach, _f32p))
     return srgb, reach
+
+
+def draw_cut_check(parsed, order, model_view, projection, width: int, height: int):
+    """(covered pixels the draw's box cut would leave out, covered pixels,
+    pinned box pixels, cut box pixels) over the splats of order
+    (or_draw_cut_check)."""
+    out = np.zeros(4, np.uint64)
+    o = np.ascontiguousarray(order, np.uint32)
+    mv = np.ascontiguousarray(model_view, np.float32).reshape(16)
+    pr = np.ascontiguousarray(projection, np.float32).reshape(16)
+    lib().or_draw_cut_check(_ptr(parsed.centers, _f32p), _ptr(parsed.covariances, _f32p), _ptr(o, _u32p), o.size,
+                            _ptr(mv, _f32p), _ptr(pr, _f32p), width, height,
+                            out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)))
+    return tuple(int(v) for v in out)
 
 
 def draw(parsed, order, model_view, projection, width: int, height: int, background=None, shaded=None):

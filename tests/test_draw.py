@@ -47,6 +47,45 @@ def test_oracle_draws_one_splat_at_the_centre():
     assert not faint.any()                                                    # reach <= 0: not drawn
 
 
+def _cut_cases():
+    """Clouds for the box cut's check: seeded scale spreads from specks to
+    splats wider than the image, seen close up, at odd and large sizes."""
+    for seed in range(14):
+        if seed in (11, 13):   # the two slowest (billions of box pixels); the others cover their ranges
+            continue
+        rng = np.random.default_rng(100 + seed)
+        n = 3000
+        rec = W.records_from(rng.uniform(-10, 10, size=(n, 3)), rng)
+        rec["scale"] = np.exp(rng.normal([-5.0, -3.0, -1.5, -0.5][seed % 4], 1.5, size=(n, 3))).astype(np.float32)
+        w, h = [(64, 48), (333, 197), (1920, 1080), (4096, 2160)][(seed // 4) % 4]
+        d = rng.normal(size=3)
+        d /= np.linalg.norm(d)
+        mv = W.look_at(d * rng.uniform(6, 40), (0, 0, 0))
+        yield rec.tobytes(), mv, camera.perspective(W.FOV_Y, w / h, W.NEAR), w, h
+
+
+def test_box_cut_leaves_no_covered_pixel_out():
+    """The draw keeps, of each splat's pinned pixel box, the pixels within
+    the quad's half-extents (plus a margin); the oracle's coverage test,
+    pixel by pixel, finds no covered pixel outside that cut on the bench's
+    draw, the real capture and clouds of extreme scales and sizes."""
+    import os
+    cases = list(_cut_cases())
+    job = W.clusters_1m(seed=1)
+    cases.append((job.bytes(), job.view.model_view, job.view.projection, 1920, 1080))
+    for name in ("cactus_posed_16384", "cactus_front_16384"):
+        g = np.load(os.path.join(os.path.dirname(__file__), "golden", f"{name}.npz"))
+        cases.append((g["records"].tobytes(), g["model_view"], g["projection"], 1920, 1080))
+    covered = box = cut = 0
+    for data, mv, pr, w, h in cases:
+        parsed = O.parse_splat(data)
+        order, _ = O.sort_view(parsed, mv, pr, (float(w), float(h)), 0.0, threads=4)
+        missed, c, b, k = O.draw_cut_check(parsed, order, mv, pr, w, h)
+        assert missed == 0
+        covered, box, cut = covered + c, box + b, cut + k
+    assert covered > 10**7 and cut < box
+
+
 def _sorted(ctx, job, cull=0.5):
     import torch
     from winding_b200 import make_view, parse_splats

@@ -22,7 +22,16 @@
 //     space). That offset is the fragment's varying
 //     (it varies linearly over the quad, as the reference interpolates it).
 //     Pixels are only considered within the quad's bounding box widened by a
-//     pixel, the same box on both sides.
+//     pixel, the same box on both sides. The library keeps, of that box, the
+//     pixels whose centre lies within the quad's half-extents (hx, hy) of
+//     its centre, plus a margin of 1/64 pixel and 2^-16 of the extent: a
+//     covered pixel's offset has |ox|, |oy| <= qm, so its centre lies within
+//     qm (la |ax| + lc |ay|) = hx across and hy down, and the margin is far
+//     above the rounding of the coverage test (a few ulps of coordinates
+//     below 4096). The cut leaves out no covered pixel (the oracle counts
+//     them on the tests' clouds: none), so the image is the same, while the
+//     tiles, pairs and fragments it saves are many (a small splat's box is
+//     mostly its margins: at clusters-1M the cut keeps 26 % of the pixels).
 //   - the fragment: alpha = min(0.99, exp(-dot(offset, offset)) a), dropped
 //     below 1/255; colour = decodeSRGB(rgb bytes) from a table (the f32
 //     nearest ((c + 0.055) / 1.055)^2.4 above 0.04045, c / 12.92 below, c
@@ -150,10 +159,19 @@ __global__ void __launch_bounds__(256) prepare_kernel(const JobDesc* __restrict_
                 q.g = tables[(word >> 8) & 255u];
                 q.b = tables[(word >> 16) & 255u];
                 if (isfinite(q.cx) && isfinite(q.cy) && isfinite(hx) && isfinite(hy)) {
-                    const float fx0 = fmaxf(floorf(fsub(fsub(q.cx, hx), 1.5f)), 0.0f);
-                    const float fx1 = fminf(ceilf(fadd(fadd(q.cx, hx), 0.5f)), (float)(width - 1));
-                    const float fy0 = fmaxf(floorf(fsub(fsub(q.cy, hy), 1.5f)), 0.0f);
-                    const float fy1 = fminf(ceilf(fadd(fadd(q.cy, hy), 0.5f)), (float)(height - 1));
+                    // The pinned box, cut to the pixels whose centre lies
+                    // within (hx, hy) of the splat's centre plus a margin of
+                    // 1/64 pixel and 2^-16 of the extent (see the head).
+                    const float mx = fadd(fadd(hx, 0.015625f), fmul(hx, 1.0f / 65536.0f));
+                    const float my = fadd(fadd(hy, 0.015625f), fmul(hy, 1.0f / 65536.0f));
+                    const float fx0 = fmaxf(fmaxf(floorf(fsub(fsub(q.cx, hx), 1.5f)), 0.0f),
+                                            ceilf(fsub(fsub(q.cx, mx), 0.5f)));
+                    const float fx1 = fminf(fminf(ceilf(fadd(fadd(q.cx, hx), 0.5f)), (float)(width - 1)),
+                                            floorf(fsub(fadd(q.cx, mx), 0.5f)));
+                    const float fy0 = fmaxf(fmaxf(floorf(fsub(fsub(q.cy, hy), 1.5f)), 0.0f),
+                                            ceilf(fsub(fsub(q.cy, my), 0.5f)));
+                    const float fy1 = fminf(fminf(ceilf(fadd(fadd(q.cy, hy), 0.5f)), (float)(height - 1)),
+                                            floorf(fsub(fadd(q.cy, my), 0.5f)));
                     if (fx0 <= fx1 && fy0 <= fy1) {
                         q.x0 = (int)fx0;
                         q.x1 = (int)fx1;
