@@ -318,7 +318,7 @@ int ws_draw(ws_ctx* ctx, const ws_cloud* cloud, const ws_view* view, const uint3
 
 /* Which tiles ws_draw blends with four warps to each pair of pixel rows
  * instead of one: those whose splat list holds min_splats or more (a power
- * of two; 0: none; 1: every tile with a splat; default 1024). The image is
+ * of two; 0: none; 1: every tile with a splat; default 256). The image is
  * the same either way; only the time differs. */
 int ws_set_draw_crowded(ws_ctx* ctx, uint32_t min_splats);
 

@@ -151,12 +151,12 @@ def test_crowded_tile_kernel_matches_oracle(ctx, crowd_min):
         with pytest.raises(WsError, match="power of two"):
             ctx.set_draw_crowded(1000)
     finally:
-        ctx.set_draw_crowded(1024)
+        ctx.set_draw_crowded(256)
         sp.destroy()
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("crowd_min", [1, 1024])
+@pytest.mark.parametrize("crowd_min", [1, 256, 1024])
 def test_draw_of_the_real_capture(ctx, crowd_min):
     """16,384 splats of the reference's real capture (the cactus fixture),
     sorted and drawn at 1920 x 1080, against the oracle's draw."""
@@ -183,7 +183,7 @@ def test_draw_of_the_real_capture(ctx, crowd_min):
         assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
         assert (got[..., 3] > 0).mean() > 0.01
     finally:
-        ctx.set_draw_crowded(1024)
+        ctx.set_draw_crowded(256)
         sp.destroy()
 
 

@@ -75,7 +75,7 @@ struct ws_ctx {
     std::vector<struct ws_cloud*> freed;   // freed clouds, kept as refusable handles
     wsort::DevBuf thr_d;              // particle depth thresholds, uploaded on first use
     wsort::DevBuf draw_d, pairs_d;    // ws_draw: per-splat quads and scans; (tile, splat) pairs
-    uint32_t draw_crowd_min = 1024;   // ws_draw: lists this long or longer take the crowded-tile kernel
+    uint32_t draw_crowd_min = 256;    // ws_draw: lists this long or longer take the crowded-tile kernel
     // Capture loads: two chunks of a file on their way to the device (pinned
     // host, device), each free again once its event has passed.
     wsort::HostBuf load_h[2];
