@@ -520,9 +520,9 @@ __global__ void __launch_bounds__(256) blend_kernel(const Quad* __restrict__ qua
 // warps take chunk i's items, a lane an item, and write each nonzero alpha
 // into a splat x pixel table in shared memory, and each pixel's own thread
 // walks its column of chunk i - 1's table in splat order, blends the nonzero
-// entries and clears them, while chunk i + 2 is copied in. The values and
-// the order of every operation on a pixel are blend_kernel's, so the image
-// is the same to the bit. One CTA of 1024 threads an SM (its registers keep
+// entries and clears them, while chunks i + 2 and i + 3 are copied in. The
+// values and the order of every operation on a pixel are blend_kernel's, so
+// the image is the same to the bit. One CTA of 1024 threads an SM (its registers keep
 // it alone there), looping over the crowded tiles, longest first.
 constexpr int kCrowdThreads = 1024;
 constexpr uint32_t kCrowdChunk = 64;                     // splats a stage
@@ -532,7 +532,7 @@ constexpr uint32_t kCrowdEvalWarps = kCrowdThreads / 32 - kCrowdLister - 1;   //
 constexpr uint32_t kCrowdBatch = 2;                      // items a lane evaluates at once
 constexpr uint32_t kCrowdRead = 8;                       // table entries a blending thread reads at once
 struct CrowdSmem {
-    Quad staged[4][kCrowdChunk];                         // chunk i in staged[i % 4]
+    Quad staged[5][kCrowdChunk];                         // chunk i in staged[i % 5]
     float alpha[2][kCrowdChunk][kTilePx * kTilePx];      // chunk i's alphas in alpha[i % 2]; 0 where none
     uint32_t start[2][kCrowdChunk + 1];                  // chunk i's items: splat e's start in start[i % 2][e]
     uint32_t box[2][kCrowdChunk];                        // and its box (crowd_box)
@@ -591,7 +591,7 @@ __global__ void __launch_bounds__(kCrowdThreads, 1) crowd_kernel(const Quad* __r
         // items' starts (an inclusive scan of the box sizes; lane l holds
         // splats l and 32 + l).
         auto list_boxes = [&](uint32_t c) {
-            const uint32_t m = chunk_len(c), b = c % 4;
+            const uint32_t m = chunk_len(c), b = c % 5;
             uint32_t* st = sm.start[c & 1];
             uint32_t* bt = sm.box[c & 1];
             uint32_t n[2];
@@ -621,22 +621,24 @@ __global__ void __launch_bounds__(kCrowdThreads, 1) crowd_kernel(const Quad* __r
             if (lane == 0) st[0] = 0;
         };
         __syncthreads();   // the previous tile's last reads of the tables are done
+        // Every thread commits one copy group a stage (empty past the end),
+        // so waiting until one group is pending leaves the latest chunk's
+        // copy in flight: each chunk has two stages to arrive.
         stage(index_of(0), 0);
         stage(index_of(1), 1);
-        uint32_t next = index_of(2);
-        cp_async_wait_none();
+        stage(index_of(2), 2);
+        uint32_t next = index_of(3);
+        cp_async_wait_one();
         __syncthreads();   // chunks 0 and 1 are staged
         if (lister && chunks) list_boxes(0);
         for (uint32_t i = 0; i <= chunks; ++i) {
-            cp_async_wait_none();
+            cp_async_wait_one();
             __syncthreads();   // chunk i + 1 is staged and chunk i listed; chunk i - 2 is no longer read
-            if (i + 2 < chunks) {
-                stage(next, (i + 2) % 4);
-                next = index_of(i + 3);
-            }
+            stage(next, (i + 3) % 5);
+            next = index_of(i + 4);
             if (blender) {
                 if (i == 0) continue;
-                const uint32_t c = i - 1, b = c % 4, m = chunk_len(c);
+                const uint32_t c = i - 1, b = c % 5, m = chunk_len(c);
                 float* col = &sm.alpha[c & 1][0][threadIdx.x];
                 // Entries past the chunk's end are 0 (never written), so
                 // reading them in groups is harmless.
@@ -660,7 +662,7 @@ __global__ void __launch_bounds__(kCrowdThreads, 1) crowd_kernel(const Quad* __r
             } else if (lister) {
                 if (i + 1 < chunks) list_boxes(i + 1);
             } else if (i < chunks) {
-                const uint32_t b = i % 4;
+                const uint32_t b = i % 5;
                 const uint32_t* st = sm.start[i & 1];
                 const uint32_t* bt = sm.box[i & 1];
                 const uint32_t total = st[kCrowdChunk];
