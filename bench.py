@@ -76,8 +76,8 @@ def peak_hbm():
 
 def ncu_traffic(workload: str, cull: float):
     """DRAM bytes per launch of the sort kernel from the committed ncu summary
-    (profiles/traffic.txt: `<workload> <cull> <bytes>` lines), or None."""
-    path = os.path.join(ROOT, "profiles", "traffic.txt")
+    (profiles/sort_kernel_traffic.txt: `<workload> <cull> <bytes>` lines), or None."""
+    path = os.path.join(ROOT, "profiles", "sort_kernel_traffic.txt")
     try:
         for line in open(path):
             parts = line.split()
