@@ -58,8 +58,10 @@ def parse_args():
     ap.add_argument("--cull", type=float, default=0.5)
     ap.add_argument("--no-suite", action="store_true", help="skip the slab-6M / mixed-64 side measurements")
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU baseline sample length")
-    ap.add_argument("--tile", type=int, default=0, help="fixed tile size (skips the autotuner; with --ctas)")
-    ap.add_argument("--ctas", type=int, default=0, help="fixed resident CTAs per SM (with --tile)")
+    ap.add_argument("--tile", type=int, default=0,
+                    help="fixed least splats a segment covers (skips the autotuner; with --ctas)")
+    ap.add_argument("--ctas", type=int, default=0, help="fixed kernel variant: 1 or 2 CTAs per SM (with --tile)")
+    ap.add_argument("--segs", type=int, default=1, help="fixed segments per resident CTA (with --tile)")
     ap.add_argument("--only", default="", choices=["", "particles-64", "shade-1M", "decode", "draw-1M"],
                     help="run one side measurement alone and print its result (no bench line)")
     return ap.parse_args()
@@ -312,10 +314,10 @@ def _run_wsort(args, rank, world, local_rank, torch):
     from winding_b200 import autotune
     fixed = bool(args.tile and args.ctas)
     if fixed:
-        ctx.set_params(tile=args.tile, ctas_per_sm=args.ctas)
+        ctx.set_params(tile=args.tile, ctas_per_sm=args.ctas, segs_per_cta=args.segs)
     plain = plain_measure(ctx, torch, jobs, 0, args.warmup, flush)   # load + warm
     if fixed:
-        tuned = {autotune.bucket(plain["splats"]): (args.tile, args.ctas)}
+        tuned = {autotune.bucket(plain["splats"]): (args.tile, args.ctas, args.segs)}
     else:
         tuned = autotune.tune(ctx, [list(zip(plain["clouds"], plain["views"]))])
     if dist:
@@ -380,7 +382,8 @@ def _run_wsort(args, rank, world, local_rank, torch):
                    "cull": args.cull, "viewport": [1920, 1080], "l2": "flushed (256 MiB write) before each step",
                    "parallelism": (f"jobs sharded over {world} ranks" if sharded else f"replicas x{world}")
                    if world > 1 else "single GPU",
-                   "tuned": {str(b): {"tile": t, "ctas_per_sm": c} for b, (t, c) in tuned.items()}},
+                   "tuned": {str(b): {"tile": t, "ctas_per_sm": c, "segs_per_cta": g}
+                             for b, (t, c, g) in tuned.items()}},
         "e2e": {"value": e2e_value, "unit": "Msplats/s", "h2d_bytes_per_step": view_bytes, "d2h_bytes_per_step": d2h,
                 "call": "ws_sort(WS_HOST_OUTPUT) into a pinned host buffer: the order and the survivor count, "
                         "the reference's outputs (its keys stay unsorted on the device and are never read back)"},
@@ -399,7 +402,7 @@ def _run_wsort(args, rank, world, local_rank, torch):
         p = ctx.params
         line["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                             "frac": achieved / peak, "traffic": traffic, "peak_source": src,
-                            "kernel": f"wsort::sort_kernel (tile {p.tile}, {p.ctas_per_sm} CTAs/SM)",
+                            "kernel": "wsort::sort_kernel",
                             "kernel_us_per_step": kernel_s * 1e6, "algorithmic_bytes_per_step": algo,
                             "algorithmic_bytes": "32 N + 8 S",
                             "layout_bytes_per_step": lay,

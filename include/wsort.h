@@ -435,17 +435,18 @@ int ws_selftest_wait(ws_ctx* ctx, uint32_t spin_limit);
 /* ------------------------------------------------------------ tuning */
 
 /*
- * Kernel parameters. tile: splats one work item of the key and digit passes
- * covers (1024, 2048 or 4096). ctas_per_sm: the kernel variant's resident
- * CTAs per SM (2, 3 or 4, or 6 with tile 1024; 0 picks 3), which bounds its
- * registers per thread. spin_limit: polls a device-side wait makes before it gives up
- * with WS_ERR_TIMEOUT.
+ * Kernel parameters. The launch's jobs, laid end to end, are cut into about
+ * segs_per_cta segments per resident CTA (0: 1), each of at least `tile`
+ * splats (a multiple of 256); a segment is one work item of each phase.
+ * ctas_per_sm: 1 (0 too) runs CTAs of 1024 threads, one an SM; 2 runs CTAs
+ * of 512 threads, two an SM. spin_limit: polls a device-side wait makes
+ * before it gives up with WS_ERR_TIMEOUT.
  */
 typedef struct ws_params {
     uint32_t tile;
     uint32_t ctas_per_sm;
     uint32_t spin_limit;
-    uint32_t reserved;
+    uint32_t segs_per_cta;
 } ws_params;
 
 int ws_get_params(const ws_ctx* ctx, ws_params* out);
@@ -477,13 +478,13 @@ int ws_timing_read(ws_ctx* ctx, double* kernel_ms, uint64_t* launches);
  * claimed, when its dependency wait ended and when it finished, and the SM
  * it ran on. ws_trace_read waits for the last launch and copies up to `cap`
  * records of it; *n receives how many it has. phase: 0 keys, 1 low-digit
- * scan, 2 low-digit scatter, 3 high-digit counts, 4 high-digit scan,
- * 5 high-digit scatter.
+ * pass, 2 high-digit pass; segment: the launch's segment the item covered.
  */
 typedef struct ws_trace_rec {
     uint64_t claim_ns, start_ns, end_ns;
-    uint32_t job, phase, tile, sm;
-    uint64_t mark_ns[3];   /* digit passes: inputs staged, ranked, staged for writing (0: none) */
+    uint32_t job, phase, segment, sm;
+    uint64_t mark_ns[3];   /* keys: -, first sub-tile swept, last; digit passes: prefix known, first
+                              sub-tile staged, last (0: none) */
 } ws_trace_rec;
 
 int ws_trace(ws_ctx* ctx, int enable);

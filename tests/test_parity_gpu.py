@@ -227,24 +227,26 @@ def test_bench_workload_mixed_64_batched(ctx):
             sp.destroy()
 
 
-@pytest.mark.parametrize("tile,ctas", [(1024, 2), (1024, 3), (1024, 4), (1024, 6), (2048, 2), (2048, 3), (2048, 4),
-                                       (4096, 2), (4096, 3), (4096, 4)])
-def test_kernel_variants_do_not_change_the_result(ctx, tile, ctas):
+# (least splats a segment covers, CTAs per SM, segments per CTA): one segment
+# per job up to hundreds in many look-back groups, both kernel variants.
+@pytest.mark.parametrize("tile,ctas,segs", [(2048, 1, 1), (2048, 2, 1), (8192, 1, 2), (1 << 20, 1, 1), (256, 1, 4),
+                                            (256, 2, 4), (512, 2, 16), (1024, 1, 64)])
+def test_kernel_variants_do_not_change_the_result(ctx, tile, ctas, segs):
     old = ctx.params
     try:
-        ctx.set_params(tile=tile, ctas_per_sm=ctas)
+        ctx.set_params(tile=tile, ctas_per_sm=ctas, segs_per_cta=segs)
         check_job(ctx, W.clusters_1m(seed=41, n=120_001))
     finally:
-        ctx.set_params(tile=old.tile, ctas_per_sm=old.ctas_per_sm)
+        ctx.set_params(tile=old.tile, ctas_per_sm=old.ctas_per_sm, segs_per_cta=old.segs_per_cta)
 
 
 def test_missing_kernel_variant_is_refused(ctx):
     old = ctx.params
-    for tile, ctas in [(2048, 6), (4096, 6), (1024, 5), (1024, 1), (3000, 3)]:
-        with pytest.raises(WsError, match="tile|ctas_per_sm"):
-            ctx.set_params(tile=tile, ctas_per_sm=ctas)
+    for tile, ctas, segs in [(777, 1, 1), (0, 1, 1), (128, 1, 1), (2048, 3, 1), (2048, 4, 1), (2048, 1, 65)]:
+        with pytest.raises(WsError, match="tile|ctas_per_sm|segs_per_cta"):
+            ctx.set_params(tile=tile, ctas_per_sm=ctas, segs_per_cta=segs)
     p = ctx.params
-    assert (p.tile, p.ctas_per_sm) == (old.tile, old.ctas_per_sm)
+    assert (p.tile, p.ctas_per_sm, p.segs_per_cta) == (old.tile, old.ctas_per_sm, old.segs_per_cta)
 
 
 def test_full_size_slab_properties(ctx):

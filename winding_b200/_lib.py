@@ -90,7 +90,7 @@ class WsParams(ctypes.Structure):
         ("tile", ctypes.c_uint32),
         ("ctas_per_sm", ctypes.c_uint32),
         ("spin_limit", ctypes.c_uint32),
-        ("reserved", ctypes.c_uint32),
+        ("segs_per_cta", ctypes.c_uint32),
     ]
 
 
@@ -141,7 +141,7 @@ class WsTraceRec(ctypes.Structure):
         ("end_ns", ctypes.c_uint64),
         ("job", ctypes.c_uint32),
         ("phase", ctypes.c_uint32),
-        ("tile", ctypes.c_uint32),
+        ("segment", ctypes.c_uint32),
         ("sm", ctypes.c_uint32),
         ("mark_ns", ctypes.c_uint64 * 3),
     ]

@@ -1,14 +1,16 @@
-"""The sort's autotuner: tile size and kernel variant per launch size.
+"""The sort's autotuner: kernel variant and segment sizing per launch size.
 
-For a workload (or synthetic clouds of given sizes), every candidate
-(tile 1024 / 2048 / 4096 x 2 / 3 / 4 resident CTAs per SM, and tile 1024 x 6)
-is timed with the
-library's own CUDA-event kernel timing (ws_timing) over a few launches, and
-the fastest is installed in the context's tuning table for that launch size
-(floor(log2(total splats)), ws_set_tuning). Results persist in a JSON cache
-keyed by the GPU's name, so later processes load them instead of measuring.
+A candidate is (tile, ctas_per_sm, segs_per_cta): the least splats a segment
+covers, the kernel variant (1: CTAs of 1024 threads, one an SM; 2: CTAs of
+512 threads, two an SM) and the segments cut per resident CTA. For a
+workload (or synthetic clouds of given sizes) every candidate is timed with
+the library's own CUDA-event kernel timing (ws_timing) over a few launches,
+and the fastest is installed in the context's tuning table for that launch
+size (floor(log2(total splats)), ws_set_tuning). Results persist in a JSON
+cache keyed by the GPU's name, so later processes load them instead of
+measuring.
 
-    table = autotune.tune(ctx, [(splats, view)], cache="~/.cache/wsort_tuning.json")
+    table = autotune.tune(ctx, [[(splats, view)]], cache="~/.cache/wsort_tuning.json")
 """
 from __future__ import annotations
 
@@ -17,9 +19,10 @@ import os
 
 from . import _lib
 
-TILES = (1024, 2048, 4096)
-CTAS = (2, 3, 4)
-CANDIDATES = tuple((t, c) for t in TILES for c in CTAS) + ((1024, 6),)
+TILES = (1024, 2048, 8192)
+CTAS = (1, 2)
+SEGS = (1, 2, 4)
+CANDIDATES = tuple((t, c, s) for t in TILES for c in CTAS for s in SEGS)
 
 
 def bucket(splats: int) -> int:
@@ -58,34 +61,41 @@ def _time_jobs(ctx, jobs, reps: int) -> float:
     return ms / max(n, 1)
 
 
-def measure(ctx, jobs, reps: int = 5) -> list[tuple[float, int, int]]:
-    """(ms, tile, ctas) for every candidate on one batch of jobs."""
+def measure(ctx, jobs, reps: int = 5, candidates=CANDIDATES) -> list[tuple[float, tuple[int, int, int]]]:
+    """(ms, candidate) for every candidate on one batch of jobs, fastest first."""
     saved = ctx.params
     table_off = (_lib.WsParams * 1)()
     ctx.check(ctx.lib.ws_set_tuning(ctx.handle, table_off, 0))
     out = []
     try:
-        for tile, ctas in CANDIDATES:
-            ctx.set_params(tile=tile, ctas_per_sm=ctas)
-            out.append((_time_jobs(ctx, jobs, reps), tile, ctas))
+        for cand in candidates:
+            tile, ctas, segs = cand
+            ctx.set_params(tile=tile, ctas_per_sm=ctas, segs_per_cta=segs)
+            out.append((_time_jobs(ctx, jobs, reps), tuple(cand)))
     finally:
-        ctx.set_params(tile=saved.tile, ctas_per_sm=saved.ctas_per_sm)
+        ctx.set_params(tile=saved.tile, ctas_per_sm=saved.ctas_per_sm, segs_per_cta=saved.segs_per_cta)
     return sorted(out)
 
 
-def install(ctx, table: dict[int, tuple[int, int]]) -> None:
-    """Installs {bucket: (tile, ctas)} as the context's tuning table."""
+def install(ctx, table: dict[int, tuple[int, int, int]]) -> None:
+    """Installs {bucket: (tile, ctas, segs)} as the context's tuning table."""
     n = max(table) + 1 if table else 0
     arr = (_lib.WsParams * max(n, 1))()
     spin = ctx.params.spin_limit
-    for b, (tile, ctas) in table.items():
+    for b, (tile, ctas, segs) in table.items():
         arr[b].tile = tile
         arr[b].ctas_per_sm = ctas
+        arr[b].segs_per_cta = segs
         arr[b].spin_limit = spin
     ctx.check(ctx.lib.ws_set_tuning(ctx.handle, arr, n))
 
 
-def tune(ctx, workloads, cache: str | None = None, reps: int = 5, force: bool = False) -> dict[int, tuple[int, int]]:
+def _valid(v) -> bool:
+    return isinstance(v, (list, tuple)) and len(v) == 3 and tuple(v[:1]) != (0,)
+
+
+def tune(ctx, workloads, cache: str | None = None, reps: int = 5, force: bool = False,
+         candidates=CANDIDATES) -> dict[int, tuple[int, int, int]]:
     """workloads: batches, each a list of (splats, view). Measures each (unless
     its size bucket is in the cache), installs the table and returns it."""
     key = gpu_name(ctx.device)
@@ -96,13 +106,12 @@ def tune(ctx, workloads, cache: str | None = None, reps: int = 5, force: bool = 
                 stored = json.load(f)
         except (OSError, ValueError):
             stored = {}
-    table = {int(b): tuple(v) for b, v in stored.get(key, {}).items()}
+    table = {int(b): tuple(v) for b, v in stored.get(key, {}).items() if _valid(v)}
     for jobs in workloads:
         b = bucket(sum(sp.count for sp, _ in jobs))
         if b in table and not force:
             continue
-        ms, tile, ctas = measure(ctx, jobs, reps)[0]
-        table[b] = (tile, ctas)
+        table[b] = measure(ctx, jobs, reps, candidates)[0][1]
     install(ctx, table)
     if cache:
         stored[key] = {str(b): list(v) for b, v in sorted(table.items())}
@@ -113,14 +122,14 @@ def tune(ctx, workloads, cache: str | None = None, reps: int = 5, force: bool = 
     return table
 
 
-def load(ctx, cache: str) -> dict[int, tuple[int, int]]:
+def load(ctx, cache: str) -> dict[int, tuple[int, int, int]]:
     """Installs a cached table for this GPU, if there is one."""
     path = os.path.expanduser(cache)
     if not os.path.exists(path):
         return {}
     with open(path) as f:
         stored = json.load(f)
-    table = {int(b): tuple(v) for b, v in stored.get(gpu_name(ctx.device), {}).items()}
+    table = {int(b): tuple(v) for b, v in stored.get(gpu_name(ctx.device), {}).items() if _valid(v)}
     if table:
         install(ctx, table)
     return table

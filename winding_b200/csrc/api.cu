@@ -16,10 +16,6 @@
 #include <vector>
 
 namespace wsort {
-cudaError_t launch_sort(const JobDesc* jobs, const uint2* items, uint32_t n_items, LaunchCtl* lctl, uint32_t* err,
-                        uint32_t tile, int minb, uint32_t spin_limit, int grid, cudaStream_t stream,
-                        TraceRec* trace);
-int sort_occupancy(uint32_t tile, int minb);
 cudaError_t launch_decode(const void* records, uint32_t n, float4* centers, float2* cov, int8_t* sexp,
                           uint32_t* bounds, uint32_t* bad, int sms, cudaStream_t stream);
 
@@ -92,29 +88,131 @@ static size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 uint32_t pad_splats(uint32_t n) { return (uint32_t)align_up(n ? n : 1, kPadSplats); }
 
-// Tile count and scratch footprint of one job.
-void job_shape(uint32_t n, const ws_params& p, uint32_t* tiles, size_t* bytes) {
-    const uint32_t n1 = n ? n : 1;
-    *tiles = (n1 + p.tile - 1) / p.tile;
-    const size_t np = pad_splats(n);
-    size_t b = 0;
-    b += align_up(np * 2, 256);                        // k16
-    b += align_up(np / 8, 256);                        // mask
-    b += align_up(np * 2, 256);                        // key_b
-    b += align_up(np * 4, 256);                        // idx_b
-    b += 2 * align_up((size_t)*tiles * 1024, 256);     // cnt_lo, cnt_hi
-    *bytes = b;
+static uint32_t npad_of(uint32_t n) { return (uint32_t)align_up(n, kSegAlign); }
+
+// Threads per CTA of the kernel variant p selects: 1024 (one CTA an SM) or
+// 512 (two).
+static int threads_of(const ws_params& p) { return p.ctas_per_sm == 2 ? 512 : 1024; }
+
+// The segments: the jobs laid end to end (each padded to kSegAlign) are cut
+// into chunks of `chunk` splats, about segs_per_cta per resident CTA and no
+// smaller than p.tile; a segment is one job's part of one chunk. Then the
+// scratch: the launch counters and every job's control region (zeroed
+// before a launch), then per job its key, survivor-bit, intermediate and
+// count arrays.
+void shape_launch(const uint32_t* ns, int njobs, const ws_params& p, int sms, LaunchShape& S) {
+    S.threads = threads_of(p);
+    const int want = S.threads == 512 ? 2 : 1;
+    const int occ = sort_occupancy(S.threads);
+    S.grid = sms * std::max(1, std::min(want, occ));
+    uint64_t total = 0;
+    for (int j = 0; j < njobs; ++j) total += npad_of(ns[j]);
+    const uint64_t target = (uint64_t)S.grid * std::max(1u, p.segs_per_cta);
+    uint64_t chunk = (total + target - 1) / std::max<uint64_t>(target, 1);
+    chunk = std::max<uint64_t>(chunk, p.tile ? p.tile : 2048);
+    chunk = align_up(chunk, kSegAlign);
+    S.chunk = (uint32_t)std::min<uint64_t>(chunk, 0x80000000ull);
+    S.regular = njobs == 1;
+    S.segs.clear();
+    S.nseg.assign(njobs, 0);
+    S.seg0.assign(njobs, 0);
+    uint64_t v = 0;   // position in the laid-end-to-end splats
+    for (int j = 0; j < njobs; ++j) {
+        const uint32_t np = npad_of(ns[j]);
+        S.seg0[j] = (uint32_t)S.segs.size();
+        uint32_t at = 0, local = 0;
+        do {
+            const uint64_t boundary = (v / S.chunk + 1) * S.chunk;
+            const uint32_t end = (uint32_t)std::min<uint64_t>(np, at + (boundary - v));
+            S.segs.push_back(SegDesc{(uint32_t)j, at, end, local++});
+            v += end - at;
+            at = end;
+        } while (at < np);
+        S.nseg[j] = local;
+    }
+    if (S.regular) {
+        // The kernel's own cut of a lone job: consecutive chunks from 0.
+        const uint32_t np = npad_of(ns[0]);
+        const uint32_t k = np ? (np + S.chunk - 1) / S.chunk : 1;
+        S.segs.clear();
+        for (uint32_t q = 0; q < k; ++q)
+            S.segs.push_back(SegDesc{0u, std::min(q * S.chunk, np), std::min(q * S.chunk + S.chunk, np), q});
+        S.nseg[0] = k;
+    }
+    size_t off = 256;   // LaunchCtl
+    S.ctl_off.resize(njobs);
+    for (int j = 0; j < njobs; ++j) {
+        S.ctl_off[j] = off;
+        off += job_ctl_bytes(S.nseg[j]);
+    }
+    S.ctl_bytes = off;
+    S.arr_off.resize(njobs);
+    for (int j = 0; j < njobs; ++j) {
+        S.arr_off[j] = off;
+        const size_t np = std::max<size_t>(npad_of(ns[j]), kSegAlign);
+        off += align_up(np * 2, 256);                       // k16
+        off += align_up(np / 8, 256);                       // survivor bits
+        off += align_up(np * 2, 256);                       // key_b
+        off += align_up(np * 4, 256);                       // idx_b
+        off += align_up((size_t)S.nseg[j] * 2 * 1024, 256); // per-segment counts, both digits
+    }
+    S.bytes = off;
 }
 
-size_t launch_scratch_bytes(const uint32_t* ns, int njobs, const ws_params& p) {
-    size_t total = align_up(sizeof(LaunchCtl) + (size_t)njobs * sizeof(JobCtl), 256);
-    for (int j = 0; j < njobs; ++j) {
-        uint32_t tiles;
-        size_t b;
-        job_shape(ns[j], p, &tiles, &b);
-        total += b;
-    }
-    return total;
+void place_job(JobDesc& d, uint32_t n, int j, const LaunchShape& S, char* scratch) {
+    d.n = n;
+    d.npad = npad_of(n);
+    d.seg0 = S.seg0[j];
+    d.nseg = S.nseg[j];
+    d.ngroups = (d.nseg + kGroup - 1) / kGroup;
+    d.ctl = reinterpret_cast<uint32_t*>(scratch + S.ctl_off[j]);
+    char* at = scratch + S.arr_off[j];
+    const size_t np = std::max<size_t>(d.npad, kSegAlign);
+    d.k16 = reinterpret_cast<uint16_t*>(at);
+    at += align_up(np * 2, 256);
+    d.mask = reinterpret_cast<uint32_t*>(at);
+    at += align_up(np / 8, 256);
+    d.key_b = reinterpret_cast<uint16_t*>(at);
+    at += align_up(np * 2, 256);
+    d.idx_b = reinterpret_cast<uint32_t*>(at);
+    at += align_up(np * 4, 256);
+    d.agg = reinterpret_cast<uint32_t*>(at);
+}
+
+size_t table_bytes(int njobs, const LaunchShape& S) {
+    return (size_t)njobs * sizeof(JobDesc) + (S.regular ? 0 : S.segs.size() * sizeof(SegDesc));
+}
+
+void write_table(void* dst, const JobDesc* jobs, int njobs, const LaunchShape& S) {
+    char* p = static_cast<char*>(dst);
+    if (p != reinterpret_cast<const char*>(jobs)) std::memcpy(p, jobs, (size_t)njobs * sizeof(JobDesc));
+    if (!S.regular)
+        std::memcpy(p + (size_t)njobs * sizeof(JobDesc), S.segs.data(), S.segs.size() * sizeof(SegDesc));
+}
+
+LaunchDesc launch_desc(const void* d_table, int njobs, const LaunchShape& S, char* scratch, uint32_t* err,
+                       uint32_t spin_limit, TraceRec* trace) {
+    LaunchDesc L;
+    std::memset(&L, 0, sizeof(L));
+    L.jobs = static_cast<const JobDesc*>(d_table);
+    L.segs = S.regular ? nullptr
+                       : reinterpret_cast<const SegDesc*>(static_cast<const char*>(d_table) +
+                                                          (size_t)njobs * sizeof(JobDesc));
+    L.nseg = (uint32_t)S.segs.size();
+    L.chunk = S.chunk;
+    L.first_phase = 0;
+    L.spin_limit = spin_limit;
+    L.lctl = reinterpret_cast<LaunchCtl*>(scratch);
+    L.err = err;
+    L.trace = trace;
+    return L;
+}
+
+// Scratch bytes of a launch of njobs jobs of ns[j] elements.
+size_t launch_scratch_bytes(const uint32_t* ns, int njobs, const ws_params& p, int sms) {
+    LaunchShape S;
+    shape_launch(ns, njobs, p, sms, S);
+    return S.bytes;
 }
 
 // The per-view shortcuts the keys phase may take, proved here on the host:
@@ -175,41 +273,13 @@ void view_shortcuts(const ws_view& v, const ws_cloud* c, uint32_t* fast, uint32_
     *keep_q = qf;
 }
 
-// Fills job descriptors and lays the scratch out from `scratch`.
-// A job's tiles, scan items and scratch regions (job_shape's layout), from
-// `at` on; advances `at` past them.
-// `alone`: the job is its launch's only one (see kRedHiTiles).
-static void assign_scratch(JobDesc& d, uint32_t n, const ws_params& p, char*& at, bool alone) {
-    size_t bytes;
-    job_shape(n, p, &d.tiles, &bytes);
-    d.scan_items = d.tiles <= kSmallScanTiles ? kSmallScanItems : kScanItems;
-    d.red_hi = alone && d.tiles <= kRedHiTiles ? 1u : 0u;
-    d.hi_items = d.red_hi ? d.tiles : (d.tiles + kCountSpan - 1) / kCountSpan;
-    const size_t np = pad_splats(n);
-    d.k16 = reinterpret_cast<uint16_t*>(at);
-    at += align_up(np * 2, 256);
-    d.mask = reinterpret_cast<uint32_t*>(at);
-    at += align_up(np / 8, 256);
-    d.key_b = reinterpret_cast<uint16_t*>(at);
-    at += align_up(np * 2, 256);
-    d.idx_b = reinterpret_cast<uint32_t*>(at);
-    at += align_up(np * 4, 256);
-    d.cnt_lo = reinterpret_cast<uint32_t*>(at);
-    at += align_up((size_t)d.tiles * 1024, 256);
-    d.cnt_hi = reinterpret_cast<uint32_t*>(at);
-    at += align_up((size_t)d.tiles * 1024, 256);
-}
-
 // Emitter jobs (ws_sort_particles): the ring, the view and the outputs.
-static void layout_emitters(JobDesc* out, const ws_emitter* em, int njobs, const ws_params& p, char* scratch,
+static void layout_emitters(JobDesc* out, const ws_emitter* em, int njobs, const LaunchShape& S, char* scratch,
                             const float* thr) {
-    char* at = scratch + align_up(sizeof(LaunchCtl) + (size_t)njobs * sizeof(JobCtl), 256);
-    JobCtl* ctls = reinterpret_cast<JobCtl*>(scratch + sizeof(LaunchCtl));
     for (int j = 0; j < njobs; ++j) {
         JobDesc& d = out[j];
         std::memset(&d, 0, sizeof(d));
         d.kind = kJobParticles;
-        d.n = em[j].capacity;
         d.idx_base = em[j].offset;
         d.pool = static_cast<const float4*>(em[j].pool);
         d.thr = thr;
@@ -220,14 +290,11 @@ static void layout_emitters(JobDesc* out, const ws_emitter* em, int njobs, const
         d.order = em[j].order;
         d.keys = em[j].keys;
         d.count = em[j].count;
-        assign_scratch(d, em[j].capacity, p, at, njobs == 1);
-        d.ctl = reinterpret_cast<uint32_t*>(&ctls[j]);
+        place_job(d, em[j].capacity, j, S, scratch);
     }
 }
 
-void layout_jobs(JobDesc* out, const ws_job* jobs, int njobs, const ws_params& p, char* scratch) {
-    char* at = scratch + align_up(sizeof(LaunchCtl) + (size_t)njobs * sizeof(JobCtl), 256);
-    JobCtl* ctls = reinterpret_cast<JobCtl*>(scratch + sizeof(LaunchCtl));
+void layout_jobs(JobDesc* out, const ws_job* jobs, int njobs, const LaunchShape& S, char* scratch) {
     for (int j = 0; j < njobs; ++j) {
         const ws_cloud* c = jobs[j].cloud;
         JobDesc& d = out[j];
@@ -239,7 +306,6 @@ void layout_jobs(JobDesc* out, const ws_job* jobs, int njobs, const ws_params& p
             d.bmin[k] = c->bmin[k];
             d.bmax[k] = c->bmax[k];
         }
-        d.n = c->n;
         std::memcpy(d.mv, jobs[j].view.model_view, sizeof(d.mv));
         std::memcpy(d.proj, jobs[j].view.projection, sizeof(d.proj));
         d.viewport[0] = jobs[j].view.viewport[0];
@@ -249,48 +315,8 @@ void layout_jobs(JobDesc* out, const ws_job* jobs, int njobs, const ws_params& p
         d.keys = jobs[j].keys;
         d.count = jobs[j].count;
         view_shortcuts(jobs[j].view, c, &d.fast_transform, &d.keep_byte, &d.keep_q);
-        assign_scratch(d, c->n, p, at, njobs == 1);
-        d.ctl = reinterpret_cast<uint32_t*>(&ctls[j]);
+        place_job(d, c->n, j, S, scratch);
     }
-}
-
-// Items of one phase of one job.
-static void push_phase(std::vector<uint2>& items, const JobDesc& d, uint32_t job, uint32_t phase) {
-    const uint32_t count = (phase == kPhaseScanLo || phase == kPhaseScanHi) ? d.scan_items
-                           : phase == kPhaseCountHi ? (d.red_hi ? 0u : d.hi_items)
-                                                    : d.tiles;
-    for (uint32_t t = 0; t < count; ++t) items.push_back(make_uint2(job, (phase << kPhaseShift) | t));
-}
-
-// Work items, phase major: every job's keys (largest job first), then every
-// job's low scan, low pass, and so on. An item's dependency (the phase
-// before it, of its job) was queued a whole phase earlier, so a CTA rarely
-// waits except at the end of a phase; within a phase the largest jobs come
-// first, whose dependencies finished first.
-void build_items(std::vector<uint2>& items, const JobDesc* jobs, int njobs) {
-    items.clear();
-    std::vector<int> by_size(njobs);
-    for (int j = 0; j < njobs; ++j) by_size[j] = j;
-    std::stable_sort(by_size.begin(), by_size.end(), [&](int a, int b) { return jobs[a].n > jobs[b].n; });
-    for (uint32_t k = 0; k < kPhases; ++k)
-        for (int j : by_size) push_phase(items, jobs[j], (uint32_t)j, k);
-}
-
-// Resident CTAs per SM the kernel variant is built for: ctas_per_sm, or 3.
-int variant_minb(const ws_params& p) {
-    if (p.ctas_per_sm == 6 && p.tile == 1024) return 6;
-    return p.ctas_per_sm >= 2 && p.ctas_per_sm <= 4 ? (int)p.ctas_per_sm : 3;
-}
-
-int grid_for(ws_ctx* ctx, size_t n_items) {
-    const int minb = variant_minb(ctx->params);
-    const int ti = ctx->params.tile == 1024 ? 0 : ctx->params.tile == 2048 ? 1 : 2;
-    int& cached = ctx->occupancy[ti][minb - 2];   // minb is 2..6
-    if (cached == 0) cached = sort_occupancy(ctx->params.tile, minb);
-    int per_sm = cached < 1 ? 1 : cached;
-    size_t g = (size_t)ctx->sms * per_sm;
-    if (g > n_items) g = n_items ? n_items : 1;
-    return (int)g;
 }
 
 int check_view(ws_ctx* ctx, const ws_view* v) {
@@ -312,9 +338,6 @@ int check_cloud(ws_ctx* ctx, const ws_cloud* c) {
     return WS_OK;
 }
 
-// Stages, uploads and launches a batch on ctx's scratch. The stream waits for
-// the context's previous launch, so one scratch is never shared by two
-// launches in flight.
 // The parameters a launch of `splats` splats in total runs with.
 const ws_params& params_for(const ws_ctx* ctx, uint64_t splats) {
     int b = 0;
@@ -326,81 +349,65 @@ const ws_params& params_for(const ws_ctx* ctx, uint64_t splats) {
 // A lone job's staging in one launch: its description (passed by value with
 // the launch, so no host-to-device copy) into the job table, and the launch's
 // and the job's counters zeroed.
-__global__ void __launch_bounds__(256) stage_kernel(const __grid_constant__ JobDesc job, JobDesc* __restrict__ dst,
-                                                    uint32_t* __restrict__ ctl, uint32_t ctl_words) {
-    static_assert(sizeof(JobDesc) % 4 == 0, "copied in words");
+__global__ void __launch_bounds__(1024) stage_kernel(const __grid_constant__ JobDesc job, JobDesc* __restrict__ dst,
+                                                     uint32_t* __restrict__ ctl, uint32_t ctl_words) {
+    static_assert(sizeof(JobDesc) % 16 == 0, "copied in words");
     const uint32_t* src = reinterpret_cast<const uint32_t*>(&job);
     uint32_t* d = reinterpret_cast<uint32_t*>(dst);
     for (uint32_t k = threadIdx.x; k < sizeof(JobDesc) / 4; k += blockDim.x) d[k] = src[k];
-    for (uint32_t k = threadIdx.x; k < ctl_words; k += blockDim.x) ctl[k] = 0;
+    uint4* c4 = reinterpret_cast<uint4*>(ctl);
+    for (uint32_t k = threadIdx.x; k < ctl_words / 4; k += blockDim.x) c4[k] = make_uint4(0, 0, 0, 0);
 }
 
 // One persistent launch over `njobs` jobs of ns[j] elements each; `fill`
 // writes the job table (kind-specific fields and scratch) into pinned
-// staging, given the scratch base, with ctx->params already the launch's.
+// staging, given the launch's shape and the scratch base. The stream waits
+// for the context's previous launch, so one scratch is never shared by two
+// launches in flight.
 template <class Fill>
 static int launch_jobs(ws_ctx* ctx, const std::vector<uint32_t>& ns, int njobs, Fill fill, cudaStream_t stream) {
     cudaError_t e;
     uint64_t splats = 0;
     for (int j = 0; j < njobs; ++j) splats += ns[j];
-    const ws_params saved = ctx->params;
-    ctx->params = params_for(ctx, splats);   // restored below
-    struct Restore {
-        ws_ctx* c;
-        ws_params p;
-        ~Restore() { c->params = p; }
-    } restore{ctx, saved};
-    const size_t need = launch_scratch_bytes(ns.data(), njobs, ctx->params);
-    if (need > ctx->scratch.bytes) {
+    const ws_params& P = params_for(ctx, splats);
+    const bool same = ctx->shape_valid && ctx->last_ns == ns && !std::memcmp(&ctx->last_params, &P, sizeof(P));
+    if (!same) {
+        shape_launch(ns.data(), njobs, P, ctx->sms, ctx->shape);
+        ctx->last_ns = ns;
+        ctx->last_params = P;
+        ctx->shape_valid = true;
+    }
+    const LaunchShape& S = ctx->shape;
+    if (S.bytes > ctx->scratch.bytes) {
         // The old scratch may still be read by a launch in flight.
         if ((e = cudaEventSynchronize(ctx->launched)) != cudaSuccess) return cuda_error(ctx, e, "ws_sort");
-        if ((e = ctx->scratch.ensure(need)) != cudaSuccess) return cuda_error(ctx, e, "ws_sort scratch");
+        if ((e = ctx->scratch.ensure(S.bytes)) != cudaSuccess) return cuda_error(ctx, e, "ws_sort scratch");
     }
     // Pinned staging is rewritten only after its previous upload finished.
     if ((e = cudaEventSynchronize(ctx->staged)) != cudaSuccess) return cuda_error(ctx, e, "ws_sort");
-    if ((e = ctx->jobs_h.ensure((size_t)njobs * sizeof(JobDesc))) != cudaSuccess)
-        return cuda_error(ctx, e, "ws_sort staging");
-    if ((e = ctx->jobs_d.ensure((size_t)njobs * sizeof(JobDesc))) != cudaSuccess)
-        return cuda_error(ctx, e, "ws_sort job table");
-    JobDesc* hj = static_cast<JobDesc*>(ctx->jobs_h.p);
-    fill(hj, static_cast<char*>(ctx->scratch.p));
-
-    // Items depend only on the job sizes and the tiles: reuse the last upload
-    // when they are unchanged.
-    bool same = ctx->items_valid && ctx->last_ns == ns && ctx->last_tile == ctx->params.tile;
-    if (!same) {
-        build_items(ctx->items, hj, njobs);
-        if ((e = ctx->items_h.ensure(ctx->items.size() * sizeof(uint2))) != cudaSuccess)
-            return cuda_error(ctx, e, "ws_sort staging");
-        if (ctx->items.size() * sizeof(uint2) > ctx->items_d.bytes) {
-            if ((e = cudaEventSynchronize(ctx->launched)) != cudaSuccess) return cuda_error(ctx, e, "ws_sort");
-            if ((e = ctx->items_d.ensure(ctx->items.size() * sizeof(uint2))) != cudaSuccess)
-                return cuda_error(ctx, e, "ws_sort items");
-        }
-        std::memcpy(ctx->items_h.p, ctx->items.data(), ctx->items.size() * sizeof(uint2));
+    const size_t tb = table_bytes(njobs, S);
+    if ((e = ctx->jobs_h.ensure(tb)) != cudaSuccess) return cuda_error(ctx, e, "ws_sort staging");
+    if (tb > ctx->jobs_d.bytes) {
+        if ((e = cudaEventSynchronize(ctx->launched)) != cudaSuccess) return cuda_error(ctx, e, "ws_sort");
+        if ((e = ctx->jobs_d.ensure(tb)) != cudaSuccess) return cuda_error(ctx, e, "ws_sort job table");
     }
+    JobDesc* hj = static_cast<JobDesc*>(ctx->jobs_h.p);
+    char* scratch = static_cast<char*>(ctx->scratch.p);
+    fill(hj, S, scratch);
+    write_table(ctx->jobs_h.p, hj, njobs, S);
     if (stream != ctx->stream) cudaStreamWaitEvent(stream, ctx->launched, 0);
-    const size_t ctl_bytes = sizeof(LaunchCtl) + (size_t)njobs * sizeof(JobCtl);
     if (njobs == 1) {
-        stage_kernel<<<1, 256, 0, stream>>>(*hj, static_cast<JobDesc*>(ctx->jobs_d.p),
-                                            static_cast<uint32_t*>(ctx->scratch.p), (uint32_t)(ctl_bytes / 4));
+        stage_kernel<<<1, 1024, 0, stream>>>(*hj, static_cast<JobDesc*>(ctx->jobs_d.p),
+                                             reinterpret_cast<uint32_t*>(scratch), (uint32_t)(S.ctl_bytes / 4));
         if ((e = cudaGetLastError()) != cudaSuccess) return cuda_error(ctx, e, "ws_sort staging");
-    } else if ((e = cudaMemcpyAsync(ctx->jobs_d.p, hj, (size_t)njobs * sizeof(JobDesc), cudaMemcpyHostToDevice,
-                                    stream)) != cudaSuccess) {
+    } else if ((e = cudaMemcpyAsync(ctx->jobs_d.p, ctx->jobs_h.p, tb, cudaMemcpyHostToDevice, stream)) !=
+               cudaSuccess) {
         return cuda_error(ctx, e, "ws_sort upload");
     }
-    if (!same) {
-        if ((e = cudaMemcpyAsync(ctx->items_d.p, ctx->items_h.p, ctx->items.size() * sizeof(uint2),
-                                 cudaMemcpyHostToDevice, stream)) != cudaSuccess)
-            return cuda_error(ctx, e, "ws_sort upload");
-        ctx->last_ns = ns;
-        ctx->last_tile = ctx->params.tile;
-        ctx->items_valid = true;
-    }
     cudaEventRecord(ctx->staged, stream);
-    if (njobs != 1 && (e = cudaMemsetAsync(ctx->scratch.p, 0, ctl_bytes, stream)) != cudaSuccess)
+    if (njobs != 1 && (e = cudaMemsetAsync(scratch, 0, S.ctl_bytes, stream)) != cudaSuccess)
         return cuda_error(ctx, e, "ws_sort reset");
-    const size_t n_items = ctx->items.size();
+    const size_t n_items = (size_t)kPhases * S.segs.size();
     cudaEvent_t t_stop = nullptr;
     if (ctx->timing) {
         if (ctx->timing_used == ctx->timing_events.size()) {
@@ -417,12 +424,12 @@ static int launch_jobs(ws_ctx* ctx, const std::vector<uint32_t>& ns, int njobs, 
     if (ctx->tracing) {
         if ((e = ctx->trace_d.ensure(n_items * sizeof(TraceRec))) != cudaSuccess) return cuda_error(ctx, e, "ws_trace");
         trace = static_cast<TraceRec*>(ctx->trace_d.p);
-        ctx->trace_items = ctx->items;
-        ctx->trace_grid = grid_for(ctx, n_items);
+        ctx->trace_segs = S.segs;
+        ctx->trace_first_phase = 0;
+        ctx->trace_grid = (int)std::min<size_t>(S.grid, S.segs.size());
     }
-    e = launch_sort(static_cast<JobDesc*>(ctx->jobs_d.p), static_cast<uint2*>(ctx->items_d.p), (uint32_t)n_items,
-                    static_cast<LaunchCtl*>(ctx->scratch.p), ctx->err_d, ctx->params.tile,
-                    variant_minb(ctx->params), ctx->params.spin_limit, grid_for(ctx, n_items), stream, trace);
+    const LaunchDesc L = launch_desc(ctx->jobs_d.p, njobs, S, scratch, ctx->err_d, P.spin_limit, trace);
+    e = launch_sort(L, S.threads, (int)std::min<size_t>(S.grid, S.segs.size()), stream);
     if (e != cudaSuccess) return cuda_error(ctx, e, "ws_sort launch");
     if (t_stop) cudaEventRecord(t_stop, stream);
     cudaEventRecord(ctx->launched, stream);
@@ -438,18 +445,15 @@ int run_given_keys(ws_ctx* ctx, const uint16_t* keys, uint32_t n, uint32_t* orde
     std::vector<uint32_t> ns(1, n);
     return launch_jobs(
         ctx, ns, 1,
-        [&](JobDesc* hj, char* scratch) {
-            char* at = scratch + align_up(sizeof(LaunchCtl) + sizeof(JobCtl), 256);
+        [&](JobDesc* hj, const LaunchShape& S, char* scratch) {
             JobDesc& d = hj[0];
             std::memset(&d, 0, sizeof(d));
             d.kind = kJobKeys;
-            d.n = n;
             d.keys_in = keys;
             d.order = order;
             d.keys = sorted;
             d.count = count;
-            assign_scratch(d, n, ctx->params, at, true);
-            d.ctl = reinterpret_cast<uint32_t*>(scratch + sizeof(LaunchCtl));
+            place_job(d, n, 0, S, scratch);
         },
         stream);
 }
@@ -458,7 +462,8 @@ int run_batch(ws_ctx* ctx, const ws_job* jobs, int njobs, cudaStream_t stream) {
     std::vector<uint32_t> ns(njobs);
     for (int j = 0; j < njobs; ++j) ns[j] = jobs[j].cloud->n;
     return launch_jobs(
-        ctx, ns, njobs, [&](JobDesc* hj, char* scratch) { layout_jobs(hj, jobs, njobs, ctx->params, scratch); },
+        ctx, ns, njobs,
+        [&](JobDesc* hj, const LaunchShape& S, char* scratch) { layout_jobs(hj, jobs, njobs, S, scratch); },
         stream);
 }
 
@@ -526,8 +531,9 @@ extern "C" int ws_create(ws_ctx** out, int device) {
     }
     cudaMemset(ctx->err_d, 0, 4 * sizeof(uint32_t));
     ctx->params.tile = 2048;
-    ctx->params.ctas_per_sm = 4;
+    ctx->params.ctas_per_sm = 1;
     ctx->params.spin_limit = 1u << 22;
+    ctx->params.segs_per_cta = 1;
     *out = ctx;
     return WS_OK;
 }
@@ -539,13 +545,11 @@ extern "C" int ws_destroy(ws_ctx* ctx) {
     cudaDeviceSynchronize();
     ctx->scratch.release();
     ctx->jobs_d.release();
-    ctx->items_d.release();
     ctx->out_d.release();
     ctx->thr_d.release();
     ctx->draw_d.release();
     ctx->pairs_d.release();
     ctx->jobs_h.release();
-    ctx->items_h.release();
     ctx->count_h.release();
     for (int b = 0; b < 2; ++b) {
         ctx->load_h[b].release();
@@ -583,12 +587,14 @@ extern "C" int ws_get_params(const ws_ctx* ctx, ws_params* out) {
 
 // The kernel variants that exist: tile 1024, 2048 or 4096 with 2, 3 or 4
 // resident CTAs per SM (0 picks 3), and tile 1024 with 6.
+// The kernel variants that exist: 1024 threads a CTA (one CTA an SM) or 512
+// (two); segments no smaller than `tile` splats, a multiple of 256.
 static const char* params_problem(const ws_params* p) {
-    if (p->tile != 1024 && p->tile != 2048 && p->tile != 4096) return "tile must be 1024, 2048 or 4096";
+    if (p->tile < kSegAlign || p->tile > (1u << 24) || p->tile % kSegAlign)
+        return "tile must be a multiple of 256 from 256 to 2^24";
     if (p->spin_limit == 0) return "spin_limit must be positive";
-    const bool ok = p->ctas_per_sm == 0 || (p->ctas_per_sm >= 2 && p->ctas_per_sm <= 4) ||
-                    (p->ctas_per_sm == 6 && p->tile == 1024);
-    if (!ok) return "ctas_per_sm must be 0, 2, 3 or 4 (or 6 with tile 1024)";
+    if (p->ctas_per_sm > 2) return "ctas_per_sm must be 0, 1 or 2";
+    if (p->segs_per_cta > 64) return "segs_per_cta must be 0 to 64";
     return nullptr;
 }
 
@@ -606,7 +612,7 @@ extern "C" int ws_set_tuning(ws_ctx* ctx, const ws_params* table, int n) {
         }
     for (int b = 0; b < 32; ++b) ctx->tuning[b] = b < n ? table[b] : ws_params{};
     ctx->tuning_n = n;
-    ctx->items_valid = false;
+    ctx->shape_valid = false;
     return WS_OK;
 }
 
@@ -614,7 +620,7 @@ extern "C" int ws_set_params(ws_ctx* ctx, const ws_params* p) {
     if (!ctx || !p) return WS_ERR_ARG;
     if (const char* why = params_problem(p)) return set_error(ctx, WS_ERR_ARG, "ws_set_params: %s", why);
     ctx->params = *p;
-    ctx->items_valid = false;
+    ctx->shape_valid = false;
     return WS_OK;
 }
 
@@ -917,42 +923,33 @@ extern "C" int ws_selftest_wait(ws_ctx* ctx, uint32_t spin_limit) {
     cudaSetDevice(ctx->device);
     cudaError_t e;
     if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return cuda_error(ctx, e, "ws_selftest_wait");
-    // One job of 4096 given keys whose keys items are not queued: its scan
-    // items wait for a count that nothing raises.
+    // One job of 4096 given keys whose keys items are left out of the launch:
+    // its low-pass items wait for a completion count that nothing raises.
     const uint32_t n = 4096;
+    LaunchShape S;
+    shape_launch(&n, 1, ctx->params, ctx->sms, S);
+    ctx->shape_valid = false;   // the context's scratch is reused below
     const size_t keys_bytes = 16384, out_bytes = 3 * 4 * (size_t)n + 256;
-    const size_t sort_bytes = launch_scratch_bytes(&n, 1, ctx->params);
-    if ((e = ctx->scratch.ensure(sort_bytes + keys_bytes + out_bytes)) != cudaSuccess)
+    if ((e = ctx->scratch.ensure(S.bytes + keys_bytes + out_bytes)) != cudaSuccess)
         return cuda_error(ctx, e, "ws_selftest_wait scratch");
     char* base = static_cast<char*>(ctx->scratch.p);
-    uint16_t* keys = reinterpret_cast<uint16_t*>(base + sort_bytes);
-    uint32_t* outs = reinterpret_cast<uint32_t*>(base + sort_bytes + keys_bytes);
+    uint16_t* keys = reinterpret_cast<uint16_t*>(base + S.bytes);
+    uint32_t* outs = reinterpret_cast<uint32_t*>(base + S.bytes + keys_bytes);
     JobDesc d;
     std::memset(&d, 0, sizeof(d));
     d.kind = kJobKeys;
-    d.n = n;
     d.keys_in = keys;
     d.order = outs;
     d.keys = outs + n;
     d.count = outs + 2 * n;
-    char* at = base + align_up(sizeof(LaunchCtl) + sizeof(JobCtl), 256);
-    assign_scratch(d, n, ctx->params, at, true);
-    d.ctl = reinterpret_cast<uint32_t*>(base + sizeof(LaunchCtl));
-    std::vector<uint2> items;
-    for (uint32_t t = 0; t < d.scan_items; ++t) items.push_back(make_uint2(0u, (kPhaseScanLo << kPhaseShift) | t));
-    if ((e = ctx->jobs_d.ensure(sizeof(JobDesc))) != cudaSuccess ||
-        (e = ctx->items_d.ensure(items.size() * sizeof(uint2))) != cudaSuccess)
-        return cuda_error(ctx, e, "ws_selftest_wait");
-    ctx->items_valid = false;   // the item upload below replaces the cached list
+    place_job(d, n, 0, S, base);
+    if ((e = ctx->jobs_d.ensure(sizeof(JobDesc))) != cudaSuccess) return cuda_error(ctx, e, "ws_selftest_wait");
     if ((e = cudaMemcpy(ctx->jobs_d.p, &d, sizeof(d), cudaMemcpyHostToDevice)) != cudaSuccess ||
-        (e = cudaMemcpy(ctx->items_d.p, items.data(), items.size() * sizeof(uint2), cudaMemcpyHostToDevice)) !=
-            cudaSuccess ||
-        (e = cudaMemset(base, 0, sizeof(LaunchCtl) + sizeof(JobCtl))) != cudaSuccess ||
-        (e = cudaMemset(keys, 0, keys_bytes)) != cudaSuccess)
+        (e = cudaMemset(base, 0, S.ctl_bytes)) != cudaSuccess || (e = cudaMemset(keys, 0, keys_bytes)) != cudaSuccess)
         return cuda_error(ctx, e, "ws_selftest_wait");
-    e = launch_sort(static_cast<JobDesc*>(ctx->jobs_d.p), static_cast<uint2*>(ctx->items_d.p), (uint32_t)items.size(),
-                    static_cast<LaunchCtl*>(ctx->scratch.p), ctx->err_d, ctx->params.tile, variant_minb(ctx->params),
-                    spin_limit, 2, ctx->stream, nullptr);
+    LaunchDesc L = launch_desc(ctx->jobs_d.p, 1, S, base, ctx->err_d, spin_limit, nullptr);
+    L.first_phase = kPhaseLow;
+    e = launch_sort(L, S.threads, 2, ctx->stream);
     if (e != cudaSuccess) return cuda_error(ctx, e, "ws_selftest_wait launch");
     if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return cuda_error(ctx, e, "ws_selftest_wait");
     return take_device_error(ctx);
@@ -1022,8 +1019,8 @@ extern "C" int ws_sort_batch_shaded(ws_ctx* ctx, int njobs, const ws_job* jobs, 
     for (int j = 0; j < njobs; ++j) ns[j] = jobs[j].cloud->n;
     return launch_jobs(
         ctx, ns, njobs,
-        [&](JobDesc* hj, char* scratch) {
-            layout_jobs(hj, jobs, njobs, ctx->params, scratch);
+        [&](JobDesc* hj, const LaunchShape& S, char* scratch) {
+            layout_jobs(hj, jobs, njobs, S, scratch);
             for (int j = 0; j < njobs; ++j) {
                 const ws_cloud* c = jobs[j].cloud;
                 if (!c->sh) continue;
@@ -1123,7 +1120,7 @@ extern "C" int ws_sort_particles(ws_ctx* ctx, int n, const ws_emitter* emitters,
     const float* thr = static_cast<const float*>(ctx->thr_d.p);
     return launch_jobs(
         ctx, ns, n,
-        [&](JobDesc* hj, char* scratch) { layout_emitters(hj, emitters, n, ctx->params, scratch, thr); },
+        [&](JobDesc* hj, const LaunchShape& S, char* scratch) { layout_emitters(hj, emitters, n, S, scratch, thr); },
         stream_p ? static_cast<cudaStream_t>(stream_p) : ctx->stream);
 }
 
@@ -1133,9 +1130,9 @@ struct ws_plan {
     ws_ctx* ctx;
     int njobs;
     std::vector<ws_job> jobs;
-    DevBuf scratch, jobs_d, items_d;
+    DevBuf scratch, jobs_d;
     HostBuf jobs_h;
-    uint32_t n_items;
+    LaunchShape shape;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     cudaEvent_t done = nullptr;
@@ -1154,13 +1151,7 @@ extern "C" int ws_plan_create(ws_ctx* ctx, int njobs, const ws_job* jobs, ws_pla
     cudaSetDevice(ctx->device);
     uint64_t splats = 0;
     for (int j = 0; j < njobs; ++j) splats += jobs[j].cloud->n;
-    const ws_params saved = ctx->params;
-    ctx->params = params_for(ctx, splats);   // restored below
-    struct Restore {
-        ws_ctx* c;
-        ws_params p;
-        ~Restore() { c->params = p; }
-    } restore{ctx, saved};
+    const ws_params& P = params_for(ctx, splats);
     ws_plan* p = new (std::nothrow) ws_plan();
     if (!p) return set_error(ctx, WS_ERR_NOMEM, "ws_plan_create: out of host memory");
     p->ctx = ctx;
@@ -1169,25 +1160,18 @@ extern "C" int ws_plan_create(ws_ctx* ctx, int njobs, const ws_job* jobs, ws_pla
     std::vector<uint32_t> ns(njobs);
     for (int j = 0; j < njobs; ++j) ns[j] = jobs[j].cloud->n;
     cudaError_t e;
-    const size_t need = launch_scratch_bytes(ns.data(), njobs, ctx->params);
-    if ((e = p->scratch.ensure(need)) != cudaSuccess || (e = p->jobs_d.ensure(njobs * sizeof(JobDesc))) != cudaSuccess ||
-        (e = p->jobs_h.ensure(njobs * sizeof(JobDesc))) != cudaSuccess ||
+    LaunchShape& S = p->shape;
+    shape_launch(ns.data(), njobs, P, ctx->sms, S);
+    const size_t tb = table_bytes(njobs, S);
+    if ((e = p->scratch.ensure(S.bytes)) != cudaSuccess || (e = p->jobs_d.ensure(tb)) != cudaSuccess ||
+        (e = p->jobs_h.ensure(tb)) != cudaSuccess ||
         (e = cudaEventCreateWithFlags(&p->done, cudaEventDisableTiming)) != cudaSuccess) {
         ws_plan_destroy(p);
         return cuda_error(ctx, e, "ws_plan_create");
     }
     JobDesc* hj = static_cast<JobDesc*>(p->jobs_h.p);
-    layout_jobs(hj, jobs, njobs, ctx->params, static_cast<char*>(p->scratch.p));
-    std::vector<uint2> items;
-    build_items(items, hj, njobs);
-    p->n_items = (uint32_t)items.size();
-    if ((e = p->items_d.ensure(items.size() * sizeof(uint2))) != cudaSuccess ||
-        (e = cudaMemcpy(p->items_d.p, items.data(), items.size() * sizeof(uint2), cudaMemcpyHostToDevice)) !=
-            cudaSuccess) {
-        ws_plan_destroy(p);
-        return cuda_error(ctx, e, "ws_plan_create");
-    }
-    p->grid = grid_for(ctx, items.size());
+    layout_jobs(hj, jobs, njobs, S, static_cast<char*>(p->scratch.p));
+    write_table(p->jobs_h.p, hj, njobs, S);
     // Capture: upload the job table from pinned memory, reset the counters,
     // launch.
     cudaStream_t cs;
@@ -1197,11 +1181,11 @@ extern "C" int ws_plan_create(ws_ctx* ctx, int njobs, const ws_job* jobs, ws_pla
     }
     e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
-        cudaMemcpyAsync(p->jobs_d.p, hj, njobs * sizeof(JobDesc), cudaMemcpyHostToDevice, cs);
-        cudaMemsetAsync(p->scratch.p, 0, sizeof(LaunchCtl) + (size_t)njobs * sizeof(JobCtl), cs);
-        launch_sort(static_cast<JobDesc*>(p->jobs_d.p), static_cast<uint2*>(p->items_d.p), p->n_items,
-                    static_cast<LaunchCtl*>(p->scratch.p), ctx->err_d, ctx->params.tile,
-                    variant_minb(ctx->params), ctx->params.spin_limit, p->grid, cs, nullptr);
+        cudaMemcpyAsync(p->jobs_d.p, p->jobs_h.p, tb, cudaMemcpyHostToDevice, cs);
+        cudaMemsetAsync(p->scratch.p, 0, S.ctl_bytes, cs);
+        const LaunchDesc L = launch_desc(p->jobs_d.p, njobs, S, static_cast<char*>(p->scratch.p), ctx->err_d,
+                                         P.spin_limit, nullptr);
+        launch_sort(L, S.threads, (int)std::min<size_t>(S.grid, S.segs.size()), cs);
         e = cudaStreamEndCapture(cs, &p->graph);
     }
     if (e == cudaSuccess) e = cudaGraphInstantiate(&p->exec, p->graph, 0);
@@ -1230,6 +1214,8 @@ extern "C" int ws_plan_set_views(ws_plan* p, const ws_view* views) {
         hj[j].viewport[0] = views[j].viewport[0];
         hj[j].viewport[1] = views[j].viewport[1];
         hj[j].cull = views[j].cull;
+        // The culling shortcuts are proved for one view: prove them again.
+        view_shortcuts(views[j], p->jobs[j].cloud, &hj[j].fast_transform, &hj[j].keep_byte, &hj[j].keep_q);
         p->jobs[j].view = views[j];
     }
     return WS_OK;
@@ -1263,7 +1249,6 @@ extern "C" int ws_plan_destroy(ws_plan* p) {
     if (p->graph) cudaGraphDestroy(p->graph);
     p->scratch.release();
     p->jobs_d.release();
-    p->items_d.release();
     p->jobs_h.release();
     delete p;
     return WS_OK;
@@ -1345,7 +1330,8 @@ extern "C" int ws_trace_read(ws_ctx* ctx, ws_trace_rec* out, size_t cap, size_t*
     cudaError_t e = cudaStreamSynchronize(ctx->stream);
     if (e == cudaSuccess) e = cudaEventSynchronize(ctx->launched);
     if (e != cudaSuccess) return cuda_error(ctx, e, "ws_trace_read");
-    const size_t items = ctx->trace_items.size();
+    const size_t nseg = ctx->trace_segs.size();
+    const size_t items = (kPhases - ctx->trace_first_phase) * nseg;
     *n = items;
     if (!out || cap == 0 || !ctx->trace_d.p) return WS_OK;
     std::vector<TraceRec> recs(items);
@@ -1355,9 +1341,10 @@ extern "C" int ws_trace_read(ws_ctx* ctx, ws_trace_rec* out, size_t cap, size_t*
         out[k].claim_ns = recs[k].claim;
         out[k].start_ns = recs[k].start;
         out[k].end_ns = recs[k].end;
-        out[k].job = ctx->trace_items[k].x;
-        out[k].phase = ctx->trace_items[k].y >> kPhaseShift;
-        out[k].tile = ctx->trace_items[k].y & kTileMask;
+        const SegDesc& sd = ctx->trace_segs[k % nseg];
+        out[k].job = sd.job;
+        out[k].phase = ctx->trace_first_phase + (uint32_t)(k / nseg);
+        out[k].segment = (uint32_t)(k % nseg);
         out[k].sm = recs[k].sm;
         for (int q = 0; q < 3; ++q) out[k].mark_ns[q] = recs[k].mark[q];
     }

@@ -14,10 +14,9 @@
 // Set-up: the first call on a device (with that device current) takes the
 // array's device address with cudaGetSymbolAddress and keeps it; make that
 // first call before any stream capture. Every call then queues three kernels
-// on the stream: one that writes the job description and work list into the
-// array and clears the counters that must start at zero, the sort kernel of
-// ws_sort itself, and one that turns a device-side error into *count =
-// 0xFFFFFFFF. All calls share the one array, which keeps the last call's
+// on the stream: one that writes the job description into the array and
+// clears the counters that must start at zero, the sort kernel of ws_sort
+// itself, and one that turns a device-side error into *count = 0xFFFFFFFF. All calls share the one array, which keeps the last call's
 // contents: calls whose work overlaps on the GPU (other streams, other host
 // threads) race on it and must be serialised by the caller.
 #include "wsort.h"
@@ -30,35 +29,21 @@
 
 namespace wsort {
 
-cudaError_t launch_sort(const JobDesc* jobs, const uint2* items, uint32_t n_items, LaunchCtl* lctl, uint32_t* err,
-                        uint32_t tile, int minb, uint32_t spin_limit, int grid, cudaStream_t stream,
-                        TraceRec* trace);
-int sort_occupancy(uint32_t tile, int minb);
-size_t launch_scratch_bytes(const uint32_t* ns, int njobs, const ws_params& p);
-void layout_jobs(JobDesc* out, const ws_job* jobs, int njobs, const ws_params& p, char* scratch);
+void layout_jobs(JobDesc* out, const ws_job* jobs, int njobs, const LaunchShape& S, char* scratch);
 
 namespace {
 
 // Fixed kernel parameters of this entry point (the library's defaults).
-constexpr uint32_t kTile = 2048;
-constexpr int kMinBlocks = 4;
+constexpr uint32_t kMinSegment = 2048;
 constexpr uint32_t kSpinLimit = 1u << 22;
 
-// Tiles of the largest cloud, and the work items of one job of that size:
-// keys, low pass and high pass one per tile, high-digit counts one per two
-// tiles (none when the low pass counts them), and the two scans one per
-// digit value.
-constexpr uint32_t kMaxTiles = (WS_NOALLOC_MAX_SPLATS + kTile - 1) / kTile;
-constexpr uint32_t kMaxItems = 3 * kMaxTiles + (kMaxTiles + kCountSpan - 1) / kCountSpan + 2 * kScanItems;
-
 // Layout of the array: the sort's scratch for one job of up to
-// WS_NOALLOC_MAX_SPLATS splats (checked against launch_scratch_bytes on every
-// call), then the job description, the error words and the work items.
+// WS_NOALLOC_MAX_SPLATS splats (checked against the launch's shape on every
+// call), then the job description and the error words.
 constexpr size_t kSortBytes = 10u << 20;
 constexpr size_t kJobOffset = kSortBytes;
 constexpr size_t kErrOffset = kJobOffset + ((sizeof(JobDesc) + 255) / 256) * 256;
-constexpr size_t kItemsOffset = kErrOffset + 256;
-constexpr size_t kScratchBytes = kItemsOffset + (size_t)kMaxItems * sizeof(uint2);
+constexpr size_t kScratchBytes = kErrOffset + 256;
 
 static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 
@@ -66,27 +51,16 @@ constexpr int kMaxDevices = 64;
 std::mutex g_setup_mutex;
 void* g_scratch_addr[kMaxDevices] = {};
 
-// Writes the job description and its work list into g_scratch and clears the
-// per-launch and per-job counters and the error words.
-__global__ void noalloc_setup_kernel(JobDesc desc, uint32_t tiles, uint32_t clear_bytes) {
+// Writes the job description into g_scratch and clears the launch's and the
+// job's counters (the first clear_bytes of the array) and the error words.
+__global__ void noalloc_setup_kernel(const __grid_constant__ JobDesc desc, uint32_t clear_bytes) {
     JobDesc* job = reinterpret_cast<JobDesc*>(g_scratch + kJobOffset);
-    uint2* items = reinterpret_cast<uint2*>(g_scratch + kItemsOffset);
     uint32_t* err = reinterpret_cast<uint32_t*>(g_scratch + kErrOffset);
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t stride = gridDim.x * blockDim.x;
     if (tid == 0) *job = desc;
     if (tid < 4) err[tid] = 0;
     for (uint32_t k = tid; k < clear_bytes / 4; k += stride) reinterpret_cast<uint32_t*>(g_scratch)[k] = 0;
-    // The phases in order: keys, low scan, low pass, high counts, high scan,
-    // high pass (the order ws_sort's work list has for a single job).
-    const uint32_t scans = desc.scan_items;
-    const uint32_t hi_counts = desc.red_hi ? 0u : desc.hi_items;
-    const uint32_t counts[kPhases] = {tiles, scans, tiles, hi_counts, scans, tiles};
-    uint32_t first = 0;
-    for (uint32_t ph = 0; ph < kPhases; ++ph) {
-        for (uint32_t t = tid; t < counts[ph]; t += stride) items[first + t] = make_uint2(0u, (ph << kPhaseShift) | t);
-        first += counts[ph];
-    }
 }
 
 // A device-side wait that gave up leaves its code in the error words; the
@@ -97,6 +71,8 @@ __global__ void noalloc_check_kernel(uint32_t* count) {
 }
 
 // The array's device address on the current device, taken once per device.
+// The address is kept for the life of the process; a cudaDeviceReset on that
+// device would make it stale (this library never resets a device).
 int scratch_address(int device, char** out) {
     if (device < 0 || device >= kMaxDevices) return WS_ERR_ARG;
     std::lock_guard<std::mutex> lock(g_setup_mutex);
@@ -127,14 +103,16 @@ extern "C" int ws_sort_noalloc(const ws_cloud* cloud, const ws_view* view, uint3
     if (cloud->n > WS_NOALLOC_MAX_SPLATS) return WS_ERR_CAPACITY;
 
     ws_params p{};
-    p.tile = kTile;
-    p.ctas_per_sm = kMinBlocks;
+    p.tile = kMinSegment;
+    p.ctas_per_sm = 1;
     p.spin_limit = kSpinLimit;
+    p.segs_per_cta = 1;
     const uint32_t n = cloud->n;
-    if (launch_scratch_bytes(&n, 1, p) > kSortBytes) return WS_ERR_CAPACITY;
-
     const int device = cloud->ctx->device;
     if (cudaSetDevice(device) != cudaSuccess) return WS_ERR_CUDA;
+    LaunchShape S;
+    shape_launch(&n, 1, p, cloud->ctx->sms, S);
+    if (S.bytes > kSortBytes) return WS_ERR_CAPACITY;
     char* base = nullptr;
     int rc = scratch_address(device, &base);
     if (rc) return rc;
@@ -147,25 +125,15 @@ extern "C" int ws_sort_noalloc(const ws_cloud* cloud, const ws_view* view, uint3
     job.keys = keys;
     job.count = count;
     JobDesc desc;
-    layout_jobs(&desc, &job, 1, p, base);
+    layout_jobs(&desc, &job, 1, S, base);
 
-    const uint32_t tiles = desc.tiles;
-    const uint32_t n_items = 3 * tiles + (desc.red_hi ? 0u : desc.hi_items) + 2 * desc.scan_items;
-    const uint32_t clear_bytes = (uint32_t)(((sizeof(LaunchCtl) + sizeof(JobCtl)) + 3) / 4 * 4);
-    int sms = 0;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    int per_sm = sort_occupancy(kTile, kMinBlocks);
-    if (per_sm < 1) per_sm = 1;
-    int grid = sms * per_sm;
-    if ((uint32_t)grid > n_items) grid = (int)n_items;
-
-    noalloc_setup_kernel<<<8, 256, 0, stream>>>(desc, tiles, clear_bytes);
+    noalloc_setup_kernel<<<8, 256, 0, stream>>>(desc, (uint32_t)S.ctl_bytes);
     cudaError_t e = cudaGetLastError();
-    if (e == cudaSuccess)
-        e = launch_sort(reinterpret_cast<const JobDesc*>(base + kJobOffset),
-                        reinterpret_cast<const uint2*>(base + kItemsOffset), n_items,
-                        reinterpret_cast<LaunchCtl*>(base), reinterpret_cast<uint32_t*>(base + kErrOffset), kTile,
-                        kMinBlocks, kSpinLimit, grid, stream, nullptr);
+    if (e == cudaSuccess) {
+        const LaunchDesc L = launch_desc(base + kJobOffset, 1, S, base, reinterpret_cast<uint32_t*>(base + kErrOffset),
+                                         kSpinLimit, nullptr);
+        e = launch_sort(L, S.threads, (int)std::min<size_t>(S.grid, S.segs.size()), stream);
+    }
     if (e == cudaSuccess) {
         noalloc_check_kernel<<<1, 1, 0, stream>>>(count);
         e = cudaGetLastError();

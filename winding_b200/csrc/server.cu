@@ -28,14 +28,8 @@
 #include <vector>
 
 namespace wsort {
-cudaError_t launch_sort(const JobDesc* jobs, const uint2* items, uint32_t n_items, LaunchCtl* lctl, uint32_t* err,
-                        uint32_t tile, int minb, uint32_t spin_limit, int grid, cudaStream_t stream,
-                        TraceRec* trace);
-int sort_occupancy(uint32_t tile, int minb);
-int variant_minb(const ws_params& p);
-size_t launch_scratch_bytes(const uint32_t* ns, int njobs, const ws_params& p);
-void layout_jobs(JobDesc* out, const ws_job* jobs, int njobs, const ws_params& p, char* scratch);
-void build_items(std::vector<uint2>& items, const JobDesc* jobs, int njobs);
+size_t launch_scratch_bytes(const uint32_t* ns, int njobs, const ws_params& p, int sms);
+void layout_jobs(JobDesc* out, const ws_job* jobs, int njobs, const LaunchShape& S, char* scratch);
 
 namespace {
 
@@ -120,11 +114,11 @@ struct Slot {
     cudaStream_t stream = nullptr;
     cudaEvent_t done = nullptr;
     uint32_t* err_d = nullptr;
-    JobDesc* h_jobs = nullptr;      // pinned
-    JobDesc* d_jobs = nullptr;
-    uint2* h_items = nullptr;       // pinned
-    uint2* d_items = nullptr;
-    size_t cap_jobs = 0, cap_items = 0;
+    uint32_t* err_h = nullptr;      // pinned: the launch's error words, copied back before `done`
+    char* h_table = nullptr;        // pinned: the job and segment table
+    char* d_table = nullptr;
+    size_t cap_table = 0;           // bytes, sized at creation for the largest batch
+    LaunchShape shape;              // the batch in flight
     char* scratch = nullptr;        // in the arena, for the batch in flight
     size_t scratch_bytes = 0;
     std::vector<Request*> batch;
@@ -168,30 +162,19 @@ struct ws_server {
 
 namespace {
 
-// Grows a slot's staging for njobs jobs and n_items work items.
-cudaError_t ensure_staging(Slot& s, size_t njobs, size_t n_items) {
-    cudaError_t e = cudaSuccess;
-    if (njobs > s.cap_jobs) {
-        if (s.h_jobs) cudaFreeHost(s.h_jobs);
-        if (s.d_jobs) cudaFree(s.d_jobs);
-        s.h_jobs = nullptr;
-        s.d_jobs = nullptr;
-        s.cap_jobs = 0;
-        if ((e = cudaHostAlloc(&s.h_jobs, njobs * sizeof(JobDesc), cudaHostAllocDefault)) != cudaSuccess) return e;
-        if ((e = cudaMalloc(&s.d_jobs, njobs * sizeof(JobDesc))) != cudaSuccess) return e;
-        s.cap_jobs = njobs;
-    }
-    if (n_items > s.cap_items) {
-        if (s.h_items) cudaFreeHost(s.h_items);
-        if (s.d_items) cudaFree(s.d_items);
-        s.h_items = nullptr;
-        s.d_items = nullptr;
-        s.cap_items = 0;
-        const size_t cap = n_items + n_items / 2;
-        if ((e = cudaHostAlloc(&s.h_items, cap * sizeof(uint2), cudaHostAllocDefault)) != cudaSuccess) return e;
-        if ((e = cudaMalloc(&s.d_items, cap * sizeof(uint2))) != cudaSuccess) return e;
-        s.cap_items = cap;
-    }
+// Sizes a slot's table staging for `bytes` (at creation; again only if a
+// batch ever needs more, which the creation-time bound rules out).
+cudaError_t ensure_table(Slot& s, size_t bytes) {
+    if (bytes <= s.cap_table) return cudaSuccess;
+    if (s.h_table) cudaFreeHost(s.h_table);
+    if (s.d_table) cudaFree(s.d_table);
+    s.h_table = nullptr;
+    s.d_table = nullptr;
+    s.cap_table = 0;
+    cudaError_t e;
+    if ((e = cudaHostAlloc(reinterpret_cast<void**>(&s.h_table), bytes, cudaHostAllocDefault)) != cudaSuccess) return e;
+    if ((e = cudaMalloc(reinterpret_cast<void**>(&s.d_table), bytes)) != cudaSuccess) return e;
+    s.cap_table = bytes;
     return cudaSuccess;
 }
 
@@ -227,7 +210,7 @@ bool form_batch(ws_server* S, Slot& slot) {
         uint64_t total = 0;
         for (uint32_t v : ns) total += v;
         slot.params = batch_params(S, total);
-        const size_t need = launch_scratch_bytes(ns.data(), (int)ns.size(), slot.params);
+        const size_t need = launch_scratch_bytes(ns.data(), (int)ns.size(), slot.params, S->sms);
         slot.scratch = S->arena.alloc(need);
         if (slot.scratch) {
             slot.scratch_bytes = need;
@@ -266,27 +249,27 @@ bool launch_batch(ws_server* S, Slot& slot) {
     // The staging of this slot's previous launch has been consumed: the slot
     // is only reused after its completion.
     const ws_params& P = slot.params;
+    std::vector<uint32_t> ns(nj);
+    for (int j = 0; j < nj; ++j) ns[j] = slot.batch[j]->n;
+    LaunchShape& SH = slot.shape;
+    shape_launch(ns.data(), nj, P, S->sms, SH);
     std::vector<JobDesc> descs(nj);
-    layout_jobs(descs.data(), jobs.data(), nj, P, slot.scratch);
-    std::vector<uint2> items;
-    build_items(items, descs.data(), nj);
-    if (ensure_staging(slot, nj, items.size()) != cudaSuccess) return false;
-    std::memcpy(slot.h_jobs, descs.data(), nj * sizeof(JobDesc));
-    std::memcpy(slot.h_items, items.data(), items.size() * sizeof(uint2));
+    layout_jobs(descs.data(), jobs.data(), nj, SH, slot.scratch);
+    const size_t tb = table_bytes(nj, SH);
+    if (ensure_table(slot, tb) != cudaSuccess) return false;
+    write_table(slot.h_table, descs.data(), nj, SH);
     cudaError_t e;
-    if ((e = cudaMemcpyAsync(slot.d_jobs, slot.h_jobs, nj * sizeof(JobDesc), cudaMemcpyHostToDevice, slot.stream)) ||
-        (e = cudaMemcpyAsync(slot.d_items, slot.h_items, items.size() * sizeof(uint2), cudaMemcpyHostToDevice,
-                             slot.stream)) ||
-        (e = cudaMemsetAsync(slot.scratch, 0, sizeof(LaunchCtl) + (size_t)nj * sizeof(JobCtl), slot.stream)) ||
+    if ((e = cudaMemcpyAsync(slot.d_table, slot.h_table, tb, cudaMemcpyHostToDevice, slot.stream)) ||
+        (e = cudaMemsetAsync(slot.scratch, 0, SH.ctl_bytes, slot.stream)) ||
         (e = cudaMemsetAsync(slot.err_d, 0, 2 * sizeof(uint32_t), slot.stream)))
         return false;
-    int per_sm = sort_occupancy(P.tile, variant_minb(P));
-    if (per_sm < 1) per_sm = 1;
-    size_t grid = (size_t)S->sms * per_sm;
-    if (grid > items.size()) grid = items.size();
-    e = launch_sort(slot.d_jobs, slot.d_items, (uint32_t)items.size(), reinterpret_cast<LaunchCtl*>(slot.scratch),
-                    slot.err_d, P.tile, variant_minb(P), P.spin_limit, (int)grid, slot.stream, nullptr);
+    const LaunchDesc L = launch_desc(slot.d_table, nj, SH, slot.scratch, slot.err_d, P.spin_limit, nullptr);
+    e = launch_sort(L, SH.threads, (int)std::min<size_t>(SH.grid, SH.segs.size()), slot.stream);
     if (e != cudaSuccess) return false;
+    // The error words come back with the batch: the completion thread reads
+    // them from pinned memory once the event has passed.
+    if ((e = cudaMemcpyAsync(slot.err_h, slot.err_d, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, slot.stream)))
+        return false;
     return cudaEventRecord(slot.done, slot.stream) == cudaSuccess;
 }
 
@@ -360,7 +343,10 @@ void completer_loop(ws_server* S) {
         lock.unlock();
         cudaError_t e = cudaEventSynchronize(oldest->done);
         uint32_t err[2] = {0, 0};
-        if (e == cudaSuccess) e = cudaMemcpy(err, oldest->err_d, sizeof(err), cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess) {
+            err[0] = oldest->err_h[0];
+            err[1] = oldest->err_h[1];
+        }
         const double t = now_ms();
         lock.lock();
         const bool ok = e == cudaSuccess && err[0] == 0;
@@ -422,14 +408,26 @@ extern "C" int ws_server_create(ws_ctx* ctx, const ws_server_opts* opts, ws_serv
         delete S;
         return WS_ERR_NOMEM;
     }
+    // Each slot's table staging is sized now for the largest batch, so a
+    // launch never allocates (an allocation or free there would synchronise
+    // the device and stall the other slot): max_batch jobs and their
+    // segments, at most segs_per_cta a resident CTA plus one a job, for the
+    // parameters of any launch size.
+    uint32_t per_cta = std::max(1u, S->params.segs_per_cta);
+    for (int b = 0; b < S->tuning_n; ++b) per_cta = std::max(per_cta, S->tuning[b].segs_per_cta);
+    const size_t max_segs = (size_t)S->sms * 2 * per_cta + (size_t)S->opts.max_batch;
+    const size_t table = (size_t)S->opts.max_batch * sizeof(JobDesc) + max_segs * sizeof(SegDesc);
     S->slots.resize(S->opts.streams);
     for (Slot& s : S->slots) {
         if (cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking) != cudaSuccess ||
             cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming) != cudaSuccess ||
-            cudaMalloc(&s.err_d, 16) != cudaSuccess || cudaMemset(s.err_d, 0, 16) != cudaSuccess) {
+            cudaMalloc(&s.err_d, 16) != cudaSuccess || cudaMemset(s.err_d, 0, 16) != cudaSuccess ||
+            cudaHostAlloc(reinterpret_cast<void**>(&s.err_h), 16, cudaHostAllocDefault) != cudaSuccess ||
+            ensure_table(s, table) != cudaSuccess) {
             ws_server_destroy(S);
             return WS_ERR_CUDA;
         }
+        s.err_h[0] = s.err_h[1] = 0;
     }
     S->dispatcher = std::thread(dispatcher_loop, S);
     S->completer = std::thread(completer_loop, S);
@@ -444,7 +442,7 @@ extern "C" int ws_server_submit(ws_server* S, const ws_cloud* cloud, const ws_vi
     if (cloud->ctx != S->ctx) return WS_ERR_ARG;
     if (!(view->cull >= 0.0f && std::isfinite(view->cull))) return WS_ERR_ARG;
     const uint32_t n = cloud->n;
-    if (output_bytes(n) + launch_scratch_bytes(&n, 1, S->params) > S->arena.size()) return WS_ERR_NOMEM;
+    if (output_bytes(n) + launch_scratch_bytes(&n, 1, S->params, S->sms) > S->arena.size()) return WS_ERR_NOMEM;
     Request* r = new (std::nothrow) Request();
     if (!r) return WS_ERR_NOMEM;
     r->cloud = cloud;
@@ -602,10 +600,9 @@ extern "C" int ws_server_destroy(ws_server* S) {
         if (s.done) cudaEventDestroy(s.done);
         if (s.stream) cudaStreamDestroy(s.stream);
         if (s.err_d) cudaFree(s.err_d);
-        if (s.h_jobs) cudaFreeHost(s.h_jobs);
-        if (s.d_jobs) cudaFree(s.d_jobs);
-        if (s.h_items) cudaFreeHost(s.h_items);
-        if (s.d_items) cudaFree(s.d_items);
+        if (s.err_h) cudaFreeHost(s.err_h);
+        if (s.h_table) cudaFreeHost(s.h_table);
+        if (s.d_table) cudaFree(s.d_table);
     }
     for (auto& kv : S->reqs) delete kv.second;
     S->arena.release();

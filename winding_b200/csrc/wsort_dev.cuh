@@ -19,61 +19,53 @@ namespace wsort {
 
 constexpr uint32_t kBuckets = 65536u;     // render/splats.js:64
 constexpr uint32_t kCulled = 0xFFFFFFFFu;
-constexpr int kThreads = 256;             // threads per CTA of every sort kernel
-constexpr int kWarps = kThreads / 32;
 constexpr uint32_t kPadSplats = 4096;     // resident clouds are padded to this multiple
 
 // Error codes a kernel leaves in the context's error word.
-constexpr uint32_t kErrWaitPhase = 1;     // a phase dependency never completed
+constexpr uint32_t kErrWaitPhase = 1;     // a dependency (phase, look-back or copy) never completed
 constexpr uint32_t kErrBounds = 3;        // a scatter position fell outside the output
 
-// Phases of one job, in dependency order. Each waits for the whole of the
-// one before it.
-//   Keys     per tile of splats: cull, key, survivor bit, low-digit counts
-//   ScanLo   per digit: scan over tiles of the low-digit counts
-//   Low      per tile of splats: stable rank by the low key byte, scatter;
-//            in a job that counts its high digits here (red_hi) also adds
-//            each element to the count of its high digit in the output tile
-//            it lands in (one atomic add per run of equal cells in a warp)
-//   CountHi  per two tiles of the low pass's output: high-digit counts
-//            (none in a red_hi job)
-//   ScanHi   per digit: scan over tiles of the high-digit counts
-//   High     per tile of the low pass's output: stable rank by the high
-//            byte, scatter the final order and keys
-constexpr uint32_t kPhaseKeys = 0, kPhaseScanLo = 1, kPhaseLow = 2, kPhaseCountHi = 3, kPhaseScanHi = 4,
-                   kPhaseHigh = 5, kPhases = 6;
-constexpr uint32_t kCountSpan = 2;        // tiles one CountHi item covers
-// A job alone in its launch with at most this many tiles counts its high
-// digits in the low pass (red_hi): a phase fewer on the critical path. In a
-// batch, CountHi items overlap other jobs' work and cost less than the atomic
-// adds; in a larger job of concentrated keys the adds meet on few counts.
-constexpr uint32_t kRedHiTiles = 1024;
-constexpr uint32_t kScanItems = 256;      // scan items per pass of a large job: one per digit value
-constexpr uint32_t kSmallScanTiles = 64;  // a job of at most this many tiles scans in ...
-constexpr uint32_t kSmallScanItems = 8;   // ... this many items per pass, 32 digit values each
+// The sort of one job is three phases, each split into the same segments
+// (contiguous splat ranges of the job, one work item each):
+//   Keys   cull, 16-bit key, survivor bit; the segment's low-digit counts
+//          (published for the look-back) and the job's totals of both digits
+//   Low    after the job's keys: stable rank by the low key byte, scatter
+//          (key, splat index) to the job's intermediate arrays
+//   High   after the job's low pass: a proportional slice of the
+//          intermediate arrays; its high-digit counts, a look-back over the
+//          earlier slices, stable rank by the high byte, scatter the final
+//          order and keys
+constexpr uint32_t kPhaseKeys = 0, kPhaseLow = 1, kPhaseHigh = 2, kPhases = 3;
+constexpr uint32_t kSegAlign = 256;       // segment boundaries are multiples of this (splats)
+constexpr uint32_t kGroup = 16;           // segments per look-back group
+constexpr int kKeysIPT = 4;               // splats per thread in one sub-tile of a keys item
+constexpr int kDigitIPT = 8;              // elements per thread in one sub-tile of a digit pass
+constexpr int kSubHist = 8;               // lane-interleaved sub-histograms for counting
 
-// One (cloud, view) to sort, as the persistent kernel reads it.
+// One (cloud, view) to sort, as the kernel reads it.
 struct alignas(16) JobDesc {
     // cloud (resident)
     const float4* centers;      // x, y, z, colour word bits; padded to kPadSplats
     const float2* cov;          // 6 f32 a splat as 3 float2; padded likewise
     const int8_t* sexp;         // per splat: max |covariance entry| <= 2^sexp; padded likewise
     double bmin[3], bmax[3];    // box around the centres
-    uint32_t n;
-    uint32_t tiles;             // tiles of splats (Keys, Low) = tiles of the low pass's output (High)
-    // Per-view shortcuts the host proves exact (see keys_tile):
+    uint32_t n;                 // elements
+    uint32_t npad;              // n rounded up to kSegAlign: the range the segments cover
+    // Per-view shortcuts the host proves exact (see keys_item):
     uint32_t fast_transform;    // affine model-view, reverse-Z perspective, no overflow possible
     uint32_t keep_byte;         // alpha bytes at or above this pass the footprint cull when ...
     float keep_q;               // ... keep_q 2^sexp <= 100 d^2 (+inf: never)
-    uint32_t scan_items;        // items of each scan phase: kSmallScanItems (small job) or 256 (one per digit)
-    uint32_t kind;              // kJobSplats or kJobParticles
+    uint32_t kind;              // kJobSplats, kJobParticles or kJobKeys
     uint32_t idx_base;          // added to every element index the order holds (a ring's first slot)
     // view: the values the reference writes into its Cloud uniform
     float mv[16];
     float proj[16];
     float viewport[2];
     float cull;
-    uint32_t red_hi;            // 1: the low pass counts the high digits (no CountHi items)
+    // segments
+    uint32_t seg0;              // the launch's index of the job's first segment
+    uint32_t nseg;              // the job's segments
+    uint32_t ngroups;           // look-back groups: ceil(nseg / kGroup)
     // outputs
     uint32_t* order;            // >= n
     uint32_t* keys;             // >= n, or null
@@ -83,9 +75,8 @@ struct alignas(16) JobDesc {
     uint32_t* mask;             // survivor bits, one word per 32 splats
     uint16_t* key_b;            // low pass output: keys
     uint32_t* idx_b;            // low pass output: splat indices
-    uint32_t* cnt_lo;           // 256 x tiles (digit major): low-digit counts, then prefixes over tiles
-    uint32_t* cnt_hi;           // 256 x tiles: the same for the high digit
-    uint32_t* ctl;              // JobCtl
+    uint32_t* agg;              // 2 x nseg x 256: per segment, low-digit then high-digit counts
+    uint32_t* ctl;              // JobCtl, then the look-back words (zeroed before a launch)
     // particles (kind == kJobParticles): one emitter's ring of the pool
     const float4* pool;         // the pool: two float4 a particle (position, age; velocity, lifetime)
     const float* thr;           // kParticleBuckets depth thresholds of the log-depth buckets
@@ -99,8 +90,7 @@ struct alignas(16) JobDesc {
     uint32_t sh_words;          // 32-bit words a splat: ceil(3 x coefficients / 2)
     // given keys (kind == kJobKeys): n 16-bit keys, every element a survivor
     const uint16_t* keys_in;
-    uint32_t hi_items;          // items that publish as CountHi: its own, or the low pass's (red_hi)
-    uint32_t pad1[3];
+    uint32_t pad1[2];
 };
 
 constexpr uint32_t kJobSplats = 0, kJobParticles = 1, kJobKeys = 2;
@@ -108,13 +98,30 @@ constexpr uint32_t kJobSplats = 0, kJobParticles = 1, kJobKeys = 2;
 // 12 bits of log2 depth over [2^-10, 2^20].
 constexpr uint32_t kParticleBuckets = 4096u;
 
-// Per-job counters, zeroed before a launch.
+// Per-job counters, zeroed before a launch. The look-back words follow:
+// gsum[2][ngroups][256] (per group, the sum of its segments' counts: low,
+// high), gdone[ngroups] (high-count items finished, per group) and
+// flag[nseg] (a segment's high-digit counts are published).
 struct JobCtl {
     uint32_t tot[2][256];       // survivors per digit value: low byte, high byte
-    uint32_t done[8];           // items finished, per phase
-    uint32_t pad[8];
+    uint32_t keys_done;         // keys items finished
+    uint32_t low_done;          // low items finished
+    uint32_t pad[14];
 };
 static_assert(sizeof(JobCtl) % 64 == 0, "JobCtl size");
+
+// Bytes of a job's zeroed control region (JobCtl and its look-back words).
+__host__ __device__ inline size_t job_ctl_bytes(uint32_t nseg) {
+    const size_t ng = (nseg + kGroup - 1) / kGroup;
+    const size_t b = sizeof(JobCtl) + (2 * ng * 256 + ng + nseg) * sizeof(uint32_t);
+    return (b + 255) / 256 * 256;
+}
+
+// One job's share of a chunk of a batch: splats [a, b) of job `job`, its
+// segment number `local` among the job's segments.
+struct alignas(16) SegDesc {
+    uint32_t job, a, b, local;
+};
 
 // Per-launch counters, zeroed before a launch.
 struct LaunchCtl {
@@ -123,17 +130,29 @@ struct LaunchCtl {
     uint32_t pad[14];
 };
 
+// What one launch sorts. Work item t is phase first_phase + t / nseg of
+// segment t % nseg: every segment's keys, then every low pass, then every
+// high pass. Segments come from `segs`, or, for a launch of one job
+// (segs null), are the job's consecutive ranges of `chunk` splats.
+struct LaunchDesc {
+    const JobDesc* jobs;
+    const SegDesc* segs;
+    uint32_t nseg;              // segments in the launch
+    uint32_t chunk;             // one job: splats a segment covers
+    uint32_t first_phase;       // phases before it are left out (the failure self-test)
+    uint32_t spin_limit;        // polls a wait makes before it gives up
+    struct LaunchCtl* lctl;
+    uint32_t* err;              // code, work item
+    struct TraceRec* trace;     // or null
+};
+
 // One work item's timeline, when tracing: globaltimer ns at the claim of its
 // ticket, after its dependency wait, and at its end; and the SM it ran on.
 struct TraceRec {
     uint64_t claim, start, end;
     uint32_t item, sm;
-    uint64_t mark[3];           // digit passes: inputs staged, ranked, staged for writing
+    uint64_t mark[3];           // phase-specific points inside the item (0: none)
 };
-
-// Work item: x = job, y = phase << 29 | tile.
-constexpr uint32_t kPhaseShift = 29;
-constexpr uint32_t kTileMask = (1u << kPhaseShift) - 1;
 
 // ---------------------------------------------------------------- f32 ops
 __device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }

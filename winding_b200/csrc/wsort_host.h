@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "wsort.h"
+#include "wsort_dev.cuh"
 
 namespace wsort {
 
@@ -41,6 +42,33 @@ constexpr uint32_t kCloudMagic = 0x57534F52u;   // "WSOR"
 int set_error(ws_ctx* ctx, int code, const char* fmt, ...);
 int cuda_error(ws_ctx* ctx, cudaError_t e, const char* what);
 
+// How one launch's jobs are cut into segments, and where its scratch lies.
+struct LaunchShape {
+    int threads = 1024;                 // per CTA: 1024 (one CTA an SM) or 512 (two)
+    int grid = 0;                       // CTAs launched
+    uint32_t chunk = 0;                 // splats a chunk covers
+    bool regular = false;               // one job: the kernel computes its segments
+    std::vector<SegDesc> segs;          // every segment, in launch order
+    std::vector<uint32_t> nseg, seg0;   // per job
+    std::vector<size_t> ctl_off;        // per job: its control region, from the scratch base
+    std::vector<size_t> arr_off;        // per job: its arrays, from the scratch base
+    size_t ctl_bytes = 0;               // LaunchCtl and every control region: zeroed before a launch
+    size_t bytes = 0;                   // the whole scratch
+};
+
+// The launch of `njobs` jobs of ns[j] elements with parameters p on a GPU
+// of `sms` SMs.
+void shape_launch(const uint32_t* ns, int njobs, const ws_params& p, int sms, LaunchShape& S);
+// Job j's segment fields and scratch pointers (n elements) in `scratch`.
+void place_job(JobDesc& d, uint32_t n, int j, const LaunchShape& S, char* scratch);
+// Bytes of the table a launch reads: the jobs, then (unless regular) the segments.
+size_t table_bytes(int njobs, const LaunchShape& S);
+void write_table(void* dst, const JobDesc* jobs, int njobs, const LaunchShape& S);
+LaunchDesc launch_desc(const void* d_table, int njobs, const LaunchShape& S, char* scratch, uint32_t* err,
+                       uint32_t spin_limit, TraceRec* trace);
+cudaError_t launch_sort(const LaunchDesc& L, int threads, int grid, cudaStream_t stream);
+int sort_occupancy(int threads);
+
 }  // namespace wsort
 
 struct ws_ctx {
@@ -56,11 +84,10 @@ struct ws_ctx {
     wsort::DevBuf scratch, jobs_d, items_d, out_d;
     wsort::HostBuf jobs_h, items_h, count_h;
     uint32_t* err_d = nullptr;        // sticky device error: code, work item
-    std::vector<uint2> items;
+    wsort::LaunchShape shape;         // the last launch's shape, reused while ns and params repeat
     std::vector<uint32_t> last_ns;
-    uint32_t last_tile = 0;
-    bool items_valid = false;
-    int occupancy[3][5] = {};         // resident sort CTAs per SM, by tile and variant (2..6)
+    ws_params last_params{};
+    bool shape_valid = false;
     uint64_t launches = 0;
     // kernel timing (ws_timing): event pairs recorded around each launch
     bool timing = false;
@@ -70,7 +97,8 @@ struct ws_ctx {
     // item tracing (ws_trace): the last traced launch's records and items
     bool tracing = false;
     wsort::DevBuf trace_d;
-    std::vector<uint2> trace_items;
+    std::vector<wsort::SegDesc> trace_segs;
+    uint32_t trace_first_phase = 0;
     int trace_grid = 0;
     std::vector<struct ws_cloud*> freed;   // freed clouds, kept as refusable handles
     wsort::DevBuf thr_d;              // particle depth thresholds, uploaded on first use

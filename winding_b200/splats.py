@@ -88,7 +88,11 @@ class Context:
         self.check(self.lib.ws_get_params(self.handle, ctypes.byref(p)))
         return p
 
-    def set_params(self, tile=None, ctas_per_sm=None, spin_limit=None) -> None:
+    def set_params(self, tile=None, ctas_per_sm=None, spin_limit=None, segs_per_cta=None) -> None:
+        """Kernel parameters (ws_params): tile = the least splats a segment
+        covers, ctas_per_sm = 1 (1024-thread CTAs) or 2 (512-thread),
+        segs_per_cta = segments per resident CTA, spin_limit = polls before a
+        device-side wait gives up."""
         p = self.params
         if tile is not None:
             p.tile = tile
@@ -96,6 +100,8 @@ class Context:
             p.ctas_per_sm = ctas_per_sm
         if spin_limit is not None:
             p.spin_limit = spin_limit
+        if segs_per_cta is not None:
+            p.segs_per_cta = segs_per_cta
         self.check(self.lib.ws_set_params(self.handle, ctypes.byref(p)))
 
     def load(self, data) -> "Splats":
@@ -197,13 +203,13 @@ class Context:
 
     def trace_read(self) -> np.ndarray:
         """The last traced launch's work items as a structured array
-        (claim_ns, start_ns, end_ns, job, phase, tile, sm, mark_ns)."""
+        (claim_ns, start_ns, end_ns, job, phase, segment, sm, mark_ns)."""
         n = ctypes.c_size_t()
         self.check(self.lib.ws_trace_read(self.handle, None, 0, ctypes.byref(n)))
         recs = (_lib.WsTraceRec * max(n.value, 1))()
         self.check(self.lib.ws_trace_read(self.handle, recs, n.value, ctypes.byref(n)))
         dt = np.dtype([("claim_ns", "<u8"), ("start_ns", "<u8"), ("end_ns", "<u8"), ("job", "<u4"),
-                       ("phase", "<u4"), ("tile", "<u4"), ("sm", "<u4"), ("mark_ns", "<u8", (3,))])
+                       ("phase", "<u4"), ("segment", "<u4"), ("sm", "<u4"), ("mark_ns", "<u8", (3,))])
         return np.frombuffer(bytes(recs), dtype=dt, count=n.value).copy()
 
     # device buffers, for callers without torch
