@@ -1,11 +1,12 @@
 """Writes the golden fixtures of the parity tests (run from the repo root):
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [path/to/demo/cactus.splat]
 
 Each case is a small seeded cloud from winding_b200.workloads with one view,
 or a seeded subset of the reference's real capture (demo/cactus.splat, a
-3D Gaussian Splatting scan by Steam Studio released CC0, read from the
-reference checkout when it is present) with a framing or a posed view;
+3D Gaussian Splatting scan by Steam Studio released CC0, read from the path
+given as the first argument, the file in a checkout of the reference; without
+it those two fixtures are left as they are) with a framing or a posed view;
 the expected survivor order and keys come from the CPU oracle (oracle/), which
 is itself cross-checked against a second restatement (oracle/pyoracle.py) and
 the reference's known-answer tests in tests/test_oracle.py. Stored per case:
@@ -24,16 +25,15 @@ from oracle import oracle  # noqa: E402
 from winding_b200 import workloads as W  # noqa: E402
 
 CULLS = (0.0, 0.5)
-CACTUS = "/root/reference/demo/cactus.splat"
 CACTUS_SUBSET = 16384
 
 
-def cactus_cases():
+def cactus_cases(path):
     """Two seeded subsets of the capture (records kept in file order): one
     seen from +z at the fitted distance, one from a seeded direction."""
-    if not os.path.exists(CACTUS):
+    if not path or not os.path.exists(path):
         return
-    rec = np.fromfile(CACTUS, dtype=W.RECORD)
+    rec = np.fromfile(path, dtype=W.RECORD)
     for name, seed, posed in (("cactus_front_16384", 21, False), ("cactus_posed_16384", 22, True)):
         rng = np.random.default_rng(seed)
         sub = rec[np.sort(rng.choice(len(rec), CACTUS_SUBSET, replace=False))]
@@ -48,18 +48,19 @@ def cactus_cases():
         yield name, W.Job(sub, view, "capture")
 
 
-def cases():
+def cases(capture=None):
     yield "uniform_3000", W.uniform_100k(seed=11, n=3000)
     yield "clusters_3000", W.clusters_1m(seed=12, n=3000)
     yield "slab_4000", W.slab_6m(seed=13, n=4000)
     rng = np.random.default_rng(14)
     rec = W.scene("cluster", 2500, 15)
     yield "posed_2500", W.Job(rec, W.View(W.random_pose(rng), W.perspective(W.FOV_Y, W.ASPECT, W.NEAR)), "cluster")
-    yield from cactus_cases()
+    yield from cactus_cases(capture)
 
 
 def main():
-    for name, job in cases():
+    capture = sys.argv[1] if len(sys.argv) > 1 else None
+    for name, job in cases(capture):
         parsed = oracle.parse_splat(job.bytes())
         out = {
             "records": np.frombuffer(job.bytes(), np.uint8),

@@ -175,10 +175,30 @@ def scene(kind: str, n: int, seed: int) -> np.ndarray:
 KINDS = ("cluster", "slab", "uniform")
 
 
+def scaled_counts(rng: np.random.Generator, jobs: int, lo: int, hi: int, total: int) -> np.ndarray:
+    """`jobs` counts drawn log-uniform in [lo, hi], then scaled by one common
+    factor (each clipped to [lo, hi]) so that they add up to `total`: the
+    draw's shape, the workload's stated size."""
+    raw = np.exp(rng.uniform(math.log(lo), math.log(hi), size=jobs))
+    a, b = 1e-3, 1e3
+    for _ in range(200):
+        f = math.sqrt(a * b)
+        if np.clip(raw * f, lo, hi).sum() < total:
+            a = f
+        else:
+            b = f
+    counts = np.clip(np.floor(raw * math.sqrt(a * b)), lo, hi).astype(np.int64)
+    counts[int(np.argmin(counts))] += total - int(counts.sum())   # the rounding remainder, on the smallest job
+    return counts
+
+
 def mixed_64(seed: int = 3, jobs: int = 64, lo: int = 10_000, hi: int = 2_000_000,
-             cull: float = 0.5) -> list[Job]:
+             cull: float = 0.5, total: int = 25_000_000) -> list[Job]:
+    """64 (scene, view) jobs of about 25M splats in all: counts log-uniform in
+    [10k, 2M] scaled to the total, scenes cycling cluster / slab / uniform,
+    cameras on spheres of radius 20-60 looking at the origin."""
     rng = np.random.default_rng(seed)
-    counts = np.exp(rng.uniform(math.log(lo), math.log(hi), size=jobs)).astype(np.int64)
+    counts = scaled_counts(rng, jobs, lo, hi, total)
     proj = perspective(FOV_Y, ASPECT, NEAR)
     out = []
     for j in range(jobs):
