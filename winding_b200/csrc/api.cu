@@ -273,6 +273,56 @@ void view_shortcuts(const ws_view& v, const ws_cloud* c, uint32_t* fast, uint32_
     *keep_q = qf;
 }
 
+double host_depth_range(const float mv[16], const double bmin[3], const double bmax[3], int* visible,
+                        float* depth_min, float* depth_scale);
+
+// The view's constants for the keys phase, computed here once per job with
+// the same IEEE operations (f32 products and quotients, the FP64 depth range;
+// built with -ffp-contract=off) as the device's make_consts.
+void fill_view_consts(JobDesc& d) {
+    ViewConsts& c = d.vc;
+    std::memset(&c, 0, sizeof(c));
+    for (int k = 0; k < 16; ++k) {
+        c.mv[k] = d.mv[k];
+        c.proj[k] = d.proj[k];
+    }
+    const float p0 = d.proj[0], p5 = d.proj[5];
+    c.fx = (p0 * d.viewport[0]) * 0.5f;
+    c.fy = (p5 * d.viewport[1]) * 0.5f;
+    c.xlo = -1.3f / p0;
+    c.xhi = 1.3f / p0;
+    c.ylo = -1.3f / p5;
+    c.yhi = 1.3f / p5;
+    c.cull = d.cull;
+    c.persp = d.proj[15] == 0.0f;
+    c.keep_q = d.keep_q;
+    c.keep_byte = d.keep_byte;
+    c.fast = d.fast_transform != 0;
+    host_depth_range(d.mv, d.bmin, d.bmax, &c.visible, &c.depth_min, &c.depth_scale);
+    // makeKeys drops a splat when unpack4x8unorm(colour).a * 255 <= 1
+    // (render/splats.js:169-170): alpha = byte / 255 rounded to f32, so the
+    // test is monotone in the byte and is a threshold on it.
+    c.faint_max = 0;
+    for (uint32_t b = 0; b < 256; ++b) {
+        const float alpha = (float)b / 255.0f;
+        if (alpha * 255.0f <= 1.0f) c.faint_max = b;
+    }
+    // The footprint bound's constants, each rounded up by a relative 1e-4
+    // (far more than the rounding of the few operations that form them).
+    auto up = [](double v) {
+        const float f = (float)(std::fabs(v) * 1.0001);
+        return std::isfinite(f) ? f : INFINITY;
+    };
+    const float* M = d.mv;
+    c.afx = up(c.fx);
+    c.afy = up(c.fy);
+    c.r0 = up(std::fabs((double)M[0]) + std::fabs((double)M[4]) + std::fabs((double)M[8]));
+    c.r1 = up(std::fabs((double)M[1]) + std::fabs((double)M[5]) + std::fabs((double)M[9]));
+    c.r2 = up(std::fabs((double)M[2]) + std::fabs((double)M[6]) + std::fabs((double)M[10]));
+    c.xcap = up(c.xhi);
+    c.ycap = up(c.yhi);
+}
+
 // Emitter jobs (ws_sort_particles): the ring, the view and the outputs.
 static void layout_emitters(JobDesc* out, const ws_emitter* em, int njobs, const LaunchShape& S, char* scratch,
                             const float* thr) {
@@ -315,6 +365,7 @@ void layout_jobs(JobDesc* out, const ws_job* jobs, int njobs, const LaunchShape&
         d.keys = jobs[j].keys;
         d.count = jobs[j].count;
         view_shortcuts(jobs[j].view, c, &d.fast_transform, &d.keep_byte, &d.keep_q);
+        fill_view_consts(d);
         place_job(d, c->n, j, S, scratch);
     }
 }
@@ -429,7 +480,7 @@ static int launch_jobs(ws_ctx* ctx, const std::vector<uint32_t>& ns, int njobs, 
         ctx->trace_grid = (int)std::min<size_t>(S.grid, S.segs.size());
     }
     const LaunchDesc L = launch_desc(ctx->jobs_d.p, njobs, S, scratch, ctx->err_d, P.spin_limit, trace);
-    e = launch_sort(L, S.threads, (int)std::min<size_t>(S.grid, S.segs.size()), stream);
+    e = launch_sort(L, S.threads, (int)std::min<size_t>(S.grid, S.segs.size()), ctx->sms, stream);
     if (e != cudaSuccess) return cuda_error(ctx, e, "ws_sort launch");
     if (t_stop) cudaEventRecord(t_stop, stream);
     cudaEventRecord(ctx->launched, stream);
@@ -949,7 +1000,7 @@ extern "C" int ws_selftest_wait(ws_ctx* ctx, uint32_t spin_limit) {
         return cuda_error(ctx, e, "ws_selftest_wait");
     LaunchDesc L = launch_desc(ctx->jobs_d.p, 1, S, base, ctx->err_d, spin_limit, nullptr);
     L.first_phase = kPhaseLow;
-    e = launch_sort(L, S.threads, 2, ctx->stream);
+    e = launch_sort(L, S.threads, 2, ctx->sms, ctx->stream);
     if (e != cudaSuccess) return cuda_error(ctx, e, "ws_selftest_wait launch");
     if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return cuda_error(ctx, e, "ws_selftest_wait");
     return take_device_error(ctx);
@@ -1185,7 +1236,7 @@ extern "C" int ws_plan_create(ws_ctx* ctx, int njobs, const ws_job* jobs, ws_pla
         cudaMemsetAsync(p->scratch.p, 0, S.ctl_bytes, cs);
         const LaunchDesc L = launch_desc(p->jobs_d.p, njobs, S, static_cast<char*>(p->scratch.p), ctx->err_d,
                                          P.spin_limit, nullptr);
-        launch_sort(L, S.threads, (int)std::min<size_t>(S.grid, S.segs.size()), cs);
+        launch_sort(L, S.threads, (int)std::min<size_t>(S.grid, S.segs.size()), ctx->sms, cs);
         e = cudaStreamEndCapture(cs, &p->graph);
     }
     if (e == cudaSuccess) e = cudaGraphInstantiate(&p->exec, p->graph, 0);
@@ -1216,6 +1267,7 @@ extern "C" int ws_plan_set_views(ws_plan* p, const ws_view* views) {
         hj[j].cull = views[j].cull;
         // The culling shortcuts are proved for one view: prove them again.
         view_shortcuts(views[j], p->jobs[j].cloud, &hj[j].fast_transform, &hj[j].keep_byte, &hj[j].keep_q);
+        fill_view_consts(hj[j]);
         p->jobs[j].view = views[j];
     }
     return WS_OK;

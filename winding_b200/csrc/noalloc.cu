@@ -132,7 +132,7 @@ extern "C" int ws_sort_noalloc(const ws_cloud* cloud, const ws_view* view, uint3
     if (e == cudaSuccess) {
         const LaunchDesc L = launch_desc(base + kJobOffset, 1, S, base, reinterpret_cast<uint32_t*>(base + kErrOffset),
                                          kSpinLimit, nullptr);
-        e = launch_sort(L, S.threads, (int)std::min<size_t>(S.grid, S.segs.size()), stream);
+        e = launch_sort(L, S.threads, (int)std::min<size_t>(S.grid, S.segs.size()), cloud->ctx->sms, stream);
     }
     if (e == cudaSuccess) {
         noalloc_check_kernel<<<1, 1, 0, stream>>>(count);

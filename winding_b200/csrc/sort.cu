@@ -50,46 +50,48 @@
 
 namespace wsort {
 
+// Shared memory of a keys CTA (NT threads).
 template <int NT>
-struct SortSmem {
-    static constexpr int W = NT / 32;
+struct KeysSmem {
     static constexpr int TK = NT * kKeysIPT;     // splats of a keys sub-tile
-    static constexpr int TD = NT * kDigitIPT;    // elements of a digit-pass sub-tile
-    alignas(8) uint64_t bar[2];                  // the keys staging buffers' mbarriers
+    alignas(8) uint64_t bar[2];                  // the staging buffers' mbarriers
     float alpha[256];                            // unpack4x8unorm(..).a: byte / 255, correctly rounded
     ViewConsts vc;
-    int vc_job;                                  // job whose constants vc holds
     uint32_t next;                               // the ticket this CTA works on next
+    uint32_t drain;
+    uint32_t abort;
+    uint32_t pending;                            // staging buffers with a copy in flight (bits)
+    uint32_t qn;
+    uint64_t mark[3];                            // tracing: timestamps inside an item
+    uint32_t hist[kSubHist][512];                // low digit at [s][..256), high at [s][256..)
+    uint32_t queue[2 * TK];                      // splats whose footprint must be evaluated
+    alignas(128) float4 centers[2][TK];
+    int8_t sexp[2][TK];
+};
+
+// Shared memory of a digit-pass CTA (NT threads).
+template <int NT>
+struct DigitSmem {
+    static constexpr int W = NT / 32;
+    static constexpr int TD = NT * kDigitIPT;    // elements of a sub-tile
+    uint32_t next;
     uint32_t drain;
     uint32_t abort;
     uint32_t total;                              // survivors of the item's job
     uint32_t tile_total;                         // elements of the current sub-tile
-    uint32_t pending;                            // staging buffers with a copy in flight (bits)
     uint32_t scan[W];
-    uint64_t mark[3];                            // tracing: timestamps inside an item
+    uint64_t mark[3];
     uint32_t dstart[256];                        // start of each digit in the pass's output
     uint32_t gbase[256];                         // dstart plus the segments before this one
     uint32_t run[256];                           // placed by the item's earlier sub-tiles
     uint32_t gofs[256];                          // gbase + run - sub-tile start, per digit
     uint32_t lstart[256];                        // sub-tile start of each digit
     uint32_t part[NT / 256][256];                // partial sums of the look-back
-    union alignas(128) U {
-        struct K {
-            float4 centers[2][TK];
-            int8_t sexp[2][TK];
-            uint32_t maskw[TK / 32];             // survivor bits of the sub-tile
-            uint16_t queue[TK];                  // splats whose footprint must be evaluated
-            uint32_t qn;
-            uint32_t hist[kSubHist][512];        // low digit at [s][..256), high at [s][256..)
-        } k;
-        struct P {
-            uint32_t wmask[W][256];              // per warp and digit: lanes of the round
-            uint16_t wcnt[W][256];               // per warp and digit: count, then the warp's start
-            uint16_t skey[TD];                   // the sub-tile staged in output order
-            uint32_t sidx[TD];
-            uint32_t hist[kSubHist][256];        // high pass: the segment's counts
-        } p;
-    } u;
+    uint32_t wmask[W][256];                      // per warp and digit: lanes of the round
+    uint16_t wcnt[W][256];                       // per warp and digit: count, then the warp's start
+    uint16_t skey[TD];                           // the sub-tile staged in output order
+    uint32_t sidx[TD];
+    uint32_t hist[kSubHist][256];                // high pass: the segment's counts
 };
 
 // The index of digit d's counter in sub-histogram s: rotated by 4 s, so that
@@ -157,7 +159,7 @@ struct KeysStage {
 // Waits (bounded) for buffer b's copy. Every thread calls it and flips its
 // own copy of the parity bit. False if the wait gave up.
 template <int NT>
-__device__ __forceinline__ bool stage_wait(SortSmem<NT>& sm, KeysStage& ks, uint32_t b, const LaunchDesc& L,
+__device__ __forceinline__ bool stage_wait(KeysSmem<NT>& sm, KeysStage& ks, uint32_t b, const LaunchDesc& L,
                                            uint32_t item) {
     const uint32_t par = (ks.parity >> b) & 1u;
     uint32_t spins = 0;
@@ -175,8 +177,8 @@ __device__ __forceinline__ bool stage_wait(SortSmem<NT>& sm, KeysStage& ks, uint
 
 // Waits (thread 0, bounded) until *p >= need. Returns false, uniformly
 // across the CTA, if the wait gave up (or another CTA raised an error).
-template <int NT>
-__device__ bool wait_count(const uint32_t* p, uint32_t need, SortSmem<NT>& sm, const LaunchDesc& L, uint32_t item) {
+template <class SM>
+__device__ bool wait_count(const uint32_t* p, uint32_t need, SM& sm, const LaunchDesc& L, uint32_t item) {
     if (threadIdx.x == 0) {
         uint32_t spins = 0;
         sm.abort = 0;
@@ -196,7 +198,7 @@ __device__ bool wait_count(const uint32_t* p, uint32_t need, SortSmem<NT>& sm, c
 // The start of each digit in a pass's output: an exclusive scan of the job's
 // 256 digit totals into sm.dstart, their sum into sm.total.
 template <int NT>
-__device__ void digit_starts(const uint32_t* tot, SortSmem<NT>& sm) {
+__device__ void digit_starts(const uint32_t* tot, DigitSmem<NT>& sm) {
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     uint32_t v = 0, x = 0;
     if (tid < 256) {
@@ -230,7 +232,7 @@ __device__ void digit_starts(const uint32_t* tot, SortSmem<NT>& sm) {
 // of segments g kGroup .. ls-1 (all published before this is called).
 template <int NT>
 __device__ void segment_prefix(const uint32_t* gsum, const uint32_t* agg, uint32_t g, uint32_t ls,
-                               SortSmem<NT>& sm) {
+                               DigitSmem<NT>& sm) {
     constexpr uint32_t P = NT / 256;
     const uint32_t d = threadIdx.x & 255u, p = threadIdx.x >> 8;
     const uint32_t g0 = g * kGroup;
@@ -255,19 +257,31 @@ __device__ void segment_prefix(const uint32_t* gsum, const uint32_t* agg, uint32
 
 // ---------------------------------------------------------------- keys
 //
-// Footprint shortcut (exact): for a perspective view the host proves
-// keep_q 2^sexp <= 100 d^2 implies every entry of |T| |Sigma| |T|^T is at most
-// 100 (T = J W, d = -view.z, sexp the splat's covariance exponent bound), and
-// then the pinned computation of the area cannot fall below 1.85, whatever
-// the rounding: the 2D covariance differs from a positive semi-definite one
-// by at most 7.1 u * 100 per entry, which moves (xx + .3)(yy + .3) - xy^2 at
-// most 0.0025 below 0.09. So alpha * area >= RN(alpha * 1.85) >= cull for
-// every alpha byte >= keep_byte, and such a splat is kept without its
-// footprint (or its covariance) being computed. The same analysis bounds the
-// pinned area from above for any G = the largest entry of |T| |Sigma| |T|^T
-// (G <= 1.002 keep_q 2^sexp / d^2): every 2D entry is at most G (1 + 8.2u),
-// so the area is at most 2 pi (1.00001 G + 0.3)(1 + 5u); a splat with alpha
-// times that below cull is culled, again without its footprint.
+// Footprint shortcut (exact). makeKeys culls a splat when
+// RN(alpha * area) < cull, area = 2 pi sqrt(max(det, 0)), det =
+// (xx + .3)(yy + .3) - xy^2 of the pinned 2D covariance T Sigma T^T
+// (render/splats.js:102-124, :174-178). For a perspective view, with
+// d = -view.z: |J00| = |fx| / d, |J02| = |fx| |x'| / d where |x'| =
+// min(|view.x| / d, 1.3 / |p00|) is the clamped slope, and likewise for row 1;
+// so the absolute row sums of T = J W are at most A = |fx| / d (r0 + |x'| r2)
+// and B = |fy| / d (r1 + |y'| r2), r_k the absolute row sums of the
+// model-view's 3x3, and with every |Sigma_ij| <= m = 2^sexp, every entry of
+// |T| |Sigma| |T|^T in row 0 is at most A^2 m and in row 1 at most B^2 m. The
+// kernel evaluates these bounds with approximate operations and a 1.002
+// margin (far above their few ulps, and the few ulps by which the pinned T
+// exceeds the real one), giving ga, gb.
+//  * Kept: if ga, gb <= 100, the pinned 2D covariance differs from a positive
+//    semi-definite one by at most 7.1 u * 100 per entry, which moves det at
+//    most 0.0025 below 0.09; so area >= 1.85 whatever the rounding, and every
+//    alpha byte >= keep_byte (RN(alpha * 1.85) >= cull, proved by the host)
+//    is kept without its footprint (or its covariance) being computed.
+//  * Culled: each pinned entry is at most g (1 + 8.2u) and the pinned area at
+//    most 2 pi sqrt((ga (1 + 8.2u) + .3)(gb (1 + 8.2u) + .3)) (1 + 5u). The
+//    kernel compares the square of alpha times that, with a further 1.0002
+//    (which also covers the rounding of the comparison's own few operations
+//    and of cull^2), against cull^2; below it, RN(alpha * area) < cull and
+//    the splat is culled, again without its footprint.
+// Splats that neither test decides are queued for the pinned computation.
 
 // Counts a survivor's two digits into the lane's sub-histograms.
 __device__ __forceinline__ void count_key(uint32_t* hist, uint32_t key, uint32_t s) {
@@ -276,104 +290,91 @@ __device__ __forceinline__ void count_key(uint32_t* hist, uint32_t key, uint32_t
 }
 
 // Sweep 1 of a keys sub-tile: tests, keys and the footprint shortcut. Every
-// splat's key slot is written now (the passes read only the slots whose
-// survivor bit is set), with the survivor bits and digit counts of the
-// splats already decided; the ones whose footprint must still be evaluated
-// go to a queue. kFast: the fast transform, the view's constants in
-// registers (FastView).
+// splat's key slot and survivor word are written now (the passes read only
+// the slots whose survivor bit is set), with the digit counts of the splats
+// already decided; the ones whose footprint must still be evaluated go to
+// the queue. Every test is evaluated for every splat and combined as
+// predicates, so a warp does not split on the data. kFast: the fast
+// transform, the view's constants in registers (FastView).
 template <bool kFast, int NT>
-__device__ __forceinline__ void keys_sweep(const ViewConsts& c, SortSmem<NT>& sm, uint32_t buf, uint32_t base,
-                                           uint32_t cnt, uint32_t n, bool fp, uint16_t* k16) {
+__device__ __forceinline__ void keys_sweep(const ViewConsts& c, KeysSmem<NT>& sm, uint32_t buf, uint32_t base,
+                                           uint32_t cnt, uint32_t n, bool fp, uint16_t* k16, uint32_t* mask) {
     const uint32_t tid = threadIdx.x, lane = tid & 31u;
     const uint32_t s = lane & (kSubHist - 1);
     FastView fv;
     if constexpr (kFast) fv = fast_view_of(c);
     const bool persp = c.persp;
-    const float keep_q = c.keep_q, cull = c.cull;
-    const uint32_t keep_byte = c.keep_byte;
-    const float4* centers = sm.u.k.centers[buf];
-    const int8_t* sexp = sm.u.k.sexp[buf];
-#pragma unroll
+    const float cull = c.cull;
+    const float afx = c.afx, afy = c.afy, r0 = c.r0, r1 = c.r1, r2 = c.r2, xcap = c.xcap, ycap = c.ycap;
+    const uint32_t keep_byte = c.keep_byte, faint_max = c.faint_max;
+    const float4* centers = sm.centers[buf];
+    const int8_t* sexp = sm.sexp[buf];
+#pragma unroll 1
     for (int r = 0; r < kKeysIPT; ++r) {
         const uint32_t at = (uint32_t)r * NT + tid;
         if (at >= cnt) break;   // uniform across the warp: cnt is a multiple of 32
-        uint32_t key = 0;
-        bool kept = false, pending = false;
-        if (base + at < n) {
-            const float4 p = centers[at];
-            float view[4];
-            bool inside;
-            if constexpr (kFast) {
-                fast_view(fv, p.x, p.y, p.z, view);
-                inside = fast_in_frustum(fv, view);
-            } else {
-                view_of(c, p.x, p.y, p.z, view);
-                inside = in_frustum(c, view);
-            }
-            if (inside) {
-                const uint32_t byte = __float_as_uint(p.w) >> 24;
+        const float4 p = centers[at];
+        float view[4];
+        bool inside;
+        uint32_t key;
+        if constexpr (kFast) {
+            fast_view(fv, p.x, p.y, p.z, view);
+            inside = fast_in_frustum(fv, view);
+            key = fast_depth_key(fv, view);
+        } else {
+            view_of(c, p.x, p.y, p.z, view);
+            inside = in_frustum(c, view);
+            key = depth_key(c, view);
+        }
+        const uint32_t byte = __float_as_uint(p.w) >> 24;
+        // too faint to reach 1/255 at or below faint_max
+        bool kept = base + at < n && inside && byte > faint_max;
+        bool pending = false;
+        if (fp) {
+            bool keep_sc = false, cull_sc = false;
+            if (persp) {
                 const float alpha = sm.alpha[byte];
-                if (!(fmul(alpha, 255.0f) <= 1.0f)) {   // else too faint to reach 1/255
-                    if constexpr (kFast)
-                        key = fast_depth_key(fv, view);
-                    else
-                        key = depth_key(c, view);
-                    kept = true;
-                    if (fp) {
-                        bool decided = false;
-                        if (persp) {
-                            const float d = -view[2];
-                            // keep_q 2^sexp, exactly: sexp is in [-100, 127] and
-                            // keep_q >= 2^-20, so the product is a normal float
-                            // (or +inf).
-                            const float pow2 = __int_as_float((int(sexp[at]) + 127) << 23);
-                            const float q = fmul(keep_q, pow2);
-                            const float dd = fmul(d, d);
-                            if (byte >= keep_byte && q <= fmul(100.0f, dd)) {
-                                decided = true;   // kept
-                            } else if (dd > 1e-30f && dd < 1e30f && q < 1e30f) {
-                                // An upper bound of G: the approximate quotient is
-                                // within a few ulps, far inside the 1.002 margin.
-                                const float g = fmul(1.002f, __fdividef(q, dd));
-                                const float top =
-                                    fmul(fmul(fmul(alpha, 6.2832f), fadd(fmul(g, 1.00001f), 0.3f)), 1.0001f);
-                                if (top < cull) {
-                                    kept = false;
-                                    decided = true;
-                                }
-                            }
-                        }
-                        if (!decided) {
-                            kept = false;
-                            pending = true;
-                        }
-                    }
-                }
+                const float d = -view[2];
+                // The splat's covariance bound 2^sexp, exactly (sexp is in
+                // [-100, 127]).
+                const float m = __int_as_float((int(sexp[at]) + 127) << 23);
+                // A, B and ga, gb of the shortcut above, from this splat's
+                // own position.
+                const float rd = __fdividef(1.0f, d);
+                const float ax = fminf(fabsf(view[0]) * rd, xcap), ay = fminf(fabsf(view[1]) * rd, ycap);
+                const float A = afx * rd * (r0 + ax * r2), B = afy * rd * (r1 + ay * r2);
+                const float ga = 1.002f * (A * A) * m, gb = 1.002f * (B * B) * m;
+                keep_sc = byte >= keep_byte && ga <= 100.0f && gb <= 100.0f;
+                const float t = alpha * 6.2832f;
+                const float top2 = t * t * ((ga * 1.00001f + 0.3f) * (gb * 1.00001f + 0.3f)) * 1.0002f;
+                cull_sc = !keep_sc && top2 < cull * cull;
             }
+            pending = kept && !keep_sc && !cull_sc;
+            kept = kept && keep_sc;
         }
         k16[base + at] = (uint16_t)key;
         const uint32_t kb = __ballot_sync(0xffffffffu, kept);
-        if (lane == 0) sm.u.k.maskw[at >> 5] = kb;
-        if (kept) count_key(&sm.u.k.hist[0][0], key, s);
+        if (lane == 0) mask[(base + at) >> 5] = kb;
+        if (kept) count_key(&sm.hist[0][0], key, s);
         const uint32_t pend = __ballot_sync(0xffffffffu, pending);
         if (pend) {
             uint32_t first = 0;
-            if (lane == (uint32_t)(__ffs(pend) - 1)) first = atomicAdd(&sm.u.k.qn, (uint32_t)__popc(pend));
+            if (lane == (uint32_t)(__ffs(pend) - 1)) first = atomicAdd(&sm.qn, (uint32_t)__popc(pend));
             first = __shfl_sync(0xffffffffu, first, __ffs(pend) - 1);
-            if (pending) sm.u.k.queue[first + __popc(pend & lanemask_lt())] = (uint16_t)at;
+            if (pending) sm.queue[first + __popc(pend & lanemask_lt())] = base + at;
         }
     }
 }
 
 // Issues the bulk copies of one keys sub-tile into staging buffer b (thread 0).
 template <int NT>
-__device__ __forceinline__ void stage_issue(const JobDesc& J, SortSmem<NT>& sm, uint32_t b, uint32_t base,
+__device__ __forceinline__ void stage_issue(const JobDesc& J, KeysSmem<NT>& sm, uint32_t b, uint32_t base,
                                             uint32_t cnt, bool fp) {
     fence_proxy_async();
     const uint32_t bytes = cnt * 16u + (fp ? cnt : 0u);
     mbar_expect_tx(&sm.bar[b], bytes);
-    bulk_copy(sm.u.k.centers[b], J.centers + base, cnt * 16u, &sm.bar[b]);
-    if (fp) bulk_copy(sm.u.k.sexp[b], J.sexp + base, cnt, &sm.bar[b]);
+    bulk_copy(sm.centers[b], J.centers + base, cnt * 16u, &sm.bar[b]);
+    if (fp) bulk_copy(sm.sexp[b], J.sexp + base, cnt, &sm.bar[b]);
     sm.pending |= 1u << b;
 }
 
@@ -381,7 +382,7 @@ __device__ __forceinline__ void stage_issue(const JobDesc& J, SortSmem<NT>& sm, 
 // low pass's look-back), its group's sum, the job's totals of both digits;
 // then the item's completion.
 template <int NT>
-__device__ void keys_publish(const JobDesc& J, uint32_t ls, SortSmem<NT>& sm) {
+__device__ void keys_publish(const JobDesc& J, uint32_t ls, KeysSmem<NT>& sm) {
     JobCtl* ctl = reinterpret_cast<JobCtl*>(J.ctl);
     __syncthreads();
     const uint32_t d = threadIdx.x;
@@ -389,8 +390,8 @@ __device__ void keys_publish(const JobDesc& J, uint32_t ls, SortSmem<NT>& sm) {
         uint32_t lo = 0, hi = 0;
 #pragma unroll
         for (uint32_t s = 0; s < (uint32_t)kSubHist; ++s) {
-            lo += sm.u.k.hist[s][sub_slot(s, d)];
-            hi += sm.u.k.hist[s][256u + sub_slot(s, d)];
+            lo += sm.hist[s][sub_slot(s, d)];
+            hi += sm.hist[s][256u + sub_slot(s, d)];
         }
         J.agg[(size_t)ls * 256 + d] = lo;
         if (lo) {
@@ -406,25 +407,64 @@ __device__ void keys_publish(const JobDesc& J, uint32_t ls, SortSmem<NT>& sm) {
 }
 
 template <int NT>
-__device__ void zero_keys_hist(SortSmem<NT>& sm) {
-    uint32_t* h = &sm.u.k.hist[0][0];
+__device__ void zero_keys_hist(KeysSmem<NT>& sm) {
+    uint32_t* h = &sm.hist[0][0];
     for (uint32_t k = threadIdx.x; k < (uint32_t)kSubHist * 512u; k += NT) h[k] = 0;
 }
 
-// Keys of one segment of splats, in sub-tiles of TK splats staged by bulk
-// copies (double-buffered).
+// The queued splats' footprints, densely (a warp evaluates 32 of them at
+// once, whichever sub-tiles they came from): a kept splat sets its survivor
+// bit and counts its digits (its key is already out). Each thread's next
+// splat is fetched while it evaluates the current one, so the records'
+// latency overlaps the arithmetic.
 template <int NT>
-__device__ void keys_item(const JobDesc& J, int job, const SegDesc& sd, SortSmem<NT>& sm, KeysStage& ks,
-                          const LaunchDesc& L, uint32_t item) {
-    constexpr uint32_t TK = SortSmem<NT>::TK;
-    const uint32_t tid = threadIdx.x;
-    if (tid == 0) {
-        if (sm.vc_job != job) {
-            make_consts(J, sm.vc);
-            sm.vc_job = job;
-        }
-        sm.u.k.qn = 0;
+__device__ void keys_footprints(const JobDesc& J, KeysSmem<NT>& sm) {
+    const ViewConsts& c = sm.vc;
+    const uint32_t qn = sm.qn;
+    uint32_t e = threadIdx.x, i_n = 0;
+    float4 p_n = make_float4(0.f, 0.f, 0.f, 0.f);
+    float2 a_n = make_float2(0.f, 0.f), b_n = a_n, c_n = a_n;
+    if (e < qn) {
+        i_n = sm.queue[e];
+        p_n = __ldg(&J.centers[i_n]);
+        a_n = __ldcs(&J.cov[3 * (size_t)i_n]);
+        b_n = __ldcs(&J.cov[3 * (size_t)i_n + 1]);
+        c_n = __ldcs(&J.cov[3 * (size_t)i_n + 2]);
     }
+    for (; e < qn; e += NT) {
+        const uint32_t i = i_n;
+        const float4 p = p_n;
+        const float sg[6] = {a_n.x, a_n.y, b_n.x, b_n.y, c_n.x, c_n.y};
+        if (e + NT < qn) {
+            i_n = sm.queue[e + NT];
+            p_n = __ldg(&J.centers[i_n]);
+            a_n = __ldcs(&J.cov[3 * (size_t)i_n]);
+            b_n = __ldcs(&J.cov[3 * (size_t)i_n + 1]);
+            c_n = __ldcs(&J.cov[3 * (size_t)i_n + 2]);
+        }
+        float view[4];
+        view_of(c, p.x, p.y, p.z, view);
+        const float alpha = sm.alpha[__float_as_uint(p.w) >> 24];
+        if (footprint_keeps(c, view, sg, alpha)) {
+            atomicOr(&J.mask[i >> 5], 1u << (i & 31u));
+            count_key(&sm.hist[0][0], depth_key(c, view), threadIdx.x & (kSubHist - 1));
+        }
+    }
+}
+
+// Keys of one segment of splats, in sub-tiles of TK splats staged by bulk
+// copies (double-buffered). Sweep 1 writes every splat's key slot and
+// survivor word; splats whose footprint must be evaluated are queued and
+// evaluated together when the queue fills or the segment ends.
+template <int NT>
+__device__ void keys_item(const JobDesc& J, const SegDesc& sd, KeysSmem<NT>& sm, KeysStage& ks, const LaunchDesc& L,
+                          uint32_t item) {
+    constexpr uint32_t TK = KeysSmem<NT>::TK;
+    const uint32_t tid = threadIdx.x;
+    static_assert(sizeof(ViewConsts) % 4 == 0, "copied in words");
+    for (uint32_t k = tid; k < sizeof(ViewConsts) / 4; k += NT)
+        reinterpret_cast<uint32_t*>(&sm.vc)[k] = reinterpret_cast<const uint32_t*>(&J.vc)[k];
+    if (tid == 0) sm.qn = 0;
     zero_keys_hist(sm);
     __syncthreads();
     const ViewConsts& c = sm.vc;
@@ -432,61 +472,47 @@ __device__ void keys_item(const JobDesc& J, int job, const SegDesc& sd, SortSmem
     const bool fp = c.cull > 0.0f;
     const uint32_t a = sd.a, b = sd.b, n = J.n;
     uint16_t* const k16 = J.k16;
+    uint32_t* const mask = J.mask;
     if (any && a < b && tid == 0) stage_issue(J, sm, ks.buf, a, min(TK, b - a), fp);
     for (uint32_t base = a; base < b; base += TK) {
         const uint32_t cnt = min(TK, b - base);
         const uint32_t buf = ks.buf;
         if (any) {
             if (tid == 0 && base + TK < b) stage_issue(J, sm, buf ^ 1u, base + TK, min(TK, b - base - TK), fp);
+            const uint64_t w0 = L.trace && tid == 0 ? global_ns() : 0;
             if (!stage_wait(sm, ks, buf, L, item)) sm.drain = 1;
-            if (tid == 0) sm.pending &= ~(1u << buf);
+            if (tid == 0) {
+                sm.pending &= ~(1u << buf);
+                if (L.trace) sm.mark[0] += global_ns() - w0;   // time spent waiting for staged records
+            }
             if (c.fast)
-                keys_sweep<true>(c, sm, buf, base, cnt, n, fp, k16);
+                keys_sweep<true>(c, sm, buf, base, cnt, n, fp, k16, mask);
             else
-                keys_sweep<false>(c, sm, buf, base, cnt, n, fp, k16);
+                keys_sweep<false>(c, sm, buf, base, cnt, n, fp, k16, mask);
+            ks.buf ^= 1u;
         } else {
             // Wholly behind the camera: no survivors.
-            for (uint32_t at = tid; at < cnt; at += NT) k16[base + at] = 0;
-            for (uint32_t w = tid; w < cnt / 32; w += NT) sm.u.k.maskw[w] = 0;
+            for (uint32_t w = tid; w < cnt / 32; w += NT) mask[(base >> 5) + w] = 0;
         }
-        __syncthreads();
+        __syncthreads();   // the staging buffer is free again; the queue is complete
         if (tid == 0 && base == a) sm.mark[1] = global_ns();
-        // Sweep 2: the queued footprints, densely; a kept splat sets its bit
-        // and counts its digits (its key is already out).
-        const uint32_t qn = sm.u.k.qn;
-        const float4* centers = sm.u.k.centers[buf];
-        for (uint32_t e = tid; e < qn; e += NT) {
-            const uint32_t at = sm.u.k.queue[e];
-            const size_t i = base + at;
-            const float4 p = centers[at];
-            float view[4];
-            view_of(c, p.x, p.y, p.z, view);
-            const float2 a2 = __ldcs(&J.cov[3 * i]);
-            const float2 b2 = __ldcs(&J.cov[3 * i + 1]);
-            const float2 c2 = __ldcs(&J.cov[3 * i + 2]);
-            const float sg[6] = {a2.x, a2.y, b2.x, b2.y, c2.x, c2.y};
-            const float alpha = sm.alpha[__float_as_uint(p.w) >> 24];
-            if (footprint_keeps(c, view, sg, alpha)) {
-                atomicOr(&sm.u.k.maskw[at >> 5], 1u << (at & 31u));
-                count_key(&sm.u.k.hist[0][0], depth_key(c, view), tid & (kSubHist - 1));
-            }
+        if (sm.qn > TK) {   // room for one more sub-tile's worth
+            keys_footprints(J, sm);
+            __syncthreads();
+            if (tid == 0) sm.qn = 0;
+            __syncthreads();
         }
-        __syncthreads();
-        for (uint32_t w = tid; w < cnt / 32; w += NT) J.mask[(base >> 5) + w] = sm.u.k.maskw[w];
-        // The shade pass, fused: every survivor of the sub-tile (its survivor
-        // bit is final here, its centre still staged) gets its colour as seen
-        // from the eye.
-        if (J.sh) {
-            for (uint32_t at = tid; at < cnt; at += NT) {
-                if (!((sm.u.k.maskw[at >> 5] >> (at & 31u)) & 1u)) continue;
-                const float4 p = centers[at];
-                J.shaded[base + at] = shade_splat(J.sh, J.sh_words, J.sh_degree, base + at, p.x, p.y, p.z,
-                                                  __float_as_uint(p.w), J.eye);
-            }
+    }
+    if (sm.qn) keys_footprints(J, sm);
+    __syncthreads();
+    // The shade pass, fused: every survivor of the segment (its survivor bit
+    // final) gets its colour as seen from the eye.
+    if (J.sh) {
+        for (uint32_t i = a + tid; i < b; i += NT) {
+            if (!((__ldcg(&mask[i >> 5]) >> (i & 31u)) & 1u)) continue;
+            const float4 p = __ldg(&J.centers[i]);
+            J.shaded[i] = shade_splat(J.sh, J.sh_words, J.sh_degree, i, p.x, p.y, p.z, __float_as_uint(p.w), J.eye);
         }
-        if (tid == 0) sm.u.k.qn = 0;
-        __syncthreads();   // the buffer, the survivor words and the queue are free again
-        if (any) ks.buf ^= 1u;
     }
     if (tid == 0) sm.mark[2] = global_ns();
     keys_publish(J, sd.local, sm);
@@ -502,7 +528,7 @@ __device__ void keys_item(const JobDesc& J, int job, const SegDesc& sd, SortSmem
 // above), starting from an estimate by log2f and correcting it; the key is
 // 4095 - bucket, far first.
 template <int NT>
-__device__ void particle_keys_item(const JobDesc& J, const SegDesc& sd, SortSmem<NT>& sm) {
+__device__ void particle_keys_item(const JobDesc& J, const SegDesc& sd, KeysSmem<NT>& sm) {
     const uint32_t tid = threadIdx.x, lane = tid & 31u, s = lane & (kSubHist - 1);
     zero_keys_hist(sm);
     __syncthreads();
@@ -533,7 +559,7 @@ __device__ void particle_keys_item(const JobDesc& J, const SegDesc& sd, SortSmem
         k16[i] = (uint16_t)key;
         const uint32_t kb = __ballot_sync(0xffffffffu, live);
         if (lane == 0) J.mask[i >> 5] = kb;
-        if (live) count_key(&sm.u.k.hist[0][0], key, s);
+        if (live) count_key(&sm.hist[0][0], key, s);
     }
     keys_publish(J, sd.local, sm);
 }
@@ -542,13 +568,13 @@ __device__ void particle_keys_item(const JobDesc& J, const SegDesc& sd, SortSmem
 // element survives with its key; the low pass reads the keys in place, so
 // only the counts are made here.
 template <int NT>
-__device__ void given_keys_item(const JobDesc& J, const SegDesc& sd, SortSmem<NT>& sm) {
+__device__ void given_keys_item(const JobDesc& J, const SegDesc& sd, KeysSmem<NT>& sm) {
     const uint32_t tid = threadIdx.x, s = (tid & 31u) & (kSubHist - 1);
     zero_keys_hist(sm);
     __syncthreads();
     const uint32_t end = min(sd.b, J.n);
 #pragma unroll 4
-    for (uint32_t i = sd.a + tid; i < end; i += NT) count_key(&sm.u.k.hist[0][0], __ldg(&J.keys_in[i]), s);
+    for (uint32_t i = sd.a + tid; i < end; i += NT) count_key(&sm.hist[0][0], __ldg(&J.keys_in[i]), s);
     keys_publish(J, sd.local, sm);
 }
 
@@ -558,11 +584,11 @@ __device__ void given_keys_item(const JobDesc& J, const SegDesc& sd, SortSmem<NT
 // byte, over the segment's splats; PASS 1: the high byte, over its slice of
 // the low pass's output).
 template <int PASS, int NT>
-__device__ void digit_item(const JobDesc& J, const SegDesc& sd, SortSmem<NT>& sm, const LaunchDesc& L,
+__device__ void digit_item(const JobDesc& J, const SegDesc& sd, DigitSmem<NT>& sm, const LaunchDesc& L,
                            uint32_t item) {
-    constexpr int W = SortSmem<NT>::W;
+    constexpr int W = DigitSmem<NT>::W;
     constexpr uint32_t IPT = kDigitIPT;
-    constexpr uint32_t TD = SortSmem<NT>::TD;
+    constexpr uint32_t TD = DigitSmem<NT>::TD;
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
     JobCtl* ctl = reinterpret_cast<JobCtl*>(J.ctl);
     uint32_t* const look = J.ctl + sizeof(JobCtl) / 4;
@@ -572,8 +598,11 @@ __device__ void digit_item(const JobDesc& J, const SegDesc& sd, SortSmem<NT>& sm
     uint32_t* const agg = J.agg + (size_t)PASS * J.nseg * 256;
     const uint32_t ls = sd.local, g = ls / kGroup;
 
-    // The job's previous phase, every segment of it.
-    if (!wait_count(PASS == 0 ? &ctl->keys_done : &ctl->low_done, J.nseg, sm, L, item)) return;
+    // The job's previous phase, every segment of it: finished with the
+    // previous kernel, unless this launch left it out (the failure self-test,
+    // whose wait never ends).
+    if (L.first_phase > kPhaseKeys && !wait_count(PASS == 0 ? &ctl->keys_done : &ctl->low_done, J.nseg, sm, L, item))
+        return;
     digit_starts(ctl->tot[PASS], sm);
     const uint32_t S = sm.total;   // the job's survivors
     uint32_t lo, hi;
@@ -587,7 +616,7 @@ __device__ void digit_item(const JobDesc& J, const SegDesc& sd, SortSmem<NT>& sm
         lo = J.npad ? (uint32_t)((uint64_t)sd.a * S / J.npad) : 0u;
         hi = J.npad ? (uint32_t)((uint64_t)sd.b * S / J.npad) : 0u;
         // The slice's high-digit counts, published for the later segments.
-        uint32_t* h = &sm.u.p.hist[0][0];
+        uint32_t* h = &sm.hist[0][0];
         for (uint32_t k = tid; k < (uint32_t)kSubHist * 256u; k += NT) h[k] = 0;
         __syncthreads();
         const uint32_t s = lane & (kSubHist - 1);
@@ -610,30 +639,36 @@ __device__ void digit_item(const JobDesc& J, const SegDesc& sd, SortSmem<NT>& sm
         if (tid == 0) {
             st_release(&flag[ls], 1u);
             red_release_add(&gdone[g], 1u);
+        }
+        if (warp == 0) {
             // The look-back: every earlier group complete, every earlier
             // segment of this group published (all have smaller tickets).
+            // Lane k polls the k-th of these words, so one round trip
+            // covers 32 of them.
+            const uint32_t nflags = ls - g * kGroup, targets = g + nflags;
             uint32_t spins = 0;
-            sm.abort = 0;
-            for (uint32_t q = 0; q < g && !sm.abort; ++q) {
-                const uint32_t need = min(kGroup, J.nseg - q * kGroup);
-                while (ld_acquire(&gdone[q]) < need) {
+            bool fail = false;
+            for (uint32_t t0 = 0; t0 < targets && !fail; t0 += 32) {
+                const uint32_t t = t0 + lane;
+                bool met = t >= targets;
+                for (;;) {
+                    if (!met) {
+                        if (t < g)
+                            met = ld_acquire(&gdone[t]) >= min(kGroup, J.nseg - t * kGroup);
+                        else
+                            met = ld_acquire(&flag[g * kGroup + (t - g)]) != 0;
+                    }
+                    if (__all_sync(0xffffffffu, met)) break;
                     if (++spins > L.spin_limit || *(volatile uint32_t*)L.err) {
-                        raise_error(L.err, kErrWaitPhase, item);
-                        sm.abort = 1;
+                        fail = true;
                         break;
                     }
                     __nanosleep(32);
                 }
             }
-            for (uint32_t q = g * kGroup; q < ls && !sm.abort; ++q) {
-                while (ld_acquire(&flag[q]) == 0) {
-                    if (++spins > L.spin_limit || *(volatile uint32_t*)L.err) {
-                        raise_error(L.err, kErrWaitPhase, item);
-                        sm.abort = 1;
-                        break;
-                    }
-                    __nanosleep(32);
-                }
+            if (lane == 0) {
+                sm.abort = fail;
+                if (fail) raise_error(L.err, kErrWaitPhase, item);
             }
         }
         __syncthreads();
@@ -652,12 +687,12 @@ __device__ void digit_item(const JobDesc& J, const SegDesc& sd, SortSmem<NT>& sm
     uint32_t* const order = J.order;
     uint32_t* const keys_out = J.keys;
     const uint32_t lt = lanemask_lt();
-    uint32_t* const wm = sm.u.p.wmask[warp];
-    uint16_t* const wc = sm.u.p.wcnt[warp];
+    uint32_t* const wm = sm.wmask[warp];
+    uint16_t* const wc = sm.wcnt[warp];
     {
-        uint32_t* z = &sm.u.p.wmask[0][0];
+        uint32_t* z = &sm.wmask[0][0];
         for (uint32_t k = tid; k < (uint32_t)W * 256u; k += NT) z[k] = 0;
-        uint32_t* zc = reinterpret_cast<uint32_t*>(&sm.u.p.wcnt[0][0]);
+        uint32_t* zc = reinterpret_cast<uint32_t*>(&sm.wcnt[0][0]);
         for (uint32_t k = tid; k < (uint32_t)W * 128u; k += NT) zc[k] = 0;
     }
     __syncthreads();
@@ -713,8 +748,8 @@ __device__ void digit_item(const JobDesc& J, const SegDesc& sd, SortSmem<NT>& sm
         if (tid < 256) {
 #pragma unroll 8
             for (int w = 0; w < W; ++w) {
-                const uint32_t c = sm.u.p.wcnt[w][tid];
-                sm.u.p.wcnt[w][tid] = (uint16_t)tc;
+                const uint32_t c = sm.wcnt[w][tid];
+                sm.wcnt[w][tid] = (uint16_t)tc;
                 tc += c;
             }
             x = tc;
@@ -743,8 +778,8 @@ __device__ void digit_item(const JobDesc& J, const SegDesc& sd, SortSmem<NT>& sm
             if (key[r] == 0xFFFFFFFFu) continue;
             const uint32_t d = PASS == 0 ? (key[r] & 255u) : ((key[r] >> 8) & 255u);
             const uint32_t slot = sm.lstart[d] + wc[d] + rk[r];
-            sm.u.p.skey[slot] = (uint16_t)key[r];
-            sm.u.p.sidx[slot] = idx[r];
+            sm.skey[slot] = (uint16_t)key[r];
+            sm.sidx[slot] = idx[r];
         }
         if (tid == 0 && base == lo) sm.mark[1] = global_ns();
         __syncthreads();
@@ -753,12 +788,12 @@ __device__ void digit_item(const JobDesc& J, const SegDesc& sd, SortSmem<NT>& sm
         // meanwhile (nothing reads them until the next sub-tile's ranks).
         const uint32_t tt = sm.tile_total;
         {
-            uint32_t* zc = reinterpret_cast<uint32_t*>(&sm.u.p.wcnt[0][0]);
+            uint32_t* zc = reinterpret_cast<uint32_t*>(&sm.wcnt[0][0]);
             for (uint32_t k = tid; k < (uint32_t)W * 128u; k += NT) zc[k] = 0;
         }
 #pragma unroll 4
         for (uint32_t i = tid; i < tt; i += NT) {
-            const uint32_t k = sm.u.p.skey[i];
+            const uint32_t k = sm.skey[i];
             const uint32_t d = PASS == 0 ? (k & 255u) : (k >> 8);
             const uint32_t gp = sm.gofs[d] + i;
             if (gp >= S) {   // only reachable if counts disagree: record, do not write
@@ -767,9 +802,9 @@ __device__ void digit_item(const JobDesc& J, const SegDesc& sd, SortSmem<NT>& sm
             }
             if (PASS == 0) {
                 key_b[gp] = (uint16_t)k;
-                idx_b[gp] = sm.u.p.sidx[i];
+                idx_b[gp] = sm.sidx[i];
             } else {
-                __stcs(&order[gp], sm.u.p.sidx[i]);
+                __stcs(&order[gp], sm.sidx[i]);
                 if (keys_out) __stcs(&keys_out[gp], k);
             }
         }
@@ -783,81 +818,91 @@ __device__ void digit_item(const JobDesc& J, const SegDesc& sd, SortSmem<NT>& sm
     }
 }
 
-// ---------------------------------------------------------------- the kernel
+// ---------------------------------------------------------------- the kernels
 
-template <int NT>
-__global__ void __launch_bounds__(NT, 1024 / NT) sort_kernel(const __grid_constant__ LaunchDesc L) {
+// Lets the stream's next kernel (launched with programmatic stream
+// serialization) schedule its CTAs once every CTA here has called it or
+// exited; that kernel still waits in griddepcontrol.wait until this grid has
+// finished and its writes are visible.
+__device__ __forceinline__ void allow_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void wait_prerequisites() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+// Work item `seg` of the launch: from the segment table, or the lone job's
+// consecutive chunks.
+__device__ __forceinline__ SegDesc segment_of(const LaunchDesc& L, uint32_t seg) {
+    if (L.segs) return L.segs[seg];
+    SegDesc sd;
+    const uint32_t npad = L.jobs[0].npad;
+    sd.job = 0;
+    sd.a = min(seg * L.chunk, npad);
+    sd.b = min(sd.a + L.chunk, npad);
+    sd.local = seg;
+    return sd;
+}
+
+template <class SM>
+__device__ __forceinline__ void claim_next(SM& sm, uint32_t* ticket, uint32_t* err) {
+    if (threadIdx.x == 0) {
+        sm.next = atomicAdd(ticket, 1u);
+        sm.drain = *(volatile uint32_t*)err;
+    }
+}
+
+__device__ __forceinline__ void trace_item(const LaunchDesc& L, uint32_t slot, uint32_t it, uint64_t claim,
+                                           uint64_t start, const uint64_t* mark) {
+    TraceRec r;
+    r.claim = claim;
+    r.start = start;
+    r.end = global_ns();
+    r.item = it;
+    r.sm = sm_id();
+    for (int q = 0; q < 3; ++q) r.mark[q] = mark[q];
+    L.trace[slot] = r;
+}
+
+// The keys phase: one work item per segment.
+template <int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) keys_kernel(const __grid_constant__ LaunchDesc L) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    SortSmem<NT>& sm = *reinterpret_cast<SortSmem<NT>*>(smem_raw);
+    KeysSmem<NT>& sm = *reinterpret_cast<KeysSmem<NT>*>(smem_raw);
     const uint32_t tid = threadIdx.x;
-    if (tid < 256) sm.alpha[tid] = fdiv(float(tid), 255.0f);
+    for (uint32_t k = tid; k < 256; k += NT) sm.alpha[k] = fdiv(float(k), 255.0f);
     if (tid == 0) {
-        sm.vc_job = -1;
         sm.pending = 0;
         mbar_init(&sm.bar[0]);
         mbar_init(&sm.bar[1]);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         fence_proxy_async();
-        sm.next = atomicAdd(&L.lctl->ticket, 1u);
-        sm.drain = *(volatile uint32_t*)L.err;
     }
+    wait_prerequisites();   // the job table and the zeroed counters
+    claim_next(sm, &L.lctl->ticket[kPhaseKeys], L.err);
     KeysStage ks{0u, 0u};
-    const uint32_t n_items = (kPhases - L.first_phase) * L.nseg;
     uint64_t t_claim = 0, t_start = 0;
     if (L.trace && tid == 0) t_claim = global_ns();
     for (;;) {
         __syncthreads();   // the previous item's shared state is no longer read
         const uint32_t it = sm.next;
-        if (it >= n_items) break;
-        const uint32_t phase = L.first_phase + it / L.nseg;
-        const uint32_t seg = it % L.nseg;
-        SegDesc sd;
-        if (L.segs) {
-            sd = L.segs[seg];
-        } else {
-            const uint32_t npad = L.jobs[0].npad;
-            sd.job = 0;
-            sd.a = min(seg * L.chunk, npad);
-            sd.b = min(sd.a + L.chunk, npad);
-            sd.local = seg;
-        }
+        if (it >= L.nseg) break;
+        const SegDesc sd = segment_of(L, it);
         const JobDesc& J = L.jobs[sd.job];
-        const bool work = !sm.drain;   // after an error: claim the remaining items, do no work
-        if (work) {
+        if (!sm.drain) {   // after an error: claim the remaining items, do no work
             if (L.trace && tid == 0) {
                 t_start = global_ns();
                 sm.mark[0] = sm.mark[1] = sm.mark[2] = 0;
             }
-            if (phase == kPhaseKeys) {
-                if (J.kind == kJobParticles)
-                    particle_keys_item(J, sd, sm);
-                else if (J.kind == kJobKeys)
-                    given_keys_item(J, sd, sm);
-                else
-                    keys_item(J, (int)sd.job, sd, sm, ks, L, it);
-            } else if (phase == kPhaseLow) {
-                digit_item<0>(J, sd, sm, L, it);
-            } else {
-                digit_item<1>(J, sd, sm, L, it);
-            }
+            if (J.kind == kJobParticles)
+                particle_keys_item(J, sd, sm);
+            else if (J.kind == kJobKeys)
+                given_keys_item(J, sd, sm);
+            else
+                keys_item(J, sd, sm, ks, L, it);
             __syncthreads();
+            if (L.trace && tid == 0) trace_item(L, it, it, t_claim, t_start, sm.mark);
         }
-        if (tid == 0) {
-            if (work && L.trace) {
-                TraceRec r;
-                r.claim = t_claim;
-                r.start = t_start;
-                r.end = global_ns();
-                r.item = it;
-                r.sm = sm_id();
-                for (int q = 0; q < 3; ++q) r.mark[q] = sm.mark[q];
-                L.trace[it] = r;
-            }
-            sm.next = atomicAdd(&L.lctl->ticket, 1u);
-            sm.drain = *(volatile uint32_t*)L.err;
-            if (L.trace) t_claim = global_ns();
-        }
+        claim_next(sm, &L.lctl->ticket[kPhaseKeys], L.err);
+        if (L.trace && tid == 0) t_claim = global_ns();
     }
+    allow_dependents();
     // No bulk copy into this CTA's shared memory outlives it (one is only
     // left in flight if a wait gave up).
     if (tid == 0) {
@@ -867,47 +912,124 @@ __global__ void __launch_bounds__(NT, 1024 / NT) sort_kernel(const __grid_consta
             while (!mbar_try_wait(&sm.bar[b], (ks.parity >> b) & 1u) && ++spins < L.spin_limit) {
             }
         }
-        atomicAdd(&L.lctl->exited, 1u);
     }
 }
 
-template <int NT>
-static cudaError_t prepare_variant() {
-    static bool done = false;   // the attribute is per function, set once per process
+// A digit pass (PASS 0: low byte, 1: high byte): one work item per segment.
+template <int PASS, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) digit_kernel(const __grid_constant__ LaunchDesc L) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    DigitSmem<NT>& sm = *reinterpret_cast<DigitSmem<NT>*>(smem_raw);
+    const uint32_t tid = threadIdx.x;
+    wait_prerequisites();   // the previous pass has finished
+    claim_next(sm, &L.lctl->ticket[kPhaseLow + PASS], L.err);
+    uint64_t t_claim = 0, t_start = 0;
+    if (L.trace && tid == 0) t_claim = global_ns();
+    for (;;) {
+        __syncthreads();
+        const uint32_t it = sm.next;
+        if (it >= L.nseg) break;
+        const SegDesc sd = segment_of(L, it);
+        const JobDesc& J = L.jobs[sd.job];
+        if (!sm.drain) {
+            if (L.trace && tid == 0) {
+                t_start = global_ns();
+                sm.mark[0] = sm.mark[1] = sm.mark[2] = 0;
+            }
+            digit_item<PASS>(J, sd, sm, L, it);
+            __syncthreads();
+            if (L.trace && tid == 0) trace_item(L, (kPhaseLow + PASS) * L.nseg + it, it, t_claim, t_start, sm.mark);
+        }
+        claim_next(sm, &L.lctl->ticket[kPhaseLow + PASS], L.err);
+        if (L.trace && tid == 0) t_claim = global_ns();
+    }
+    allow_dependents();
+}
+
+// Keys CTAs: 768 threads, one an SM (up to 85 registers a thread).
+constexpr int kKeysThreads = 768;
+
+template <class K>
+static cudaError_t set_smem(K kernel, size_t bytes) {
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+// A launch that may begin while the stream's previous kernel finishes (its
+// CTAs wait in griddepcontrol.wait).
+template <class K>
+static cudaError_t launch_dependent(K kernel, int grid, int threads, size_t smem, cudaStream_t stream,
+                                    const LaunchDesc& L) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3((unsigned)threads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, L);
+}
+
+template <int NT, int MINB>
+static cudaError_t prepare_digit() {
+    static bool done = false;   // the attributes are per function, set once per process
     if (done) return cudaSuccess;
-    const cudaError_t e = cudaFuncSetAttribute(sort_kernel<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               (int)sizeof(SortSmem<NT>));
+    cudaError_t e;
+    if ((e = set_smem(digit_kernel<0, NT, MINB>, sizeof(DigitSmem<NT>))) != cudaSuccess) return e;
+    if ((e = set_smem(digit_kernel<1, NT, MINB>, sizeof(DigitSmem<NT>))) != cudaSuccess) return e;
+    done = true;
+    return cudaSuccess;
+}
+
+static cudaError_t prepare_keys() {
+    static bool done = false;
+    if (done) return cudaSuccess;
+    const cudaError_t e = set_smem(keys_kernel<kKeysThreads, 1>, sizeof(KeysSmem<kKeysThreads>));
     if (e == cudaSuccess) done = true;
     return e;
 }
 
-template <int NT>
-static cudaError_t launch_variant(const LaunchDesc& L, int grid, cudaStream_t stream) {
-    cudaError_t e = prepare_variant<NT>();
+template <int NT, int MINB>
+static cudaError_t launch_digits(const LaunchDesc& L, int grid, cudaStream_t stream) {
+    cudaError_t e = prepare_digit<NT, MINB>();
     if (e != cudaSuccess) return e;
-    sort_kernel<NT><<<grid, NT, sizeof(SortSmem<NT>), stream>>>(L);
-    return cudaGetLastError();
+    if (L.first_phase <= kPhaseLow &&
+        (e = launch_dependent(digit_kernel<0, NT, MINB>, grid, NT, sizeof(DigitSmem<NT>), stream, L)) != cudaSuccess)
+        return e;
+    return launch_dependent(digit_kernel<1, NT, MINB>, grid, NT, sizeof(DigitSmem<NT>), stream, L);
 }
 
-// Host-side launcher: `threads` per CTA is 1024 (one CTA an SM) or 512 (two).
-cudaError_t launch_sort(const LaunchDesc& L, int threads, int grid, cudaStream_t stream) {
-    if (threads == 512) return launch_variant<512>(L, grid, stream);
-    return launch_variant<1024>(L, grid, stream);
+// Host-side launcher: the keys kernel (unless L.first_phase leaves it out),
+// one CTA an SM, then the two digit passes, `grid` CTAs of `threads` threads:
+// 1024 (one CTA an SM) or 512 (two).
+cudaError_t launch_sort(const LaunchDesc& L, int threads, int grid, int sms, cudaStream_t stream) {
+    cudaError_t e;
+    if (L.first_phase == kPhaseKeys) {
+        if ((e = prepare_keys()) != cudaSuccess) return e;
+        const int kg = (int)min((uint32_t)sms, L.nseg);
+        if ((e = launch_dependent(keys_kernel<kKeysThreads, 1>, kg, kKeysThreads, sizeof(KeysSmem<kKeysThreads>),
+                                  stream, L)) != cudaSuccess)
+            return e;
+    }
+    if (threads == 512) return launch_digits<512, 2>(L, grid, stream);
+    return launch_digits<1024, 1>(L, grid, stream);
 }
 
-template <int NT>
-static int occupancy_variant() {
+template <int NT, int MINB>
+static int occupancy_digit() {
     int blocks = 0;
-    if (prepare_variant<NT>() != cudaSuccess) return 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, sort_kernel<NT>, NT, sizeof(SortSmem<NT>));
+    if (prepare_digit<NT, MINB>() != cudaSuccess) return 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, digit_kernel<0, NT, MINB>, NT, sizeof(DigitSmem<NT>));
     return blocks;
 }
 
-// Resident CTAs per SM of the variant with `threads` threads.
+// Resident digit-pass CTAs per SM of the variant with `threads` threads.
 int sort_occupancy(int threads) {
     static int cached[2] = {0, 0};
     const int k = threads == 512 ? 1 : 0;
-    if (!cached[k]) cached[k] = k ? occupancy_variant<512>() : occupancy_variant<1024>();
+    if (!cached[k]) cached[k] = k ? occupancy_digit<512, 2>() : occupancy_digit<1024, 1>();
     return cached[k];
 }
 

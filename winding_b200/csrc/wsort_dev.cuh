@@ -42,6 +42,29 @@ constexpr int kKeysIPT = 4;               // splats per thread in one sub-tile o
 constexpr int kDigitIPT = 8;              // elements per thread in one sub-tile of a digit pass
 constexpr int kSubHist = 8;               // lane-interleaved sub-histograms for counting
 
+// Per-view constants of one job, computed once (by the host for a sort, by
+// make_consts for the draw). Each is the same IEEE operation on the same
+// operands the per-splat WGSL evaluates, so hoisting them changes no bit.
+struct ViewConsts {
+    float mv[16];
+    float proj[16];
+    float keep_q;
+    uint32_t keep_byte;
+    int fast;
+    float fx, fy;               // p[0][0] * viewport.x * 0.5, p[1][1] * viewport.y * 0.5
+    float xlo, xhi, ylo, yhi;   // -1.3 / p[0][0], 1.3 / p[0][0], and for p[1][1]
+    float cull;
+    float depth_min, depth_scale;
+    int persp;                  // p[3][3] == 0
+    int visible;                // far > 0
+    uint32_t faint_max;         // alpha bytes up to this are too faint: unpack(byte) * 255 <= 1
+    // Upper bounds (rounded up) for the per-splat footprint bound of the keys
+    // phase: |fx|, |fy|, the absolute row sums of the model-view's 3x3 (rows
+    // 0, 1, 2), and |1.3 / p[0][0]|, |1.3 / p[1][1]|.
+    float afx, afy, r0, r1, r2, xcap, ycap;
+    uint32_t pad[1];
+};
+
 // One (cloud, view) to sort, as the kernel reads it.
 struct alignas(16) JobDesc {
     // cloud (resident)
@@ -62,6 +85,7 @@ struct alignas(16) JobDesc {
     float proj[16];
     float viewport[2];
     float cull;
+    ViewConsts vc;              // the view's constants, filled by the host
     // segments
     uint32_t seg0;              // the launch's index of the job's first segment
     uint32_t nseg;              // the job's segments
@@ -125,15 +149,14 @@ struct alignas(16) SegDesc {
 
 // Per-launch counters, zeroed before a launch.
 struct LaunchCtl {
-    uint32_t ticket;            // next work item
-    uint32_t exited;            // CTAs that left the loop
-    uint32_t pad[14];
+    uint32_t ticket[3];         // next work item of each phase's kernel
+    uint32_t pad[13];
 };
 
-// What one launch sorts. Work item t is phase first_phase + t / nseg of
-// segment t % nseg: every segment's keys, then every low pass, then every
-// high pass. Segments come from `segs`, or, for a launch of one job
-// (segs null), are the job's consecutive ranges of `chunk` splats.
+// What one launch sorts: three kernels (keys, low pass, high pass), each
+// with one work item per segment, claimed in order. Segments come from
+// `segs`, or, for a launch of one job (segs null), are the job's consecutive
+// ranges of `chunk` splats.
 struct LaunchDesc {
     const JobDesc* jobs;
     const SegDesc* segs;
@@ -244,23 +267,6 @@ __device__ __forceinline__ uint32_t shade_splat(const uint32_t* sh, uint32_t wor
     return pack_unorm8(__fadd_rn(r, c.x)) | (pack_unorm8(__fadd_rn(gr, c.y)) << 8) |
            (pack_unorm8(__fadd_rn(bl, c.z)) << 16) | (pack_unorm8(al) << 24);
 }
-
-// Per-view constants of one job, computed once per work item. Each is the
-// same IEEE operation on the same operands the per-splat WGSL evaluates, so
-// hoisting them changes no bit.
-struct ViewConsts {
-    float mv[16];
-    float proj[16];
-    float keep_q;
-    uint32_t keep_byte;
-    int fast;
-    float fx, fy;               // p[0][0] * viewport.x * 0.5, p[1][1] * viewport.y * 0.5
-    float xlo, xhi, ylo, yhi;   // -1.3 / p[0][0], 1.3 / p[0][0], and for p[1][1]
-    float cull;
-    float depth_min, depth_scale;
-    int persp;                  // p[3][3] == 0
-    int visible;                // far > 0
-};
 
 // The depth range in FP64 (render/splats.js:561-582).
 __device__ __forceinline__ void depth_range(const JobDesc& J, float* depth_min, float* depth_scale,

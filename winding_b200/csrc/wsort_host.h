@@ -66,7 +66,7 @@ size_t table_bytes(int njobs, const LaunchShape& S);
 void write_table(void* dst, const JobDesc* jobs, int njobs, const LaunchShape& S);
 LaunchDesc launch_desc(const void* d_table, int njobs, const LaunchShape& S, char* scratch, uint32_t* err,
                        uint32_t spin_limit, TraceRec* trace);
-cudaError_t launch_sort(const LaunchDesc& L, int threads, int grid, cudaStream_t stream);
+cudaError_t launch_sort(const LaunchDesc& L, int threads, int grid, int sms, cudaStream_t stream);
 int sort_occupancy(int threads);
 
 }  // namespace wsort
