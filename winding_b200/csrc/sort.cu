@@ -697,34 +697,52 @@ __device__ void digit_item(const JobDesc& J, const SegDesc& sd, DigitSmem<NT>& s
     }
     __syncthreads();
 
+    // Element e of a sub-tile at b0 goes to warp w = (e - b0) / (32 IPT),
+    // round r, lane e % 32: warps, rounds and lanes follow the element order.
+    // Each sub-tile's inputs are loaded one sub-tile ahead (nk, nx), so their
+    // latency overlaps the previous sub-tile's ranks, staging and writes.
+    uint32_t nk[IPT], nx[IPT];
+#define WS_FETCH(b0)                                                                \
+    _Pragma("unroll") for (uint32_t r = 0; r < IPT; ++r) {                        \
+        const uint32_t e = (b0) + (warp * IPT + r) * 32u + lane;                  \
+        nk[r] = 0xFFFFFFFFu;                                                        \
+        nx[r] = 0;                                                                  \
+        if (e < hi) {                                                               \
+            if (PASS == 1) {                                                        \
+                nk[r] = __ldcg(&kin[e]);                                            \
+                nx[r] = __ldcg(&idx_in[e]);                                         \
+            } else if (given) {                                                     \
+                /* given keys are read only below n */                             \
+                if (e < n) nk[r] = __ldcg(&kin[e]);                                 \
+                nx[r] = 0xFFFFFFFFu;                                                \
+            } else {                                                                \
+                nk[r] = __ldcg(&kin[e]);                                            \
+                nx[r] = __ldcg(&mask[e >> 5]);                                      \
+            }                                                                       \
+        }                                                                           \
+    }
+    if (lo < hi) {
+        WS_FETCH(lo)
+    }
     for (uint32_t base = lo; base < hi; base += TD) {
-        // Load: warp w takes elements base + 32 (IPT w + r) + lane, rounds
-        // r in order, so warps, rounds and lanes follow the element order.
-        uint32_t key[IPT], idx[IPT], rk[IPT];
+        // kr: the key in bits 0-15 and its rank within the warp's digit
+        // above, or 0xFFFFFFFF for no element.
+        uint32_t kr[IPT], ix[IPT];
 #pragma unroll
         for (uint32_t r = 0; r < IPT; ++r) {
-            const uint32_t e = base + (warp * IPT + r) * 32u + lane;
-            key[r] = 0xFFFFFFFFu;
-            idx[r] = 0;
-            if (e < hi) {
-                if (PASS == 0) {
-                    // Given keys are read only below n (the segments run to
-                    // the next multiple of 256).
-                    if (given ? e < n : ((__ldcg(&mask[e >> 5]) >> lane) & 1u)) key[r] = __ldcg(&kin[e]);
-                    idx[r] = idx_base + e;
-                } else {
-                    key[r] = __ldcg(&kin[e]);
-                    idx[r] = __ldcg(&idx_in[e]);
-                }
-            }
+            const bool v = nk[r] != 0xFFFFFFFFu && (PASS == 1 || ((nx[r] >> lane) & 1u));
+            kr[r] = v ? nk[r] : 0xFFFFFFFFu;
+            ix[r] = nx[r];
+        }
+        if (base + TD < hi) {
+            WS_FETCH(base + TD)
         }
         // Rank within the warp, round by round.
 #pragma unroll
         for (uint32_t r = 0; r < IPT; ++r) {
-            const bool v = key[r] != 0xFFFFFFFFu;
-            rk[r] = 0;
+            const bool v = kr[r] != 0xFFFFFFFFu;
             if (__any_sync(0xffffffffu, v)) {
-                const uint32_t d = PASS == 0 ? (key[r] & 255u) : ((key[r] >> 8) & 255u);
+                const uint32_t d = PASS == 0 ? (kr[r] & 255u) : ((kr[r] >> 8) & 255u);
                 if (v) atomicOr(&wm[d], 1u << lane);
                 __syncwarp();
                 uint32_t peers = 0, prior = 0;
@@ -738,7 +756,7 @@ __device__ void digit_item(const JobDesc& J, const SegDesc& sd, DigitSmem<NT>& s
                     wc[d] = (uint16_t)(prior + __popc(peers));
                 }
                 __syncwarp();
-                rk[r] = prior + __popc(peers & lt);
+                if (v) kr[r] |= (prior + __popc(peers & lt)) << 16;
             }
         }
         __syncthreads();
@@ -775,11 +793,11 @@ __device__ void digit_item(const JobDesc& J, const SegDesc& sd, DigitSmem<NT>& s
         // Stage in sub-tile order (digit, then element order).
 #pragma unroll
         for (uint32_t r = 0; r < IPT; ++r) {
-            if (key[r] == 0xFFFFFFFFu) continue;
-            const uint32_t d = PASS == 0 ? (key[r] & 255u) : ((key[r] >> 8) & 255u);
-            const uint32_t slot = sm.lstart[d] + wc[d] + rk[r];
-            sm.skey[slot] = (uint16_t)key[r];
-            sm.sidx[slot] = idx[r];
+            if (kr[r] == 0xFFFFFFFFu) continue;
+            const uint32_t d = PASS == 0 ? (kr[r] & 255u) : ((kr[r] >> 8) & 255u);
+            const uint32_t slot = sm.lstart[d] + wc[d] + (kr[r] >> 16);
+            sm.skey[slot] = (uint16_t)kr[r];
+            sm.sidx[slot] = PASS == 0 ? idx_base + base + (warp * IPT + r) * 32u + lane : ix[r];
         }
         if (tid == 0 && base == lo) sm.mark[1] = global_ns();
         __syncthreads();
@@ -810,6 +828,7 @@ __device__ void digit_item(const JobDesc& J, const SegDesc& sd, DigitSmem<NT>& s
         }
         __syncthreads();
     }
+#undef WS_FETCH
     if (tid == 0) sm.mark[2] = global_ns();
     if (PASS == 0) {
         __threadfence();
