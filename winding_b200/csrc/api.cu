@@ -321,6 +321,31 @@ void fill_view_consts(JobDesc& d) {
     c.r2 = up(std::fabs((double)M[2]) + std::fabs((double)M[6]) + std::fabs((double)M[10]));
     c.xcap = up(c.xhi);
     c.ycap = up(c.yhi);
+    // det_min[b]: the least f32 det that makeKeys keeps with alpha byte b,
+    // found by bisection over the ordered non-negative f32 values (the test
+    // is monotone in det: max, the square root and the two products are).
+    for (uint32_t b = 0; b < 256; ++b) {
+        const float alpha = (float)b / 255.0f;
+        auto kept = [&](float det) {
+            const float area = 6.2831853f * std::sqrt(std::fmax(det, 0.0f));
+            return !(alpha * area < d.cull);
+        };
+        if (kept(0.0f)) {
+            c.det_min[b] = -INFINITY;
+            continue;
+        }
+        uint32_t lo = 0, hi = 0x7f800000u;   // kept(lo) false, kept(+inf) true
+        while (hi - lo > 1) {
+            const uint32_t mid = lo + (hi - lo) / 2;
+            float f;
+            std::memcpy(&f, &mid, 4);
+            if (kept(f))
+                hi = mid;
+            else
+                lo = mid;
+        }
+        std::memcpy(&c.det_min[b], &hi, 4);
+    }
 }
 
 // Emitter jobs (ws_sort_particles): the ring, the view and the outputs.

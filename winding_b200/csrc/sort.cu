@@ -275,12 +275,12 @@ __device__ void segment_prefix(const uint32_t* gsum, const uint32_t* agg, uint32
 //    most 0.0025 below 0.09; so area >= 1.85 whatever the rounding, and every
 //    alpha byte >= keep_byte (RN(alpha * 1.85) >= cull, proved by the host)
 //    is kept without its footprint (or its covariance) being computed.
-//  * Culled: each pinned entry is at most g (1 + 8.2u) and the pinned area at
-//    most 2 pi sqrt((ga (1 + 8.2u) + .3)(gb (1 + 8.2u) + .3)) (1 + 5u). The
-//    kernel compares the square of alpha times that, with a further 1.0002
-//    (which also covers the rounding of the comparison's own few operations
-//    and of cull^2), against cull^2; below it, RN(alpha * area) < cull and
-//    the splat is culled, again without its footprint.
+//  * Culled: each pinned entry is at most g (1 + 8.2u) and the pinned det at
+//    most (ga (1 + 8.2u) + .3)(gb (1 + 8.2u) + .3)(1 + 3u); the kernel forms
+//    that with a further 1.0001 (which covers its own few roundings) and
+//    compares it with det_min[byte], the least det the cull keeps for the
+//    splat's alpha byte (found exactly by the host); below it the splat is
+//    culled, again without its footprint.
 // Splats that neither test decides are queued for the pinned computation.
 
 // Counts a survivor's two digits into the lane's sub-histograms.
@@ -333,7 +333,6 @@ __device__ __forceinline__ void keys_sweep(const ViewConsts& c, KeysSmem<NT>& sm
         if (fp) {
             bool keep_sc = false, cull_sc = false;
             if (persp) {
-                const float alpha = sm.alpha[byte];
                 const float d = -view[2];
                 // The splat's covariance bound 2^sexp, exactly (sexp is in
                 // [-100, 127]).
@@ -345,9 +344,9 @@ __device__ __forceinline__ void keys_sweep(const ViewConsts& c, KeysSmem<NT>& sm
                 const float A = afx * rd * (r0 + ax * r2), B = afy * rd * (r1 + ay * r2);
                 const float ga = 1.002f * (A * A) * m, gb = 1.002f * (B * B) * m;
                 keep_sc = byte >= keep_byte && ga <= 100.0f && gb <= 100.0f;
-                const float t = alpha * 6.2832f;
-                const float top2 = t * t * ((ga * 1.00001f + 0.3f) * (gb * 1.00001f + 0.3f)) * 1.0002f;
-                cull_sc = !keep_sc && top2 < cull * cull;
+                // det's pinned value is at most (ga (1 + 8.2u) + .3)(gb (1 +
+                // 8.2u) + .3)(1 + 3u); below the byte's threshold, culled.
+                cull_sc = !keep_sc && ((ga * 1.00001f + 0.3f) * (gb * 1.00001f + 0.3f)) * 1.0001f < c.det_min[byte];
             }
             pending = kept && !keep_sc && !cull_sc;
             kept = kept && keep_sc;
@@ -444,8 +443,54 @@ __device__ void keys_footprints(const JobDesc& J, KeysSmem<NT>& sm) {
         }
         float view[4];
         view_of(c, p.x, p.y, p.z, view);
-        const float alpha = sm.alpha[__float_as_uint(p.w) >> 24];
-        if (footprint_keeps(c, view, sg, alpha)) {
+        const float thr = c.det_min[__float_as_uint(p.w) >> 24];
+        // A filter first: det from the same inputs with fast arithmetic (fused
+        // products, an approximate reciprocal), and a bound on how far the
+        // pinned det can lie from it: every intermediate of both is within
+        // about 30 ulps of its real value, relative to the magnitudes
+        // |T| |Sigma| |T|^T (ga, gb below), so 2^-16 of
+        // (ga + .3)(gb + .3) + ga gb bounds the difference with room to spare.
+        // Outside that band of the threshold the decision is the pinned one's;
+        // inside, the pinned det decides.
+        float J00 = c.fx, J11 = c.fy, J02 = 0.0f, J12 = 0.0f;
+        if (c.persp) {
+            const float rd = __fdividef(1.0f, -view[2]);
+            J00 = c.fx * rd;
+            J11 = c.fy * rd;
+            J02 = J00 * fminf(fmaxf(view[0] * rd, c.xlo), c.xhi);
+            J12 = J11 * fminf(fmaxf(view[1] * rd, c.ylo), c.yhi);
+        }
+        float T0[3], T1[3], ta = 0.0f, tb = 0.0f;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            T0[k] = __fmaf_rn(J00, c.mv[k * 4 + 0], J02 * c.mv[k * 4 + 2]);
+            T1[k] = __fmaf_rn(J11, c.mv[k * 4 + 1], J12 * c.mv[k * 4 + 2]);
+            ta += fabsf(T0[k]);
+            tb += fabsf(T1[k]);
+        }
+        const float S[3][3] = {{sg[0], sg[1], sg[2]}, {sg[1], sg[3], sg[4]}, {sg[2], sg[4], sg[5]}};
+        float U0[3], U1[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            U0[k] = __fmaf_rn(T0[0], S[0][k], __fmaf_rn(T0[1], S[1][k], T0[2] * S[2][k]));
+            U1[k] = __fmaf_rn(T1[0], S[0][k], __fmaf_rn(T1[1], S[1][k], T1[2] * S[2][k]));
+        }
+        const float xx = __fmaf_rn(U0[0], T0[0], __fmaf_rn(U0[1], T0[1], U0[2] * T0[2]));
+        const float xy = __fmaf_rn(U1[0], T0[0], __fmaf_rn(U1[1], T0[1], U1[2] * T0[2]));
+        const float yy = __fmaf_rn(U1[0], T1[0], __fmaf_rn(U1[1], T1[1], U1[2] * T1[2]));
+        const float det = __fmaf_rn(xx + 0.3f, yy + 0.3f, -(xy * xy));
+        const float ms = fmaxf(fmaxf(fmaxf(fabsf(sg[0]), fabsf(sg[1])), fmaxf(fabsf(sg[2]), fabsf(sg[3]))),
+                               fmaxf(fabsf(sg[4]), fabsf(sg[5])));
+        const float ga = ta * ta * ms, gb = tb * tb * ms;
+        const float err = 1.52587890625e-5f * __fmaf_rn(ga + 0.3f, gb + 0.3f, ga * gb);
+        bool keep;
+        if (det - err >= thr)
+            keep = true;
+        else if (det + err < thr)
+            keep = false;
+        else
+            keep = fmaxf(footprint_det(c, view, sg), 0.0f) >= thr;   // the max of makeKeys' sqrt(max(det, 0))
+        if (keep) {
             atomicOr(&J.mask[i >> 5], 1u << (i & 31u));
             count_key(&sm.hist[0][0], depth_key(c, view), threadIdx.x & (kSubHist - 1));
         }

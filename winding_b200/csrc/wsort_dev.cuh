@@ -63,6 +63,12 @@ struct ViewConsts {
     // 0, 1, 2), and |1.3 / p[0][0]|, |1.3 / p[1][1]|.
     float afx, afy, r0, r1, r2, xcap, ycap;
     uint32_t pad[1];
+    // The footprint cull as a threshold on det, per alpha byte b: makeKeys
+    // keeps the splat exactly when det >= det_min[b] (the host's bisection
+    // over f32 values of the monotone test !(alpha * (2 pi sqrt(max(det, 0)))
+    // < cull), each operation rounded as the kernels round it; -inf: kept
+    // whatever det).
+    float det_min[256];
 };
 
 // One (cloud, view) to sort, as the kernel reads it.
@@ -437,6 +443,14 @@ __device__ __forceinline__ uint32_t fast_depth_key(const FastView& f, const floa
 }
 
 // The footprint cull (render/splats.js:172-178): true when the splat is kept.
+// The pinned 2D covariance's det = (xx + .3)(yy + .3) - xy^2
+// (render/splats.js:174-178).
+__device__ __forceinline__ float footprint_det(const ViewConsts& c, const float view[4], const float s[6]) {
+    float fxx, fxy, fyy;
+    footprint2d(c, view, s, &fxx, &fxy, &fyy);
+    return fsub(fmul(fadd(fxx, 0.3f), fadd(fyy, 0.3f)), fmul(fxy, fxy));
+}
+
 __device__ __forceinline__ bool footprint_keeps(const ViewConsts& c, const float view[4], const float s[6],
                                                 float alpha) {
     float fxx, fxy, fyy;
