@@ -207,6 +207,18 @@ typedef struct ws_job {
 int ws_sort_batch(ws_ctx* ctx, int njobs, const ws_job* jobs, void* stream);
 
 /*
+ * ws_sort_batch with host outputs: the same one launch for all jobs, then
+ * each job's survivors and count into host memory -- the loop of
+ * SplatPass._encodeSort (src/render/splats.js:678-696) with the reference's
+ * outputs (order, args.instanceCount) read back. jobs[j].order, .keys (may
+ * be NULL) and .count are host memory; when every one is pinned
+ * (cudaHostAlloc / registered), one kernel writes them all and the call
+ * synchronises once, else the counts come back first and then the orders.
+ * Returns when the outputs are filled.
+ */
+int ws_sort_batch_host(ws_ctx* ctx, int njobs, const ws_job* jobs, void* stream);
+
+/*
  * A batch frozen into a CUDA graph: the job set (clouds, output buffers) is
  * fixed at creation; views can change between launches with
  * ws_plan_set_views, which waits for the plan's previous launch to finish

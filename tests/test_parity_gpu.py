@@ -335,6 +335,49 @@ def test_a_wait_that_runs_out_is_reported_and_the_context_recovers(ctx):
     check_job(ctx, W.uniform_100k(seed=77, n=50_000))
 
 
+@pytest.mark.parametrize("pinned", [True, False])
+def test_batch_with_host_outputs(ctx, pinned):
+    """ws_sort_batch_host: every job's count, order and keys in host memory
+    equal ws_sort_batch's device results (one copy kernel into pinned
+    buffers, or counts then orders into pageable ones), twice in a row."""
+    import ctypes
+
+    import torch
+    base = W.clusters_1m(seed=60, n=250_000)
+    parts = [base.records[:70_001], base.records[:1], base.records[:0], base.records]
+    clouds = [parse_splats(r, ctx) if len(r) else None for r in parts]
+    try:
+        live = [c for c in clouds if c is not None]
+        specs, dev, host = [], [], []
+        for sp in live:
+            view = make_view(base.view.model_view, base.view.projection, base.view.viewport, 0.5)
+            n = max(sp.count, 1)
+            o = torch.empty(n, dtype=torch.int32, device="cuda")
+            k = torch.empty(n, dtype=torch.int32, device="cuda")
+            c = torch.zeros(1, dtype=torch.int32, device="cuda")
+            dev.append((o, k, c))
+            ho, hk, hc = (torch.full((n,), -1, dtype=torch.int32), torch.full((n,), -1, dtype=torch.int32),
+                          torch.zeros(1, dtype=torch.int32))
+            if pinned:
+                ho, hk, hc = ho.pin_memory(), hk.pin_memory(), hc.pin_memory()
+            host.append((ho, hk, hc))
+            specs.append((sp, view))
+        ctx.sort_batch([(sp, v, o.data_ptr(), k.data_ptr(), c.data_ptr()) for (sp, v), (o, k, c) in zip(specs, dev)])
+        ctx.sync()
+        for _ in range(2):
+            ctx.sort_batch_host([(sp, v, ho.data_ptr(), hk.data_ptr(), hc.data_ptr())
+                                 for (sp, v), (ho, hk, hc) in zip(specs, host)])
+            for (o, k, c), (ho, hk, hc) in zip(dev, host):
+                s = int(c.item())
+                assert int(hc[0]) == s
+                assert np.array_equal(ho[:s].numpy(), o[:s].cpu().numpy())
+                assert np.array_equal(hk[:s].numpy(), k[:s].cpu().numpy())
+    finally:
+        for sp in clouds:
+            if sp is not None:
+                sp.destroy()
+
+
 def test_host_output_into_pinned_buffers(ctx):
     """ws_sort with pinned host outputs takes the direct path (the survivors
     written into the host buffers by a kernel, one synchronisation); the

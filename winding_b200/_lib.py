@@ -166,6 +166,7 @@ SIGNATURES = {
     "ws_depth_range": (ctypes.c_int, [vp, f32p, ctypes.POINTER(ctypes.c_int), f32p, f32p]),
     "ws_sort": (ctypes.c_int, [vp, vp, ctypes.POINTER(WsView), vp, vp, vp, ctypes.c_int, vp]),
     "ws_sort_batch": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(WsJob), vp]),
+    "ws_sort_batch_host": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(WsJob), vp]),
     "ws_plan_create": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(WsJob), ctypes.POINTER(vp)]),
     "ws_plan_set_views": (ctypes.c_int, [vp, ctypes.POINTER(WsView)]),
     "ws_plan_launch": (ctypes.c_int, [vp, vp]),

@@ -276,6 +276,60 @@ void view_shortcuts(const ws_view& v, const ws_cloud* c, uint32_t* fast, uint32_
 double host_depth_range(const float mv[16], const double bmin[3], const double bmax[3], int* visible,
                         float* depth_min, float* depth_scale);
 
+// det_min[b]: the least f32 det that makeKeys keeps with alpha byte b under
+// `cull`, found by bisection over the ordered non-negative f32 values (the
+// test is monotone in det: max, the square root and the two products are);
+// -inf when it keeps every det. The table depends on cull alone: the last few
+// are kept, so a frame loop's calls (one cull) compute it once.
+static void det_thresholds(float cull, float out[256]) {
+    struct Entry {
+        uint32_t bits;
+        float t[256];
+    };
+    static std::mutex mu;
+    static std::vector<Entry> cache;
+    static size_t next = 0;
+    uint32_t bits;
+    std::memcpy(&bits, &cull, 4);
+    std::lock_guard<std::mutex> lock(mu);
+    for (const Entry& e : cache)
+        if (e.bits == bits) {
+            std::memcpy(out, e.t, sizeof(e.t));
+            return;
+        }
+    Entry e;
+    e.bits = bits;
+    for (uint32_t b = 0; b < 256; ++b) {
+        const float alpha = (float)b / 255.0f;
+        auto kept = [&](float det) {
+            const float area = 6.2831853f * std::sqrt(std::fmax(det, 0.0f));
+            return !(alpha * area < cull);
+        };
+        if (kept(0.0f)) {
+            e.t[b] = -INFINITY;
+            continue;
+        }
+        uint32_t lo = 0, hi = 0x7f800000u;   // kept(lo) false, kept(+inf) true
+        while (hi - lo > 1) {
+            const uint32_t mid = lo + (hi - lo) / 2;
+            float f;
+            std::memcpy(&f, &mid, 4);
+            if (kept(f))
+                hi = mid;
+            else
+                lo = mid;
+        }
+        std::memcpy(&e.t[b], &hi, 4);
+    }
+    std::memcpy(out, e.t, sizeof(e.t));
+    if (cache.size() < 8) {
+        cache.push_back(e);
+    } else {
+        cache[next] = e;
+        next = (next + 1) % cache.size();
+    }
+}
+
 // The view's constants for the keys phase, computed here once per job with
 // the same IEEE operations (f32 products and quotients, the FP64 depth range;
 // built with -ffp-contract=off) as the device's make_consts.
@@ -321,31 +375,7 @@ void fill_view_consts(JobDesc& d) {
     c.r2 = up(std::fabs((double)M[2]) + std::fabs((double)M[6]) + std::fabs((double)M[10]));
     c.xcap = up(c.xhi);
     c.ycap = up(c.yhi);
-    // det_min[b]: the least f32 det that makeKeys keeps with alpha byte b,
-    // found by bisection over the ordered non-negative f32 values (the test
-    // is monotone in det: max, the square root and the two products are).
-    for (uint32_t b = 0; b < 256; ++b) {
-        const float alpha = (float)b / 255.0f;
-        auto kept = [&](float det) {
-            const float area = 6.2831853f * std::sqrt(std::fmax(det, 0.0f));
-            return !(alpha * area < d.cull);
-        };
-        if (kept(0.0f)) {
-            c.det_min[b] = -INFINITY;
-            continue;
-        }
-        uint32_t lo = 0, hi = 0x7f800000u;   // kept(lo) false, kept(+inf) true
-        while (hi - lo > 1) {
-            const uint32_t mid = lo + (hi - lo) / 2;
-            float f;
-            std::memcpy(&f, &mid, 4);
-            if (kept(f))
-                hi = mid;
-            else
-                lo = mid;
-        }
-        std::memcpy(&c.det_min[b], &hi, 4);
-    }
+    det_thresholds(d.cull, c.det_min);
 }
 
 // Emitter jobs (ws_sort_particles): the ring, the view and the outputs.
@@ -459,28 +489,32 @@ static int launch_jobs(ws_ctx* ctx, const std::vector<uint32_t>& ns, int njobs, 
         if ((e = cudaEventSynchronize(ctx->launched)) != cudaSuccess) return cuda_error(ctx, e, "ws_sort");
         if ((e = ctx->scratch.ensure(S.bytes)) != cudaSuccess) return cuda_error(ctx, e, "ws_sort scratch");
     }
-    // Pinned staging is rewritten only after its previous upload finished.
-    if ((e = cudaEventSynchronize(ctx->staged)) != cudaSuccess) return cuda_error(ctx, e, "ws_sort");
     const size_t tb = table_bytes(njobs, S);
-    if ((e = ctx->jobs_h.ensure(tb)) != cudaSuccess) return cuda_error(ctx, e, "ws_sort staging");
     if (tb > ctx->jobs_d.bytes) {
         if ((e = cudaEventSynchronize(ctx->launched)) != cudaSuccess) return cuda_error(ctx, e, "ws_sort");
         if ((e = ctx->jobs_d.ensure(tb)) != cudaSuccess) return cuda_error(ctx, e, "ws_sort job table");
     }
-    JobDesc* hj = static_cast<JobDesc*>(ctx->jobs_h.p);
     char* scratch = static_cast<char*>(ctx->scratch.p);
-    fill(hj, S, scratch);
-    write_table(ctx->jobs_h.p, hj, njobs, S);
     if (stream != ctx->stream) cudaStreamWaitEvent(stream, ctx->launched, 0);
     if (njobs == 1) {
-        stage_kernel<<<1, 1024, 0, stream>>>(*hj, static_cast<JobDesc*>(ctx->jobs_d.p),
+        // A lone job's description travels with the staging kernel's launch:
+        // no pinned buffer, so nothing to wait for before writing it.
+        JobDesc one;
+        fill(&one, S, scratch);
+        stage_kernel<<<1, 1024, 0, stream>>>(one, static_cast<JobDesc*>(ctx->jobs_d.p),
                                              reinterpret_cast<uint32_t*>(scratch), (uint32_t)(S.ctl_bytes / 4));
         if ((e = cudaGetLastError()) != cudaSuccess) return cuda_error(ctx, e, "ws_sort staging");
-    } else if ((e = cudaMemcpyAsync(ctx->jobs_d.p, ctx->jobs_h.p, tb, cudaMemcpyHostToDevice, stream)) !=
-               cudaSuccess) {
-        return cuda_error(ctx, e, "ws_sort upload");
+    } else {
+        // Pinned staging is rewritten only after its previous upload finished.
+        if ((e = cudaEventSynchronize(ctx->staged)) != cudaSuccess) return cuda_error(ctx, e, "ws_sort");
+        if ((e = ctx->jobs_h.ensure(tb)) != cudaSuccess) return cuda_error(ctx, e, "ws_sort staging");
+        JobDesc* hj = static_cast<JobDesc*>(ctx->jobs_h.p);
+        fill(hj, S, scratch);
+        write_table(ctx->jobs_h.p, hj, njobs, S);
+        if ((e = cudaMemcpyAsync(ctx->jobs_d.p, ctx->jobs_h.p, tb, cudaMemcpyHostToDevice, stream)) != cudaSuccess)
+            return cuda_error(ctx, e, "ws_sort upload");
+        cudaEventRecord(ctx->staged, stream);
     }
-    cudaEventRecord(ctx->staged, stream);
     if (njobs != 1 && (e = cudaMemsetAsync(scratch, 0, S.ctl_bytes, stream)) != cudaSuccess)
         return cuda_error(ctx, e, "ws_sort reset");
     const size_t n_items = (size_t)kPhases * S.segs.size();
@@ -622,6 +656,8 @@ extern "C" int ws_destroy(ws_ctx* ctx) {
     ctx->scratch.release();
     ctx->jobs_d.release();
     ctx->out_d.release();
+    ctx->copy_d.release();
+    ctx->copy_h.release();
     ctx->thr_d.release();
     ctx->draw_d.release();
     ctx->pairs_d.release();
@@ -988,6 +1024,122 @@ extern "C" int ws_sort_batch(ws_ctx* ctx, int njobs, const ws_job* jobs, void* s
     }
     cudaSetDevice(ctx->device);
     return run_batch(ctx, jobs, njobs, stream_p ? static_cast<cudaStream_t>(stream_p) : ctx->stream);
+}
+
+// One job's results on their way to host memory (ws_sort_batch_host): the
+// device outputs and the device addresses of the caller's pinned buffers.
+struct HostCopy {
+    const uint32_t* order;
+    const uint32_t* keys;       // or null
+    const uint32_t* count;
+    uint32_t* horder;
+    uint32_t* hkeys;            // or null
+    uint32_t* hcount;
+    uint32_t n;                 // the job's splats: no count read back exceeds it
+    uint32_t pad[3];
+};
+
+// Every job's survivors into mapped host memory: blockIdx.y is the job, the
+// x blocks stride over its survivors; consecutive threads write consecutive
+// words. Block (0, j) writes the count.
+__global__ void __launch_bounds__(256) copy_jobs_kernel(const HostCopy* __restrict__ jobs) {
+    const HostCopy J = jobs[blockIdx.y];
+    // After a device error a job's count may never have been written: the
+    // copy stays inside the job's buffers whatever it holds.
+    const uint32_t c = min(*J.count, J.n);
+    if (blockIdx.x == 0 && threadIdx.x == 0) *J.hcount = c;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < c; i += gridDim.x * blockDim.x) {
+        J.horder[i] = J.order[i];
+        if (J.hkeys) J.hkeys[i] = J.keys[i];
+    }
+}
+
+extern "C" int ws_sort_batch_host(ws_ctx* ctx, int njobs, const ws_job* jobs, void* stream_p) {
+    NvtxRange nvtx("ws_sort_batch_host");
+    if (!ctx) return WS_ERR_ARG;
+    if (njobs < 0 || (njobs && !jobs)) return set_error(ctx, WS_ERR_ARG, "ws_sort_batch_host: bad job list");
+    if (njobs == 0) return WS_OK;
+    if (njobs > (1 << 16)) return set_error(ctx, WS_ERR_ARG, "ws_sort_batch_host: too many jobs");
+    for (int j = 0; j < njobs; ++j) {
+        int rc;
+        if ((rc = check_cloud(ctx, jobs[j].cloud)) || (rc = check_view(ctx, &jobs[j].view))) return rc;
+        if (!jobs[j].order || !jobs[j].count)
+            return set_error(ctx, WS_ERR_ARG, "ws_sort_batch_host: job %d has no output", j);
+    }
+    cudaSetDevice(ctx->device);
+    cudaStream_t stream = stream_p ? static_cast<cudaStream_t>(stream_p) : ctx->stream;
+    cudaError_t e;
+    // Device outputs, one region per job: order, keys, count.
+    std::vector<size_t> off(njobs);
+    size_t words = 0;
+    for (int j = 0; j < njobs; ++j) {
+        off[j] = words;
+        words += align_up(2 * (size_t)jobs[j].cloud->n + 1, 64);
+    }
+    if ((e = cudaEventSynchronize(ctx->launched)) != cudaSuccess) return cuda_error(ctx, e, "ws_sort_batch_host");
+    if ((e = ctx->out_d.ensure(words * sizeof(uint32_t) + 256)) != cudaSuccess)
+        return cuda_error(ctx, e, "ws_sort_batch_host output");
+    uint32_t* d = static_cast<uint32_t*>(ctx->out_d.p);
+    std::vector<ws_job> dj(jobs, jobs + njobs);
+    std::vector<HostCopy> hc(njobs);
+    bool direct = true;
+    for (int j = 0; j < njobs; ++j) {
+        const size_t n = jobs[j].cloud->n;
+        dj[j].order = d + off[j];
+        dj[j].keys = jobs[j].keys ? d + off[j] + n : nullptr;
+        dj[j].count = d + off[j] + 2 * n;
+        HostCopy& h = hc[j];
+        std::memset(&h, 0, sizeof(h));
+        h.order = dj[j].order;
+        h.keys = dj[j].keys;
+        h.count = dj[j].count;
+        h.horder = mapped_alias(jobs[j].order);
+        h.hkeys = jobs[j].keys ? mapped_alias(jobs[j].keys) : nullptr;
+        h.hcount = mapped_alias(jobs[j].count);
+        h.n = (uint32_t)n;
+        direct = direct && h.horder && h.hcount && (!jobs[j].keys || h.hkeys);
+    }
+    int rc = run_batch(ctx, dj.data(), njobs, stream);
+    if (rc) return rc;
+    if (direct) {
+        // The copy table's pinned staging is free: every call ends with a
+        // synchronisation.
+        const size_t tb = (size_t)njobs * sizeof(HostCopy);
+        if ((e = ctx->copy_h.ensure(tb)) != cudaSuccess || (e = ctx->copy_d.ensure(tb)) != cudaSuccess)
+            return cuda_error(ctx, e, "ws_sort_batch_host staging");
+        std::memcpy(ctx->copy_h.p, hc.data(), tb);
+        uint32_t* hw = static_cast<uint32_t*>(ctx->count_h.p);
+        uint32_t max_n = 0;
+        for (int j = 0; j < njobs; ++j) max_n = std::max(max_n, jobs[j].cloud->n);
+        const uint32_t bx = std::max(1u, std::min((max_n + 2047) / 2048, 64u));
+        if ((e = cudaMemcpyAsync(ctx->copy_d.p, ctx->copy_h.p, tb, cudaMemcpyHostToDevice, stream)) != cudaSuccess)
+            return cuda_error(ctx, e, "ws_sort_batch_host upload");
+        copy_jobs_kernel<<<dim3(bx, (unsigned)njobs), 256, 0, stream>>>(static_cast<const HostCopy*>(ctx->copy_d.p));
+        if ((e = cudaGetLastError()) != cudaSuccess ||
+            (e = cudaMemcpyAsync(hw, ctx->err_d, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
+            (e = cudaStreamSynchronize(stream)) != cudaSuccess)
+            return cuda_error(ctx, e, "ws_sort_batch_host");
+        if (hw[0]) return take_device_error(ctx);
+        return WS_OK;
+    }
+    // Pageable outputs: the counts first, then each job's survivors.
+    std::vector<uint32_t> counts(njobs);
+    for (int j = 0; j < njobs; ++j)
+        if ((e = cudaMemcpyAsync(&counts[j], dj[j].count, 4, cudaMemcpyDeviceToHost, stream)) != cudaSuccess)
+            return cuda_error(ctx, e, "ws_sort_batch_host");
+    if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return cuda_error(ctx, e, "ws_sort_batch_host");
+    if ((rc = take_device_error(ctx))) return rc;
+    for (int j = 0; j < njobs; ++j) {
+        *jobs[j].count = counts[j];
+        if (!counts[j]) continue;
+        if ((e = cudaMemcpyAsync(jobs[j].order, dj[j].order, (size_t)counts[j] * 4, cudaMemcpyDeviceToHost, stream)) !=
+                cudaSuccess ||
+            (jobs[j].keys && (e = cudaMemcpyAsync(jobs[j].keys, dj[j].keys, (size_t)counts[j] * 4,
+                                                  cudaMemcpyDeviceToHost, stream)) != cudaSuccess))
+            return cuda_error(ctx, e, "ws_sort_batch_host download");
+    }
+    if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return cuda_error(ctx, e, "ws_sort_batch_host download");
+    return WS_OK;
 }
 
 // -------------------------------------------------------------- self-test

@@ -304,7 +304,6 @@ __device__ __forceinline__ void keys_sweep(const ViewConsts& c, KeysSmem<NT>& sm
     FastView fv;
     if constexpr (kFast) fv = fast_view_of(c);
     const bool persp = c.persp;
-    const float cull = c.cull;
     const float afx = c.afx, afy = c.afy, r0 = c.r0, r1 = c.r1, r2 = c.r2, xcap = c.xcap, ycap = c.ycap;
     const uint32_t keep_byte = c.keep_byte, faint_max = c.faint_max;
     const float4* centers = sm.centers[buf];

@@ -81,7 +81,8 @@ struct ws_ctx {
     ws_params params{};
     ws_params tuning[32] = {};        // per floor(log2(splats)); tile 0: unset
     int tuning_n = 0;
-    wsort::DevBuf scratch, jobs_d, items_d, out_d;
+    wsort::DevBuf scratch, jobs_d, items_d, out_d, copy_d;
+    wsort::HostBuf copy_h;            // ws_sort_batch_host: the copy table, pinned
     wsort::HostBuf jobs_h, items_h, count_h;
     uint32_t* err_d = nullptr;        // sticky device error: code, work item
     wsort::LaunchShape shape;         // the last launch's shape, reused while ns and params repeat

@@ -138,6 +138,20 @@ class Context:
             arr[j].count = c
         self.check(self.lib.ws_sort_batch(self.handle, len(jobs), arr, stream))
 
+    def sort_batch_host(self, jobs: list[tuple], stream: int | None = None) -> None:
+        """jobs as sort_batch, with host pointers (pinned for the one-copy
+        path): every job's count, order and keys (or None) filled on return
+        (ws_sort_batch_host)."""
+        arr = (WsJob * len(jobs))()
+        for j, (sp, view, o, k, c) in enumerate(jobs):
+            sp._check_alive()
+            arr[j].cloud = sp.handle
+            arr[j].view = view
+            arr[j].order = o
+            arr[j].keys = k
+            arr[j].count = c
+        self.check(self.lib.ws_sort_batch_host(self.handle, len(jobs), arr, stream))
+
     def sort_batch_shaded(self, jobs: list[tuple], shades: list[tuple], stream: int | None = None) -> None:
         """jobs as sort_batch; shades: per job (eye, shaded_ptr), the eye in
         the cloud's space and a device array of its cloud's count words that
