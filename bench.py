@@ -1,32 +1,39 @@
 """Benchmark of the splat depth-key + stable counting sort on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                    [--workload clusters-1M|uniform-100k|slab-6M|mixed-64] [--cull C]
+                    [--workload mixed-64|clusters-1M|uniform-100k|slab-6M] [--cull C]
 
-One step is one sort of one batch of synthetic splats: for the default
-workload (clusters-1M: 1,000,000 splats from 32 Gaussian clusters, one view
-framing them, cull 0.5) one plain ws_sort of the resident cloud. Prints one
-JSON line:
+One step is one pass of the sort over one batch of synthetic splats. The
+default workload, mixed-64, is 64 (scene, view) jobs of 10k-2M splats (25M in
+all, cull 0.5), every job's cloud resident in HBM; one step is one
+graph-captured launch of the batch (ws_plan_launch: the job table up, the
+counters reset, the keys kernel and the two digit passes over all 64 jobs).
+Prints one JSON line:
 
-  value        Msplats/s (whole job, all ranks), cloud resident in HBM,
-               outputs to device memory, CUDA events on the launching stream,
-               L2 flushed (a 256 MiB write) before every timed step
-  e2e          the same metric through the public call a user makes
-               (ws_sort with host outputs): per step the view goes up and the
-               count, permutation and keys come back to pinned host memory
-  roofline     the sort kernel's algorithmic bytes / its event-timed duration
-               against the measured HBM copy bandwidth
+  value        Msplats/s (whole job, all ranks), outputs to device memory,
+               CUDA events on the launching stream, L2 flushed (a 256 MiB
+               write) before every timed step
+  e2e          the same metric through the public batch call with host
+               outputs (ws_sort_batch_host): per step every job's survivor
+               count and order come back to pinned host memory; the bytes
+               each way are the library's own copy counters
+  roofline     32 N + 8 S summed over the jobs / the sort kernels' event-timed
+               duration, against the measured HBM copy bandwidth
   cpu_baseline the CPU oracle (C++ restatement of the reference's path, all
-               host threads) on a bounded sample of the same workload
-  suite        the other measured targets: the plain kernel at 6M splats
-               (slab-6M) and batched vs plain on the 64-job mixed workload
+               host threads) on a bounded sample of the same jobs
+  batch        the same 64 jobs as 64 plain ws_sort calls, as one ws_sort_batch
+               call and as the graph launch
+  suite        the other measured targets: clusters-1M and slab-6M as plain
+               single-cloud sorts, the served stream, particles, shading,
+               decoding and drawing
 
---impl reference times the reference's algorithm on the host CPU instead
-(the oracle port; the reference's own JavaScript needs Node, which this
-machine does not have) and prints the same line with "impl": "reference".
-With N > 1 (torchrun), every rank sorts its own replica of the workload
-(weak scaling, no collective on the data path); the time is the max over
-ranks.
+--workload clusters-1M (or uniform-100k, slab-6M) makes one plain ws_sort of
+that cloud the step instead. --impl reference times the reference's
+algorithm on the host CPU over the same jobs (the oracle port; the
+reference's own JavaScript needs Node, which this machine does not have) and
+prints the same line with "impl": "reference". With N > 1 (torchrun) every
+rank sorts its own batch of 64 jobs (other seeds), weak scaling with no
+collective on the data path; the time is the max over ranks.
 """
 from __future__ import annotations
 
@@ -53,10 +60,10 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="wsort", choices=["wsort", "reference"])
-    ap.add_argument("--workload", default="clusters-1M",
-                    choices=["clusters-1M", "uniform-100k", "slab-6M", "mixed-64"])
+    ap.add_argument("--workload", default="mixed-64",
+                    choices=["mixed-64", "clusters-1M", "uniform-100k", "slab-6M"])
     ap.add_argument("--cull", type=float, default=0.5)
-    ap.add_argument("--no-suite", action="store_true", help="skip the slab-6M / mixed-64 side measurements")
+    ap.add_argument("--no-suite", action="store_true", help="skip the side measurements")
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU baseline sample length")
     ap.add_argument("--tile", type=int, default=0,
                     help="fixed least splats a segment covers (skips the autotuner; with --ctas)")
@@ -194,8 +201,8 @@ def run_reference(args, rank: int):
         "unit": "Msplats/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 keys, u32 sort", "data": "synthetic (seeded)",
-        "config": {"workload": args.workload, "splats_per_step": total // args.steps, "cull": args.cull,
-                   "viewport": [1920, 1080]},
+        "config": {"workload": args.workload, "jobs": len(jobs), "splats_per_step": total // args.steps,
+                   "cull": args.cull, "viewport": [1920, 1080]},
         "cpu_baseline": {"value": value, "unit": "Msplats/s", "cores": threads, "kind": "port",
                          "sample": f"{args.steps} steps of the full workload; C++ restatement of the reference's "
                                    f"makeKeys + stable counting sort (the reference's JavaScript needs Node, absent)"},
@@ -204,13 +211,18 @@ def run_reference(args, rank: int):
     print(json.dumps(line), flush=True)
 
 
-def timed_sorts(ctx, torch, steps, flush, fn):
+def timed_sorts(ctx, torch, steps, flush, fn, host_start=False):
     """Runs fn() `steps` times, each bracketed by CUDA events on torch's
-    current stream with an L2 flush before it. Returns total ms."""
+    current stream with an L2 flush before it. Returns total ms. host_start:
+    the flush finishes before the start event is recorded, so a call's host
+    work before its first launch is inside the bracket (the end-to-end
+    measurements)."""
     stream = torch.cuda.current_stream()
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
     for a, b in evs:
         flush.zero_()
+        if host_start:
+            stream.synchronize()
         a.record(stream)
         fn()
         b.record(stream)
@@ -218,10 +230,10 @@ def timed_sorts(ctx, torch, steps, flush, fn):
     return sum(a.elapsed_time(b) for a, b in evs)
 
 
-def plain_measure(ctx, torch, jobs, steps, warmup, flush):
-    """Plain ws_sort per job (device outputs). Returns dict with totals."""
+def load_jobs(ctx, torch, jobs):
+    """Each job's cloud resident on the device, its view, and device outputs
+    (order, keys, count)."""
     from winding_b200 import make_view, parse_splats
-    stream = torch.cuda.current_stream().cuda_stream
     clouds, outs, views = [], [], []
     for j in jobs:
         sp = parse_splats(j.records, ctx)
@@ -232,21 +244,50 @@ def plain_measure(ctx, torch, jobs, steps, warmup, flush):
         clouds.append(sp)
         outs.append((o, k, c))
         views.append(make_view(j.view.model_view, j.view.projection, j.view.viewport, j.view.cull))
+    return {"clouds": clouds, "views": views, "outs": outs, "splats": sum(sp.count for sp in clouds)}
+
+
+def time_plain(ctx, torch, p, steps, warmup, flush):
+    """One plain ws_sort per job (device outputs) per step; fills p's ms,
+    kernel_ms, launches and survivors."""
+    stream = torch.cuda.current_stream().cuda_stream
 
     def one():
-        for sp, v, (o, k, c) in zip(clouds, views, outs):
+        for sp, v, (o, k, c) in zip(p["clouds"], p["views"], p["outs"]):
             ctx.sort_device(sp, v, o.data_ptr(), k.data_ptr(), c.data_ptr(), stream)
 
     for _ in range(warmup):
         one()
     torch.cuda.synchronize()
     ctx.timing(True)
-    ms = timed_sorts(ctx, torch, steps, flush, one)
-    kms, launches = ctx.timing_read()
+    p["ms"] = timed_sorts(ctx, torch, steps, flush, one)
+    p["kernel_ms"], p["launches"] = ctx.timing_read()
     ctx.timing(False)
-    survivors = [int(c.item()) for _, _, c in outs]
-    return {"clouds": clouds, "views": views, "outs": outs, "ms": ms, "kernel_ms": kms, "launches": launches,
-            "survivors": survivors, "splats": sum(sp.count for sp in clouds)}
+    p["survivors"] = [int(c.item()) for _, _, c in p["outs"]]
+    return p
+
+
+def plain_measure(ctx, torch, jobs, steps, warmup, flush):
+    """Plain ws_sort per job (device outputs). Returns dict with totals."""
+    return time_plain(ctx, torch, load_jobs(ctx, torch, jobs), steps, warmup, flush)
+
+
+def tune_batch(ctx, p, args):
+    """The launch parameters: fixed from the command line, or the autotuner's
+    choice per size bucket (each bucket's first job alone, and the whole
+    batch)."""
+    from winding_b200 import autotune
+    if args.tile and args.ctas:
+        ctx.set_params(tile=args.tile, ctas_per_sm=args.ctas, segs_per_cta=args.segs)
+        return {autotune.bucket(p["splats"]): (args.tile, args.ctas, args.segs)}
+    pairs = list(zip(p["clouds"], p["views"]))
+    per_bucket = {}
+    for pair in pairs:
+        per_bucket.setdefault(autotune.bucket(pair[0].count), pair)
+    sets = [[pr] for pr in per_bucket.values()]
+    if len(pairs) > 1:
+        sets.append(pairs)
+    return autotune.tune(ctx, sets)
 
 
 def survivors_at_cull0(ctx, torch, plain):
@@ -302,111 +343,11 @@ def _run_wsort(args, rank, world, local_rank, torch):
         if rank == 0:
             print(json.dumps({"only": args.only, "result": result}), flush=True)
         return
-    jobs = make_jobs(args.workload, args.cull, seed_offset=0)
-    # A batch of independent jobs is split across ranks (no collective on
-    # the data path); a single cloud runs as one replica per rank.
-    all_splats = sum(len(j.records) for j in jobs)
-    sharded = world > 1 and len(jobs) > 1
-    if sharded:
-        from winding_b200 import shard
-        jobs = [jobs[i] for i in shard.my_jobs([len(j.records) for j in jobs], rank, world)]
-
-    from winding_b200 import autotune
-    fixed = bool(args.tile and args.ctas)
-    if fixed:
-        ctx.set_params(tile=args.tile, ctas_per_sm=args.ctas, segs_per_cta=args.segs)
-    plain = plain_measure(ctx, torch, jobs, 0, args.warmup, flush)   # load + warm
-    if fixed:
-        tuned = {autotune.bucket(plain["splats"]): (args.tile, args.ctas, args.segs)}
+    if args.workload == "mixed-64":
+        line, jobs = batch_line(args, rank, world, dist, ctx, torch, flush)
     else:
-        tuned = autotune.tune(ctx, [list(zip(plain["clouds"], plain["views"]))])
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    clocks = Clocks(local_rank)
-    clocks.start()
-    ctx.timing(True)
-    stream = torch.cuda.current_stream().cuda_stream
-
-    def one():
-        for sp, v, (o, k, c) in zip(plain["clouds"], plain["views"], plain["outs"]):
-            ctx.sort_device(sp, v, o.data_ptr(), k.data_ptr(), c.data_ptr(), stream)
-
-    ms = timed_sorts(ctx, torch, args.steps, flush, one)
-    kms, launches = ctx.timing_read()
-    ctx.timing(False)
-    clk = clocks.stop()
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    splats_per_step = plain["splats"]
-    job_splats = all_splats if sharded else splats_per_step * world
-    value = job_splats * args.steps / (ms_max / 1e3) / 1e6
-    survivors = [int(c.item()) for _, _, c in plain["outs"]]
-
-    # End to end through the public call: host outputs, every step.
-    n_max = max(sp.count for sp in plain["clouds"])
-    host_order = torch.empty(n_max, dtype=torch.int32).pin_memory()
-    import ctypes
-    cnt = ctypes.c_uint32()
-    from winding_b200 import _lib
-
-    def one_e2e():
-        for sp, v in zip(plain["clouds"], plain["views"]):
-            ctx.check(ctx.lib.ws_sort(ctx.handle, sp.handle, ctypes.byref(v), host_order.data_ptr(),
-                                      None, ctypes.byref(cnt), _lib.WS_HOST_OUTPUT, stream))
-
-    for _ in range(2):
-        one_e2e()
-    e2e_steps = max(3, min(args.steps, 20))
-    e2e_ms = timed_sorts(ctx, torch, e2e_steps, flush, one_e2e)
-    view_bytes = 35 * 4 * len(jobs)
-    if dist:
-        t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_value = job_splats * e2e_steps / (e2e_ms / 1e3) / 1e6
-    d2h = sum(4 + 4 * s for s in survivors)
-
-    line = {
-        "metric": "Msplats/s sorted (bit-exact stable order)", "value": value, "unit": "Msplats/s",
-        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
-        "higher_is_better": True, "scaling": "strong" if sharded else "weak", "vs_baseline": None,
-        "dtype": "f32 keys, u32 sort",
-        "data": "synthetic (seeded)",
-        "config": {"workload": args.workload, "splats_per_step": splats_per_step, "survivors_per_step": sum(survivors),
-                   "cull": args.cull, "viewport": [1920, 1080], "l2": "flushed (256 MiB write) before each step",
-                   "parallelism": (f"jobs sharded over {world} ranks" if sharded else f"replicas x{world}")
-                   if world > 1 else "single GPU",
-                   "tuned": {str(b): {"tile": t, "ctas_per_sm": c, "segs_per_cta": g}
-                             for b, (t, c, g) in tuned.items()}},
-        "e2e": {"value": e2e_value, "unit": "Msplats/s", "h2d_bytes_per_step": view_bytes, "d2h_bytes_per_step": d2h,
-                "call": "ws_sort(WS_HOST_OUTPUT) into a pinned host buffer: the order and the survivor count, "
-                        "the reference's outputs (its keys stay unsorted on the device and are never read back)"},
-        # each ws_sort of a lone job is two launches, the staging kernel and the sort
-        "gpu_launches": launches * (2 if len(jobs) == 1 else 1),
-        "clocks": clk,
-    }
+        line, jobs = single_line(args, rank, world, dist, ctx, torch, flush)
     if rank == 0:
-        peak, src = peak_hbm()
-        front = survivors_at_cull0(ctx, torch, plain) if args.cull > 0 else survivors
-        algo = sum(algorithmic_bytes(sp.count, s) for sp, s in zip(plain["clouds"], survivors))
-        lay = sum(layout_bytes(sp.count, f, s, args.cull) for sp, f, s in zip(plain["clouds"], front, survivors))
-        kernel_s = kms / max(launches, 1) / 1e3 * len(jobs)   # per step
-        achieved = algo / kernel_s / 1e9
-        traffic = ncu_traffic(args.workload, args.cull)
-        p = ctx.params
-        line["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                            "frac": achieved / peak, "traffic": traffic, "peak_source": src,
-                            "kernel": "wsort::sort_kernel",
-                            "kernel_us_per_step": kernel_s * 1e6, "algorithmic_bytes_per_step": algo,
-                            "algorithmic_bytes": "32 N + 8 S",
-                            "layout_bytes_per_step": lay,
-                            "layout_frac": lay / kernel_s / 1e9 / peak}
         if world == 1:
             v, sample = cpu_baseline(jobs, args.cpu_seconds, os.cpu_count() or 1)
             v1, sample1 = cpu_baseline(jobs, max(args.cpu_seconds / 3, 1.0), 1)
@@ -421,71 +362,240 @@ def _run_wsort(args, rank, world, local_rank, torch):
                 line["suite"] = suite(ctx, torch, flush, args)
             except Exception as exc:   # the headline line still prints
                 line["suite"] = {"error": f"{type(exc).__name__}: {exc}"}
-    if rank == 0:
         print(json.dumps(line), flush=True)
-    for sp in plain["clouds"]:
-        sp.destroy()
     ctx.close()
 
 
-def suite(ctx, torch, flush, args):
-    """Side measurements of the two targets: the plain kernel at 6M splats
-    against the HBM roofline, and batched vs plain on the mixed workload."""
-    out = {}
-    peak, src = peak_hbm()
-    from winding_b200 import autotune
-    # slab-6M, plain kernel
-    jobs = make_jobs("slab-6M", 0.5)
-    p = plain_measure(ctx, torch, jobs, 0, 0, flush)
-    slab_tuned = autotune.tune(ctx, [list(zip(p["clouds"], p["views"]))])
-    for sp in p["clouds"]:
-        sp.destroy()
-    p = plain_measure(ctx, torch, jobs, 20, 3, flush)
-    n = p["splats"]
-    algo = sum(algorithmic_bytes(sp.count, s) for sp, s in zip(p["clouds"], p["survivors"]))
-    kernel_s = p["kernel_ms"] / p["launches"] / 1e3
-    out["slab-6M"] = {"splats": n, "survivors": p["survivors"][0], "kernel_us": kernel_s * 1e6,
-                      "step_us": p["ms"] / 20 * 1e3, "msplats_s": n / (p["ms"] / 20 / 1e3) / 1e6,
-                      "achieved_gbs": algo / kernel_s / 1e9, "frac": algo / kernel_s / 1e9 / peak,
-                      "peak_source": src, "traffic": ncu_traffic("slab-6M", 0.5),
-                      "tuned": {str(b): list(v) for b, v in slab_tuned.items()}}
-    for sp in p["clouds"]:
-        sp.destroy()
-    del p
-    # mixed-64: 64 plain calls vs one batched launch vs the graph-captured plan,
-    # each tuned for its own launch sizes
-    jobs = make_jobs("mixed-64", 0.5)
-    p = plain_measure(ctx, torch, jobs, 0, 0, flush)
-    pairs = list(zip(p["clouds"], p["views"]))
-    per_bucket = {}
-    for pair in pairs:
-        per_bucket.setdefault(autotune.bucket(pair[0].count), pair)
-    mixed_tuned = autotune.tune(ctx, [[pr] for pr in per_bucket.values()] + [pairs])
-    for sp in p["clouds"]:
-        sp.destroy()
-    p = plain_measure(ctx, torch, jobs, 10, 2, flush)
-    total = p["splats"]
+def max_over_ranks(dist, torch, ms):
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def batch_line(args, rank, world, dist, ctx, torch, flush):
+    """The default step: the 64 mixed jobs as one graph-captured launch."""
+    jobs = make_jobs("mixed-64", args.cull, seed_offset=rank)   # each rank its own batch: weak scaling
+    p = load_jobs(ctx, torch, jobs)
+    time_plain(ctx, torch, p, 0, 1, flush)   # warm
+    tuned = tune_batch(ctx, p, args)
+    stream = torch.cuda.current_stream().cuda_stream
     specs = [(sp, v, o.data_ptr(), k.data_ptr(), c.data_ptr())
              for sp, v, (o, k, c) in zip(p["clouds"], p["views"], p["outs"])]
-    stream = torch.cuda.current_stream().cuda_stream
+    plan = ctx.plan(specs)
+    for _ in range(args.warmup):
+        plan.launch(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(local_rank_of(torch))
+    clocks.start()
+    ms = timed_sorts(ctx, torch, args.steps, flush, lambda: plan.launch(stream))
+    clk = clocks.stop()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ms_max = max_over_ranks(dist, torch, ms)
+    plan.close()
+    total = p["splats"]
+    survivors = [int(c.item()) for _, _, c in p["outs"]]
+    value = total * world * args.steps / (ms_max / 1e3) / 1e6
+
+    # The same launch through ws_sort_batch, its three kernels bracketed by
+    # the library's timing events: the kernel time of the roofline.
+    reps = 10
     for _ in range(2):
         ctx.sort_batch(specs, stream)
-    b_ms = timed_sorts(ctx, torch, 10, flush, lambda: ctx.sort_batch(specs, stream))
-    plan = ctx.plan(specs)
+    ctx.timing(True)
+    b_ms = timed_sorts(ctx, torch, reps, flush, lambda: ctx.sort_batch(specs, stream))
+    kms, launches = ctx.timing_read()
+    ctx.timing(False)
+    kernel_s = kms / max(launches, 1) / 1e3
+
+    # End to end through the public batch call: every job's count and order
+    # into pinned host memory, every step.
+    host = [(torch.empty(max(sp.count, 1), dtype=torch.int32).pin_memory(), torch.zeros(1, dtype=torch.int32)
+             .pin_memory()) for sp in p["clouds"]]
+    hspecs = [(sp, v, ho.data_ptr(), None, hc.data_ptr()) for sp, v, (ho, hc) in zip(p["clouds"], p["views"], host)]
     for _ in range(2):
-        plan.launch(stream)
-    g_ms = timed_sorts(ctx, torch, 10, flush, lambda: plan.launch(stream))
-    plan.close()
-    plain_rate = total * 10 / (p["ms"] / 1e3) / 1e6
-    batch_rate = total * 10 / (b_ms / 1e3) / 1e6
-    graph_rate = total * 10 / (g_ms / 1e3) / 1e6
-    out["mixed-64"] = {"jobs": len(jobs), "splats": total, "plain_msplats_s": plain_rate,
-                       "batched_msplats_s": batch_rate, "graph_msplats_s": graph_rate,
-                       "batched_vs_plain": batch_rate / plain_rate, "graph_vs_plain": graph_rate / plain_rate,
-                       "plain_ms_per_step": p["ms"] / 10, "graph_ms_per_step": g_ms / 10,
-                       "tuned": {str(b): list(v) for b, v in mixed_tuned.items()}}
+        ctx.sort_batch_host(hspecs, stream)
+    e2e_steps = max(3, min(args.steps, 20))
+    ctx.copy_stats(reset=True)
+    e2e_ms = timed_sorts(ctx, torch, e2e_steps, flush, lambda: ctx.sort_batch_host(hspecs, stream), host_start=True)
+    h2d, d2h = ctx.copy_stats(reset=True)
+    e2e_ms = max_over_ranks(dist, torch, e2e_ms)
+    e2e_value = total * world * e2e_steps / (e2e_ms / 1e3) / 1e6
+    assert all(int(hc[0]) == s for (_, hc), s in zip(host, survivors))
+
+    line = {
+        "metric": "Msplats/s sorted (bit-exact stable order)", "value": value, "unit": "Msplats/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 keys, u32 sort", "data": "synthetic (seeded)",
+        "config": {"workload": "mixed-64", "jobs": len(jobs), "splats_per_step": total * world,
+                   "survivors_per_step": sum(survivors), "job_splats": [10_000, 2_000_000], "cull": args.cull,
+                   "viewport": [1920, 1080], "l2": "flushed (256 MiB write) before each step",
+                   "launch": "ws_plan_launch: one graph (job table upload, counter reset, keys kernel, low and high "
+                             "digit passes over all jobs)",
+                   "parallelism": f"each of {world} ranks sorts its own 64-job batch, no collective"
+                   if world > 1 else "single GPU",
+                   "tuned": {str(b): {"tile": t, "ctas_per_sm": c, "segs_per_cta": g}
+                             for b, (t, c, g) in tuned.items()}},
+        "e2e": {"value": e2e_value, "unit": "Msplats/s", "h2d_bytes_per_step": h2d // e2e_steps,
+                "d2h_bytes_per_step": d2h // e2e_steps,
+                "call": "ws_sort_batch_host: one launch for all 64 jobs, then every job's survivor count and order "
+                        "into pinned host buffers (the reference's outputs; its keys are never read back)"},
+        "gpu_launches": 3 * args.steps,
+        "clocks": clk,
+    }
+    if rank == 0:
+        peak, src = peak_hbm()
+        algo = sum(algorithmic_bytes(sp.count, s) for sp, s in zip(p["clouds"], survivors))
+        achieved = algo / kernel_s / 1e9
+        line["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                            "frac": achieved / peak, "traffic": ncu_traffic("mixed-64", args.cull),
+                            "peak_source": src,
+                            "kernel": "wsort::keys_kernel + digit_kernel<0> + digit_kernel<1>, one batched launch",
+                            "kernel_us_per_step": kernel_s * 1e6, "algorithmic_bytes_per_step": algo,
+                            "algorithmic_bytes": "32 N + 8 S summed over the jobs"}
+        # the same 64 jobs as 64 plain calls
+        time_plain(ctx, torch, p, reps, 2, flush)
+        plain_rate = total * reps / (p["ms"] / 1e3) / 1e6
+        graph_rate = value / world
+        batch_rate = total * reps / (b_ms / 1e3) / 1e6
+        line["batch"] = {"plain_msplats_s": plain_rate, "batch_call_msplats_s": batch_rate,
+                         "graph_msplats_s": graph_rate, "graph_vs_plain": graph_rate / plain_rate,
+                         "batch_call_vs_plain": batch_rate / plain_rate,
+                         "plain_ms_per_step": p["ms"] / reps, "graph_ms_per_step": ms_max / args.steps,
+                         "plain": "64 ws_sort calls (device outputs), each its own launch"}
     for sp in p["clouds"]:
         sp.destroy()
+    return line, jobs
+
+
+def local_rank_of(torch):
+    return torch.cuda.current_device()
+
+
+def single_line(args, rank, world, dist, ctx, torch, flush):
+    """One cloud (clusters-1M, uniform-100k or slab-6M): one plain ws_sort a
+    step, one replica per rank."""
+    jobs = make_jobs(args.workload, args.cull, seed_offset=0)
+    p = load_jobs(ctx, torch, jobs)
+    time_plain(ctx, torch, p, 0, args.warmup, flush)
+    tuned = tune_batch(ctx, p, args)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(local_rank_of(torch))
+    clocks.start()
+    time_plain(ctx, torch, p, args.steps, 0, flush)
+    clk = clocks.stop()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ms_max = max_over_ranks(dist, torch, p["ms"])
+    splats = p["splats"]
+    value = splats * world * args.steps / (ms_max / 1e3) / 1e6
+    survivors = p["survivors"]
+    kms, launches = p["kernel_ms"], p["launches"]
+
+    e2e_value, h2d, d2h, e2e_steps = single_e2e(ctx, torch, p, args.steps, flush)
+    e2e_ms = max_over_ranks(dist, torch, splats * e2e_steps / e2e_value / 1e3)
+    e2e_value = splats * world * e2e_steps / (e2e_ms / 1e3) / 1e6
+    line = {
+        "metric": "Msplats/s sorted (bit-exact stable order)", "value": value, "unit": "Msplats/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 keys, u32 sort", "data": "synthetic (seeded)",
+        "config": {"workload": args.workload, "splats_per_step": splats * world,
+                   "survivors_per_step": sum(survivors), "cull": args.cull, "viewport": [1920, 1080],
+                   "l2": "flushed (256 MiB write) before each step",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "tuned": {str(b): {"tile": t, "ctas_per_sm": c, "segs_per_cta": g}
+                             for b, (t, c, g) in tuned.items()}},
+        "e2e": {"value": e2e_value, "unit": "Msplats/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "call": "ws_sort(WS_HOST_OUTPUT) into a pinned host buffer: the order and the survivor count, "
+                        "the reference's outputs (its keys stay unsorted on the device and are never read back)"},
+        # a lone job's ws_sort: the staging kernel, the keys kernel, two digit passes
+        "gpu_launches": 4 * launches,
+        "clocks": clk,
+    }
+    if rank == 0:
+        peak, src = peak_hbm()
+        front = survivors_at_cull0(ctx, torch, p) if args.cull > 0 else survivors
+        algo = sum(algorithmic_bytes(sp.count, s) for sp, s in zip(p["clouds"], survivors))
+        lay = sum(layout_bytes(sp.count, f, s, args.cull) for sp, f, s in zip(p["clouds"], front, survivors))
+        kernel_s = kms / max(launches, 1) / 1e3
+        achieved = algo / kernel_s / 1e9
+        line["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                            "frac": achieved / peak, "traffic": ncu_traffic(args.workload, args.cull),
+                            "peak_source": src, "kernel": "wsort::keys_kernel + digit_kernel<0> + digit_kernel<1>",
+                            "kernel_us_per_step": kernel_s * 1e6, "algorithmic_bytes_per_step": algo,
+                            "algorithmic_bytes": "32 N + 8 S", "layout_bytes_per_step": lay,
+                            "layout_frac": lay / kernel_s / 1e9 / peak}
+    for sp in p["clouds"]:
+        sp.destroy()
+    return line, jobs
+
+
+def single_e2e(ctx, torch, p, steps, flush):
+    """ws_sort with host outputs (the order and the count into a pinned
+    buffer) per step: (Msplats/s, h2d and d2h bytes a step, steps)."""
+    import ctypes
+    from winding_b200 import _lib
+    stream = torch.cuda.current_stream().cuda_stream
+    n_max = max(sp.count for sp in p["clouds"])
+    host_order = torch.empty(max(n_max, 1), dtype=torch.int32).pin_memory()
+    cnt = ctypes.c_uint32()
+
+    def one():
+        for sp, v in zip(p["clouds"], p["views"]):
+            ctx.check(ctx.lib.ws_sort(ctx.handle, sp.handle, ctypes.byref(v), host_order.data_ptr(),
+                                      None, ctypes.byref(cnt), _lib.WS_HOST_OUTPUT, stream))
+
+    for _ in range(2):
+        one()
+    e2e_steps = max(3, min(steps, 20))
+    ctx.copy_stats(reset=True)
+    ms = timed_sorts(ctx, torch, e2e_steps, flush, one, host_start=True)
+    h2d, d2h = ctx.copy_stats(reset=True)
+    return p["splats"] * e2e_steps / (ms / 1e3) / 1e6, h2d // e2e_steps, d2h // e2e_steps, e2e_steps
+
+
+def suite(ctx, torch, flush, args):
+    """Side measurements: the single-cloud sorts (clusters-1M, slab-6M)
+    against the HBM roofline with their end-to-end rates, mixed-64 batched vs
+    plain when it is not the headline, the served stream, particles,
+    shading, decoding and drawing."""
+    out = {}
+    peak, src = peak_hbm()
+    for name in ("clusters-1M", "slab-6M"):
+        if name == args.workload:
+            continue
+        p = load_jobs(ctx, torch, make_jobs(name, 0.5))
+        time_plain(ctx, torch, p, 0, 2, flush)
+        tuned = tune_batch(ctx, p, argparse.Namespace(tile=0, ctas=0, segs=1))
+        time_plain(ctx, torch, p, 20, 3, flush)
+        n = p["splats"]
+        algo = sum(algorithmic_bytes(sp.count, s) for sp, s in zip(p["clouds"], p["survivors"]))
+        kernel_s = p["kernel_ms"] / p["launches"] / 1e3
+        e2e, h2d, d2h, _ = single_e2e(ctx, torch, p, 20, flush)
+        out[name] = {"splats": n, "survivors": p["survivors"][0], "kernel_us": kernel_s * 1e6,
+                     "step_us": p["ms"] / 20 * 1e3, "msplats_s": n / (p["ms"] / 20 / 1e3) / 1e6,
+                     "achieved_gbs": algo / kernel_s / 1e9, "frac": algo / kernel_s / 1e9 / peak,
+                     "peak_source": src, "traffic": ncu_traffic(name, 0.5),
+                     "e2e_msplats_s": e2e, "e2e_h2d_bytes": h2d, "e2e_d2h_bytes": d2h,
+                     "tuned": {str(b): list(v) for b, v in tuned.items()}}
+        for sp in p["clouds"]:
+            sp.destroy()
+        del p
+    if args.workload != "mixed-64":
+        line, _ = batch_line(argparse.Namespace(cull=0.5, warmup=3, steps=10, tile=0, ctas=0, segs=1), 0, 1, None,
+                             ctx, torch, flush)
+        out["mixed-64"] = {"graph_msplats_s": line["value"], "e2e_msplats_s": line["e2e"]["value"],
+                           "frac": line["roofline"]["frac"], **line["batch"]}
     try:
         out["served-16"] = served(ctx, args)
     except Exception as exc:
@@ -627,23 +737,30 @@ def decode_suite(ctx, torch, flush, peak):
     return out
 
 
-def served(ctx, args, rate_hz: float = 2000.0, seconds: float = 2.0):
-    """Config 4: a Poisson stream of random-pose requests over 16 resident
+def served(ctx, args, rates=(2000.0, 20000.0), seconds: float = 0.5, repeats: int = 5):
+    """Config 4: Poisson streams of random-pose requests over 16 resident
     scenes of 50k-4M splats, through the server (continuous batching) and,
-    on the same arrival schedule, through one plain ws_sort per request."""
+    on the same arrival schedule, through one plain ws_sort per request. Per
+    arrival rate: one warm-up run, then `repeats` runs of `seconds` each,
+    reported as the median with the spread (min, max). Then a saturated
+    queue (every request submitted at once)."""
     import threading
+    import ctypes as _ct
+    import torch
     from winding_b200 import make_view, parse_splats, workloads as W
     from winding_b200.server import Server
     scenes = [parse_splats(rec, ctx) for rec in W.served_16()]
     resident = sum(sp.count for sp in scenes) * 40
-    arrivals = W.poisson_arrivals(rate_hz, seconds)
-    rng = np.random.default_rng(6)
     proj = W.perspective(W.FOV_Y, W.ASPECT, W.NEAR)
-    reqs = [(int(rng.integers(0, len(scenes))), make_view(W.random_pose(rng), proj, W.VIEWPORT, 0.5))
-            for _ in arrivals]
-    splats = sum(scenes[k].count for k, _ in reqs)
 
-    def run(submit, collect):
+    def requests(rate, dur, seed):
+        arrivals = W.poisson_arrivals(rate, dur, seed=seed)
+        rng = np.random.default_rng(seed + 1)
+        reqs = [(int(rng.integers(0, len(scenes))), make_view(W.random_pose(rng), proj, W.VIEWPORT, 0.5))
+                for _ in arrivals]
+        return arrivals, reqs
+
+    def run(arrivals, reqs, submit, collect):
         """Submits on the arrival schedule from one thread, collects from another;
         returns (seconds from the first arrival to the last result, latencies in
         ms from each request's scheduled arrival to its result)."""
@@ -674,15 +791,10 @@ def served(ctx, args, rate_hz: float = 2000.0, seconds: float = 2.0):
         srv.result(t)      # the result is on the device, as the reference's draw reads it
         srv.release(t)
 
-    with Server(ctx, memory_budget=8 << 30, max_batch=64, streams=2) as srv:
-        wall, lat = run(lambda sp, v: srv.submit(sp, v), lambda t: collect(srv, t))
-        st = srv.stats()
-    import torch
     n_max = max(sp.count for sp in scenes)
     o = torch.empty(n_max, dtype=torch.int32, device="cuda")
     k = torch.empty(n_max, dtype=torch.int32, device="cuda")
     c = torch.zeros(1, dtype=torch.int32, device="cuda")
-    import ctypes as _ct
     cnt = _ct.c_uint32()
 
     def plain(sp, v):
@@ -690,42 +802,73 @@ def served(ctx, args, rate_hz: float = 2000.0, seconds: float = 2.0):
         ctx.sort_device(sp, v, o.data_ptr(), k.data_ptr(), c.data_ptr())
         ctx.check(ctx.lib.ws_device_download(ctx.handle, c.data_ptr(), _ct.byref(cnt), 4, None))
 
-    plain_wall, plain_lat = run(plain, lambda res: None)
+    def spread(vals):
+        return {"median": float(np.median(vals)), "min": float(np.min(vals)), "max": float(np.max(vals))}
+
+    out = {"scenes": len(scenes), "resident_bytes": resident, "seconds_per_run": seconds, "repeats": repeats,
+           "latency": "scheduled arrival to the result ready in device memory, count known on the host"}
+    with Server(ctx, memory_budget=8 << 30, max_batch=64, streams=2) as srv:
+        for rate in rates:
+            warm_a, warm_r = requests(rate, 0.1, 99)
+            run(warm_a, warm_r, lambda sp, v: srv.submit(sp, v), lambda t: collect(srv, t))
+            run(warm_a, warm_r, plain, lambda res: None)
+            s_rate, s_p50, s_p99, s_batch, p_rate, p_p50, p_p99, n_req = [], [], [], [], [], [], [], []
+            for r in range(repeats):
+                arrivals, reqs = requests(rate, seconds, 5 + 17 * r)
+                splats = sum(scenes[q].count for q, _ in reqs)
+                before = srv.stats()
+                wall, lat = run(arrivals, reqs, lambda sp, v: srv.submit(sp, v), lambda t: collect(srv, t))
+                after = srv.stats()
+                batches = after["batches"] - before["batches"]
+                s_rate.append(splats / wall / 1e6)
+                s_p50.append(float(np.percentile(lat, 50)))
+                s_p99.append(float(np.percentile(lat, 99)))
+                s_batch.append(len(reqs) / max(batches, 1))
+                wall, lat = run(arrivals, reqs, plain, lambda res: None)
+                p_rate.append(splats / wall / 1e6)
+                p_p50.append(float(np.percentile(lat, 50)))
+                p_p99.append(float(np.percentile(lat, 99)))
+                n_req.append(len(reqs))
+            out[f"{int(rate)}hz"] = {
+                "requests_per_run": spread(n_req), "served_msplats_s": spread(s_rate),
+                "served_p50_ms": spread(s_p50), "served_p99_ms": spread(s_p99), "mean_batch": spread(s_batch),
+                "plain_msplats_s": spread(p_rate), "plain_p50_ms": spread(p_p50), "plain_p99_ms": spread(p_p99),
+                "served_vs_plain": float(np.median(s_rate) / np.median(p_rate))}
+        st = srv.stats()
+        out["overlapped_batches"] = st["overlapped_batches"]
+        out["admission_waits"] = st["admission_waits"]
+        out["device_p50_ms"] = st["p50_ms"]
+        out["device_p99_ms"] = st["p99_ms"]
 
     # Saturated: every request queued at once (a closed queue), so the server
     # batches as many as it admits; against one plain sort per request.
-    burst = reqs[:1024]
-    burst_splats = sum(scenes[k].count for k, _ in burst)
+    _, burst = requests(20000.0, 0.06, 7)
+    burst = burst[:1024]
+    burst_splats = sum(scenes[q].count for q, _ in burst)
+    sat_s, sat_p, sat_b = [], [], []
     with Server(ctx, memory_budget=8 << 30, max_batch=64, streams=2) as srv:
-        t0 = time.perf_counter()
-        tickets = [srv.submit(scenes[sc], v) for sc, v in burst]
-        for tk in tickets:
-            collect(srv, tk)
-        sat_wall = time.perf_counter() - t0
-        sat = srv.stats()
-    t0 = time.perf_counter()
-    for sc, v in burst:
-        plain(scenes[sc], v)
-    sat_plain_wall = time.perf_counter() - t0
+        for r in range(repeats + 1):
+            before = srv.stats()
+            t0 = time.perf_counter()
+            tickets = [srv.submit(scenes[sc], v) for sc, v in burst]
+            for tk in tickets:
+                collect(srv, tk)
+            wall = time.perf_counter() - t0
+            after = srv.stats()
+            t0 = time.perf_counter()
+            for sc, v in burst:
+                plain(scenes[sc], v)
+            p_wall = time.perf_counter() - t0
+            if r:   # the first round is the warm-up
+                sat_s.append(burst_splats / wall / 1e6)
+                sat_p.append(burst_splats / p_wall / 1e6)
+                sat_b.append(len(burst) / max(after["batches"] - before["batches"], 1))
+    out["saturated"] = {"requests": len(burst), "splats": burst_splats, "served_msplats_s": spread(sat_s),
+                        "plain_msplats_s": spread(sat_p), "mean_batch": spread(sat_b),
+                        "served_vs_plain": float(np.median(sat_s) / np.median(sat_p))}
     for sp in scenes:
         sp.destroy()
-    return {
-        "saturated": {"requests": len(burst), "splats": burst_splats,
-                      "served_msplats_s": burst_splats / sat_wall / 1e6,
-                      "plain_msplats_s": burst_splats / sat_plain_wall / 1e6,
-                      "served_vs_plain": sat_plain_wall / sat_wall, "mean_batch": sat["mean_batch"],
-                      "batches": sat["batches"]},
-        "requests": len(reqs), "rate_hz": rate_hz, "scenes": len(scenes), "resident_bytes": resident,
-        "splats": splats,
-        "served_msplats_s": splats / wall / 1e6, "served_p50_ms": float(np.percentile(lat, 50)),
-        "served_p99_ms": float(np.percentile(lat, 99)),
-        "device_p50_ms": st["p50_ms"], "device_p99_ms": st["p99_ms"], "mean_batch": st["mean_batch"],
-        "batches": st["batches"], "overlapped_batches": st["overlapped_batches"],
-        "admission_waits": st["admission_waits"],
-        "plain_msplats_s": splats / plain_wall / 1e6, "plain_p50_ms": float(np.percentile(plain_lat, 50)),
-        "plain_p99_ms": float(np.percentile(plain_lat, 99)),
-        "latency": "scheduled arrival to the result ready in device memory, count known on the host",
-    }
+    return out
 
 
 def main():

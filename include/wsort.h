@@ -485,6 +485,15 @@ int ws_timing(ws_ctx* ctx, int enable);
 int ws_timing_read(ws_ctx* ctx, double* kernel_ms, uint64_t* launches);
 
 /*
+ * Bytes the sort calls of ctx moved between host and device since creation
+ * (or the last reset): job tables and launch parameters up; counts, error
+ * words and the survivors of host-output calls down. reset != 0 zeroes both
+ * after reading. Resident clouds, plans' graph uploads and device-output
+ * results are not counted.
+ */
+int ws_copy_stats(ws_ctx* ctx, uint64_t* h2d_bytes, uint64_t* d2h_bytes, int reset);
+
+/*
  * Work-item tracing: while enabled, each sort launch of ctx (not plans)
  * stamps every work item with the GPU's global timer when its ticket was
  * claimed, when its dependency wait ended and when it finished, and the SM

@@ -365,8 +365,13 @@ def test_batch_with_host_outputs(ctx, pinned):
         ctx.sort_batch([(sp, v, o.data_ptr(), k.data_ptr(), c.data_ptr()) for (sp, v), (o, k, c) in zip(specs, dev)])
         ctx.sync()
         for _ in range(2):
+            ctx.copy_stats(reset=True)
             ctx.sort_batch_host([(sp, v, ho.data_ptr(), hk.data_ptr(), hc.data_ptr())
                                  for (sp, v), (ho, hk, hc) in zip(specs, host)])
+            # the error words, then per job its count and its survivors' order and keys
+            h2d, d2h = ctx.copy_stats()
+            assert d2h == 8 + sum(4 + 8 * int(c.item()) for _, _, c in dev)
+            assert h2d > 0
             for (o, k, c), (ho, hk, hc) in zip(dev, host):
                 s = int(c.item())
                 assert int(hc[0]) == s

@@ -200,6 +200,8 @@ SIGNATURES = {
     "ws_server_get_stats": (ctypes.c_int, [vp, ctypes.POINTER(WsServerStats)]),
     "ws_server_destroy": (ctypes.c_int, [vp]),
     "ws_set_tuning": (ctypes.c_int, [vp, ctypes.POINTER(WsParams), ctypes.c_int]),
+    "ws_copy_stats": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64),
+                                     ctypes.c_int]),
     "ws_timing": (ctypes.c_int, [vp, ctypes.c_int]),
     "ws_timing_read": (ctypes.c_int, [vp, f64p, ctypes.POINTER(ctypes.c_uint64)]),
     "ws_trace": (ctypes.c_int, [vp, ctypes.c_int]),

@@ -504,6 +504,7 @@ static int launch_jobs(ws_ctx* ctx, const std::vector<uint32_t>& ns, int njobs, 
         stage_kernel<<<1, 1024, 0, stream>>>(one, static_cast<JobDesc*>(ctx->jobs_d.p),
                                              reinterpret_cast<uint32_t*>(scratch), (uint32_t)(S.ctl_bytes / 4));
         if ((e = cudaGetLastError()) != cudaSuccess) return cuda_error(ctx, e, "ws_sort staging");
+        ctx->h2d_bytes += sizeof(JobDesc);
     } else {
         // Pinned staging is rewritten only after its previous upload finished.
         if ((e = cudaEventSynchronize(ctx->staged)) != cudaSuccess) return cuda_error(ctx, e, "ws_sort");
@@ -513,6 +514,7 @@ static int launch_jobs(ws_ctx* ctx, const std::vector<uint32_t>& ns, int njobs, 
         write_table(ctx->jobs_h.p, hj, njobs, S);
         if ((e = cudaMemcpyAsync(ctx->jobs_d.p, ctx->jobs_h.p, tb, cudaMemcpyHostToDevice, stream)) != cudaSuccess)
             return cuda_error(ctx, e, "ws_sort upload");
+        ctx->h2d_bytes += tb;
         cudaEventRecord(ctx->staged, stream);
     }
     if (njobs != 1 && (e = cudaMemsetAsync(scratch, 0, S.ctl_bytes, stream)) != cudaSuccess)
@@ -992,6 +994,7 @@ extern "C" int ws_sort(ws_ctx* ctx, const ws_cloud* cloud, const ws_view* view, 
             return cuda_error(ctx, e, "ws_sort");
         if (hc[1]) return take_device_error(ctx);
         *count = hc[0];
+        ctx->d2h_bytes += 12 + (size_t)hc[0] * (keys ? 8 : 4);
         return WS_OK;
     }
     if ((e = cudaMemcpyAsync(hc, job.count, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
@@ -1001,6 +1004,7 @@ extern "C" int ws_sort(ws_ctx* ctx, const ws_cloud* cloud, const ws_view* view, 
     if (hc[1]) return take_device_error(ctx);
     const uint32_t s = hc[0];
     *count = s;
+    ctx->d2h_bytes += 12 + (size_t)s * (keys ? 8 : 4);
     if (s) {
         if ((e = cudaMemcpyAsync(order, job.order, (size_t)s * 4, cudaMemcpyDeviceToHost, stream)) != cudaSuccess)
             return cuda_error(ctx, e, "ws_sort download");
@@ -1120,6 +1124,9 @@ extern "C" int ws_sort_batch_host(ws_ctx* ctx, int njobs, const ws_job* jobs, vo
             (e = cudaStreamSynchronize(stream)) != cudaSuccess)
             return cuda_error(ctx, e, "ws_sort_batch_host");
         if (hw[0]) return take_device_error(ctx);
+        ctx->h2d_bytes += tb;
+        ctx->d2h_bytes += 8;
+        for (int j = 0; j < njobs; ++j) ctx->d2h_bytes += 4 + (size_t)*jobs[j].count * (jobs[j].keys ? 8 : 4);
         return WS_OK;
     }
     // Pageable outputs: the counts first, then each job's survivors.
@@ -1129,8 +1136,10 @@ extern "C" int ws_sort_batch_host(ws_ctx* ctx, int njobs, const ws_job* jobs, vo
             return cuda_error(ctx, e, "ws_sort_batch_host");
     if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return cuda_error(ctx, e, "ws_sort_batch_host");
     if ((rc = take_device_error(ctx))) return rc;
+    ctx->d2h_bytes += 8;
     for (int j = 0; j < njobs; ++j) {
         *jobs[j].count = counts[j];
+        ctx->d2h_bytes += 4 + (size_t)counts[j] * (jobs[j].keys ? 8 : 4);
         if (!counts[j]) continue;
         if ((e = cudaMemcpyAsync(jobs[j].order, dj[j].order, (size_t)counts[j] * 4, cudaMemcpyDeviceToHost, stream)) !=
                 cudaSuccess ||
@@ -1523,6 +1532,14 @@ extern "C" int ws_timing(ws_ctx* ctx, int enable) {
     ctx->timing = enable != 0;
     ctx->timing_used = 0;
     ctx->timing_launches = 0;
+    return WS_OK;
+}
+
+extern "C" int ws_copy_stats(ws_ctx* ctx, uint64_t* h2d_bytes, uint64_t* d2h_bytes, int reset) {
+    if (!ctx) return WS_ERR_ARG;
+    if (h2d_bytes) *h2d_bytes = ctx->h2d_bytes;
+    if (d2h_bytes) *d2h_bytes = ctx->d2h_bytes;
+    if (reset) ctx->h2d_bytes = ctx->d2h_bytes = 0;
     return WS_OK;
 }
 

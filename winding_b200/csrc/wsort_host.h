@@ -90,6 +90,9 @@ struct ws_ctx {
     ws_params last_params{};
     bool shape_valid = false;
     uint64_t launches = 0;
+    // host <-> device bytes the sort calls moved (ws_copy_stats): job tables
+    // and launch parameters up, counts, error words and survivors down
+    uint64_t h2d_bytes = 0, d2h_bytes = 0;
     // kernel timing (ws_timing): event pairs recorded around each launch
     bool timing = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> timing_events;

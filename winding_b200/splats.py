@@ -212,6 +212,13 @@ class Context:
         self.check(self.lib.ws_timing_read(self.handle, ctypes.byref(ms), ctypes.byref(n)))
         return ms.value, n.value
 
+    def copy_stats(self, reset: bool = False) -> tuple[int, int]:
+        """(host-to-device, device-to-host) bytes the sort calls moved (ws_copy_stats)."""
+        h = ctypes.c_uint64()
+        d = ctypes.c_uint64()
+        self.check(self.lib.ws_copy_stats(self.handle, ctypes.byref(h), ctypes.byref(d), int(reset)))
+        return h.value, d.value
+
     def trace(self, enable: bool = True) -> None:
         self.check(self.lib.ws_trace(self.handle, int(enable)))
 
