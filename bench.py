@@ -51,6 +51,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 FALLBACK_HBM_GBS = 6650.0
+ALGORITHMS = ("three-phase", "one-CTA radix", "one-CTA counting")
 L2_FLUSH_BYTES = 256 << 20
 
 
@@ -278,8 +279,8 @@ def tune_batch(ctx, p, args):
     batch)."""
     from winding_b200 import autotune
     if args.tile and args.ctas:
-        ctx.set_params(tile=args.tile, ctas_per_sm=args.ctas, segs_per_cta=args.segs)
-        return {autotune.bucket(p["splats"]): (args.tile, args.ctas, args.segs)}
+        ctx.set_params(tile=args.tile, ctas_per_sm=args.ctas, segs_per_cta=args.segs, algorithm=0)
+        return {autotune.bucket(p["splats"]): (args.tile, args.ctas, args.segs, 0)}
     pairs = list(zip(p["clouds"], p["views"]))
     per_bucket = {}
     for pair in pairs:
@@ -440,8 +441,8 @@ def batch_line(args, rank, world, dist, ctx, torch, flush):
                              "digit passes over all jobs)",
                    "parallelism": f"each of {world} ranks sorts its own 64-job batch, no collective"
                    if world > 1 else "single GPU",
-                   "tuned": {str(b): {"tile": t, "ctas_per_sm": c, "segs_per_cta": g}
-                             for b, (t, c, g) in tuned.items()}},
+                   "tuned": {str(b): {"tile": t, "ctas_per_sm": c, "segs_per_cta": g, "algorithm": ALGORITHMS[a]}
+                             for b, (t, c, g, a) in tuned.items()}},
         "e2e": {"value": e2e_value, "unit": "Msplats/s", "h2d_bytes_per_step": h2d // e2e_steps,
                 "d2h_bytes_per_step": d2h // e2e_steps,
                 "call": "ws_sort_batch_host: one launch for all 64 jobs, then every job's survivor count and order "
@@ -513,8 +514,8 @@ def single_line(args, rank, world, dist, ctx, torch, flush):
                    "survivors_per_step": sum(survivors), "cull": args.cull, "viewport": [1920, 1080],
                    "l2": "flushed (256 MiB write) before each step",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                   "tuned": {str(b): {"tile": t, "ctas_per_sm": c, "segs_per_cta": g}
-                             for b, (t, c, g) in tuned.items()}},
+                   "tuned": {str(b): {"tile": t, "ctas_per_sm": c, "segs_per_cta": g, "algorithm": ALGORITHMS[a]}
+                             for b, (t, c, g, a) in tuned.items()}},
         "e2e": {"value": e2e_value, "unit": "Msplats/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "call": "ws_sort(WS_HOST_OUTPUT) into a pinned host buffer: the order and the survivor count, "
                         "the reference's outputs (its keys stay unsorted on the device and are never read back)"},

@@ -452,13 +452,19 @@ int ws_selftest_wait(ws_ctx* ctx, uint32_t spin_limit);
  * splats (a multiple of 256); a segment is one work item of each phase.
  * ctas_per_sm: 1 (0 too) runs CTAs of 1024 threads, one an SM; 2 runs CTAs
  * of 512 threads, two an SM. spin_limit: polls a device-side wait makes
- * before it gives up with WS_ERR_TIMEOUT.
+ * before it gives up with WS_ERR_TIMEOUT. algorithm: 0 sorts in three phases
+ * (keys, low digit, high digit) over segments of every job; 1 and 2 give each
+ * job one CTA that sorts it in shared memory in one kernel, by two 8-bit
+ * passes (1) or by one counting pass over all 65536 keys (2) — for launches
+ * whose jobs are all of splats with at most 16384 each (others, and traced
+ * launches, take the three phases). The result is the same whichever runs.
  */
 typedef struct ws_params {
     uint32_t tile;
     uint32_t ctas_per_sm;
     uint32_t spin_limit;
     uint32_t segs_per_cta;
+    uint32_t algorithm;
 } ws_params;
 
 int ws_get_params(const ws_ctx* ctx, ws_params* out);

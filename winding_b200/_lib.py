@@ -91,7 +91,12 @@ class WsParams(ctypes.Structure):
         ("ctas_per_sm", ctypes.c_uint32),
         ("spin_limit", ctypes.c_uint32),
         ("segs_per_cta", ctypes.c_uint32),
+        ("algorithm", ctypes.c_uint32),
     ]
+
+
+ALGO_PHASES, ALGO_ONE_RADIX, ALGO_ONE_COUNT = 0, 1, 2
+ONE_CTA_MAX = 16384   # largest job of splats the one-CTA sorts take
 
 
 class WsServerOpts(ctypes.Structure):

@@ -195,6 +195,7 @@ LaunchDesc launch_desc(const void* d_table, int njobs, const LaunchShape& S, cha
     LaunchDesc L;
     std::memset(&L, 0, sizeof(L));
     L.jobs = static_cast<const JobDesc*>(d_table);
+    L.njobs = (uint32_t)njobs;
     L.segs = S.regular ? nullptr
                        : reinterpret_cast<const SegDesc*>(static_cast<const char*>(d_table) +
                                                           (size_t)njobs * sizeof(JobDesc));
@@ -452,6 +453,14 @@ const ws_params& params_for(const ws_ctx* ctx, uint64_t splats) {
     return ctx->params;
 }
 
+// The one-CTA sorts take a launch when every job is one of splats of at
+// most kOneMax.
+bool one_cta_takes(const JobDesc* jobs, int njobs) {
+    for (int j = 0; j < njobs; ++j)
+        if (jobs[j].kind != kJobSplats || jobs[j].n > kOneMax) return false;
+    return true;
+}
+
 // A lone job's staging in one launch: its description (passed by value with
 // the launch, so no host-to-device copy) into the job table, and the launch's
 // and the job's counters zeroed.
@@ -496,11 +505,14 @@ static int launch_jobs(ws_ctx* ctx, const std::vector<uint32_t>& ns, int njobs, 
     }
     char* scratch = static_cast<char*>(ctx->scratch.p);
     if (stream != ctx->stream) cudaStreamWaitEvent(stream, ctx->launched, 0);
+    // The one-CTA sorts take launches of small jobs of splats (not traced).
+    bool one_cta = P.algorithm != kAlgoPhases && !ctx->tracing;
     if (njobs == 1) {
         // A lone job's description travels with the staging kernel's launch:
         // no pinned buffer, so nothing to wait for before writing it.
         JobDesc one;
         fill(&one, S, scratch);
+        one_cta = one_cta && one_cta_takes(&one, 1);
         stage_kernel<<<1, 1024, 0, stream>>>(one, static_cast<JobDesc*>(ctx->jobs_d.p),
                                              reinterpret_cast<uint32_t*>(scratch), (uint32_t)(S.ctl_bytes / 4));
         if ((e = cudaGetLastError()) != cudaSuccess) return cuda_error(ctx, e, "ws_sort staging");
@@ -511,6 +523,7 @@ static int launch_jobs(ws_ctx* ctx, const std::vector<uint32_t>& ns, int njobs, 
         if ((e = ctx->jobs_h.ensure(tb)) != cudaSuccess) return cuda_error(ctx, e, "ws_sort staging");
         JobDesc* hj = static_cast<JobDesc*>(ctx->jobs_h.p);
         fill(hj, S, scratch);
+        one_cta = one_cta && one_cta_takes(hj, njobs);
         write_table(ctx->jobs_h.p, hj, njobs, S);
         if ((e = cudaMemcpyAsync(ctx->jobs_d.p, ctx->jobs_h.p, tb, cudaMemcpyHostToDevice, stream)) != cudaSuccess)
             return cuda_error(ctx, e, "ws_sort upload");
@@ -541,7 +554,8 @@ static int launch_jobs(ws_ctx* ctx, const std::vector<uint32_t>& ns, int njobs, 
         ctx->trace_grid = (int)std::min<size_t>(S.grid, S.segs.size());
     }
     const LaunchDesc L = launch_desc(ctx->jobs_d.p, njobs, S, scratch, ctx->err_d, P.spin_limit, trace);
-    e = launch_sort(L, S.threads, (int)std::min<size_t>(S.grid, S.segs.size()), ctx->sms, stream);
+    e = one_cta ? launch_one(L, P.algorithm, stream)
+                : launch_sort(L, S.threads, (int)std::min<size_t>(S.grid, S.segs.size()), ctx->sms, stream);
     if (e != cudaSuccess) return cuda_error(ctx, e, "ws_sort launch");
     if (t_stop) cudaEventRecord(t_stop, stream);
     cudaEventRecord(ctx->launched, stream);
@@ -704,6 +718,7 @@ extern "C" int ws_get_params(const ws_ctx* ctx, ws_params* out) {
 // The kernel variants that exist: 1024 threads a CTA (one CTA an SM) or 512
 // (two); segments no smaller than `tile` splats, a multiple of 256.
 static const char* params_problem(const ws_params* p) {
+    if (p->algorithm > kAlgoOneCount) return "algorithm must be 0 (three phases), 1 (one-CTA radix) or 2 (one-CTA counting)";
     if (p->tile < kSegAlign || p->tile > (1u << 24) || p->tile % kSegAlign)
         return "tile must be a multiple of 256 from 256 to 2^24";
     if (p->spin_limit == 0) return "spin_limit must be positive";
@@ -1422,7 +1437,10 @@ extern "C" int ws_plan_create(ws_ctx* ctx, int njobs, const ws_job* jobs, ws_pla
         cudaMemsetAsync(p->scratch.p, 0, S.ctl_bytes, cs);
         const LaunchDesc L = launch_desc(p->jobs_d.p, njobs, S, static_cast<char*>(p->scratch.p), ctx->err_d,
                                          P.spin_limit, nullptr);
-        launch_sort(L, S.threads, (int)std::min<size_t>(S.grid, S.segs.size()), ctx->sms, cs);
+        if (P.algorithm != kAlgoPhases && one_cta_takes(hj, njobs))
+            launch_one(L, P.algorithm, cs);
+        else
+            launch_sort(L, S.threads, (int)std::min<size_t>(S.grid, S.segs.size()), ctx->sms, cs);
         e = cudaStreamEndCapture(cs, &p->graph);
     }
     if (e == cudaSuccess) e = cudaGraphInstantiate(&p->exec, p->graph, 0);

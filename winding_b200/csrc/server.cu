@@ -264,7 +264,9 @@ bool launch_batch(ws_server* S, Slot& slot) {
         (e = cudaMemsetAsync(slot.err_d, 0, 2 * sizeof(uint32_t), slot.stream)))
         return false;
     const LaunchDesc L = launch_desc(slot.d_table, nj, SH, slot.scratch, slot.err_d, P.spin_limit, nullptr);
-    e = launch_sort(L, SH.threads, (int)std::min<size_t>(SH.grid, SH.segs.size()), S->sms, slot.stream);
+    e = P.algorithm != kAlgoPhases && one_cta_takes(descs.data(), nj)
+            ? launch_one(L, P.algorithm, slot.stream)
+            : launch_sort(L, SH.threads, (int)std::min<size_t>(SH.grid, SH.segs.size()), S->sms, slot.stream);
     if (e != cudaSuccess) return false;
     // The error words come back with the batch: the completion thread reads
     // them from pinned memory once the event has passed.

@@ -289,6 +289,25 @@ __device__ __forceinline__ void count_key(uint32_t* hist, uint32_t key, uint32_t
     atomicAdd(&hist[s * 512u + 256u + sub_slot(s, key >> 8)], 1u);
 }
 
+// The footprint shortcut above for one splat of a perspective view: keep_sc
+// when its footprint surely passes the cull, cull_sc when it surely does not.
+__device__ __forceinline__ void shortcut(const ViewConsts& c, const float view[4], uint32_t byte, int8_t sexp, float afx,
+                                         float afy, float r0, float r1, float r2, float xcap, float ycap,
+                                         uint32_t keep_byte, bool* keep_sc, bool* cull_sc) {
+    const float d = -view[2];
+    // The splat's covariance bound 2^sexp, exactly (sexp is in [-100, 127]).
+    const float m = __int_as_float((int(sexp) + 127) << 23);
+    // A, B and ga, gb of the shortcut above, from this splat's own position.
+    const float rd = __fdividef(1.0f, d);
+    const float ax = fminf(fabsf(view[0]) * rd, xcap), ay = fminf(fabsf(view[1]) * rd, ycap);
+    const float A = afx * rd * (r0 + ax * r2), B = afy * rd * (r1 + ay * r2);
+    const float ga = 1.002f * (A * A) * m, gb = 1.002f * (B * B) * m;
+    *keep_sc = byte >= keep_byte && ga <= 100.0f && gb <= 100.0f;
+    // det's pinned value is at most (ga (1 + 8.2u) + .3)(gb (1 + 8.2u) +
+    // .3)(1 + 3u); below the byte's threshold, culled.
+    *cull_sc = !*keep_sc && ((ga * 1.00001f + 0.3f) * (gb * 1.00001f + 0.3f)) * 1.0001f < c.det_min[byte];
+}
+
 // Sweep 1 of a keys sub-tile: tests, keys and the footprint shortcut. Every
 // splat's key slot and survivor word are written now (the passes read only
 // the slots whose survivor bit is set), with the digit counts of the splats
@@ -331,22 +350,7 @@ __device__ __forceinline__ void keys_sweep(const ViewConsts& c, KeysSmem<NT>& sm
         bool pending = false;
         if (fp) {
             bool keep_sc = false, cull_sc = false;
-            if (persp) {
-                const float d = -view[2];
-                // The splat's covariance bound 2^sexp, exactly (sexp is in
-                // [-100, 127]).
-                const float m = __int_as_float((int(sexp[at]) + 127) << 23);
-                // A, B and ga, gb of the shortcut above, from this splat's
-                // own position.
-                const float rd = __fdividef(1.0f, d);
-                const float ax = fminf(fabsf(view[0]) * rd, xcap), ay = fminf(fabsf(view[1]) * rd, ycap);
-                const float A = afx * rd * (r0 + ax * r2), B = afy * rd * (r1 + ay * r2);
-                const float ga = 1.002f * (A * A) * m, gb = 1.002f * (B * B) * m;
-                keep_sc = byte >= keep_byte && ga <= 100.0f && gb <= 100.0f;
-                // det's pinned value is at most (ga (1 + 8.2u) + .3)(gb (1 +
-                // 8.2u) + .3)(1 + 3u); below the byte's threshold, culled.
-                cull_sc = !keep_sc && ((ga * 1.00001f + 0.3f) * (gb * 1.00001f + 0.3f)) * 1.0001f < c.det_min[byte];
-            }
+            if (persp) shortcut(c, view, byte, sexp[at], afx, afy, r0, r1, r2, xcap, ycap, keep_byte, &keep_sc, &cull_sc);
             pending = kept && !keep_sc && !cull_sc;
             kept = kept && keep_sc;
         }
@@ -410,6 +414,53 @@ __device__ void zero_keys_hist(KeysSmem<NT>& sm) {
     for (uint32_t k = threadIdx.x; k < (uint32_t)kSubHist * 512u; k += NT) h[k] = 0;
 }
 
+// makeKeys' footprint cull of one splat (view coordinates `view`, covariance
+// sg, threshold thr = det_min of its alpha byte): true when it keeps it.
+__device__ __forceinline__ bool footprint_keep(const ViewConsts& c, const float view[4], const float sg[6], float thr) {
+    // A filter first: det from the same inputs with fast arithmetic (fused
+    // products, an approximate reciprocal), and a bound on how far the
+    // pinned det can lie from it: every intermediate of both is within
+    // about 30 ulps of its real value, relative to the magnitudes
+    // |T| |Sigma| |T|^T (ga, gb below), so 2^-16 of
+    // (ga + .3)(gb + .3) + ga gb bounds the difference with room to spare.
+    // Outside that band of the threshold the decision is the pinned one's;
+    // inside, the pinned det decides.
+    float J00 = c.fx, J11 = c.fy, J02 = 0.0f, J12 = 0.0f;
+    if (c.persp) {
+        const float rd = __fdividef(1.0f, -view[2]);
+        J00 = c.fx * rd;
+        J11 = c.fy * rd;
+        J02 = J00 * fminf(fmaxf(view[0] * rd, c.xlo), c.xhi);
+        J12 = J11 * fminf(fmaxf(view[1] * rd, c.ylo), c.yhi);
+    }
+    float T0[3], T1[3], ta = 0.0f, tb = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        T0[k] = __fmaf_rn(J00, c.mv[k * 4 + 0], J02 * c.mv[k * 4 + 2]);
+        T1[k] = __fmaf_rn(J11, c.mv[k * 4 + 1], J12 * c.mv[k * 4 + 2]);
+        ta += fabsf(T0[k]);
+        tb += fabsf(T1[k]);
+    }
+    const float S[3][3] = {{sg[0], sg[1], sg[2]}, {sg[1], sg[3], sg[4]}, {sg[2], sg[4], sg[5]}};
+    float U0[3], U1[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        U0[k] = __fmaf_rn(T0[0], S[0][k], __fmaf_rn(T0[1], S[1][k], T0[2] * S[2][k]));
+        U1[k] = __fmaf_rn(T1[0], S[0][k], __fmaf_rn(T1[1], S[1][k], T1[2] * S[2][k]));
+    }
+    const float xx = __fmaf_rn(U0[0], T0[0], __fmaf_rn(U0[1], T0[1], U0[2] * T0[2]));
+    const float xy = __fmaf_rn(U1[0], T0[0], __fmaf_rn(U1[1], T0[1], U1[2] * T0[2]));
+    const float yy = __fmaf_rn(U1[0], T1[0], __fmaf_rn(U1[1], T1[1], U1[2] * T1[2]));
+    const float det = __fmaf_rn(xx + 0.3f, yy + 0.3f, -(xy * xy));
+    const float ms = fmaxf(fmaxf(fmaxf(fabsf(sg[0]), fabsf(sg[1])), fmaxf(fabsf(sg[2]), fabsf(sg[3]))),
+                           fmaxf(fabsf(sg[4]), fabsf(sg[5])));
+    const float ga = ta * ta * ms, gb = tb * tb * ms;
+    const float err = 1.52587890625e-5f * __fmaf_rn(ga + 0.3f, gb + 0.3f, ga * gb);
+    if (det - err >= thr) return true;
+    if (det + err < thr) return false;
+    return fmaxf(footprint_det(c, view, sg), 0.0f) >= thr;   // the max of makeKeys' sqrt(max(det, 0))
+}
+
 // The queued splats' footprints, densely (a warp evaluates 32 of them at
 // once, whichever sub-tiles they came from): a kept splat sets its survivor
 // bit and counts its digits (its key is already out). Each thread's next
@@ -442,53 +493,7 @@ __device__ void keys_footprints(const JobDesc& J, KeysSmem<NT>& sm) {
         }
         float view[4];
         view_of(c, p.x, p.y, p.z, view);
-        const float thr = c.det_min[__float_as_uint(p.w) >> 24];
-        // A filter first: det from the same inputs with fast arithmetic (fused
-        // products, an approximate reciprocal), and a bound on how far the
-        // pinned det can lie from it: every intermediate of both is within
-        // about 30 ulps of its real value, relative to the magnitudes
-        // |T| |Sigma| |T|^T (ga, gb below), so 2^-16 of
-        // (ga + .3)(gb + .3) + ga gb bounds the difference with room to spare.
-        // Outside that band of the threshold the decision is the pinned one's;
-        // inside, the pinned det decides.
-        float J00 = c.fx, J11 = c.fy, J02 = 0.0f, J12 = 0.0f;
-        if (c.persp) {
-            const float rd = __fdividef(1.0f, -view[2]);
-            J00 = c.fx * rd;
-            J11 = c.fy * rd;
-            J02 = J00 * fminf(fmaxf(view[0] * rd, c.xlo), c.xhi);
-            J12 = J11 * fminf(fmaxf(view[1] * rd, c.ylo), c.yhi);
-        }
-        float T0[3], T1[3], ta = 0.0f, tb = 0.0f;
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            T0[k] = __fmaf_rn(J00, c.mv[k * 4 + 0], J02 * c.mv[k * 4 + 2]);
-            T1[k] = __fmaf_rn(J11, c.mv[k * 4 + 1], J12 * c.mv[k * 4 + 2]);
-            ta += fabsf(T0[k]);
-            tb += fabsf(T1[k]);
-        }
-        const float S[3][3] = {{sg[0], sg[1], sg[2]}, {sg[1], sg[3], sg[4]}, {sg[2], sg[4], sg[5]}};
-        float U0[3], U1[3];
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            U0[k] = __fmaf_rn(T0[0], S[0][k], __fmaf_rn(T0[1], S[1][k], T0[2] * S[2][k]));
-            U1[k] = __fmaf_rn(T1[0], S[0][k], __fmaf_rn(T1[1], S[1][k], T1[2] * S[2][k]));
-        }
-        const float xx = __fmaf_rn(U0[0], T0[0], __fmaf_rn(U0[1], T0[1], U0[2] * T0[2]));
-        const float xy = __fmaf_rn(U1[0], T0[0], __fmaf_rn(U1[1], T0[1], U1[2] * T0[2]));
-        const float yy = __fmaf_rn(U1[0], T1[0], __fmaf_rn(U1[1], T1[1], U1[2] * T1[2]));
-        const float det = __fmaf_rn(xx + 0.3f, yy + 0.3f, -(xy * xy));
-        const float ms = fmaxf(fmaxf(fmaxf(fabsf(sg[0]), fabsf(sg[1])), fmaxf(fabsf(sg[2]), fabsf(sg[3]))),
-                               fmaxf(fabsf(sg[4]), fabsf(sg[5])));
-        const float ga = ta * ta * ms, gb = tb * tb * ms;
-        const float err = 1.52587890625e-5f * __fmaf_rn(ga + 0.3f, gb + 0.3f, ga * gb);
-        bool keep;
-        if (det - err >= thr)
-            keep = true;
-        else if (det + err < thr)
-            keep = false;
-        else
-            keep = fmaxf(footprint_det(c, view, sg), 0.0f) >= thr;   // the max of makeKeys' sqrt(max(det, 0))
+        const bool keep = footprint_keep(c, view, sg, c.det_min[__float_as_uint(p.w) >> 24]);
         if (keep) {
             atomicOr(&J.mask[i >> 5], 1u << (i & 31u));
             count_key(&sm.hist[0][0], depth_key(c, view), threadIdx.x & (kSubHist - 1));
@@ -889,6 +894,289 @@ __device__ void digit_item(const JobDesc& J, const SegDesc& sd, DigitSmem<NT>& s
 // finished and its writes are visible.
 __device__ __forceinline__ void allow_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 __device__ __forceinline__ void wait_prerequisites() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+// ---------------------------------------------------------------- one-CTA sorts
+//
+// A job of at most kOneMax splats sorted by one CTA in its shared memory, in
+// one kernel: every splat's key and survivor bit into shared memory, then
+// the survivors placed in (key, index) order, straight into the outputs.
+// kCounting: one counting pass over all 65536 keys (the counts of every key,
+// their exclusive scan, then one warp walks the splats in index order and
+// gives each the next slot of its key; a key's peers within the 32 are
+// ranked by their lanes). Otherwise two stable 8-bit passes, low digit then
+// high, all warps at once: each warp takes a contiguous run of the pass's
+// input, its per-digit starts from the counts of the runs before it.
+
+template <bool kCounting, int NT>
+struct OneSmem {
+    static constexpr int W = NT / 32;
+    ViewConsts vc;
+    uint32_t total;                              // survivors
+    uint32_t scan[32];
+    uint32_t live[kOneMax / 32];                 // survivor bits
+    uint16_t key[kOneMax];                       // each splat's key
+    // counting: the counts of all 65536 keys, two 16-bit halves a word; then
+    // each key's next slot. radix: the low pass's output (keys and indices),
+    // each warp's counts of its run per digit (then its next slot), and the
+    // lanes of a round per warp and digit.
+    union {
+        uint32_t hist[kCounting ? 32768 : 1];
+        struct {
+            uint16_t key1[kOneMax];
+            uint16_t idx1[kOneMax];
+            uint32_t off[W][256];
+            uint32_t wm[W][256];
+            uint32_t tot[256];
+        } r;
+    } u;
+};
+
+// Exclusive scan of v over the CTA's NT threads (NT <= 1024); the CTA's
+// total in *total. Every thread calls it.
+template <int NT>
+__device__ __forceinline__ uint32_t cta_exclusive_scan(uint32_t v, uint32_t* scan, uint32_t* total) {
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= (uint32_t)o) x += y;
+    }
+    if (lane == 31) scan[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = lane < (uint32_t)(NT / 32) ? scan[lane] : 0u;
+        const uint32_t w0 = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= (uint32_t)o) w += y;
+        }
+        if (lane < (uint32_t)(NT / 32)) scan[lane] = w - w0;
+        if (lane == 31) *total = w;
+    }
+    __syncthreads();
+    const uint32_t r = scan[warp] + x - v;
+    __syncthreads();   // scan[] may be reused by the caller
+    return r;
+}
+
+// One stable 8-bit pass of the one-CTA radix sort over m elements: input
+// element e is (key(e), idx(e)) when valid(e); warp w takes the elements
+// [w ch, (w + 1) ch). Each survivor goes to slot out(pos, key, idx).
+template <int NT, class In, class Out>
+__device__ __forceinline__ void one_pass(OneSmem<false, NT>& sm, uint32_t m, uint32_t shift, In in, Out out) {
+    constexpr int W = NT / 32;
+    const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+    const uint32_t ch = ((m + W - 1) / W + 31u) & ~31u;
+    const uint32_t a = min(warp * ch, m), b = min(a + ch, m);
+    for (uint32_t k = tid; k < (uint32_t)W * 256u; k += NT) {
+        (&sm.u.r.off[0][0])[k] = 0;
+        (&sm.u.r.wm[0][0])[k] = 0;
+    }
+    __syncthreads();
+    uint32_t* const off = sm.u.r.off[warp];
+    uint32_t* const wm = sm.u.r.wm[warp];
+    for (uint32_t e = a + lane; e < b; e += 32) {
+        uint32_t k, x;
+        if (in(e, &k, &x)) atomicAdd(&off[(k >> shift) & 255u], 1u);
+    }
+    __syncthreads();
+    // Digit-major starts: digit d's runs in warp order, the digits in order.
+    if (tid < 256) {
+        uint32_t run = 0;
+        for (int w = 0; w < W; ++w) {
+            const uint32_t c = sm.u.r.off[w][tid];
+            sm.u.r.off[w][tid] = run;
+            run += c;
+        }
+        sm.u.r.tot[tid] = run;
+    }
+    __syncthreads();
+    const uint32_t t = tid < 256 ? sm.u.r.tot[tid] : 0u;
+    const uint32_t start = cta_exclusive_scan<NT>(t, sm.scan, &sm.total);
+    if (tid < 256)
+        for (int w = 0; w < W; ++w) sm.u.r.off[w][tid] += start;
+    __syncthreads();
+    const uint32_t lt = lanemask_lt();
+    for (uint32_t e0 = a; e0 < b; e0 += 32) {
+        const uint32_t e = e0 + lane;
+        uint32_t k = 0, x = 0;
+        const bool v = e < b && in(e, &k, &x);
+        const uint32_t d = (k >> shift) & 255u;
+        if (v) atomicOr(&wm[d], 1u << lane);
+        __syncwarp();
+        uint32_t peers = 0, prior = 0;
+        if (v) {
+            peers = wm[d];
+            prior = off[d];
+        }
+        __syncwarp();
+        if (v && lane == 31u - __clz(peers)) {
+            wm[d] = 0;
+            off[d] = prior + __popc(peers);
+        }
+        __syncwarp();
+        if (v) out(prior + __popc(peers & lt), k, x);
+    }
+    __syncthreads();
+}
+
+template <bool kCounting, int NT>
+__global__ void __launch_bounds__(NT, 1) one_kernel(const __grid_constant__ LaunchDesc L) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    OneSmem<kCounting, NT>& sm = *reinterpret_cast<OneSmem<kCounting, NT>*>(smem_raw);
+    const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+    wait_prerequisites();   // the job table
+    if (*(volatile uint32_t*)L.err) return;
+    const JobDesc& J = L.jobs[blockIdx.x];
+    static_assert(sizeof(ViewConsts) % 4 == 0, "copied in words");
+    for (uint32_t k = tid; k < sizeof(ViewConsts) / 4; k += NT)
+        reinterpret_cast<uint32_t*>(&sm.vc)[k] = reinterpret_cast<const uint32_t*>(&J.vc)[k];
+    if (kCounting)
+        for (uint32_t k = tid; k < 32768u; k += NT) sm.u.hist[k] = 0;
+    __syncthreads();
+    const ViewConsts& c = sm.vc;
+    const uint32_t n = min(J.n, kOneMax);
+    const bool fp = c.cull > 0.0f, any = c.visible != 0;
+    // Keys and survivors, as the keys phase decides them.
+    for (uint32_t e0 = 0; e0 < n; e0 += NT) {
+        const uint32_t e = e0 + tid;
+        bool kept = false;
+        uint32_t key = 0;
+        if (e < n && any) {
+            const float4 p = __ldg(&J.centers[e]);
+            float view[4];
+            view_of(c, p.x, p.y, p.z, view);
+            key = depth_key(c, view);
+            const uint32_t byte = __float_as_uint(p.w) >> 24;
+            kept = in_frustum(c, view) && byte > c.faint_max;
+            if (kept && fp) {
+                bool keep_sc = false, cull_sc = false;
+                if (c.persp)
+                    shortcut(c, view, byte, J.sexp[e], c.afx, c.afy, c.r0, c.r1, c.r2, c.xcap, c.ycap, c.keep_byte,
+                             &keep_sc, &cull_sc);
+                if (!keep_sc) {
+                    kept = false;
+                    if (!cull_sc) {
+                        const float2 a = __ldg(&J.cov[3 * (size_t)e]), b = __ldg(&J.cov[3 * (size_t)e + 1]),
+                                     q = __ldg(&J.cov[3 * (size_t)e + 2]);
+                        const float sg[6] = {a.x, a.y, b.x, b.y, q.x, q.y};
+                        kept = footprint_keep(c, view, sg, c.det_min[byte]);
+                    }
+                }
+            }
+        }
+        if (e < n) sm.key[e] = (uint16_t)key;
+        const uint32_t kb = __ballot_sync(0xffffffffu, kept);
+        if (lane == 0 && e < n) sm.live[e >> 5] = kb;
+        if (kCounting && kept) atomicAdd(&sm.u.hist[key >> 1], 1u << ((key & 1u) * 16u));
+    }
+    __syncthreads();
+    // The shade pass, fused: every survivor's colour as seen from the eye.
+    if (J.sh)
+        for (uint32_t e = tid; e < n; e += NT)
+            if ((sm.live[e >> 5] >> (e & 31u)) & 1u) {
+                const float4 p = __ldg(&J.centers[e]);
+                J.shaded[e] = shade_splat(J.sh, J.sh_words, J.sh_degree, e, p.x, p.y, p.z, __float_as_uint(p.w), J.eye);
+            }
+    const uint32_t idx_base = J.idx_base;
+    uint32_t* const order = J.order;
+    uint32_t* const keys_out = J.keys;
+    if constexpr (kCounting) {
+        // Each thread's 65536 / NT keys: their counts' sum, the CTA's scan,
+        // then each key's first slot (below 2^16: n <= kOneMax).
+        constexpr uint32_t KW = 32768u / NT;   // words a thread owns
+        uint32_t* const h = &sm.u.hist[tid * KW];
+        uint32_t sum = 0;
+        for (uint32_t k = 0; k < KW; ++k) sum += (h[k] & 0xFFFFu) + (h[k] >> 16);
+        uint32_t run = cta_exclusive_scan<NT>(sum, sm.scan, &sm.total);
+        for (uint32_t k = 0; k < KW; ++k) {
+            const uint32_t lo = h[k] & 0xFFFFu, hi = h[k] >> 16;
+            h[k] = run | ((run + lo) << 16);
+            run += lo + hi;
+        }
+        __syncthreads();
+        if (tid == 0) *J.count = sm.total;
+        if (warp == 0) {
+            const uint32_t lt = lanemask_lt();
+            for (uint32_t b0 = 0; b0 < n; b0 += 32) {
+                const uint32_t e = b0 + lane;
+                const bool v = e < n && ((sm.live[b0 >> 5] >> lane) & 1u);
+                const uint32_t k = v ? (uint32_t)sm.key[e] : (0x10000u | lane);
+                const uint32_t peers = __match_any_sync(0xffffffffu, k);
+                const uint32_t sh = (k & 1u) * 16u;
+                const uint32_t prior = v ? (sm.u.hist[k >> 1] >> sh) & 0xFFFFu : 0u;
+                __syncwarp();
+                if (v && lane == 31u - __clz(peers)) atomicAdd(&sm.u.hist[k >> 1], (uint32_t)__popc(peers) << sh);
+                __syncwarp();
+                if (v) {
+                    const uint32_t r = prior + __popc(peers & lt);
+                    order[r] = idx_base + e;
+                    if (keys_out) keys_out[r] = k;
+                }
+            }
+        }
+    } else {
+        // Low digit: the splats (survivors only) into key1 / idx1, compacted.
+        one_pass<NT>(
+            sm, n, 0u,
+            [&](uint32_t e, uint32_t* k, uint32_t* x) {
+                *k = sm.key[e];
+                *x = e;
+                return ((sm.live[e >> 5] >> (e & 31u)) & 1u) != 0u;
+            },
+            [&](uint32_t pos, uint32_t k, uint32_t x) {
+                sm.u.r.key1[pos] = (uint16_t)k;
+                sm.u.r.idx1[pos] = (uint16_t)x;
+            });
+        const uint32_t s = sm.total;
+        if (tid == 0) *J.count = s;
+        // High digit: straight into the outputs.
+        one_pass<NT>(
+            sm, s, 8u,
+            [&](uint32_t e, uint32_t* k, uint32_t* x) {
+                *k = sm.u.r.key1[e];
+                *x = sm.u.r.idx1[e];
+                return true;
+            },
+            [&](uint32_t pos, uint32_t k, uint32_t x) {
+                order[pos] = idx_base + x;
+                if (keys_out) keys_out[pos] = k;
+            });
+    }
+}
+
+template <bool kCounting>
+static cudaError_t launch_one_variant(const LaunchDesc& L, cudaStream_t stream) {
+    static bool ready = false;   // the attribute is per function, set once per process
+    constexpr size_t bytes = sizeof(OneSmem<kCounting, kOneThreads>);
+    if (!ready) {
+        const cudaError_t e =
+            cudaFuncSetAttribute(one_kernel<kCounting, kOneThreads>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        if (e != cudaSuccess) return e;
+        ready = true;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(L.njobs);
+    cfg.blockDim = dim3(kOneThreads);
+    cfg.dynamicSmemBytes = bytes;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, one_kernel<kCounting, kOneThreads>, L);
+}
+
+// Host-side launcher of the one-CTA sorts: one CTA per job of L.jobs (every
+// one a job of splats of at most kOneMax).
+cudaError_t launch_one(const LaunchDesc& L, uint32_t algorithm, cudaStream_t stream) {
+    if (L.njobs == 0) return cudaSuccess;
+    return algorithm == kAlgoOneCount ? launch_one_variant<true>(L, stream) : launch_one_variant<false>(L, stream);
+}
+
 
 // Work item `seg` of the launch: from the segment table, or the lone job's
 // consecutive chunks.

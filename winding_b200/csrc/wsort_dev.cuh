@@ -41,6 +41,13 @@ constexpr uint32_t kGroup = 16;           // segments per look-back group
 constexpr int kKeysIPT = 4;               // splats per thread in one sub-tile of a keys item
 constexpr int kDigitIPT = 8;              // elements per thread in one sub-tile of a digit pass
 constexpr int kSubHist = 8;               // lane-interleaved sub-histograms for counting
+// The sort's algorithms (ws_params.algorithm): the three phases over
+// segments of every job (any size), or one CTA per job with the job in its
+// shared memory (jobs of splats up to kOneMax), placed by two 8-bit passes
+// or by one counting pass over all 65536 keys.
+constexpr uint32_t kAlgoPhases = 0, kAlgoOneRadix = 1, kAlgoOneCount = 2;
+constexpr uint32_t kOneMax = 16384;       // largest job the one-CTA sorts take
+constexpr int kOneThreads = 1024;
 
 // Per-view constants of one job, computed once (by the host for a sort, by
 // make_consts for the draw). Each is the same IEEE operation on the same
@@ -165,6 +172,7 @@ struct LaunchCtl {
 // ranges of `chunk` splats.
 struct LaunchDesc {
     const JobDesc* jobs;
+    uint32_t njobs;
     const SegDesc* segs;
     uint32_t nseg;              // segments in the launch
     uint32_t chunk;             // one job: splats a segment covers

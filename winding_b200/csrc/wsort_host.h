@@ -67,6 +67,10 @@ void write_table(void* dst, const JobDesc* jobs, int njobs, const LaunchShape& S
 LaunchDesc launch_desc(const void* d_table, int njobs, const LaunchShape& S, char* scratch, uint32_t* err,
                        uint32_t spin_limit, TraceRec* trace);
 cudaError_t launch_sort(const LaunchDesc& L, int threads, int grid, int sms, cudaStream_t stream);
+// Whether the one-CTA sorts take these jobs (all of splats, none above kOneMax).
+bool one_cta_takes(const JobDesc* jobs, int njobs);
+// The one-CTA sorts (kAlgoOneRadix or kAlgoOneCount): one CTA per job.
+cudaError_t launch_one(const LaunchDesc& L, uint32_t algorithm, cudaStream_t stream);
 int sort_occupancy(int threads);
 
 }  // namespace wsort

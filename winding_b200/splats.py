@@ -88,12 +88,15 @@ class Context:
         self.check(self.lib.ws_get_params(self.handle, ctypes.byref(p)))
         return p
 
-    def set_params(self, tile=None, ctas_per_sm=None, spin_limit=None, segs_per_cta=None) -> None:
+    def set_params(self, tile=None, ctas_per_sm=None, spin_limit=None, segs_per_cta=None, algorithm=None) -> None:
         """Kernel parameters (ws_params): tile = the least splats a segment
         covers, ctas_per_sm = 1 (1024-thread CTAs) or 2 (512-thread),
         segs_per_cta = segments per resident CTA, spin_limit = polls before a
-        device-side wait gives up."""
+        device-side wait gives up, algorithm = 0 (three phases), 1 (one-CTA
+        radix) or 2 (one-CTA counting) for launches of small jobs of splats."""
         p = self.params
+        if algorithm is not None:
+            p.algorithm = algorithm
         if tile is not None:
             p.tile = tile
         if ctas_per_sm is not None:
