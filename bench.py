@@ -70,8 +70,10 @@ def parse_args():
                     help="fixed least splats a segment covers (skips the autotuner; with --ctas)")
     ap.add_argument("--ctas", type=int, default=0, help="fixed kernel variant: 1 or 2 CTAs per SM (with --tile)")
     ap.add_argument("--segs", type=int, default=1, help="fixed segments per resident CTA (with --tile)")
-    ap.add_argument("--only", default="", choices=["", "particles-64", "shade-1M", "decode", "draw-1M"],
-                    help="run one side measurement alone and print its result (no bench line)")
+    ap.add_argument("--only", default="", choices=["", "particles-64", "shade-1M", "decode", "draw-1M", "sort-batch"],
+                    help="run one side measurement alone and print its result (no bench line); sort-batch: "
+                         "mixed-64 as 3 + 3 batched launches with the --tile/--ctas/--segs parameters (for a "
+                         "profiler: the 4th launch's three kernels are launches 9-11)")
     return ap.parse_args()
 
 
@@ -338,7 +340,7 @@ def _run_wsort(args, rank, world, local_rank, torch):
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device="cuda")
     if args.only:   # one side measurement alone (for a profiler, say)
         fns = {"particles-64": particles_suite, "shade-1M": shade_suite, "decode": decode_suite,
-               "draw-1M": draw_suite}
+               "draw-1M": draw_suite, "sort-batch": lambda c, t, f, pk: sort_batch_only(c, t, f, args)}
         peak, _ = peak_hbm()
         result = fns[args.only](ctx, torch, flush, peak)
         if rank == 0:
@@ -365,6 +367,29 @@ def _run_wsort(args, rank, world, local_rank, torch):
                 line["suite"] = {"error": f"{type(exc).__name__}: {exc}"}
         print(json.dumps(line), flush=True)
     ctx.close()
+
+
+def sort_batch_only(ctx, torch, flush, args):
+    """mixed-64 as batched launches (ws_sort_batch) with fixed parameters:
+    3 untimed, then 3 timed by the library's kernel events."""
+    p = load_jobs(ctx, torch, make_jobs("mixed-64", args.cull))
+    ctx.set_params(tile=args.tile or 2048, ctas_per_sm=args.ctas or 1, segs_per_cta=args.segs, algorithm=0)
+    stream = torch.cuda.current_stream().cuda_stream
+    specs = [(sp, v, o.data_ptr(), k.data_ptr(), c.data_ptr())
+             for sp, v, (o, k, c) in zip(p["clouds"], p["views"], p["outs"])]
+    for _ in range(3):
+        flush.zero_()
+        ctx.sort_batch(specs, stream)
+    ctx.timing(True)
+    timed_sorts(ctx, torch, 3, flush, lambda: ctx.sort_batch(specs, stream))
+    kms, launches = ctx.timing_read()
+    ctx.timing(False)
+    ctx.sync()
+    out = {"jobs": len(specs), "splats": p["splats"], "kernel_us": kms / max(launches, 1) * 1e3,
+           "params": [args.tile or 2048, args.ctas or 1, args.segs]}
+    for sp in p["clouds"]:
+        sp.destroy()
+    return out
 
 
 def max_over_ranks(dist, torch, ms):

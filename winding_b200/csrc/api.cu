@@ -17,7 +17,9 @@
 
 namespace wsort {
 cudaError_t launch_decode(const void* records, uint32_t n, float4* centers, float2* cov, int8_t* sexp,
-                          uint32_t* bounds, uint32_t* bad, int sms, cudaStream_t stream);
+                          uint32_t* bounds, uint32_t* bad, int sms, cudaStream_t stream, uint32_t first);
+cudaError_t stream_splat_records(ws_ctx* ctx, const uint8_t* src, uint32_t n, float4* centers, float2* cov,
+                                 int8_t* sexp, uint32_t* bounds, uint32_t* bad);
 
 int set_error(ws_ctx* ctx, int code, const char* fmt, ...) {
     char buf[512];
@@ -780,7 +782,10 @@ static int sniff(ws_ctx* ctx, const uint8_t* d, size_t nbytes) {
     return WS_OK;
 }
 
-static int decode_cloud(ws_ctx* ctx, const void* dev_records, uint32_t n, ws_cloud** out) {
+// A cloud from n .splat records: in host memory (streamed through the
+// context's pinned chunks, each decoded while the next one is copied) or on
+// the device (decoded in place).
+static int decode_cloud(ws_ctx* ctx, const void* records, bool on_host, uint32_t n, ws_cloud** out) {
     cudaError_t e;
     ws_cloud* c = new (std::nothrow) ws_cloud();
     if (!c) return set_error(ctx, WS_ERR_NOMEM, "ws_cloud: out of host memory");
@@ -803,7 +808,9 @@ static int decode_cloud(ws_ctx* ctx, const void* dev_records, uint32_t n, ws_clo
     cudaMemsetAsync(c->centers, 0, np * sizeof(float4), ctx->stream);
     cudaMemsetAsync(c->cov, 0, np * 3 * sizeof(float2), ctx->stream);
     cudaMemsetAsync(c->sexp, 0x7f, np, ctx->stream);   // padding: no shortcut
-    e = launch_decode(dev_records, n, c->centers, c->cov, c->sexp, words, words + 7, ctx->sms, ctx->stream);
+    e = on_host ? stream_splat_records(ctx, static_cast<const uint8_t*>(records), n, c->centers, c->cov, c->sexp, words,
+                                       words + 7)
+                : launch_decode(records, n, c->centers, c->cov, c->sexp, words, words + 7, ctx->sms, ctx->stream, 0);
     uint32_t back[8];
     if (e == cudaSuccess) e = cudaMemcpyAsync(back, words, sizeof(back), cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
@@ -838,17 +845,7 @@ extern "C" int ws_cloud_from_splat(ws_ctx* ctx, const uint8_t* bytes, size_t nby
     cudaSetDevice(ctx->device);
     int rc = sniff(ctx, bytes, nbytes);
     if (rc) return rc;
-    void* staging = nullptr;
-    cudaError_t e = cudaMalloc(&staging, nbytes);
-    if (e != cudaSuccess) return cuda_error(ctx, e, "ws_cloud_from_splat");
-    e = cudaMemcpyAsync(staging, bytes, nbytes, cudaMemcpyHostToDevice, ctx->stream);
-    if (e != cudaSuccess) {
-        cudaFree(staging);
-        return cuda_error(ctx, e, "ws_cloud_from_splat upload");
-    }
-    rc = decode_cloud(ctx, staging, (uint32_t)(nbytes / 32), out);
-    cudaFree(staging);
-    return rc;
+    return decode_cloud(ctx, bytes, true, (uint32_t)(nbytes / 32), out);
 }
 
 extern "C" int ws_cloud_from_device(ws_ctx* ctx, const void* dev, size_t nbytes, ws_cloud** out) {
@@ -864,7 +861,7 @@ extern "C" int ws_cloud_from_device(ws_ctx* ctx, const void* dev, size_t nbytes,
     }
     int rc = sniff(ctx, head, nbytes);
     if (rc) return rc;
-    return decode_cloud(ctx, dev, (uint32_t)(nbytes / 32), out);
+    return decode_cloud(ctx, dev, false, (uint32_t)(nbytes / 32), out);
 }
 
 extern "C" int ws_cloud_info(const ws_cloud* c, uint32_t* count, double mn[3], double mx[3]) {

@@ -32,7 +32,7 @@ __device__ __forceinline__ void covariance(float fsx, float fsy, float fsz, uint
 __global__ void __launch_bounds__(256) decode_kernel(const uint4* __restrict__ rec, uint32_t n,
                                                      float4* __restrict__ centers, float2* __restrict__ cov,
                                                      int8_t* __restrict__ sexp, uint32_t* __restrict__ bounds,
-                                                     uint32_t* __restrict__ bad) {
+                                                     uint32_t* __restrict__ bad, uint32_t first) {
     uint32_t lo[3] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu};
     uint32_t hi[3] = {0u, 0u, 0u};
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -40,7 +40,7 @@ __global__ void __launch_bounds__(256) decode_kernel(const uint4* __restrict__ r
         const uint4 b = __ldcs(&rec[2 * (size_t)i + 1]);
         const float x = __uint_as_float(a.x), y = __uint_as_float(a.y), z = __uint_as_float(a.z);
         if (!(isfinite(x) && isfinite(y) && isfinite(z))) {
-            atomicMin(bad, i);
+            atomicMin(bad, first + i);
             continue;
         }
         centers[i] = make_float4(x, y, z, __uint_as_float(b.z));
@@ -89,11 +89,15 @@ __global__ void __launch_bounds__(256) decode_kernel(const uint4* __restrict__ r
     }
 }
 
+// Decodes records [0, n) into splats first .. first + n - 1 of the cloud's
+// arrays (centers, cov and sexp point at splat 0); bad receives the least
+// cloud index of a record whose position is not finite.
 cudaError_t launch_decode(const void* records, uint32_t n, float4* centers, float2* cov, int8_t* sexp,
-                          uint32_t* bounds, uint32_t* bad, int sms, cudaStream_t stream) {
+                          uint32_t* bounds, uint32_t* bad, int sms, cudaStream_t stream, uint32_t first) {
     const uint32_t want = (n + 255) / 256;
     const uint32_t grid = want < (uint32_t)sms * 8u ? (want ? want : 1u) : (uint32_t)sms * 8u;
-    decode_kernel<<<grid, 256, 0, stream>>>(static_cast<const uint4*>(records), n, centers, cov, sexp, bounds, bad);
+    decode_kernel<<<grid, 256, 0, stream>>>(static_cast<const uint4*>(records), n, centers + first,
+                                            cov + 3 * (size_t)first, sexp + first, bounds, bad, first);
     return cudaGetLastError();
 }
 

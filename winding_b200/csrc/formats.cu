@@ -507,13 +507,13 @@ void parallel_copy(void* dst, const void* src, size_t bytes) {
 }
 
 // Streams n fixed-size records from host memory to the device, a chunk of
-// about 32 MB at a time through the context's two pinned and two device
+// about 4 MB at a time through the context's two pinned and two device
 // buffers: while one chunk crosses PCIe and is decoded (`decode(dev, first,
 // count)`, queued on the context's stream), the host copies the next one.
 // Returns the first CUDA error; the caller's decode launches are checked.
 template <class Decode>
 cudaError_t stream_records(ws_ctx* ctx, const uint8_t* src, uint32_t n, size_t stride, Decode decode) {
-    constexpr size_t kChunkBytes = 32u << 20;
+    constexpr size_t kChunkBytes = 4u << 20;
     const uint32_t per = (uint32_t)std::max<size_t>(1, std::min<size_t>(kChunkBytes / stride, n ? n : 1));
     const size_t chunk = (size_t)per * stride;
     cudaError_t e;
@@ -1316,6 +1316,22 @@ int load_sog(ws_ctx* ctx, const uint8_t* bytes, size_t nbytes, ws_decode_image d
 }
 
 }  // namespace
+
+cudaError_t launch_decode(const void* records, uint32_t n, float4* centers, float2* cov, int8_t* sexp,
+                          uint32_t* bounds, uint32_t* bad, int sms, cudaStream_t stream, uint32_t first);
+
+// n .splat records from host memory into a cloud's arrays, through the
+// pinned chunks above.
+cudaError_t stream_splat_records(ws_ctx* ctx, const uint8_t* src, uint32_t n, float4* centers, float2* cov,
+                                 int8_t* sexp, uint32_t* bounds, uint32_t* bad) {
+    cudaError_t le = cudaSuccess;
+    const cudaError_t e = stream_records(ctx, src, n, 32, [&](const uint8_t* dev, uint32_t first, uint32_t count) {
+        const cudaError_t d = launch_decode(dev, count, centers, cov, sexp, bounds, bad, ctx->sms, ctx->stream, first);
+        if (le == cudaSuccess) le = d;
+    });
+    return e != cudaSuccess ? e : le;
+}
+
 }  // namespace wsort
 
 using namespace wsort;
