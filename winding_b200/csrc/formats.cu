@@ -507,13 +507,13 @@ void parallel_copy(void* dst, const void* src, size_t bytes) {
 }
 
 // Streams n fixed-size records from host memory to the device, a chunk of
-// about 4 MB at a time through the context's two pinned and two device
+// about 32 MB at a time through the context's two pinned and two device
 // buffers: while one chunk crosses PCIe and is decoded (`decode(dev, first,
 // count)`, queued on the context's stream), the host copies the next one.
 // Returns the first CUDA error; the caller's decode launches are checked.
 template <class Decode>
 cudaError_t stream_records(ws_ctx* ctx, const uint8_t* src, uint32_t n, size_t stride, Decode decode) {
-    constexpr size_t kChunkBytes = 4u << 20;
+    constexpr size_t kChunkBytes = 32u << 20;
     const uint32_t per = (uint32_t)std::max<size_t>(1, std::min<size_t>(kChunkBytes / stride, n ? n : 1));
     const size_t chunk = (size_t)per * stride;
     cudaError_t e;

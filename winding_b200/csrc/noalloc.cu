@@ -15,8 +15,9 @@
 // array's device address with cudaGetSymbolAddress and keeps it; make that
 // first call before any stream capture. Every call then queues three kernels
 // on the stream: one that writes the job description into the array and
-// clears the counters that must start at zero, the sort kernel of ws_sort
-// itself, and one that turns a device-side error into *count = 0xFFFFFFFF. All calls share the one array, which keeps the last call's
+// clears the counters that must start at zero, the sort kernels of ws_sort
+// themselves (keys, low digit, high digit), and one that turns a device-side
+// error into *count = 0xFFFFFFFF. All calls share the one array, which keeps the last call's
 // contents: calls whose work overlaps on the GPU (other streams, other host
 // threads) race on it and must be serialised by the caller.
 #include "wsort.h"
