@@ -1,6 +1,7 @@
-// The persistent sort kernel: every (cloud, view) job's keys, survivor
-// compaction and stable two-digit radix sort, for any number of jobs, in one
-// launch.
+// The sort: every (cloud, view) job's keys, survivor compaction and stable
+// two-digit radix sort, for any number of jobs, in one launch of three
+// persistent kernels (keys, low digit, high digit), chained by programmatic
+// dependent launch; and the one-CTA sorts for small jobs.
 //
 // Reference (src/render/splats.js): makeKeys :155-186 appends survivors
 // through a global atomic and counts them into 65536 buckets; scanCounts
@@ -26,13 +27,20 @@
 // segments, waiting (bounded) only for those. The digit starts come from the
 // totals the keys phase counted.
 //
-// Items are claimed in ticket order by a persistent grid: every segment's
-// keys, then every low pass, then every high pass. An item waits only for
-// items with smaller tickets (the job's earlier phase, or its own phase's
-// earlier segments, which publish their counts before they wait), all
-// claimed by running CTAs, so the queue always drains, whatever else shares
-// the GPU. Every wait is bounded: after spin_limit polls the kernel records
-// an error and every CTA drains the remaining items without work.
+// Items are claimed in ticket order, one ticket counter per phase: every
+// segment's keys, then every low pass, then every high pass, each phase a
+// persistent kernel. Each kernel lets the next one launch as soon as all its
+// CTAs run (griddepcontrol.launch_dependents at their start); the next
+// kernel's CTAs take SMs as this one's leave, and none waits for a whole
+// grid: an item waits only for its own job's previous phase (a completion
+// count) and for its own phase's earlier segments (which publish their
+// counts before they wait). All of those have smaller tickets, claimed by
+// CTAs that are running (a kernel launches only once every CTA of the one
+// before it runs), so the queue always drains, whatever else shares the
+// GPU; and a batch's later jobs can be in their keys while its earlier jobs
+// are in their digit passes. Every wait is bounded: after spin_limit polls
+// the kernel records an error and every CTA drains the remaining items
+// without work.
 //
 // Ranking: a warp ranks 32 elements a round, in element order. Lanes with
 // the same digit find each other by an atomicOr of their lane bit into the
@@ -386,6 +394,10 @@ __device__ __forceinline__ void stage_issue(const JobDesc& J, KeysSmem<NT>& sm, 
 template <int NT>
 __device__ void keys_publish(const JobDesc& J, uint32_t ls, KeysSmem<NT>& sm) {
     JobCtl* ctl = reinterpret_cast<JobCtl*>(J.ctl);
+    // Every thread's keys and survivor words are visible on the GPU before
+    // the item is counted done: the low pass reads them after acquiring the
+    // job's count, with no grid-wide wait.
+    __threadfence();
     __syncthreads();
     const uint32_t d = threadIdx.x;
     if (d < 256) {
@@ -647,11 +659,12 @@ __device__ void digit_item(const JobDesc& J, const SegDesc& sd, DigitSmem<NT>& s
     uint32_t* const agg = J.agg + (size_t)PASS * J.nseg * 256;
     const uint32_t ls = sd.local, g = ls / kGroup;
 
-    // The job's previous phase, every segment of it: finished with the
-    // previous kernel, unless this launch left it out (the failure self-test,
-    // whose wait never ends).
-    if (L.first_phase > kPhaseKeys && !wait_count(PASS == 0 ? &ctl->keys_done : &ctl->low_done, J.nseg, sm, L, item))
-        return;
+    // The job's previous phase, every segment of it (its items have smaller
+    // tickets of the previous kernel, whose CTAs are all resident: the wait
+    // ends, unless the launch left that phase out, as the failure self-test
+    // does). A job's pass starts as soon as its own previous phase is done,
+    // while other jobs may still be in theirs.
+    if (!wait_count(PASS == 0 ? &ctl->keys_done : &ctl->low_done, J.nseg, sm, L, item)) return;
     digit_starts(ctl->tot[PASS], sm);
     const uint32_t S = sm.total;   // the job's survivors
     uint32_t lo, hi;
@@ -890,8 +903,10 @@ __device__ void digit_item(const JobDesc& J, const SegDesc& sd, DigitSmem<NT>& s
 
 // Lets the stream's next kernel (launched with programmatic stream
 // serialization) schedule its CTAs once every CTA here has called it or
-// exited; that kernel still waits in griddepcontrol.wait until this grid has
-// finished and its writes are visible.
+// exited. A kernel that calls wait_prerequisites (griddepcontrol.wait) then
+// waits until the grids before it have finished and their writes are
+// visible; the digit passes do not, and order their reads by each job's
+// completion counts instead (release by the writer, acquire by the reader).
 __device__ __forceinline__ void allow_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 __device__ __forceinline__ void wait_prerequisites() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
@@ -1226,6 +1241,9 @@ __global__ void __launch_bounds__(NT, MINB) keys_kernel(const __grid_constant__ 
         fence_proxy_async();
     }
     wait_prerequisites();   // the job table and the zeroed counters
+    // The low pass may launch now: its CTAs take the SMs this kernel's CTAs
+    // leave, and its items wait for their own job's keys.
+    allow_dependents();
     claim_next(sm, &L.lctl->ticket[kPhaseKeys], L.err);
     KeysStage ks{0u, 0u};
     uint64_t t_claim = 0, t_start = 0;
@@ -1253,7 +1271,6 @@ __global__ void __launch_bounds__(NT, MINB) keys_kernel(const __grid_constant__ 
         claim_next(sm, &L.lctl->ticket[kPhaseKeys], L.err);
         if (L.trace && tid == 0) t_claim = global_ns();
     }
-    allow_dependents();
     // No bulk copy into this CTA's shared memory outlives it (one is only
     // left in flight if a wait gave up).
     if (tid == 0) {
@@ -1272,7 +1289,9 @@ __global__ void __launch_bounds__(NT, MINB) digit_kernel(const __grid_constant__
     extern __shared__ __align__(128) unsigned char smem_raw[];
     DigitSmem<NT>& sm = *reinterpret_cast<DigitSmem<NT>*>(smem_raw);
     const uint32_t tid = threadIdx.x;
-    wait_prerequisites();   // the previous pass has finished
+    // No grid-wide wait for the previous kernel: each item waits for its own
+    // job's previous phase (digit_item). The next pass may launch now.
+    allow_dependents();
     claim_next(sm, &L.lctl->ticket[kPhaseLow + PASS], L.err);
     uint64_t t_claim = 0, t_start = 0;
     if (L.trace && tid == 0) t_claim = global_ns();
@@ -1294,7 +1313,6 @@ __global__ void __launch_bounds__(NT, MINB) digit_kernel(const __grid_constant__
         claim_next(sm, &L.lctl->ticket[kPhaseLow + PASS], L.err);
         if (L.trace && tid == 0) t_claim = global_ns();
     }
-    allow_dependents();
 }
 
 // Keys CTAs: 768 threads, one an SM (up to 85 registers a thread).
