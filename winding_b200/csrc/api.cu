@@ -12,6 +12,7 @@
 #include <cstring>
 #include <mutex>
 #include <new>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -481,8 +482,12 @@ __global__ void __launch_bounds__(1024) stage_kernel(const __grid_constant__ Job
 // staging, given the launch's shape and the scratch base. The stream waits
 // for the context's previous launch, so one scratch is never shared by two
 // launches in flight.
+// `tail`, when given, queues more kernels right after the sort's, before the
+// launch's events (so that nothing but kernels lies between them and they
+// may overlap the sort's last phase).
 template <class Fill>
-static int launch_jobs(ws_ctx* ctx, const std::vector<uint32_t>& ns, int njobs, Fill fill, cudaStream_t stream) {
+static int launch_jobs(ws_ctx* ctx, const std::vector<uint32_t>& ns, int njobs, Fill fill, cudaStream_t stream,
+                       const std::function<cudaError_t(cudaStream_t)>* tail = nullptr) {
     cudaError_t e;
     uint64_t splats = 0;
     for (int j = 0; j < njobs; ++j) splats += ns[j];
@@ -559,6 +564,7 @@ static int launch_jobs(ws_ctx* ctx, const std::vector<uint32_t>& ns, int njobs, 
     e = one_cta ? launch_one(L, P.algorithm, stream)
                 : launch_sort(L, S.threads, (int)std::min<size_t>(S.grid, S.segs.size()), ctx->sms, stream);
     if (e != cudaSuccess) return cuda_error(ctx, e, "ws_sort launch");
+    if (tail && (e = (*tail)(stream)) != cudaSuccess) return cuda_error(ctx, e, "ws_sort copy");
     if (t_stop) cudaEventRecord(t_stop, stream);
     cudaEventRecord(ctx->launched, stream);
     ++ctx->launches;
@@ -586,13 +592,14 @@ int run_given_keys(ws_ctx* ctx, const uint16_t* keys, uint32_t n, uint32_t* orde
         stream);
 }
 
-int run_batch(ws_ctx* ctx, const ws_job* jobs, int njobs, cudaStream_t stream) {
+int run_batch(ws_ctx* ctx, const ws_job* jobs, int njobs, cudaStream_t stream,
+              const std::function<cudaError_t(cudaStream_t)>* tail = nullptr) {
     std::vector<uint32_t> ns(njobs);
     for (int j = 0; j < njobs; ++j) ns[j] = jobs[j].cloud->n;
     return launch_jobs(
         ctx, ns, njobs,
         [&](JobDesc* hj, const LaunchShape& S, char* scratch) { layout_jobs(hj, jobs, njobs, S, scratch); },
-        stream);
+        stream, tail);
 }
 
 // Reads and clears the sticky device error words. Call after a sync.
@@ -1043,30 +1050,54 @@ extern "C" int ws_sort_batch(ws_ctx* ctx, int njobs, const ws_job* jobs, void* s
 }
 
 // One job's results on their way to host memory (ws_sort_batch_host): the
-// device outputs and the device addresses of the caller's pinned buffers.
+// device addresses of the caller's pinned buffers; the job's device outputs
+// and its completion count are in its job description.
 struct HostCopy {
-    const uint32_t* order;
-    const uint32_t* keys;       // or null
-    const uint32_t* count;
     uint32_t* horder;
     uint32_t* hkeys;            // or null
     uint32_t* hcount;
     uint32_t n;                 // the job's splats: no count read back exceeds it
-    uint32_t pad[3];
+    uint32_t pad[1];
 };
 
 // Every job's survivors into mapped host memory: blockIdx.y is the job, the
 // x blocks stride over its survivors; consecutive threads write consecutive
-// words. Block (0, j) writes the count.
-__global__ void __launch_bounds__(256) copy_jobs_kernel(const HostCopy* __restrict__ jobs) {
-    const HostCopy J = jobs[blockIdx.y];
+// words. It is launched right behind the sort's last pass and may start
+// while that pass runs: a block first waits (bounded) until its job's high
+// pass is complete, so early jobs cross PCIe while later ones are sorted.
+// Block (0, j) writes the count.
+__global__ void __launch_bounds__(256) copy_jobs_kernel(const JobDesc* __restrict__ jobs,
+                                                        const HostCopy* __restrict__ hc, uint32_t* err,
+                                                        uint32_t spin_limit) {
+    __shared__ uint32_t ready;
+    const JobDesc& J = jobs[blockIdx.y];
+    if (threadIdx.x == 0) {
+        const JobCtl* ctl = reinterpret_cast<const JobCtl*>(J.ctl);
+        uint32_t spins = 0;
+        ready = 1;
+        while (ld_acquire(&ctl->high_done) < J.nseg) {
+            if (*(volatile uint32_t*)err) {   // the sort failed: its error stands
+                ready = 0;
+                break;
+            }
+            if (++spins > spin_limit) {
+                if (atomicCAS(err, 0u, kErrWaitPhase) == 0u) err[1] = 0xFFFFFFFFu;
+                ready = 0;
+                break;
+            }
+            __nanosleep(64);
+        }
+    }
+    __syncthreads();
+    if (!ready) return;
+    const HostCopy H = hc[blockIdx.y];
     // After a device error a job's count may never have been written: the
     // copy stays inside the job's buffers whatever it holds.
-    const uint32_t c = min(*J.count, J.n);
-    if (blockIdx.x == 0 && threadIdx.x == 0) *J.hcount = c;
+    const uint32_t c = min(__ldcg(J.count), H.n);
+    if (blockIdx.x == 0 && threadIdx.x == 0) *H.hcount = c;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < c; i += gridDim.x * blockDim.x) {
-        J.horder[i] = J.order[i];
-        if (J.hkeys) J.hkeys[i] = J.keys[i];
+        H.horder[i] = __ldcg(&J.order[i]);
+        if (H.hkeys) H.hkeys[i] = __ldcg(&J.keys[i]);
     }
 }
 
@@ -1106,33 +1137,45 @@ extern "C" int ws_sort_batch_host(ws_ctx* ctx, int njobs, const ws_job* jobs, vo
         dj[j].count = d + off[j] + 2 * n;
         HostCopy& h = hc[j];
         std::memset(&h, 0, sizeof(h));
-        h.order = dj[j].order;
-        h.keys = dj[j].keys;
-        h.count = dj[j].count;
         h.horder = mapped_alias(jobs[j].order);
         h.hkeys = jobs[j].keys ? mapped_alias(jobs[j].keys) : nullptr;
         h.hcount = mapped_alias(jobs[j].count);
         h.n = (uint32_t)n;
         direct = direct && h.horder && h.hcount && (!jobs[j].keys || h.hkeys);
     }
-    int rc = run_batch(ctx, dj.data(), njobs, stream);
-    if (rc) return rc;
     if (direct) {
-        // The copy table's pinned staging is free: every call ends with a
+        // The copy table goes up before the sort, so that the copy kernel
+        // follows the sort's last pass directly in the stream and overlaps
+        // it. The table's pinned staging is free: every call ends with a
         // synchronisation.
         const size_t tb = (size_t)njobs * sizeof(HostCopy);
         if ((e = ctx->copy_h.ensure(tb)) != cudaSuccess || (e = ctx->copy_d.ensure(tb)) != cudaSuccess)
             return cuda_error(ctx, e, "ws_sort_batch_host staging");
         std::memcpy(ctx->copy_h.p, hc.data(), tb);
-        uint32_t* hw = static_cast<uint32_t*>(ctx->count_h.p);
+        if ((e = cudaMemcpyAsync(ctx->copy_d.p, ctx->copy_h.p, tb, cudaMemcpyHostToDevice, stream)) != cudaSuccess)
+            return cuda_error(ctx, e, "ws_sort_batch_host upload");
         uint32_t max_n = 0;
         for (int j = 0; j < njobs; ++j) max_n = std::max(max_n, jobs[j].cloud->n);
         const uint32_t bx = std::max(1u, std::min((max_n + 2047) / 2048, 64u));
-        if ((e = cudaMemcpyAsync(ctx->copy_d.p, ctx->copy_h.p, tb, cudaMemcpyHostToDevice, stream)) != cudaSuccess)
-            return cuda_error(ctx, e, "ws_sort_batch_host upload");
-        copy_jobs_kernel<<<dim3(bx, (unsigned)njobs), 256, 0, stream>>>(static_cast<const HostCopy*>(ctx->copy_d.p));
-        if ((e = cudaGetLastError()) != cudaSuccess ||
-            (e = cudaMemcpyAsync(hw, ctx->err_d, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
+        const HostCopy* table = static_cast<const HostCopy*>(ctx->copy_d.p);
+        const uint32_t spin = ctx->params.spin_limit;
+        const std::function<cudaError_t(cudaStream_t)> tail = [&](cudaStream_t s) {
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3(bx, (unsigned)njobs);
+            cfg.blockDim = dim3(256);
+            cfg.stream = s;
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+            attr[0].val.programmaticStreamSerializationAllowed = 1;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            return cudaLaunchKernelEx(&cfg, copy_jobs_kernel, static_cast<const JobDesc*>(ctx->jobs_d.p), table,
+                                      ctx->err_d, spin);
+        };
+        int rc = run_batch(ctx, dj.data(), njobs, stream, &tail);
+        if (rc) return rc;
+        uint32_t* hw = static_cast<uint32_t*>(ctx->count_h.p);
+        if ((e = cudaMemcpyAsync(hw, ctx->err_d, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
             (e = cudaStreamSynchronize(stream)) != cudaSuccess)
             return cuda_error(ctx, e, "ws_sort_batch_host");
         if (hw[0]) return take_device_error(ctx);
@@ -1141,6 +1184,8 @@ extern "C" int ws_sort_batch_host(ws_ctx* ctx, int njobs, const ws_job* jobs, vo
         for (int j = 0; j < njobs; ++j) ctx->d2h_bytes += 4 + (size_t)*jobs[j].count * (jobs[j].keys ? 8 : 4);
         return WS_OK;
     }
+    int rc = run_batch(ctx, dj.data(), njobs, stream);
+    if (rc) return rc;
     // Pageable outputs: the counts first, then each job's survivors.
     std::vector<uint32_t> counts(njobs);
     for (int j = 0; j < njobs; ++j)

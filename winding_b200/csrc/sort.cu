@@ -892,11 +892,12 @@ __device__ void digit_item(const JobDesc& J, const SegDesc& sd, DigitSmem<NT>& s
     }
 #undef WS_FETCH
     if (tid == 0) sm.mark[2] = global_ns();
-    if (PASS == 0) {
-        __threadfence();
-        __syncthreads();
-        if (tid == 0) red_release_add(&ctl->low_done, 1u);
-    }
+    // The item is counted done once every thread's writes are visible: the
+    // high pass reads the low pass's output, and a host-output copy reads the
+    // job's final order, after acquiring these counts.
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) red_release_add(PASS == 0 ? &ctl->low_done : &ctl->high_done, 1u);
 }
 
 // ---------------------------------------------------------------- the kernels
@@ -1160,6 +1161,11 @@ __global__ void __launch_bounds__(NT, 1) one_kernel(const __grid_constant__ Laun
                 if (keys_out) keys_out[pos] = k;
             });
     }
+    // The job's outputs are final: counted as all of its segments, for a
+    // host-output copy that waits on them.
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) red_release_add(&reinterpret_cast<JobCtl*>(J.ctl)->high_done, J.nseg);
 }
 
 template <bool kCounting>

@@ -143,7 +143,8 @@ struct JobCtl {
     uint32_t tot[2][256];       // survivors per digit value: low byte, high byte
     uint32_t keys_done;         // keys items finished
     uint32_t low_done;          // low items finished
-    uint32_t pad[14];
+    uint32_t high_done;         // high items finished (the job's outputs are final at nseg)
+    uint32_t pad[13];
 };
 static_assert(sizeof(JobCtl) % 64 == 0, "JobCtl size");
 
