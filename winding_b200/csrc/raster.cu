@@ -58,6 +58,7 @@
 #include "wsort_host.h"
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -510,6 +511,92 @@ __global__ void __launch_bounds__(256) blend_kernel(const Quad* __restrict__ qua
     if (inside) image[(size_t)py * width + px] = dst;
 }
 
+// Crowded tiles are drawn in bands of kBandRows rows, each band by its own
+// CTA (a tile's kBands bands on different SMs), from its own list: the
+// splats of the tile's list whose box meets the band's rows, in list order.
+// A pixel of the band gets the same splats, in the same order, as from the
+// whole list (a splat whose box misses the band has no fragment in it).
+constexpr int kBands = 4;
+constexpr int kBandRows = kTilePx / kBands;
+
+// One CTA of 1024 threads per crowded tile (persistent over them): the
+// tile's kBands band lists, compacted in list order into band_list at
+// kBands * range.x + b * length, their lengths into band_count[slot * kBands + b].
+// Each chunk of 1024 list entries: every thread's band bits, a ballot per
+// band, the warps' counts scanned by warp 0; the next chunk's entries and
+// boxes are loaded while the current one is placed.
+constexpr int kSplitThreads = 1024;
+__global__ void __launch_bounds__(kSplitThreads) band_split_kernel(const Quad* __restrict__ quads,
+                                                                   const uint32_t* __restrict__ splat_of,
+                                                                   const uint2* __restrict__ range,
+                                                                   const uint32_t* __restrict__ tile_order,
+                                                                   const uint32_t* __restrict__ n_crowded,
+                                                                   uint32_t tiles_x, uint32_t* __restrict__ band_list,
+                                                                   uint32_t* __restrict__ band_count) {
+    constexpr int W = kSplitThreads / 32;
+    __shared__ uint32_t warp_n[kBands][W];     // a chunk's count per band and warp, then their exclusive scan
+    __shared__ uint32_t run[kBands];           // placed so far, per band
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, lt = lanemask_lt();
+    const uint32_t crowded = *n_crowded;
+    for (uint32_t slot = blockIdx.x; slot < crowded; slot += gridDim.x) {
+        const uint32_t tile = tile_order[slot];
+        const int ty0 = (int)((tile / tiles_x) * kTilePx);
+        const uint2 rg = range[tile];
+        const uint32_t len = rg.y - rg.x;
+        uint32_t* const out = band_list + (size_t)kBands * rg.x;
+        if (threadIdx.x < kBands) run[threadIdx.x] = 0;
+        auto fetch = [&](uint32_t c0, uint32_t& idx, int2& ys) {
+            const uint32_t e = c0 + threadIdx.x;
+            idx = 0;
+            ys = make_int2(INT_MAX, INT_MIN);   // past the list: meets no band
+            if (e < len) {
+                idx = __ldg(&splat_of[rg.x + e]);
+                ys = make_int2(__ldg(&quads[idx].y0), __ldg(&quads[idx].y1));   // 4-byte fields, 4-byte aligned
+            }
+        };
+        uint32_t idx_n;
+        int2 ys_n;
+        fetch(0, idx_n, ys_n);
+        for (uint32_t c0 = 0; c0 < len; c0 += kSplitThreads) {
+            const uint32_t idx = idx_n;
+            const int2 ys = ys_n;
+            if (c0 + kSplitThreads < len) fetch(c0 + kSplitThreads, idx_n, ys_n);
+            uint32_t bits = 0;
+#pragma unroll
+            for (int b = 0; b < kBands; ++b)
+                if (ys.x <= ty0 + (b + 1) * kBandRows - 1 && ys.y >= ty0 + b * kBandRows) bits |= 1u << b;
+            uint32_t ballots[kBands];
+#pragma unroll
+            for (int b = 0; b < kBands; ++b) {
+                ballots[b] = __ballot_sync(0xffffffffu, (bits >> b) & 1u);
+                if (lane == 0) warp_n[b][warp] = __popc(ballots[b]);
+            }
+            __syncthreads();
+            if (warp == 0) {
+#pragma unroll
+                for (int b = 0; b < kBands; ++b) {
+                    const uint32_t v = lane < (uint32_t)W ? warp_n[b][lane] : 0u;
+                    uint32_t x = v;
+#pragma unroll
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+                        if (lane >= (uint32_t)o) x += y;
+                    }
+                    if (lane < (uint32_t)W) warp_n[b][lane] = run[b] + x - v;
+                    if (lane == 31) run[b] += x;   // W == 32: lane 31 holds the chunk's total
+                }
+            }
+            __syncthreads();
+#pragma unroll
+            for (int b = 0; b < kBands; ++b)
+                if ((bits >> b) & 1u) out[(size_t)b * len + warp_n[b][warp] + __popc(ballots[b] & lt)] = idx;
+            __syncthreads();   // warp_n is rewritten by the next chunk
+        }
+        if (threadIdx.x < kBands) band_count[slot * kBands + threadIdx.x] = run[threadIdx.x];
+        __syncthreads();
+    }
+}
+
 // Crowded tiles: the same blend, with the fragments evaluated by 23 warps
 // and blended by 8. A tile whose list runs to thousands of splats keeps the
 // warps of blend_kernel evaluating 32 pixels for every splat that reaches
@@ -549,13 +636,16 @@ __device__ __forceinline__ uint32_t crowd_box(int bx, int by, int bw) {
 }
 
 __global__ void __launch_bounds__(kCrowdThreads, 1) crowd_kernel(const Quad* __restrict__ quads,
-                                                                 const uint32_t* __restrict__ splat_of,
+                                                                 const uint32_t* __restrict__ band_list,
+                                                                 const uint32_t* __restrict__ band_count,
                                                                  const uint2* __restrict__ range,
                                                                  const uint32_t* __restrict__ tile_order,
                                                                  const uint32_t* __restrict__ n_crowded,
+                                                                 uint32_t* __restrict__ ticket,
                                                                  uint32_t width, uint32_t height, uint32_t tiles_x,
                                                                  float4* __restrict__ image) {
     extern __shared__ __align__(16) unsigned char crowd_raw[];
+    __shared__ uint32_t next_unit;
     CrowdSmem& sm = *reinterpret_cast<CrowdSmem*>(crowd_raw);
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const bool blender = threadIdx.x < kCrowdBlenders, lister = warp == kCrowdLister;
@@ -564,22 +654,34 @@ __global__ void __launch_bounds__(kCrowdThreads, 1) crowd_kernel(const Quad* __r
         float4* z = reinterpret_cast<float4*>(&sm.alpha[0][0][0]);
         for (uint32_t k = threadIdx.x; k < sizeof(sm.alpha) / 16; k += kCrowdThreads) z[k] = make_float4(0, 0, 0, 0);
     }
-    const uint32_t crowded = *n_crowded;
-    for (uint32_t slot = blockIdx.x; slot < crowded; slot += gridDim.x) {
-        const uint32_t tile = tile_order[slot];
+    const uint32_t units = *n_crowded * kBands;   // (crowded tile, band), densest tile's bands first
+    // Units are claimed in order from one counter: a CTA that finishes a
+    // short band takes the next unit, so the densest bands (claimed first)
+    // bound the kernel, not a fixed share of units.
+    for (;;) {
+        __syncthreads();   // every thread has read next_unit
+        if (threadIdx.x == 0) next_unit = atomicAdd(ticket, 1u);
+        __syncthreads();
+        const uint32_t unit = next_unit;
+        if (unit >= units) break;
+        const uint32_t tile = tile_order[unit / kBands], band = unit % kBands;
         const int tx0 = (int)((tile % tiles_x) * kTilePx), ty0 = (int)((tile / tiles_x) * kTilePx);
+        const int by0 = ty0 + (int)band * kBandRows, by1 = by0 + kBandRows - 1;   // the band's rows
         const int px = tx0 + (int)(threadIdx.x & 15), py = ty0 + (int)((threadIdx.x >> 4) & 15);
-        const bool inside = blender && px < (int)width && py < (int)height;
+        const bool mine = blender && py >= by0 && py <= by1;   // a pixel of the band
+        const bool inside = mine && px < (int)width && py < (int)height;
         float4 dst = make_float4(0, 0, 0, 0);
         if (inside) dst = image[(size_t)py * width + px];
         const uint2 rg = range[tile];
-        const uint32_t chunks = (rg.y - rg.x + kCrowdChunk - 1) / kCrowdChunk;
-        auto chunk_len = [&](uint32_t c) { return min(kCrowdChunk, rg.y - rg.x - c * kCrowdChunk); };
+        const uint32_t* const list = band_list + (size_t)kBands * rg.x + (size_t)band * (rg.y - rg.x);
+        const uint32_t count = band_count[unit];
+        const uint32_t chunks = (count + kCrowdChunk - 1) / kCrowdChunk;
+        auto chunk_len = [&](uint32_t c) { return min(kCrowdChunk, count - c * kCrowdChunk); };
         // Staging: threads 0..255 copy one 16-byte quarter of a quad each;
         // the splat index is read a chunk ahead, so its latency is hidden.
         auto index_of = [&](uint32_t c) -> uint32_t {
-            const uint32_t k = rg.x + c * kCrowdChunk + (threadIdx.x >> 2);
-            return threadIdx.x < kCrowdChunk * 4 && c < chunks && k < rg.y ? splat_of[k] : 0xffffffffu;
+            const uint32_t k = c * kCrowdChunk + (threadIdx.x >> 2);
+            return threadIdx.x < kCrowdChunk * 4 && c < chunks && k < count ? list[k] : 0xffffffffu;
         };
         auto stage = [&](uint32_t idx, uint32_t b) {
             if (idx != 0xffffffffu)
@@ -601,8 +703,8 @@ __global__ void __launch_bounds__(kCrowdThreads, 1) crowd_kernel(const Quad* __r
                 n[j] = 0;
                 if (e < m) {
                     const Quad& q = sm.staged[b][e];
-                    const int bx = max(q.x0, tx0), by = max(q.y0, ty0);
-                    const int bw = min(q.x1, tx0 + kTilePx - 1) - bx + 1, bh = min(q.y1, ty0 + kTilePx - 1) - by + 1;
+                    const int bx = max(q.x0, tx0), by = max(q.y0, by0);
+                    const int bw = min(q.x1, tx0 + kTilePx - 1) - bx + 1, bh = min(q.y1, by1) - by + 1;
                     n[j] = (uint32_t)(bw * bh);
                     bt[e] = crowd_box(bx - tx0, by - ty0, bw);
                 }
@@ -637,7 +739,7 @@ __global__ void __launch_bounds__(kCrowdThreads, 1) crowd_kernel(const Quad* __r
             stage(next, (i + 3) % 5);
             next = index_of(i + 4);
             if (blender) {
-                if (i == 0) continue;
+                if (i == 0 || !mine) continue;
                 const uint32_t c = i - 1, b = c % 5, m = chunk_len(c);
                 float* col = &sm.alpha[c & 1][0][threadIdx.x];
                 // Entries past the chunk's end are 0 (never written), so
@@ -829,7 +931,11 @@ extern "C" int ws_draw(ws_ctx* ctx, const ws_cloud* cloud, const ws_view* view, 
     const size_t o_keys = 0, o_own = o_keys + up((size_t)pairs * 2), o_sorted = o_own + up((size_t)pairs * 4);
     const size_t o_skeys = o_sorted + up((size_t)pairs * 4), o_spl = o_skeys + up((size_t)pairs * 4);
     const size_t o_pc = o_spl + up((size_t)pairs * 4);
-    if ((e = ctx->pairs_d.ensure(o_pc + 256)) != cudaSuccess) return cuda_error(ctx, e, "ws_draw scratch");
+    // and the crowded tiles' band lists (room for every pair in every band)
+    // and band lengths
+    const size_t o_band = o_pc + 256, o_bcnt = o_band + up((size_t)pairs * 4 * kBands);
+    const size_t pairs_bytes = ctx->draw_crowd_min ? o_bcnt + up((size_t)tiles * 4 * kBands) : o_pc + 256;
+    if ((e = ctx->pairs_d.ensure(pairs_bytes)) != cudaSuccess) return cuda_error(ctx, e, "ws_draw scratch");
     char* pb = static_cast<char*>(ctx->pairs_d.p);
     uint16_t* keys = reinterpret_cast<uint16_t*>(pb + o_keys);
     uint32_t* owner = reinterpret_cast<uint32_t*>(pb + o_own);
@@ -849,8 +955,15 @@ extern "C" int ws_draw(ws_ctx* ctx, const ws_cloud* cloud, const ws_view* view, 
         if ((e = cudaFuncSetAttribute(crowd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)sizeof(CrowdSmem))) != cudaSuccess)
             return cuda_error(ctx, e, "ws_draw");
-        crowd_kernel<<<std::min(tiles, (uint32_t)ctx->sms), kCrowdThreads, sizeof(CrowdSmem), stream>>>(
-            quads, splat_of, range, tile_order, n_crowded, width, height, tiles_x, reinterpret_cast<float4*>(image));
+        uint32_t* band_list = reinterpret_cast<uint32_t*>(pb + o_band);
+        uint32_t* band_count = reinterpret_cast<uint32_t*>(pb + o_bcnt);
+        uint32_t* ticket = n_crowded + 1;   // the crowded kernel's unit counter (its 256-byte slot)
+        if ((e = cudaMemsetAsync(ticket, 0, sizeof(uint32_t), stream)) != cudaSuccess) return cuda_error(ctx, e, "ws_draw");
+        band_split_kernel<<<std::min(tiles, (uint32_t)ctx->sms * 2), kSplitThreads, 0, stream>>>(
+            quads, splat_of, range, tile_order, n_crowded, tiles_x, band_list, band_count);
+        crowd_kernel<<<std::min(tiles * kBands, (uint32_t)ctx->sms), kCrowdThreads, sizeof(CrowdSmem), stream>>>(
+            quads, band_list, band_count, range, tile_order, n_crowded, ticket, width, height, tiles_x,
+            reinterpret_cast<float4*>(image));
     }
     blend_kernel<<<tiles, 256, 0, stream>>>(quads, splat_of, range, tile_order, n_crowded, width, height, tiles_x,
                                             reinterpret_cast<float4*>(image));
