@@ -63,7 +63,6 @@ template <int NT>
 struct KeysSmem {
     static constexpr int TK = NT * kKeysIPT;     // splats of a keys sub-tile
     alignas(8) uint64_t bar[2];                  // the staging buffers' mbarriers
-    float alpha[256];                            // unpack4x8unorm(..).a: byte / 255, correctly rounded
     ViewConsts vc;
     uint32_t next;                               // the ticket this CTA works on next
     uint32_t drain;
@@ -76,6 +75,9 @@ struct KeysSmem {
     alignas(128) float4 centers[2][TK];
     int8_t sexp[2][TK];
 };
+
+// The keys CTA's shared memory fits the 227 KB a block may opt into.
+static_assert(sizeof(KeysSmem<768>) <= 232448, "keys shared memory");
 
 // Shared memory of a digit-pass CTA (NT threads).
 template <int NT>
@@ -1238,7 +1240,6 @@ __global__ void __launch_bounds__(NT, MINB) keys_kernel(const __grid_constant__ 
     extern __shared__ __align__(128) unsigned char smem_raw[];
     KeysSmem<NT>& sm = *reinterpret_cast<KeysSmem<NT>*>(smem_raw);
     const uint32_t tid = threadIdx.x;
-    for (uint32_t k = tid; k < 256; k += NT) sm.alpha[k] = fdiv(float(k), 255.0f);
     if (tid == 0) {
         sm.pending = 0;
         mbar_init(&sm.bar[0]);
