@@ -6,8 +6,9 @@
 One step is one pass of the sort over one batch of synthetic splats. The
 default workload, mixed-64, is 64 (scene, view) jobs of 10k-2M splats (25M in
 all, cull 0.5), every job's cloud resident in HBM; one step is one
-graph-captured launch of the batch (ws_plan_launch: the job table up, the
-counters reset, the keys kernel and the two digit passes over all 64 jobs).
+graph-captured launch of the batch (ws_plan_launch: the counters reset, the
+keys kernel and the two digit passes over all 64 jobs; the job table with the
+views stays resident, uploaded by ws_plan_set_views).
 Prints one JSON line:
 
   value        Msplats/s (whole job, all ranks), outputs to device memory,
@@ -462,8 +463,9 @@ def batch_line(args, rank, world, dist, ctx, torch, flush):
         "config": {"workload": "mixed-64", "jobs": len(jobs), "splats_per_step": total * world,
                    "survivors_per_step": sum(survivors), "job_splats": [10_000, 2_000_000], "cull": args.cull,
                    "viewport": [1920, 1080], "l2": "flushed (256 MiB write) before each step",
-                   "launch": "ws_plan_launch: one graph (job table upload, counter reset, keys kernel, low and high "
-                             "digit passes over all jobs)",
+                   "launch": "ws_plan_launch: one graph (counter reset, keys kernel, low and high digit passes "
+                             "over all jobs; the job table with the views stays resident, uploaded by "
+                             "ws_plan_set_views)",
                    "parallelism": f"each of {world} ranks sorts its own 64-job batch, no collective"
                    if world > 1 else "single GPU",
                    "tuned": {str(b): {"tile": t, "ctas_per_sm": c, "segs_per_cta": g, "algorithm": ALGORITHMS[a]}

@@ -222,8 +222,8 @@ int ws_sort_batch_host(ws_ctx* ctx, int njobs, const ws_job* jobs, void* stream)
  * A batch frozen into a CUDA graph: the job set (clouds, output buffers) is
  * fixed at creation; views can change between launches with
  * ws_plan_set_views, which waits for the plan's previous launch to finish
- * reading them. The graph holds the upload of the views, the reset of the
- * counters and the one persistent launch.
+ * reading them and uploads the new ones. The job table stays in device
+ * memory; the graph holds the reset of the counters and the sort's launch.
  */
 int ws_plan_create(ws_ctx* ctx, int njobs, const ws_job* jobs, ws_plan** out);
 int ws_plan_set_views(ws_plan* plan, const ws_view* views);

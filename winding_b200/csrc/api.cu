@@ -1431,6 +1431,7 @@ struct ws_plan {
     cudaGraphExec_t exec = nullptr;
     cudaEvent_t done = nullptr;
     int grid;
+    size_t table_bytes = 0;   // the job table (and segment table) in jobs_h / jobs_d
 };
 
 extern "C" int ws_plan_create(ws_ctx* ctx, int njobs, const ws_job* jobs, ws_plan** out) {
@@ -1466,16 +1467,22 @@ extern "C" int ws_plan_create(ws_ctx* ctx, int njobs, const ws_job* jobs, ws_pla
     JobDesc* hj = static_cast<JobDesc*>(p->jobs_h.p);
     layout_jobs(hj, jobs, njobs, S, static_cast<char*>(p->scratch.p));
     write_table(p->jobs_h.p, hj, njobs, S);
-    // Capture: upload the job table from pinned memory, reset the counters,
-    // launch.
+    // The job table stays in device memory (uploaded here and by
+    // ws_plan_set_views); the graph resets the counters and launches.
     cudaStream_t cs;
     if ((e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking)) != cudaSuccess) {
         ws_plan_destroy(p);
         return cuda_error(ctx, e, "ws_plan_create");
     }
+    if ((e = cudaMemcpyAsync(p->jobs_d.p, p->jobs_h.p, tb, cudaMemcpyHostToDevice, cs)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(cs)) != cudaSuccess) {
+        cudaStreamDestroy(cs);
+        ws_plan_destroy(p);
+        return cuda_error(ctx, e, "ws_plan_create upload");
+    }
+    p->table_bytes = tb;
     e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
-        cudaMemcpyAsync(p->jobs_d.p, p->jobs_h.p, tb, cudaMemcpyHostToDevice, cs);
         cudaMemsetAsync(p->scratch.p, 0, S.ctl_bytes, cs);
         const LaunchDesc L = launch_desc(p->jobs_d.p, njobs, S, static_cast<char*>(p->scratch.p), ctx->err_d,
                                          P.spin_limit, nullptr);
@@ -1516,6 +1523,12 @@ extern "C" int ws_plan_set_views(ws_plan* p, const ws_view* views) {
         fill_view_consts(hj[j]);
         p->jobs[j].view = views[j];
     }
+    // The new views go up now; no launch of the plan is in flight.
+    if ((e = cudaMemcpyAsync(p->jobs_d.p, p->jobs_h.p, p->table_bytes, cudaMemcpyHostToDevice, p->ctx->stream)) !=
+            cudaSuccess ||
+        (e = cudaStreamSynchronize(p->ctx->stream)) != cudaSuccess)
+        return cuda_error(p->ctx, e, "ws_plan_set_views");
+    p->ctx->h2d_bytes += p->table_bytes;
     return WS_OK;
 }
 
