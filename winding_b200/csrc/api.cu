@@ -119,16 +119,23 @@ void shape_launch(const uint32_t* ns, int njobs, const ws_params& p, int sms, La
     S.segs.clear();
     S.nseg.assign(njobs, 0);
     S.seg0.assign(njobs, 0);
-    uint64_t v = 0;   // position in the laid-end-to-end splats
-    for (int j = 0; j < njobs; ++j) {
+    // Each job is cut into equal segments of at most a chunk (multiples of
+    // kSegAlign), and the jobs are queued largest first (ties in their given
+    // order): a phase's last items are then the small jobs' short segments,
+    // so the grid's last wave ends evenly. A job's segments stay in order,
+    // which is all the look-back needs.
+    std::vector<int> by_size(njobs);
+    for (int j = 0; j < njobs; ++j) by_size[j] = j;
+    std::stable_sort(by_size.begin(), by_size.end(), [&](int a, int b) { return ns[a] > ns[b]; });
+    for (const int j : by_size) {
         const uint32_t np = npad_of(ns[j]);
+        const uint64_t k = std::max<uint64_t>(1, (np + (uint64_t)S.chunk - 1) / S.chunk);
+        const uint32_t each = (uint32_t)align_up((np + k - 1) / k, kSegAlign);
         S.seg0[j] = (uint32_t)S.segs.size();
         uint32_t at = 0, local = 0;
         do {
-            const uint64_t boundary = (v / S.chunk + 1) * S.chunk;
-            const uint32_t end = (uint32_t)std::min<uint64_t>(np, at + (boundary - v));
+            const uint32_t end = std::min(np, at + each);
             S.segs.push_back(SegDesc{(uint32_t)j, at, end, local++});
-            v += end - at;
             at = end;
         } while (at < np);
         S.nseg[j] = local;
