@@ -597,30 +597,29 @@ __global__ void __launch_bounds__(kSplitThreads) band_split_kernel(const Quad* _
     }
 }
 
-// Crowded tiles: the same blend, with the fragments evaluated by 23 warps
-// and blended by 8. A tile whose list runs to thousands of splats keeps the
-// warps of blend_kernel evaluating 32 pixels for every splat that reaches
-// their two rows, most of them outside its box, while the SM has little else
-// to issue. Here the tile's list goes by in chunks of 64 splats, a stage
-// each: one warp lists the boxes of chunk i + 1 (each splat's box within the
-// tile and where its pixels start in a flat list of items), the evaluating
-// warps take chunk i's items, a lane an item, and write each nonzero alpha
-// into a splat x pixel table in shared memory, and each pixel's own thread
-// walks its column of chunk i - 1's table in splat order, blends the nonzero
-// entries and clears them, while chunks i + 2 and i + 3 are copied in. The
-// values and the order of every operation on a pixel are blend_kernel's, so
-// the image is the same to the bit. One CTA of 1024 threads an SM (its registers keep
-// it alone there), looping over the crowded tiles, longest first.
+// Crowded tiles: the same blend, band by band, with the fragments evaluated
+// by 29 warps and blended by 2. A band's list goes by in chunks of 128
+// splats, a stage each: one warp lists the boxes of chunk i + 1 (each
+// splat's box within the band and where its pixels start in a flat list of
+// items), the evaluating warps take chunk i's items, a lane an item, and
+// write each nonzero alpha into a splat x pixel table in shared memory, and
+// each of the band's 64 pixels walks its column of chunk i - 1's table in
+// splat order, blends the nonzero entries and clears them, while chunks
+// i + 2 and i + 3 are copied in. The values and the order of every
+// operation on a pixel are blend_kernel's, so the image is the same to the
+// bit. One CTA of 1024 threads an SM (its registers keep it alone there),
+// claiming (tile, band) units, densest tiles first.
 constexpr int kCrowdThreads = 1024;
-constexpr uint32_t kCrowdChunk = 64;                     // splats a stage
-constexpr uint32_t kCrowdBlenders = 256;                 // a thread a pixel: warps 0..7
-constexpr uint32_t kCrowdLister = kCrowdBlenders / 32;   // warp 8 lists the boxes
-constexpr uint32_t kCrowdEvalWarps = kCrowdThreads / 32 - kCrowdLister - 1;   // warps 9..31
+constexpr uint32_t kCrowdChunk = 128;                    // splats a stage
+constexpr uint32_t kBandPx = kTilePx * kBandRows;        // pixels of a band
+constexpr uint32_t kCrowdBlenders = kBandPx;             // a thread a pixel of the band: warps 0..1
+constexpr uint32_t kCrowdLister = kCrowdBlenders / 32;   // warp 2 lists the boxes
+constexpr uint32_t kCrowdEvalWarps = kCrowdThreads / 32 - kCrowdLister - 1;   // warps 3..31
 constexpr uint32_t kCrowdBatch = 2;                      // items a lane evaluates at once
 constexpr uint32_t kCrowdRead = 8;                       // table entries a blending thread reads at once
 struct CrowdSmem {
     Quad staged[5][kCrowdChunk];                         // chunk i in staged[i % 5]
-    float alpha[2][kCrowdChunk][kTilePx * kTilePx];      // chunk i's alphas in alpha[i % 2]; 0 where none
+    float alpha[2][kCrowdChunk][kBandPx];                // chunk i's alphas in alpha[i % 2]; 0 where none
     uint32_t start[2][kCrowdChunk + 1];                  // chunk i's items: splat e's start in start[i % 2][e]
     uint32_t box[2][kCrowdChunk];                        // and its box (crowd_box)
 };
@@ -667,9 +666,9 @@ __global__ void __launch_bounds__(kCrowdThreads, 1) crowd_kernel(const Quad* __r
         const uint32_t tile = tile_order[unit / kBands], band = unit % kBands;
         const int tx0 = (int)((tile % tiles_x) * kTilePx), ty0 = (int)((tile / tiles_x) * kTilePx);
         const int by0 = ty0 + (int)band * kBandRows, by1 = by0 + kBandRows - 1;   // the band's rows
-        const int px = tx0 + (int)(threadIdx.x & 15), py = ty0 + (int)((threadIdx.x >> 4) & 15);
-        const bool mine = blender && py >= by0 && py <= by1;   // a pixel of the band
-        const bool inside = mine && px < (int)width && py < (int)height;
+        // A blending thread's pixel: column t % 16, row t / 16 of the band.
+        const int px = tx0 + (int)(threadIdx.x & 15), py = by0 + (int)((threadIdx.x >> 4) & 3);
+        const bool inside = blender && px < (int)width && py < (int)height;
         float4 dst = make_float4(0, 0, 0, 0);
         if (inside) dst = image[(size_t)py * width + px];
         const uint2 rg = range[tile];
@@ -689,16 +688,17 @@ __global__ void __launch_bounds__(kCrowdThreads, 1) crowd_kernel(const Quad* __r
                            reinterpret_cast<const float4*>(&quads[idx]) + (threadIdx.x & 3));
             cp_async_commit();
         };
-        // The lister's part: chunk c's boxes within the tile and their
+        // The lister's part: chunk c's boxes within the band and their
         // items' starts (an inclusive scan of the box sizes; lane l holds
-        // splats l and 32 + l).
+        // splats l, 32 + l, 64 + l and 96 + l).
+        constexpr int kListed = (int)kCrowdChunk / 32;
         auto list_boxes = [&](uint32_t c) {
             const uint32_t m = chunk_len(c), b = c % 5;
             uint32_t* st = sm.start[c & 1];
             uint32_t* bt = sm.box[c & 1];
-            uint32_t n[2];
+            uint32_t n[kListed];
 #pragma unroll
-            for (int j = 0; j < 2; ++j) {
+            for (int j = 0; j < kListed; ++j) {
                 const uint32_t e = j * 32 + lane;
                 n[j] = 0;
                 if (e < m) {
@@ -706,20 +706,23 @@ __global__ void __launch_bounds__(kCrowdThreads, 1) crowd_kernel(const Quad* __r
                     const int bx = max(q.x0, tx0), by = max(q.y0, by0);
                     const int bw = min(q.x1, tx0 + kTilePx - 1) - bx + 1, bh = min(q.y1, by1) - by + 1;
                     n[j] = (uint32_t)(bw * bh);
-                    bt[e] = crowd_box(bx - tx0, by - ty0, bw);
+                    bt[e] = crowd_box(bx - tx0, by - by0, bw);
                 }
             }
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
-                const uint32_t y0 = __shfl_up_sync(0xffffffffu, n[0], o), y1 = __shfl_up_sync(0xffffffffu, n[1], o);
-                if (lane >= (uint32_t)o) {
-                    n[0] += y0;
-                    n[1] += y1;
+#pragma unroll
+                for (int j = 0; j < kListed; ++j) {
+                    const uint32_t y = __shfl_up_sync(0xffffffffu, n[j], o);
+                    if (lane >= (uint32_t)o) n[j] += y;
                 }
             }
-            const uint32_t half = __shfl_sync(0xffffffffu, n[0], 31);
-            st[lane + 1] = n[0];
-            st[lane + 33] = n[1] + half;
+            uint32_t before = 0;
+#pragma unroll
+            for (int j = 0; j < kListed; ++j) {
+                st[j * 32 + lane + 1] = n[j] + before;
+                before += __shfl_sync(0xffffffffu, n[j], 31);
+            }
             if (lane == 0) st[0] = 0;
         };
         __syncthreads();   // the previous tile's last reads of the tables are done
@@ -739,7 +742,7 @@ __global__ void __launch_bounds__(kCrowdThreads, 1) crowd_kernel(const Quad* __r
             stage(next, (i + 3) % 5);
             next = index_of(i + 4);
             if (blender) {
-                if (i == 0 || !mine) continue;
+                if (i == 0) continue;
                 const uint32_t c = i - 1, b = c % 5, m = chunk_len(c);
                 float* col = &sm.alpha[c & 1][0][threadIdx.x];
                 // Entries past the chunk's end are 0 (never written), so
@@ -747,12 +750,12 @@ __global__ void __launch_bounds__(kCrowdThreads, 1) crowd_kernel(const Quad* __r
                 for (uint32_t e0 = 0; e0 < m; e0 += kCrowdRead) {
                     float a[kCrowdRead];
 #pragma unroll
-                    for (uint32_t k = 0; k < kCrowdRead; ++k) a[k] = col[(e0 + k) * kTilePx * kTilePx];
+                    for (uint32_t k = 0; k < kCrowdRead; ++k) a[k] = col[(e0 + k) * kBandPx];
 #pragma unroll
                     for (uint32_t k = 0; k < kCrowdRead; ++k) {
                         const float alpha = a[k];
                         if (alpha == 0.0f) continue;
-                        col[(e0 + k) * kTilePx * kTilePx] = 0.0f;
+                        col[(e0 + k) * kBandPx] = 0.0f;
                         const Quad& q = sm.staged[b][e0 + k];
                         const float om = fsub(1.0f, alpha);
                         dst.x = fadd(fmul(q.r, alpha), fmul(dst.x, om));
@@ -789,11 +792,11 @@ __global__ void __launch_bounds__(kCrowdThreads, 1) crowd_kernel(const Quad* __r
                         const uint32_t dy = (local * (bx >> 12)) >> 16;
                         const uint32_t cx = (bx & 15u) + local - dy * w, cy = ((bx >> 4) & 15u) + dy;
                         ipx[t] = tx0 + (int)cx;
-                        ipy[t] = ty0 + (int)cy;
+                        ipy[t] = by0 + (int)cy;
                         ifx[t] = fadd((float)ipx[t], 0.5f);
                         ify[t] = fadd((float)ipy[t], 0.5f);
                         qs[t] = &sm.staged[b][e];
-                        cell[t] = e * (kTilePx * kTilePx) + cy * kTilePx + cx;
+                        cell[t] = e * kBandPx + cy * kTilePx + cx;
                     }
                     float al[kCrowdBatch];
                     fragment_alphas_at<kCrowdBatch, true>(qs, ipx, ipy, ifx, ify, al);
