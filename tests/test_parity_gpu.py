@@ -411,3 +411,49 @@ def test_host_output_into_pinned_buffers(ctx):
                 assert np.array_equal(keys[:s].numpy().view(np.uint32), want_k)
     finally:
         splats.destroy()
+
+
+def test_two_contexts_in_flight_at_once():
+    """Two contexts sorting batches from two host threads at the same time
+    (their kernels overlap on the device, as the pipelined bench runs them):
+    every result is the oracle's."""
+    import threading
+
+    import torch
+
+    from winding_b200 import Context
+    rng = np.random.default_rng(29)
+    jobs = [W.Job(W.scene(W.KINDS[j % 3], int(rng.integers(20_000, 300_000)), 970 + j),
+                  W.View(W.random_pose(rng), W.perspective(W.FOV_Y, W.ASPECT, W.NEAR), cull=0.5))
+            for j in range(8)]
+    want = [oracle_sort(O.parse_splat(j.bytes()), j.view, 0.5) for j in jobs]
+    ctxs = [Context(0), Context(0)]
+    errors = []
+
+    def run(c, k):
+        try:
+            clouds = [parse_splats(j.records, c) for j in jobs]
+            host = [(torch.full((sp.count,), -1, dtype=torch.int32).pin_memory(),
+                     torch.zeros(1, dtype=torch.int32).pin_memory()) for sp in clouds]
+            specs = [(sp, make_view(j.view.model_view, j.view.projection, j.view.viewport, 0.5), ho.data_ptr(),
+                      None, hc.data_ptr()) for sp, j, (ho, hc) in zip(clouds, jobs, host)]
+            stream = torch.cuda.Stream()
+            for _ in range(3):
+                c.sort_batch_host(specs, stream.cuda_stream)
+                for (ho, hc), (wo, _) in zip(host, want):
+                    s = int(hc[0])
+                    if s != wo.size or not np.array_equal(ho[:s].numpy().view(np.uint32), wo):
+                        errors.append(k)
+            for sp in clouds:
+                sp.destroy()
+        except Exception as exc:   # reported below, from the main thread
+            errors.append(repr(exc))
+
+    threads = [threading.Thread(target=run, args=(c, k)) for k, c in enumerate(ctxs)]
+    for th in threads:
+        th.start()
+    for th in threads:
+        th.join()
+    for c in ctxs:
+        c.close()
+    assert not errors, errors
