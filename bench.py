@@ -835,7 +835,7 @@ def decode_suite(ctx, torch, flush, peak):
     return out
 
 
-def served(ctx, args, rates=(2000.0, 20000.0), seconds: float = 0.5, repeats: int = 5):
+def served(ctx, args, rates=(2000.0, 20000.0, 50000.0), seconds: float = 0.5, repeats: int = 5):
     """Config 4: Poisson streams of random-pose requests over 16 resident
     scenes of 50k-4M splats, through the server (continuous batching) and,
     on the same arrival schedule, through one plain ws_sort per request. Per
