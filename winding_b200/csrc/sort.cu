@@ -685,10 +685,23 @@ __device__ void digit_item(const JobDesc& J, const SegDesc& sd, DigitSmem<NT>& s
         __syncthreads();
         const uint32_t s = lane & (kSubHist - 1);
         const uint16_t* kb = J.key_b;
-#pragma unroll 4
-        for (uint32_t e = lo + tid; e < hi; e += NT) {
-            const uint32_t d = __ldcg(&kb[e]) >> 8;
-            atomicAdd(&h[s * 256u + sub_slot(s, d)], 1u);
+        // The slice's keys 8 at a time (16-byte loads from its first 8-key
+        // boundary; key_b is 256-byte aligned), the few before and after it
+        // one at a time: many bytes in flight, so the count is not bound by
+        // the loads' latency.
+        const uint32_t a8 = min(hi, (lo + 7u) & ~7u), b8 = max(a8, hi & ~7u);
+        for (uint32_t e = lo + tid; e < a8; e += NT) atomicAdd(&h[s * 256u + sub_slot(s, __ldcg(&kb[e]) >> 8)], 1u);
+        for (uint32_t e = b8 + tid; e < hi; e += NT) atomicAdd(&h[s * 256u + sub_slot(s, __ldcg(&kb[e]) >> 8)], 1u);
+        const uint4* kv = reinterpret_cast<const uint4*>(kb + a8);
+#pragma unroll 2
+        for (uint32_t k = tid; k < (b8 - a8) / 8u; k += NT) {
+            const uint4 w = __ldcg(&kv[k]);
+            const uint32_t words[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                atomicAdd(&h[s * 256u + sub_slot(s, (words[q] >> 8) & 255u)], 1u);
+                atomicAdd(&h[s * 256u + sub_slot(s, words[q] >> 24)], 1u);
+            }
         }
         __syncthreads();
         if (tid < 256) {
