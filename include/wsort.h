@@ -212,9 +212,10 @@ int ws_sort_batch(ws_ctx* ctx, int njobs, const ws_job* jobs, void* stream);
  * SplatPass._encodeSort (src/render/splats.js:678-696) with the reference's
  * outputs (order, args.instanceCount) read back. jobs[j].order, .keys (may
  * be NULL) and .count are host memory; when every one is pinned
- * (cudaHostAlloc / registered), one kernel writes them all and the call
- * synchronises once, else the counts come back first and then the orders.
- * Returns when the outputs are filled.
+ * (cudaHostAlloc / registered), one kernel writes them all, starting on each
+ * job as soon as its sort is done (so it overlaps the rest of the launch),
+ * and the call synchronises once; else the counts come back first and then
+ * the orders. At most 65535 jobs. Returns when the outputs are filled.
  */
 int ws_sort_batch_host(ws_ctx* ctx, int njobs, const ws_job* jobs, void* stream);
 

@@ -1113,7 +1113,8 @@ extern "C" int ws_sort_batch_host(ws_ctx* ctx, int njobs, const ws_job* jobs, vo
     if (!ctx) return WS_ERR_ARG;
     if (njobs < 0 || (njobs && !jobs)) return set_error(ctx, WS_ERR_ARG, "ws_sort_batch_host: bad job list");
     if (njobs == 0) return WS_OK;
-    if (njobs > (1 << 16)) return set_error(ctx, WS_ERR_ARG, "ws_sort_batch_host: too many jobs");
+    // One copy grid row a job: at most 65535 (the grid's y limit).
+    if (njobs > 65535) return set_error(ctx, WS_ERR_ARG, "ws_sort_batch_host: too many jobs (at most 65535)");
     for (int j = 0; j < njobs; ++j) {
         int rc;
         if ((rc = check_cloud(ctx, jobs[j].cloud)) || (rc = check_view(ctx, &jobs[j].view))) return rc;
