@@ -636,8 +636,26 @@ __device__ void given_keys_item(const JobDesc& J, const SegDesc& sd, KeysSmem<NT
     zero_keys_hist(sm);
     __syncthreads();
     const uint32_t end = min(sd.b, J.n);
-#pragma unroll 4
-    for (uint32_t i = sd.a + tid; i < end; i += NT) count_key(&sm.hist[0][0], __ldg(&J.keys_in[i]), s);
+    // 8 keys a 16-byte load where the keys are so aligned (the segment starts
+    // on a multiple of 256), the rest one at a time.
+    const uint16_t* const kin = J.keys_in;
+    uint32_t a8 = sd.a;
+    if ((reinterpret_cast<uintptr_t>(kin + sd.a) & 15u) == 0) {
+        const uint32_t nv = end > sd.a ? (end - sd.a) / 8u : 0u;
+        const uint4* kv = reinterpret_cast<const uint4*>(kin + sd.a);
+#pragma unroll 2
+        for (uint32_t k = tid; k < nv; k += NT) {
+            const uint4 w = __ldg(&kv[k]);
+            const uint32_t words[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                count_key(&sm.hist[0][0], words[q] & 0xFFFFu, s);
+                count_key(&sm.hist[0][0], words[q] >> 16, s);
+            }
+        }
+        a8 = sd.a + nv * 8u;
+    }
+    for (uint32_t i = a8 + tid; i < end; i += NT) count_key(&sm.hist[0][0], __ldg(&kin[i]), s);
     keys_publish(J, sd.local, sm);
 }
 
