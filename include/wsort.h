@@ -329,10 +329,13 @@ int ws_particle_thresholds(float* out);
 int ws_draw(ws_ctx* ctx, const ws_cloud* cloud, const ws_view* view, const uint32_t* order, const uint32_t* count,
             const uint32_t* shaded, float* image, uint32_t width, uint32_t height, void* stream);
 
-/* Which tiles ws_draw blends with four warps to each pair of pixel rows
- * instead of one: those whose splat list holds min_splats or more (a power
- * of two; 0: none; 1: every tile with a splat; default 256). The image is
- * the same either way; only the time differs. */
+/* Which tiles ws_draw draws as crowded: those whose splat list holds
+ * min_splats or more (a power of two; 0: none; 1: every tile with a splat;
+ * default 256). A crowded tile is split into four bands of 4 rows, each with
+ * its own list (the splats whose box meets it, in order) and drawn by its
+ * own CTA, the fragments evaluated by most of the CTA's warps; the other
+ * tiles are drawn one CTA a tile. The image is the same either way; only
+ * the time differs. */
 int ws_set_draw_crowded(ws_ctx* ctx, uint32_t min_splats);
 
 /* The draw's two 256-entry tables: decodeSRGB(byte / 255) and
