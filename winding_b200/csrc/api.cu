@@ -1102,7 +1102,21 @@ __global__ void __launch_bounds__(256) copy_jobs_kernel(const JobDesc* __restric
     // copy stays inside the job's buffers whatever it holds.
     const uint32_t c = min(__ldcg(J.count), H.n);
     if (blockIdx.x == 0 && threadIdx.x == 0) *H.hcount = c;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < c; i += gridDim.x * blockDim.x) {
+    const uint32_t t0 = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+    // 16 bytes a thread where both sides are 16-byte aligned (the device
+    // outputs always are; pinned host buffers usually), the rest a word at a time.
+    uint32_t done = 0;
+    const bool wide = ((reinterpret_cast<uintptr_t>(H.horder) | reinterpret_cast<uintptr_t>(J.order)) & 15u) == 0 &&
+                      (!H.hkeys || ((reinterpret_cast<uintptr_t>(H.hkeys) | reinterpret_cast<uintptr_t>(J.keys)) & 15u) == 0);
+    if (wide) {
+        const uint32_t c4 = c / 4u;
+        for (uint32_t i = t0; i < c4; i += stride) {
+            reinterpret_cast<uint4*>(H.horder)[i] = __ldcg(reinterpret_cast<const uint4*>(J.order) + i);
+            if (H.hkeys) reinterpret_cast<uint4*>(H.hkeys)[i] = __ldcg(reinterpret_cast<const uint4*>(J.keys) + i);
+        }
+        done = c4 * 4u;
+    }
+    for (uint32_t i = done + t0; i < c; i += stride) {
         H.horder[i] = __ldcg(&J.order[i]);
         if (H.hkeys) H.hkeys[i] = __ldcg(&J.keys[i]);
     }
