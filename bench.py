@@ -506,6 +506,7 @@ def batch_line(args, rank, world, dist, ctx, torch, flush):
         plain_rate = total * reps / (p["ms"] / 1e3) / 1e6
         graph_rate = value / world
         batch_rate = total * reps / (b_ms / 1e3) / 1e6
+        line["cull0"] = cull0_batch(ctx, torch, p, flush, peak)
         line["batch"] = {"plain_msplats_s": plain_rate, "batch_call_msplats_s": batch_rate,
                          "graph_msplats_s": graph_rate, "graph_vs_plain": graph_rate / plain_rate,
                          "batch_call_vs_plain": batch_rate / plain_rate,
@@ -570,6 +571,30 @@ def pipelined_e2e(ctx, torch, jobs, p, tuned, steps):
     finally:
         ctx2.close()
     return ms, h2d, d2h
+
+
+def cull0_batch(ctx, torch, p, flush, peak, reps=5):
+    """The same jobs at cull 0 (no footprint cull), as one ws_sort_batch
+    launch: its kernels' event time, rate and roofline fraction."""
+    from winding_b200 import make_view
+    stream = torch.cuda.current_stream().cuda_stream
+    views0 = [make_view(np.ctypeslib.as_array(v.model_view), np.ctypeslib.as_array(v.projection),
+                        (v.viewport[0], v.viewport[1]), 0.0) for v in p["views"]]
+    specs = [(sp, v0, o.data_ptr(), k.data_ptr(), c.data_ptr())
+             for sp, v0, (o, k, c) in zip(p["clouds"], views0, p["outs"])]
+    for _ in range(2):
+        ctx.sort_batch(specs, stream)
+    ctx.timing(True)
+    timed_sorts(ctx, torch, reps, flush, lambda: ctx.sort_batch(specs, stream))
+    kms, launches = ctx.timing_read()
+    ctx.timing(False)
+    ctx.sync()
+    kernel_s = kms / max(launches, 1) / 1e3
+    survivors = [int(c.item()) for _, _, c in p["outs"]]
+    algo = sum(algorithmic_bytes(sp.count, s) for sp, s in zip(p["clouds"], survivors))
+    return {"kernel_us": kernel_s * 1e6, "msplats_s": p["splats"] / kernel_s / 1e6, "survivors": sum(survivors),
+            "achieved_gbs": algo / kernel_s / 1e9, "frac": algo / kernel_s / 1e9 / peak,
+            "launch": "ws_sort_batch, kernels only (events)"}
 
 
 def local_rank_of(torch):
@@ -680,7 +705,8 @@ def suite(ctx, torch, flush, args):
         algo = sum(algorithmic_bytes(sp.count, s) for sp, s in zip(p["clouds"], p["survivors"]))
         kernel_s = p["kernel_ms"] / p["launches"] / 1e3
         e2e, h2d, d2h, _ = single_e2e(ctx, torch, p, 20, flush)
-        out[name] = {"splats": n, "survivors": p["survivors"][0], "kernel_us": kernel_s * 1e6,
+        c0 = cull0_batch(ctx, torch, p, flush, peak)
+        out[name] = {"cull0": c0, "splats": n, "survivors": p["survivors"][0], "kernel_us": kernel_s * 1e6,
                      "step_us": p["ms"] / 20 * 1e3, "msplats_s": n / (p["ms"] / 20 / 1e3) / 1e6,
                      "achieved_gbs": algo / kernel_s / 1e9, "frac": algo / kernel_s / 1e9 / peak,
                      "peak_source": src, "traffic": ncu_traffic(name, 0.5),
