@@ -363,6 +363,7 @@ void fill_view_consts(JobDesc& d) {
     c.keep_q = d.keep_q;
     c.keep_byte = d.keep_byte;
     c.fast = d.fast_transform != 0;
+    c.revz = c.fast && d.proj[8] == 0.0f && d.proj[9] == 0.0f && d.proj[10] == 0.0f && d.proj[11] == -1.0f;
     host_depth_range(d.mv, d.bmin, d.bmax, &c.visible, &c.depth_min, &c.depth_scale);
     // makeKeys drops a splat when unpack4x8unorm(colour).a * 255 <= 1
     // (render/splats.js:169-170): alpha = byte / 255 rounded to f32, so the

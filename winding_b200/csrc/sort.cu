@@ -323,15 +323,16 @@ __device__ __forceinline__ void shortcut(const ViewConsts& c, const float view[4
 // the slots whose survivor bit is set), with the digit counts of the splats
 // already decided; the ones whose footprint must still be evaluated go to
 // the queue. Every test is evaluated for every splat and combined as
-// predicates, so a warp does not split on the data. kFast: the fast
-// transform, the view's constants in registers (FastView).
-template <bool kFast, int NT>
+// predicates, so a warp does not split on the data. kMode 1: the fast
+// transform, the view's constants in registers (FastView); 2: that, with a
+// reverse-Z infinite projection's frustum test (fast_in_frustum_revz).
+template <int kMode, int NT>
 __device__ __forceinline__ void keys_sweep(const ViewConsts& c, KeysSmem<NT>& sm, uint32_t buf, uint32_t base,
                                            uint32_t cnt, uint32_t n, bool fp, uint16_t* k16, uint32_t* mask) {
     const uint32_t tid = threadIdx.x, lane = tid & 31u;
     const uint32_t s = lane & (kSubHist - 1);
     FastView fv;
-    if constexpr (kFast) fv = fast_view_of(c);
+    if constexpr (kMode > 0) fv = fast_view_of(c);
     const bool persp = c.persp;
     const float afx = c.afx, afy = c.afy, r0 = c.r0, r1 = c.r1, r2 = c.r2, xcap = c.xcap, ycap = c.ycap;
     const uint32_t keep_byte = c.keep_byte, faint_max = c.faint_max;
@@ -345,9 +346,9 @@ __device__ __forceinline__ void keys_sweep(const ViewConsts& c, KeysSmem<NT>& sm
         float view[4];
         bool inside;
         uint32_t key;
-        if constexpr (kFast) {
+        if constexpr (kMode > 0) {
             fast_view(fv, p.x, p.y, p.z, view);
-            inside = fast_in_frustum(fv, view);
+            inside = kMode == 2 ? fast_in_frustum_revz(fv, view) : fast_in_frustum(fv, view);
             key = fast_depth_key(fv, view);
         } else {
             view_of(c, p.x, p.y, p.z, view);
@@ -548,10 +549,12 @@ __device__ void keys_item(const JobDesc& J, const SegDesc& sd, KeysSmem<NT>& sm,
                 sm.pending &= ~(1u << buf);
                 if (L.trace) sm.mark[0] += global_ns() - w0;   // time spent waiting for staged records
             }
-            if (c.fast)
-                keys_sweep<true>(c, sm, buf, base, cnt, n, fp, k16, mask);
+            if (c.revz)
+                keys_sweep<2>(c, sm, buf, base, cnt, n, fp, k16, mask);
+            else if (c.fast)
+                keys_sweep<1>(c, sm, buf, base, cnt, n, fp, k16, mask);
             else
-                keys_sweep<false>(c, sm, buf, base, cnt, n, fp, k16, mask);
+                keys_sweep<0>(c, sm, buf, base, cnt, n, fp, k16, mask);
             ks.buf ^= 1u;
         } else {
             // Wholly behind the camera: no survivors.

@@ -69,7 +69,7 @@ struct ViewConsts {
     // phase: |fx|, |fy|, the absolute row sums of the model-view's 3x3 (rows
     // 0, 1, 2), and |1.3 / p[0][0]|, |1.3 / p[1][1]|.
     float afx, afy, r0, r1, r2, xcap, ycap;
-    uint32_t pad[1];
+    uint32_t revz;              // fast, and P[8] = P[9] = P[10] = 0, P[11] = -1 (reverse-Z infinite)
     // The footprint cull as a threshold on det, per alpha byte b: makeKeys
     // keeps the splat exactly when det >= det_min[b] (the host's bisection
     // over f32 values of the monotone test !(alpha * (2 pi sqrt(max(det, 0)))
@@ -443,6 +443,15 @@ __device__ __forceinline__ bool fast_in_frustum(const FastView& f, const float v
     const float c2 = fadd(fmul(f.p10, view[2]), f.p14);
     const float w = fmul(f.p11, view[2]);
     return !(view[2] >= 0.0f || c2 > w || fabsf(c0) > fmul(1.3f, w) || fabsf(c1) > fmul(1.3f, w));
+}
+
+// fast_in_frustum for a projection with P[8] = P[9] = P[10] = 0 and P[11] = -1: the
+// zero products add a signed zero, which changes no comparison (|c0|, |c1|;
+// c2 is P[14] itself), and w = -1 view.z is -view.z exactly.
+__device__ __forceinline__ bool fast_in_frustum_revz(const FastView& f, const float view[4]) {
+    const float w = -view[2];
+    const float c0 = fmul(f.p0, view[0]), c1 = fmul(f.p5, view[1]);
+    return !(view[2] >= 0.0f || f.p14 > w || fabsf(c0) > fmul(1.3f, w) || fabsf(c1) > fmul(1.3f, w));
 }
 
 __device__ __forceinline__ uint32_t fast_depth_key(const FastView& f, const float view[4]) {
