@@ -448,6 +448,16 @@ int ws_inject_alloc_failures(int count);
  */
 int ws_selftest_wait(ws_ctx* ctx, uint32_t spin_limit);
 
+/*
+ * The same for ws_sort_noalloc: queues, on `stream` (NULL: the context's),
+ * one job on the library's fixed array whose first phase is left out, with
+ * `spin_limit` polls (1 to 2^20), then the check ws_sort_noalloc ends with,
+ * so that the device count *count becomes 0xFFFFFFFF as after a real wait
+ * that gave up. The context only names the device; its own scratch is not
+ * touched. Serialise it with ws_sort_noalloc calls as those are serialised.
+ */
+int ws_selftest_noalloc_wait(ws_ctx* ctx, uint32_t spin_limit, uint32_t* count, void* stream);
+
 /* ------------------------------------------------------------ tuning */
 
 /*

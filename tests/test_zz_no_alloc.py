@@ -99,6 +99,29 @@ def test_noalloc_allocates_nothing(ctx):
             sp.destroy()
 
 
+def test_noalloc_wait_that_runs_out_sets_the_count_and_the_next_call_is_exact(ctx):
+    """A job on the fixed array whose first phase is left out: its bounded
+    wait gives up, the closing check turns that into *count = 0xFFFFFFFF, and
+    the next ws_sort_noalloc on the same array is exact again."""
+    import torch
+    stream = torch.cuda.current_stream().cuda_stream
+    count = torch.zeros(1, dtype=torch.int32, device="cuda")
+    assert ctx.lib.ws_selftest_noalloc_wait(ctx.handle, 0, count.data_ptr(), stream) == _lib.WS_ERR_ARG
+    assert ctx.lib.ws_selftest_noalloc_wait(ctx.handle, 2000, count.data_ptr(), stream) == _lib.WS_OK
+    torch.cuda.synchronize()
+    assert int(count.item()) == -1
+    job = W.clusters_1m(seed=65, n=120_000)
+    splats = parse_splats(job.records, ctx)
+    try:
+        view = make_view(job.view.model_view, job.view.projection, job.view.viewport, 0.5)
+        want_o, want_k = O.sort_view(O.parse_splat(job.bytes()), job.view.model_view, job.view.projection,
+                                     job.view.viewport, 0.5)
+        order, keys = _noalloc(ctx, splats, view, torch)
+        assert np.array_equal(order, want_o) and np.array_equal(keys, want_k)
+    finally:
+        splats.destroy()
+
+
 def test_noalloc_refuses_clouds_beyond_its_fixed_size(ctx):
     import torch
     job = W.uniform_100k(seed=63, n=_lib.WS_NOALLOC_MAX_SPLATS + 1)

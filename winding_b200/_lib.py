@@ -189,6 +189,7 @@ SIGNATURES = {
     "ws_draw_tables": (ctypes.c_int, [ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]),
     "ws_set_draw_crowded": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32]),
     "ws_selftest_wait": (ctypes.c_int, [vp, ctypes.c_uint32]),
+    "ws_selftest_noalloc_wait": (ctypes.c_int, [vp, ctypes.c_uint32, vp, vp]),
     "ws_inject_alloc_failures": (ctypes.c_int, [ctypes.c_int]),
     "ws_server_cancel": (ctypes.c_int, [vp, ctypes.c_uint64]),
     "ws_cloud_harmonics": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_int), vp]),

@@ -141,3 +141,50 @@ extern "C" int ws_sort_noalloc(const ws_cloud* cloud, const ws_view* view, uint3
     }
     return e == cudaSuccess ? WS_OK : WS_ERR_CUDA;
 }
+
+extern "C" int ws_selftest_noalloc_wait(ws_ctx* ctx, uint32_t spin_limit, uint32_t* count, void* stream_p) {
+    if (!ctx || !count) return WS_ERR_ARG;
+    if (spin_limit == 0 || spin_limit > (1u << 20)) return WS_ERR_ARG;
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return WS_ERR_CUDA;
+    char* base = nullptr;
+    int rc = scratch_address(ctx->device, &base);
+    if (rc) return rc;
+    cudaStream_t stream = stream_p ? static_cast<cudaStream_t>(stream_p) : ctx->stream;
+
+    // One job of 4096 given keys, laid out on the array as ws_sort_noalloc
+    // lays out a cloud, its keys kernel left out of the launch: the low pass's
+    // items wait for a completion count that nothing raises and give up after
+    // spin_limit polls. The job's keys and outputs sit after its scratch.
+    ws_params p{};
+    p.tile = kMinSegment;
+    p.ctas_per_sm = 1;
+    p.spin_limit = spin_limit;
+    p.segs_per_cta = 1;
+    const uint32_t n = 4096;
+    LaunchShape S;
+    shape_launch(&n, 1, p, ctx->sms, S);
+    const size_t keys_off = (S.bytes + 255) / 256 * 256, out_off = keys_off + 2 * (size_t)n;
+    if (out_off + 2 * 4 * (size_t)n > kSortBytes) return WS_ERR_CAPACITY;
+    JobDesc d;
+    std::memset(&d, 0, sizeof(d));
+    d.kind = kJobKeys;
+    d.keys_in = reinterpret_cast<const uint16_t*>(base + keys_off);
+    d.order = reinterpret_cast<uint32_t*>(base + out_off);
+    d.keys = d.order + n;
+    d.count = count;
+    place_job(d, n, 0, S, base);
+
+    noalloc_setup_kernel<<<8, 256, 0, stream>>>(d, (uint32_t)S.ctl_bytes);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) {
+        LaunchDesc L = launch_desc(base + kJobOffset, 1, S, base, reinterpret_cast<uint32_t*>(base + kErrOffset),
+                                   spin_limit, nullptr);
+        L.first_phase = kPhaseLow;
+        e = launch_sort(L, S.threads, 2, ctx->sms, stream);
+    }
+    if (e == cudaSuccess) {
+        noalloc_check_kernel<<<1, 1, 0, stream>>>(count);
+        e = cudaGetLastError();
+    }
+    return e == cudaSuccess ? WS_OK : WS_ERR_CUDA;
+}
