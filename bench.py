@@ -517,22 +517,28 @@ def batch_line(args, rank, world, dist, ctx, torch, flush):
     return line, jobs
 
 
-def pipelined_e2e(ctx, torch, jobs, p, tuned, steps):
-    """ws_sort_batch_host over the 64 jobs, `steps` calls from two host
-    threads, each with its own context and stream (a second context holds its
-    own resident copy of the clouds and the same tuning). Returns (wall ms
+def pipelined_e2e(ctx, torch, jobs, p, tuned, steps, threads=2):
+    """ws_sort_batch_host over the 64 jobs, `steps` calls from `threads` host
+    threads, each with its own context and stream (each further context holds
+    its own resident copy of the clouds and the same tuning). Returns (wall ms
     from the first call to the last result, host-to-device and device-to-host
     bytes of all calls)."""
     import ctypes
     import threading
     from winding_b200 import Context, autotune
     from winding_b200._lib import WsJob
-    ctx2 = Context(ctx.device)
+    extra = []
     try:
-        autotune.install(ctx2, tuned)
-        p2 = load_jobs(ctx2, torch, jobs)
+        pairs = [(ctx, p)]
+        for _ in range(threads - 1):
+            c2 = Context(ctx.device)
+            extra.append((c2, None))
+            autotune.install(c2, tuned)
+            q2 = load_jobs(c2, torch, jobs)
+            extra[-1] = (c2, q2)
+            pairs.append((c2, q2))
         sides = []
-        for c, q in ((ctx, p), (ctx2, p2)):
+        for c, q in pairs:
             host = [(torch.empty(max(sp.count, 1), dtype=torch.int32).pin_memory(),
                      torch.zeros(1, dtype=torch.int32).pin_memory()) for sp in q["clouds"]]
             arr = (WsJob * len(host))()
@@ -552,10 +558,10 @@ def pipelined_e2e(ctx, torch, jobs, p, tuned, steps):
         for c, *_ in sides:
             c.copy_stats(reset=True)
         t0 = time.perf_counter()
-        threads = [threading.Thread(target=run, args=(side, steps // 2)) for side in sides]
-        for th in threads:
+        workers = [threading.Thread(target=run, args=(side, steps // threads)) for side in sides]
+        for th in workers:
             th.start()
-        for th in threads:
+        for th in workers:
             th.join()
         torch.cuda.synchronize()
         ms = (time.perf_counter() - t0) * 1e3
@@ -566,10 +572,12 @@ def pipelined_e2e(ctx, torch, jobs, p, tuned, steps):
         want = [int(cc.item()) for _, _, cc in p["outs"]]
         for _, _, host, _ in sides:
             assert [int(hc[0]) for _, hc in host] == want
-        for sp in p2["clouds"]:
-            sp.destroy()
     finally:
-        ctx2.close()
+        for c2, q2 in extra:
+            if q2:
+                for sp in q2["clouds"]:
+                    sp.destroy()
+            c2.close()
     return ms, h2d, d2h
 
 
