@@ -155,25 +155,36 @@ class Clocks:
                 "samples": len(sm)}
 
 
-def cpu_baseline(jobs, seconds: float, threads: int):
-    """The oracle on the host cores: full views of the workload, repeated for
-    about `seconds` (at least once). Returns (Msplats/s, sample text)."""
+def cpu_baseline(jobs, seconds: float, threads: int, runs: int = 5):
+    """The oracle on the host cores: after a warm-up sort, `runs` timed runs of
+    about seconds / runs each, every run sorting full views of the workload in
+    turn (continuing where the previous run stopped). Returns (median
+    Msplats/s, sample text with the runs' spread)."""
     from oracle import oracle as O
     parsed = [O.parse_splat(j.bytes()) for j in jobs]
-    done = 0
-    sorts = 0
-    t0 = time.perf_counter()
-    while True:
-        for p, j in zip(parsed, jobs):
-            O.sort_view(p, j.view.model_view, j.view.projection, j.view.viewport, j.view.cull, threads=threads)
-            done += p.count
+    order = sorted(range(len(jobs)), key=lambda k: parsed[k].count)
+
+    def sort(k):
+        j = jobs[k]
+        O.sort_view(parsed[k], j.view.model_view, j.view.projection, j.view.viewport, j.view.cull, threads=threads)
+        return parsed[k].count
+
+    sort(order[0])   # warm-up: the smallest view
+    rates, sorts, done_all, at = [], 0, 0, 0
+    for _ in range(runs):
+        done = 0
+        t0 = time.perf_counter()
+        while True:
+            done += sort(at % len(jobs))
+            at += 1
             sorts += 1
-            if time.perf_counter() - t0 >= seconds:
+            if time.perf_counter() - t0 >= seconds / runs:
                 break
-        if time.perf_counter() - t0 >= seconds:
-            break
-    dt = time.perf_counter() - t0
-    return done / dt / 1e6, f"{sorts} full-view sorts ({done} splats) in {dt:.1f} s"
+        rates.append(done / (time.perf_counter() - t0) / 1e6)
+        done_all += done
+    med = sorted(rates)[len(rates) // 2]
+    return med, (f"median of {runs} runs of ~{seconds / runs:.1f} s ({sorts} full-view sorts, {done_all} splats "
+                 f"in all; runs {min(rates):.1f}-{max(rates):.1f} Msplats/s)")
 
 
 def run_reference(args, rank: int):
