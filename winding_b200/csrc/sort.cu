@@ -525,6 +525,11 @@ __device__ void keys_item(const JobDesc& J, const SegDesc& sd, KeysSmem<NT>& sm,
                           uint32_t item) {
     constexpr uint32_t TK = KeysSmem<NT>::TK;
     const uint32_t tid = threadIdx.x;
+    const uint32_t a = sd.a, b = sd.b, n = J.n;
+    // The first sub-tile's copy goes out before the view's constants are
+    // staged (the staging buffers are free: the previous item ended with a
+    // barrier after its last sweep).
+    if (tid == 0 && J.vc.visible != 0 && a < b) stage_issue(J, sm, ks.buf, a, min(TK, b - a), J.vc.cull > 0.0f);
     static_assert(sizeof(ViewConsts) % 4 == 0, "copied in words");
     for (uint32_t k = tid; k < sizeof(ViewConsts) / 4; k += NT)
         reinterpret_cast<uint32_t*>(&sm.vc)[k] = reinterpret_cast<const uint32_t*>(&J.vc)[k];
@@ -534,10 +539,8 @@ __device__ void keys_item(const JobDesc& J, const SegDesc& sd, KeysSmem<NT>& sm,
     const ViewConsts& c = sm.vc;
     const bool any = c.visible != 0;
     const bool fp = c.cull > 0.0f;
-    const uint32_t a = sd.a, b = sd.b, n = J.n;
     uint16_t* const k16 = J.k16;
     uint32_t* const mask = J.mask;
-    if (any && a < b && tid == 0) stage_issue(J, sm, ks.buf, a, min(TK, b - a), fp);
     for (uint32_t base = a; base < b; base += TK) {
         const uint32_t cnt = min(TK, b - base);
         const uint32_t buf = ks.buf;
