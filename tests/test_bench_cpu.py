@@ -1,6 +1,6 @@
-"""bench.py's CPU side: the reference arm's JSON line (the contract the
-round-end run reads) and the CPU baseline's timing protocol, on the small
-uniform-100k workload."""
+"""bench.py's CPU side: the reference arm's JSON line (the one line a
+benchmark harness parses) and the CPU baseline's timing protocol, on the
+small uniform-100k workload."""
 import json
 import os
 import subprocess
