@@ -460,22 +460,14 @@ __device__ __forceinline__ uint32_t fast_depth_key(const FastView& f, const floa
     return kBuckets - 1u - bucket;
 }
 
-// The footprint cull (render/splats.js:172-178): true when the splat is kept.
-// The pinned 2D covariance's det = (xx + .3)(yy + .3) - xy^2
-// (render/splats.js:174-178).
+// The footprint cull's determinant (render/splats.js:172-178): the pinned 2D
+// covariance's det = (xx + .3)(yy + .3) - xy^2; makeKeys keeps the splat when
+// RN(alpha * 2 pi sqrt(max(det, 0))) >= cull, which the keys phase tests as
+// det >= det_min[alpha byte].
 __device__ __forceinline__ float footprint_det(const ViewConsts& c, const float view[4], const float s[6]) {
     float fxx, fxy, fyy;
     footprint2d(c, view, s, &fxx, &fxy, &fyy);
     return fsub(fmul(fadd(fxx, 0.3f), fadd(fyy, 0.3f)), fmul(fxy, fxy));
-}
-
-__device__ __forceinline__ bool footprint_keeps(const ViewConsts& c, const float view[4], const float s[6],
-                                                float alpha) {
-    float fxx, fxy, fyy;
-    footprint2d(c, view, s, &fxx, &fxy, &fyy);
-    const float det = fsub(fmul(fadd(fxx, 0.3f), fadd(fyy, 0.3f)), fmul(fxy, fxy));
-    const float area = fmul(6.2831853f, __fsqrt_rn(fmaxf(det, 0.0f)));
-    return !(fmul(alpha, area) < c.cull);
 }
 
 // key = 65535 - bucket (render/splats.js:180-181).
@@ -487,13 +479,10 @@ __device__ __forceinline__ uint32_t depth_key(const ViewConsts& c, const float v
 
 // ---------------------------------------------------------------- memory ops
 // 16-byte asynchronous copies global -> shared (cp.async, cached in L2
-// only), and the wait for all of this thread's copies.
+// only), their commit, and the waits for a thread's committed groups.
 __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
     const uint32_t dst = (uint32_t)__cvta_generic_to_shared(smem_dst);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(gsrc) : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() {
-    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 // Waits until at most one of this thread's committed copy groups is pending.
@@ -511,7 +500,6 @@ __device__ __forceinline__ void st_release(uint32_t* p, uint32_t v) {
 __device__ __forceinline__ void red_release_add(uint32_t* p, uint32_t v) {
     asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
-__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31; }
 __device__ __forceinline__ uint32_t lanemask_lt() {
     uint32_t m;
     asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
